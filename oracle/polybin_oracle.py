@@ -1,0 +1,616 @@
+"""ORACLE — test infrastructure only (the checker, never the product path).
+
+A CPU FP64 restatement of PolyBin3D's binned polyspectrum hot path, written from the
+reference's algorithm (file:line cited per function).  FFTs are scipy.fft in FP64 with
+numpy's normalisation (forward unnormalised, inverse x 1/N^3), the convention of the
+reference's `to_fourier`/`to_real` (base.py:176-229).  The O(N_bins N^3) real-space
+triplet loop runs in plain C (oracle/oracle_loops.c) via ctypes.
+
+Parity is pinned: tests/test_oracle_golden.py checks every function here against
+fixtures produced by running the reference itself (tests/golden/make_golden.py).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this.
+"""
+import ctypes
+import os
+
+import numpy as np
+import scipy.fft
+from scipy.interpolate import interp1d
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+# --------------------------------------------------------------------------------------
+# C loops
+# --------------------------------------------------------------------------------------
+_loops = None
+
+
+def _load_loops():
+    global _loops
+    if _loops is None:
+        path = os.path.join(_HERE, "liboracle_loops.so")
+        if not os.path.exists(path):
+            build_loops()
+        lib = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        I = ctypes.c_int64
+        lib.oracle_triplet_sum.argtypes = [P, P, P, I, P, I, P, ctypes.c_int]
+        lib.oracle_pair_sum.argtypes = [P, P, I, P, I, P, ctypes.c_int]
+        _loops = lib
+    return _loops
+
+
+def build_loops():
+    """Compile oracle/oracle_loops.c with gcc + OpenMP into oracle/liboracle_loops.so."""
+    import subprocess
+    src = os.path.join(_HERE, "oracle_loops.c")
+    out = os.path.join(_HERE, "liboracle_loops.so")
+    subprocess.check_call(["gcc", "-O3", "-fopenmp", "-fPIC", "-shared", src, "-o", out])
+    return out
+
+
+def triplet_sum(A, B, C, idx, nthreads=None):
+    """out[t] = sum_x A[i1]B[i2]C[i3]; A,B,C are (n_maps, ...) float64 arrays.
+    Restates assemble_b3 / sum_triplet (utils.pyx:614-636, 357-366)."""
+    lib = _load_loops()
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    C = np.ascontiguousarray(C, dtype=np.float64)
+    n_vox = int(np.prod(A.shape[1:]))
+    idx = np.ascontiguousarray(idx, dtype=np.int64).reshape(-1, 3)
+    out = np.zeros(len(idx), dtype=np.float64)
+    lib.oracle_triplet_sum(A.ctypes.data, B.ctypes.data, C.ctypes.data, n_vox,
+                           idx.ctypes.data, len(idx), out.ctypes.data,
+                           int(nthreads or os.cpu_count()))
+    return out
+
+
+def pair_sum(A, B, idx, nthreads=None):
+    """out[t] = sum_x A[i1]B[i2]  (sum_pair, utils.pyx:343-352)."""
+    lib = _load_loops()
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    n_vox = int(np.prod(A.shape[1:]))
+    idx = np.ascontiguousarray(idx, dtype=np.int64).reshape(-1, 2)
+    out = np.zeros(len(idx), dtype=np.float64)
+    lib.oracle_pair_sum(A.ctypes.data, B.ctypes.data, n_vox, idx.ctypes.data, len(idx),
+                        out.ctypes.data, int(nthreads or os.cpu_count()))
+    return out
+
+
+# --------------------------------------------------------------------------------------
+# small helpers
+# --------------------------------------------------------------------------------------
+def legendre(l, mu):
+    """Explicit Legendre polynomials, as utils.pyx:385-400."""
+    if l == 0:
+        return np.ones_like(mu)
+    if l == 1:
+        return mu
+    if l == 2:
+        return 0.5 * (3 * mu ** 2 - 1)
+    if l == 3:
+        return 0.5 * (5 * mu ** 3 - 3 * mu)
+    if l == 4:
+        return (35 * mu ** 4 - 30 * mu ** 2 + 3) / 8.0
+    raise ValueError("l > 4 unsupported")
+
+
+def real_harmonics_fourier(k_grids, lmax):
+    """Real spherical harmonics of the unit k-vector, l = 2, 4 (utils.pyx:518-609, even l)."""
+    kx, ky, kz = k_grids
+    norm = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    safe = np.where(norm == 0, 1.0, norm)
+    xh = np.where(norm == 0, 0.0, kx / safe)
+    yh = np.where(norm == 0, 0.0, ky / safe)
+    zh = np.where(norm == 0, 0.0, kz / safe)
+    out = {}
+    if lmax >= 2:
+        out[2] = np.asarray([
+            6.0 * xh * yh * np.sqrt(1.0 / 12.0),
+            3.0 * yh * zh * np.sqrt(1.0 / 3.0),
+            zh ** 2 - xh ** 2 / 2.0 - yh ** 2 / 2.0,
+            3.0 * xh * zh * np.sqrt(1.0 / 3.0),
+            (3 * xh ** 2 - 3 * yh ** 2) * np.sqrt(1.0 / 12.0)])
+    if lmax >= 4:
+        out[4] = np.asarray([
+            (420.0 * xh ** 3 * yh - 420.0 * xh * yh ** 3) * np.sqrt(1.0 / 20160.0),
+            (315.0 * xh ** 2 * yh * zh - 105.0 * yh ** 3 * zh) * np.sqrt(1.0 / 2520.0),
+            (-15.0 * xh ** 3 * yh - 15.0 * xh * yh ** 3 + 90.0 * xh * yh * zh ** 2) * np.sqrt(1.0 / 180.0),
+            (-7.5 * xh ** 2 * yh * zh - 7.5 * yh ** 3 * zh + 10.0 * yh * zh ** 3) * np.sqrt(1.0 / 10.0),
+            35.0 / 8.0 * zh ** 4 - 15.0 / 4.0 * zh ** 2 + 3.0 / 8.0,
+            (-15.0 / 2.0 * xh ** 3 * zh - 15.0 * xh * yh ** 2 * zh / 2.0 + 10.0 * xh * zh ** 3) * np.sqrt(1.0 / 10.0),
+            (-15.0 / 2.0 * xh ** 4 + 45.0 * xh ** 2 * zh ** 2 + 15.0 / 2.0 * yh ** 4 - 45.0 * yh ** 2 * zh ** 2) * np.sqrt(1.0 / 180.0),
+            (105.0 * xh ** 3 * zh - 315.0 * xh * yh ** 2 * zh) * np.sqrt(1.0 / 2520.0),
+            (105.0 * xh ** 4 - 630.0 * xh ** 2 * yh ** 2 + 105.0 * yh ** 4) * np.sqrt(1.0 / 20160.0)])
+    return out
+
+
+def pixel_window_1d(kind, x):
+    """1-D voxel windows with first-order alias corrections (base.py:231-254); x = pi*n/N."""
+    if kind == "cic":
+        s = np.sin(x) ** 2.0
+        return (1.0 - 2.0 / 3.0 * s) ** 0.5
+    if kind == "tsc":
+        s = np.sin(x) ** 2.0
+        return (1.0 - s + 2.0 / 15 * s ** 2.0) ** 0.5
+    if kind == "pcs":
+        s = np.sin(x) ** 2.0
+        return (1.0 - 4.0 / 3.0 * s + 2.0 / 5.0 * s ** 2 - 4.0 / 315.0 * s ** 3) ** 0.5
+    if kind == "interlaced-cic":
+        s = np.sinc(x / np.pi)
+        v = np.ones_like(s)
+        v[s != 0.0] = s[s != 0.0] ** 2.0
+        return v
+    if kind == "interlaced-tsc":
+        return np.sinc(x / np.pi) ** 3.0
+    if kind == "interlaced-pcs":
+        return np.sinc(x / np.pi) ** 4.0
+    raise ValueError(kind)
+
+
+# --------------------------------------------------------------------------------------
+# base geometry (base.py:20-144)
+# --------------------------------------------------------------------------------------
+class OracleBase:
+    """Grids and FFTs of the reference base class, global sightline, real FFTs."""
+
+    def __init__(self, boxsize, gridsize, Pk=None, pixel_window="none", nthreads=None):
+        self.boxsize = np.asarray(boxsize, dtype=np.float64)
+        self.gridsize = np.asarray(gridsize, dtype=int)
+        self.nthreads = nthreads or os.cpu_count()
+        self.pixel_window = pixel_window
+        self.volume = self.boxsize.prod()
+        self.kF = 2.0 * np.pi / self.boxsize                         # base.py:64
+        self.kNy = self.gridsize * self.kF * 0.5                        # base.py:65
+        if Pk is None:                                                  # base.py:68-70
+            k_tmp = np.arange(0.0, np.max(self.kNy) * 2, np.min(self.kF) / 10.0)
+            self.Pfid = np.asarray([k_tmp, 1.0 + 0.0 * k_tmp])
+        else:
+            self.Pfid = np.asarray(Pk)
+        # fftshift order on axes 0,1; 0..N/2 on axis 2  (base.py:86-91)
+        k_arrs = [np.fft.fftshift(np.arange(-self.gridsize[i] // 2, self.gridsize[i] // 2)) * self.kF[i]
+                  for i in range(2)]
+        k_arrs += [np.arange(0, self.gridsize[2] // 2 + 1) * self.kF[2]]
+        self.k_arrs = k_arrs
+        self.k_grids = np.meshgrid(*k_arrs, indexing="ij")
+        self.modk_grid = np.sqrt(self.k_grids[0] ** 2 + self.k_grids[1] ** 2 + self.k_grids[2] ** 2)
+        self.degeneracy_factor = np.asarray(1.0 + (self.k_grids[2] > 0), dtype=np.float64)   # base.py:94
+        if pixel_window != "none":                                      # base.py:106-108
+            w1d = [pixel_window_1d(pixel_window, np.pi / self.gridsize[i] * k_arrs[i] / self.kF[i])
+                   for i in range(3)]
+            self.pixel_window_grid = np.asarray(np.meshgrid(*w1d, indexing="ij")).prod(axis=0)
+        self.muk_grid = np.zeros(self.modk_grid.shape)                  # base.py:115-116
+        nz = self.modk_grid != 0
+        self.muk_grid[nz] = self.k_grids[2][nz] / self.modk_grid[nz]
+        self.Pk0_grid = interp1d(self.Pfid[0], self.Pfid[1], bounds_error=False,
+                                 fill_value=0.0)(self.modk_grid)         # base.py:122
+        self.invPk0_grid = np.zeros(self.modk_grid.shape)               # base.py:125-131
+        good = (self.Pk0_grid != 0) & np.isfinite(self.Pk0_grid)
+        self.invPk0_grid[good] = 1.0 / self.Pk0_grid[good]
+        self.Pk0_grid[~np.isfinite(self.Pk0_grid)] = 0.0
+        self.invPk0_grid[self.modk_grid == 0] = 1.0
+        self.Pk0_grid[self.modk_grid == 0] = 1.0
+
+    # FFTs, numpy normalisation (base.py:176-229)
+    def to_fourier(self, x):
+        return scipy.fft.rfftn(np.asarray(x, dtype=np.float64), axes=(0, 1, 2), workers=self.nthreads)
+
+    def to_real(self, k):
+        return scipy.fft.irfftn(k, s=tuple(self.gridsize), axes=(0, 1, 2), workers=self.nthreads)
+
+    # map utilities (utils.pyx:213-338)
+    def in_bin(self, kmin, kmax):
+        return (self.modk_grid >= kmin) & (self.modk_grid < kmax)
+
+    def fourier_filter(self, kmap, l, kmin, kmax, l2=0):
+        """Theta_b(k) L_l(mu) [L_l2(mu)] kmap  (fourier_filter / fourier_filter_ll, utils.pyx:283-320)."""
+        out = np.zeros(self.modk_grid.shape, dtype=np.complex128)
+        m = self.in_bin(kmin, kmax)
+        leg = legendre(l, self.muk_grid[m]) * legendre(l2, self.muk_grid[m])
+        out[m] = kmap[m] * leg
+        return out
+
+    def div_fourier(self, kmap, w):
+        """kmap / w with 0 where w == 0 (utils.pyx:230-243)."""
+        out = np.zeros_like(kmap, dtype=np.complex128)
+        nz = w != 0
+        out[nz] = kmap[nz] / w[nz]
+        return out
+
+    # k-bin reductions (utils.pyx:51-134); bins [k_b, k_b+1) with >= / <
+    def integrate(self, spec, k_edges, l):
+        vals = self.degeneracy_factor * (spec.real ** 2 + spec.imag ** 2) * legendre(l, self.muk_grid)
+        return np.asarray([vals[self.in_bin(k_edges[b], k_edges[b + 1])].sum()
+                           for b in range(len(k_edges) - 1)])
+
+    def cross_integrate(self, s1, s2, k_edges, l):
+        vals = self.degeneracy_factor * (s1 * np.conj(s2)).real * legendre(l, self.muk_grid)
+        return np.asarray([vals[self.in_bin(k_edges[b], k_edges[b + 1])].sum()
+                           for b in range(len(k_edges) - 1)])
+
+    def real_integrate_double(self, spec, l1, l2, k_edges):
+        vals = self.degeneracy_factor * spec ** 2 * legendre(l1, self.muk_grid) * legendre(l2, self.muk_grid)
+        return np.asarray([vals[self.in_bin(k_edges[b], k_edges[b + 1])].sum()
+                           for b in range(len(k_edges) - 1)])
+
+    def integrate_row(self, input_map, input_array, kmin, kmax):
+        """out[j] = sum_{k in [kmin,kmax)} deg Re(conj(map) * array[j])  (utils.pyx:162-179)."""
+        m = self.in_bin(kmin, kmax)
+        w = self.degeneracy_factor[m] * np.conj(input_map[m])
+        return (input_array[:, m] * w[None, :]).real.sum(axis=1)
+
+    # Gaussian random field from supplied white noise (base.py:305-353)
+    def grf_from_noise(self, noise_re, noise_im, Pk_grid=None, include_pixel_window=True):
+        """Reference draws noise_re, noise_im = np.random.randn(*N) twice after
+        np.random.seed(seed) (base.py:315-316, 332); here they are inputs."""
+        N = self.gridsize
+        rand = noise_re + 1.0j * noise_im
+        rand[0, 0, 0] = 0.0                                                     # base.py:333
+        ii, jj, kk = np.meshgrid(*[np.arange(N[i]) for i in range(3)], indexing="ij")
+        rand = 0.5 * (rand + np.conj(rand[(-ii) % N[0], (-jj) % N[1], (-kk) % N[2]]))  # 336-337
+        rand = np.ascontiguousarray(rand[:, :, :N[2] // 2 + 1])                 # 340-341
+        Pk_grid = self.Pk0_grid if Pk_grid is None else Pk_grid
+        rand = rand * np.sqrt(Pk_grid) * N.prod() / np.sqrt(self.volume)        # 344
+        if self.pixel_window != "none" and include_pixel_window:               # 347-348
+            rand = rand * self.pixel_window_grid
+        return rand
+
+    def reference_noise(self, seed):
+        """The reference's own draw: legacy MT19937 gaussians, real part first (base.py:316, 332)."""
+        rs = np.random.RandomState(seed)
+        re = rs.randn(*self.gridsize)
+        im = rs.randn(*self.gridsize)
+        return re, im
+
+    def applyAinv_fourier(self, a):
+        """A^-1 a = a invP (/W^2)  (base.py:364-389), Fourier in and out."""
+        out = a * self.invPk0_grid
+        if self.pixel_window != "none":
+            out = self.div_fourier(self.div_fourier(out, self.pixel_window_grid), self.pixel_window_grid)
+        return out
+
+
+# --------------------------------------------------------------------------------------
+# power spectrum (pspec.py)
+# --------------------------------------------------------------------------------------
+class OraclePSpec:
+    def __init__(self, base, k_bins, lmax=2, mask=None):
+        self.base = base
+        self.k_bins = np.asarray(k_bins, dtype=np.float64)
+        self.lmax = lmax
+        self.Nk = len(k_bins) - 1
+        self.Nl = lmax // 2 + 1                                      # pspec.py:38 (odd_l=False)
+        self.N_bins = self.Nk * self.Nl
+        if mask is None:                                             # pspec.py:62-81
+            self.const_mask, self.mask_mean, self.sq_mask_mean = True, 1.0, 1.0
+        else:
+            self.mask = np.asarray(mask, dtype=np.float64)
+            if np.std(self.mask) < 1e-12:
+                self.const_mask = True
+                self.mask_mean = np.mean(self.mask)
+            else:
+                self.const_mask = False
+            self.sq_mask_mean = np.mean(self.mask ** 2)
+
+    def numerator(self, data, filtering="ideal"):
+        """_compute_pk_numerator, global sightline (pspec.py:613-686); trivial S^-1."""
+        b = self.base
+        data = np.asarray(data, dtype=np.float64)
+        x = b.to_fourier(data)
+        if b.pixel_window != "none":
+            x = b.div_fourier(x, b.pixel_window_grid)
+        if filtering == "ideal":
+            x = x * b.invPk0_grid / np.sqrt(self.sq_mask_mean)
+        out = np.zeros(self.N_bins)
+        for li in range(self.Nl):
+            out[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.integrate(x, self.k_bins, 2 * li)
+        return out * b.volume / b.gridsize.prod() ** 2
+
+    def fisher_ideal(self, discreteness_correction=True):
+        """compute_fisher_ideal with the base fiducial spectrum (pspec.py:702-752)."""
+        b = self.base
+        fish = np.zeros((self.N_bins, self.N_bins))
+        if discreteness_correction:
+            for la in range(self.Nl):
+                for lb in range(self.Nl):
+                    fish[la * self.Nk:(la + 1) * self.Nk, lb * self.Nk:(lb + 1) * self.Nk] = np.diag(
+                        0.5 * b.real_integrate_double(b.invPk0_grid, 2 * la, 2 * lb, self.k_bins))
+        else:
+            d = 0.5 * b.real_integrate_double(b.invPk0_grid, 0, 0, self.k_bins)
+            for la in range(self.Nl):
+                fish[la * self.Nk:(la + 1) * self.Nk, la * self.Nk:(la + 1) * self.Nk] = np.diag(d) / (4.0 * la + 1.0)
+        return fish
+
+    def Pk_ideal(self, data, fish=None):
+        fish = self.fisher_ideal() if fish is None else fish
+        out = np.linalg.inv(fish) @ self.numerator(data, "ideal")      # pspec.py:775
+        return {"p%d" % (2 * li): out[li * self.Nk:(li + 1) * self.Nk] for li in range(self.Nl)}
+
+    def fisher_contribution(self, noise_pair):
+        """_compute_fisher global, no covariance, no theory, trivial S^-1 (pspec.py:215-493)."""
+        b = self.base
+        a = b.grf_from_noise(*noise_pair)                                # pspec.py:266
+        if not self.const_mask:
+            a_real = b.to_real(a)                                        # 268
+        Ainv = b.applyAinv_fourier(a)                                    # 328
+        if self.const_mask:                                              # 273-276
+            SinvP = self.mask_mean * a
+        else:
+            SinvP = b.to_fourier(self.mask * a_real)
+        fish = np.zeros((self.N_bins, self.N_bins))
+        scaling = 0.5 * b.volume / b.gridsize.prod() ** 2                # 390
+        for li in range(self.Nl):
+            for ki in range(self.Nk):
+                kmap = b.fourier_filter(SinvP, 2 * li, self.k_bins[ki], self.k_bins[ki + 1])
+                if self.const_mask:                                      # 296-304
+                    Q = self.mask_mean * kmap
+                else:
+                    Q = b.to_fourier(self.mask * b.to_real(kmap))
+                row = li * self.Nk + ki
+                for lp in range(self.Nl):                                # 394-401
+                    fish[row, lp * self.Nk:(lp + 1) * self.Nk] += scaling * b.cross_integrate(
+                        Ainv, Q, self.k_bins, 2 * lp)
+        return fish
+
+
+# --------------------------------------------------------------------------------------
+# bispectrum (bspec.py)
+# --------------------------------------------------------------------------------------
+def check_bin(k_bins, k_bins_squeeze, b1, b2, b3, include_partial_triangles=False):
+    """Triangle test on bin centres, or on bin edges for partial triangles (bspec.py:171-199)."""
+    ks = k_bins_squeeze
+    if include_partial_triangles:
+        k3_hi = ks[b1 + 1] + ks[b2 + 1]
+        if b1 > b2:
+            k3_lo = ks[b1] - ks[b2 + 1]
+        elif b1 == b2:
+            k3_lo = 0.0
+        else:
+            k3_lo = ks[b2] - ks[b1 + 1]
+        return not (ks[b3] >= k3_hi - 1e-10 or ks[b3 + 1] <= k3_lo + 1e-10)
+    k1 = 0.5 * (k_bins[b1] + k_bins[b1 + 1])
+    k2 = 0.5 * (ks[b2] + ks[b2 + 1])
+    k3 = 0.5 * (ks[b3] + ks[b3 + 1])
+    return not (k3 < abs(k1 - k2) or k3 > k1 + k2)
+
+
+def all_bins_list(k_bins, lmax, k_bins_squeeze=None, include_partial_triangles=False):
+    """(b1,b2,b3,l) rows, l outer, b1<=b2<=b3 (bspec.py:67-75)."""
+    k_bins = np.asarray(k_bins)
+    ks = k_bins if k_bins_squeeze is None else np.asarray(k_bins_squeeze)
+    Nk, Nks = len(k_bins) - 1, len(ks) - 1
+    rows = []
+    for l in range(0, lmax + 1, 2):
+        for b1 in range(Nk):
+            for b2 in range(b1, Nks):
+                for b3 in range(b2, Nks):
+                    if check_bin(k_bins, ks, b1, b2, b3, include_partial_triangles):
+                        rows.append((b1, b2, b3, l))
+    return np.asarray(rows, dtype=np.int64)
+
+
+class OracleBSpec:
+    def __init__(self, base, k_bins, lmax=0, mask=None, k_bins_squeeze=None,
+                 include_partial_triangles=False):
+        self.base = base
+        self.k_bins = np.asarray(k_bins, dtype=np.float64)
+        self.k_bins_squeeze = self.k_bins.copy() if k_bins_squeeze is None else np.asarray(k_bins_squeeze, dtype=np.float64)
+        self.lmax = lmax
+        self.Nk = len(self.k_bins) - 1
+        self.Nk_squeeze = len(self.k_bins_squeeze) - 1
+        self.Nl = lmax // 2 + 1
+        self.all_bins = all_bins_list(self.k_bins, lmax, self.k_bins_squeeze, include_partial_triangles)
+        self.N_bins = len(self.all_bins)
+        self.N3 = self.N_bins // self.Nl
+        if mask is None:                                                 # bspec.py:87-106
+            self.const_mask, self.mask_mean, self.cube_mask_mean = True, 1.0, 1.0
+        else:
+            self.mask = np.asarray(mask, dtype=np.float64)
+            if np.std(self.mask) < 1e-12:
+                self.const_mask = True
+                self.mask_mean = np.mean(self.mask)
+            else:
+                self.const_mask = False
+            self.cube_mask_mean = np.mean(self.mask ** 3)
+        # Pk_fid=None: unit weighting on k >= kF/10 grid (bspec.py:139-153)
+        b = base
+        k_tmp = np.arange(np.min(b.kF) / 10.0, np.max(b.kNy) * 2, np.min(b.kF) / 10.0)
+        P = interp1d(k_tmp, 1.0 + 0.0 * k_tmp, bounds_error=False, fill_value=0.0)(b.modk_grid)
+        self.invPk0 = np.zeros(P.shape)
+        self.invPk0[P != 0] = 1.0 / P[P != 0]
+
+    def triplet_index(self):
+        """Map-index triplets for assemble_b3 over maps ordered (l/2, b)."""
+        nb = self.Nk_squeeze
+        ab = self.all_bins
+        return np.stack([ab[:, 0], ab[:, 1], (ab[:, 3] // 2) * nb + ab[:, 2]], axis=1)
+
+    def symmetry_factor(self):
+        """_compute_symmetry_factor (bspec.py:222-279)."""
+        b = self.base
+        sym = []
+        for (b1, b2, b3, l) in self.all_bins[self.all_bins[:, 3] == 0]:
+            if b1 == b2 and b1 == b3:
+                sym.append(6.0)
+            elif b1 == b2 or b1 == b3 or b2 == b3:
+                sym.append(2.0)
+            else:
+                sym.append(1.0)
+        if self.lmax > 0:
+            ks = self.k_bins_squeeze
+            invP = self.invPk0.astype(np.complex128)
+            bins = np.asarray([b.to_real(b.fourier_filter(invP, 0, ks[i], ks[i + 1]))
+                               for i in range(self.Nk_squeeze)])
+            ylm = real_harmonics_fourier(b.k_grids, self.lmax)
+            for l in range(2, self.lmax + 1, 2):
+                bin23 = np.zeros_like(bins)
+                for i in range(self.Nk_squeeze):
+                    m = b.in_bin(ks[i], ks[i + 1])
+                    for y in ylm[l]:
+                        km = np.zeros(b.modk_grid.shape, dtype=np.complex128)
+                        km[m] = invP[m] * y[m]
+                        bin23[i] += b.to_real(km) ** 2
+                for (b1, b2, b3, ll) in self.all_bins[self.all_bins[:, 3] == l]:
+                    if b1 != b2 and b2 != b3:
+                        sym.append(1.0)
+                    elif b1 == b2 and b2 != b3:
+                        sym.append(2.0)
+                    elif b1 != b2 and b2 == b3:
+                        sym.append(1.0 + np.sum(bins[b1] * bin23[b3]) / np.sum(bins[b1] * bins[b3] * bins[b3]))
+                    else:
+                        sym.append(2.0 * (1.0 + 2.0 * np.sum(bins[b3] * bin23[b3]) / np.sum(bins[b3] ** 3)))
+        return np.asarray(sym)
+
+    def g_maps(self, weighted_fourier):
+        """g[l/2, b] = irfftn(Theta_b L_l x)  (bspec.py:936-956)."""
+        b = self.base
+        ks = self.k_bins_squeeze
+        g = np.zeros((self.Nl, self.Nk_squeeze) + tuple(b.gridsize))
+        for l in range(0, self.lmax + 1, 2):
+            for i in range(self.Nk_squeeze):
+                g[l // 2, i] = b.to_real(b.fourier_filter(weighted_fourier, l, ks[i], ks[i + 1]))
+        return g
+
+    def weighted_data(self, data, filtering="ideal"):
+        """S^-1 d in Fourier space (bspec.py:912-929); trivial S^-1 for 'Sinv'."""
+        b = self.base
+        x = b.to_fourier(np.asarray(data, dtype=np.float64))
+        if b.pixel_window != "none":
+            x = b.div_fourier(x, b.pixel_window_grid)
+        if filtering == "ideal":
+            x = x * self.invPk0 / self.cube_mask_mean ** (1.0 / 3.0)
+        return x
+
+    def numerator(self, data, filtering="ideal", sym=None):
+        """_compute_bk_numerator without the linear term (bspec.py:895-983)."""
+        b = self.base
+        sym = self.symmetry_factor() if sym is None else sym
+        g = self.g_maps(self.weighted_data(data, filtering))
+        flat = g.reshape(self.Nl * self.Nk_squeeze, -1)
+        B3 = triplet_sum(flat, flat, flat, self.triplet_index(), b.nthreads)
+        return B3 * b.volume / b.gridsize.prod() / sym
+
+    def fisher_ideal(self, discreteness_correction=True, sym=None):
+        """compute_fisher_ideal (bspec.py:999-1083)."""
+        b = self.base
+        sym = self.symmetry_factor() if sym is None else sym
+        ks = self.k_bins_squeeze
+        invP = self.invPk0.astype(np.complex128)
+        nb = self.Nk_squeeze
+        ab = self.all_bins[:self.N3, :3]
+        if discreteness_correction:
+            fish = np.zeros((self.N_bins, self.N_bins))
+            u = np.asarray([[b.to_real(b.fourier_filter(invP, l, ks[i], ks[i + 1])) for i in range(nb)]
+                            for l in range(0, self.lmax + 1, 2)])
+            for l in range(0, self.lmax + 1, 2):
+                for lp in range(l, self.lmax + 1, 2):
+                    ull = np.asarray([b.to_real(b.fourier_filter(invP, l, ks[i], ks[i + 1], l2=lp))
+                                      for i in range(nb)])
+                    T1 = triplet_sum(u[0], u[0], ull, ab, b.nthreads)
+                    T2 = triplet_sum(u[0], u[l // 2], u[lp // 2], ab, b.nthreads)
+                    for i in range(self.N3):
+                        b1, b2, b3 = ab[i]
+                        if b1 != b2 and b2 != b3:
+                            v = T1[i]
+                        elif b1 == b2 and b2 != b3:
+                            v = 2.0 * T1[i]
+                        elif b1 != b2 and b2 == b3:
+                            v = T2[i] + T1[i]
+                        else:
+                            v = 4.0 * T2[i] + 2.0 * T1[i]
+                        fish[l // 2 * self.N3 + i, lp // 2 * self.N3 + i] = v
+            fish = fish + fish.T - np.diag(np.diag(fish))
+            fish = fish / np.outer(sym, sym) * b.gridsize.prod() ** 2 / b.volume
+        else:
+            u0 = np.asarray([b.to_real(b.fourier_filter(invP, 0, ks[i], ks[i + 1])) for i in range(nb)])
+            Ntri = triplet_sum(u0, u0, u0, ab, b.nthreads)
+            d = np.concatenate([Ntri / (2.0 * l + 1.0) for l in range(0, self.lmax + 1, 2)])
+            fish = np.diag(d / sym) * b.gridsize.prod() ** 2 / b.volume
+        return fish
+
+    def Bk_ideal(self, data, fish=None, sym=None):
+        sym = self.symmetry_factor() if sym is None else sym
+        fish = self.fisher_ideal(sym=sym) if fish is None else fish
+        out = np.linalg.inv(fish) @ self.numerator(data, "ideal", sym=sym)   # bspec.py:1110
+        return {"b%d" % l: out[l // 2 * self.N3:(l // 2 + 1) * self.N3] for l in range(0, self.lmax + 1, 2)}
+
+    def fisher_contribution(self, noise1, noise2, sym=None, return_Q=False):
+        """_compute_fisher, global sightline, no covariance, trivial S^-1 (bspec.py:473-676)."""
+        b = self.base
+        sym = self.symmetry_factor() if sym is None else sym
+        ks = self.k_bins_squeeze
+        ab = self.all_bins
+        nks = self.Nk_squeeze
+        a1 = b.grf_from_noise(*noise1)                                   # 648-649
+        a2 = b.grf_from_noise(*noise2)
+        if not self.const_mask:
+            ar1, ar2 = b.to_real(a1), b.to_real(a2)                      # 651-653
+
+        def apply_filter(x_fourier=None, x_real=None):                   # 499-505
+            if self.const_mask:
+                return self.mask_mean * x_fourier
+            return b.to_fourier(self.mask * x_real)
+
+        def g_sets(w1, w2):
+            g1 = np.asarray([b.to_real(b.fourier_filter(w1, 0, ks[i], ks[i + 1])) for i in range(nks)])
+            g2 = np.asarray([b.to_real(b.fourier_filter(w2, 0, ks[i], ks[i + 1])) for i in range(nks)])
+            return g1, g2
+
+        def gl_maps(w, B):
+            return [b.to_real(b.fourier_filter(w, l, ks[B], ks[B + 1])) for l in range(2, self.lmax + 1, 2)]
+
+        Nh = b.modk_grid.shape
+        Q = np.zeros((self.N_bins,) + Nh, dtype=np.complex128)           # 643
+        # Q[A^-1 a] (compute_Q 'Ainv', 521-640)
+        w1, w2 = b.applyAinv_fourier(a1), b.applyAinv_fourier(a2)
+        g1, g2 = g_sets(w1, w2)
+        for B in range(nks):
+            gl1, gl2 = (gl_maps(w1, B), gl_maps(w2, B)) if self.lmax > 0 else ([], [])
+            for A in range(B + 1):
+                i1 = np.where((ab[:, 0] == A) & (ab[:, 1] == B))[0]
+                i2 = np.where((ab[:, 1] == A) & (ab[:, 2] == B))[0]
+                i3 = np.where((ab[:, 2] == B) & (ab[:, 0] == A))[0]
+                if len(i1) + len(i2) + len(i3) == 0:
+                    continue
+                ft = [b.to_fourier(g1[A] * g1[B] - g2[A] * g2[B])]
+                for l in range(2, self.lmax + 1, 2):
+                    ft.append(b.to_fourier(g1[A] * gl1[l // 2 - 1] - g2[A] * gl2[l // 2 - 1]))
+                for ii in i1:                                            # leg b3, L_l on it
+                    C, l = ab[ii, 2], ab[ii, 3]
+                    Q[ii] += b.fourier_filter(ft[0], l, ks[C], ks[C + 1])
+                for ii in i2:                                            # leg b1
+                    C, l = ab[ii, 0], ab[ii, 3]
+                    Q[ii] += b.fourier_filter(ft[l // 2], 0, ks[C], ks[C + 1])
+                for ii in i3:                                            # leg b2
+                    C, l = ab[ii, 1], ab[ii, 3]
+                    Q[ii] += b.fourier_filter(ft[l // 2], 0, ks[C], ks[C + 1])
+        for i in range(self.N_bins):                                     # 662-666
+            Q[i] = apply_filter(Q[i], None if self.const_mask else b.to_real(Q[i]))
+        # Q[S^-1 P a] rows (compute_Q 'Sinv')
+        if self.const_mask:
+            w1, w2 = apply_filter(a1), apply_filter(a2)
+        else:
+            w1, w2 = apply_filter(None, ar1), apply_filter(None, ar2)
+        g1, g2 = g_sets(w1, w2)
+        fish = np.zeros((self.N_bins, self.N_bins))
+        for B in range(nks):
+            gl1, gl2 = (gl_maps(w1, B), gl_maps(w2, B)) if self.lmax > 0 else ([], [])
+            for A in range(B + 1):
+                these = np.where((ab[:, 2] == B) & (ab[:, 0] == A))[0]
+                if len(these) == 0:
+                    continue
+                for l in range(0, self.lmax + 1, 2):
+                    if l == 0:
+                        ft = b.to_fourier(g1[A] * g1[B] - g2[A] * g2[B])
+                    else:
+                        ft = b.to_fourier(g1[A] * gl1[l // 2 - 1] - g2[A] * gl2[l // 2 - 1])
+                    for ii in these[ab[these, 3] == l]:
+                        s = ab[ii, 1]
+                        fish[ii] = b.integrate_row(ft, Q, ks[s], ks[s + 1])
+        fish = 0.5 * fish * b.volume / b.gridsize.prod() ** 2 / np.outer(sym, sym)   # 674
+        if return_Q:
+            return fish, Q
+        return fish

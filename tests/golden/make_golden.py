@@ -1,0 +1,248 @@
+"""Generate the golden fixtures under tests/golden/ by running the REFERENCE itself.
+
+Run in a container that holds the reference tree (its Python read in place, its Cython
+kernels compiled into oracle/_ref/ by oracle/build_ref.sh):
+
+    python tests/golden/make_golden.py
+
+Every input is regenerated from a seed by polybin3d_b200.synthetic (numpy), so the
+fixtures hold only the case parameters and the reference's outputs.  The Monte Carlo
+Fisher cases use the reference's own `generate_data(seed)` (legacy MT19937 noise); the
+reference's Q-maps are captured by wrapping its integrator object and recording the
+map arguments of `cross_integrate` (pspec.py:386) and `integrate_row` (bspec.py:597).
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, HERE)
+
+from polybin3d_b200 import synthetic  # noqa: E402
+from reference_harness import load_reference  # noqa: E402
+
+CASES = {}
+
+
+def case(fn):
+    CASES[fn.__name__] = fn
+    return fn
+
+
+class _Capture:
+    """Proxy around the reference's IntegrationUtils recording Q-map arguments."""
+
+    def __init__(self, inner):
+        self._inner = inner
+        self.q_rows = []
+        self.q_array = None
+
+    def cross_integrate(self, s1, s2, k_edges, l):
+        if l == 0:
+            self.q_rows.append(np.array(s2))
+        return self._inner.cross_integrate(s1, s2, k_edges, l)
+
+    def integrate_row(self, input_map, input_array, kmin, kmax):
+        if self.q_array is None:
+            self.q_array = np.array(input_array)
+        return self._inner.integrate_row(input_map, input_array, kmin, kmax)
+
+    def __getattr__(self, name):
+        return getattr(self._inner, name)
+
+
+def _quiet(fn, *a, **k):
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        return fn(*a, **k)
+
+
+@case
+def cfg1(pb):
+    """64^3, L=1000, 10 linear bins of width 2kF from kF, no window, FP64 GRF seed 0."""
+    N, L = 64, 1000.0
+    kF = 2 * np.pi / L
+    edges = kF + 2 * kF * np.arange(11)
+    data = synthetic.grf(N, L, seed=0)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="none", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=2)
+    pk = _quiet(ps.Pk_ideal, data)
+    bs = _quiet(pb.BSpec, base, edges, lmax=0)
+    bk = _quiet(bs.Bk_ideal, data)
+    out = dict(N=N, L=L, edges=edges, data_seed=0, data_kind="grf", pw="none", pk_lmax=2, bk_lmax=0,
+               pk_num=_quiet(ps.Pk_numerator_ideal, data), pk_fish=ps.fish_ideal,
+               bk_bins=bs.all_bins, bk_sym=bs.sym_factor, bk_num=_quiet(bs.Bk_numerator_ideal, data),
+               bk_fish=bs.fish_ideal)
+    for k, v in pk.items():
+        out["Pk_" + k] = v
+    for k, v in bk.items():
+        out["Bk_" + k] = v
+    return out
+
+
+@case
+def bk_l2_tsc(pb):
+    """32^3, L=500, TSC window, lmax=2, 6 bins to 0.15; float32 lognormal seed 3."""
+    N, L = 32, 500.0
+    edges = np.linspace(2 * np.pi / L, 0.15, 7)
+    data = synthetic.lognormal(N, L, seed=3)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="tsc", backend="mkl")
+    bs = _quiet(pb.BSpec, base, edges, lmax=2)
+    bk = _quiet(bs.Bk_ideal, data)
+    out = dict(N=N, L=L, edges=edges, data_seed=3, data_kind="lognormal", pw="tsc", bk_lmax=2,
+               bk_bins=bs.all_bins, bk_sym=bs.sym_factor, bk_num=_quiet(bs.Bk_numerator_ideal, data),
+               bk_fish=bs.fish_ideal)
+    for k, v in bk.items():
+        out["Bk_" + k] = v
+    bs2 = _quiet(pb.BSpec, base, edges, lmax=2)
+    out["bk_fish_nodisc"] = _quiet(bs2.compute_fisher_ideal, discreteness_correction=False)
+    return out
+
+
+@case
+def bk_squeeze_partial(pb):
+    """24^3, squeezed bins + partial triangles, lmax=0, CIC window, GRF seed 4."""
+    N, L = 24, 400.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.12, 4)
+    sq = np.concatenate([edges, [0.15, 0.18]])
+    data = synthetic.grf(N, L, seed=4)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="mkl")
+    bs = _quiet(pb.BSpec, base, edges, lmax=0, k_bins_squeeze=sq, include_partial_triangles=True)
+    bk = _quiet(bs.Bk_ideal, data)
+    out = dict(N=N, L=L, edges=edges, edges_sq=sq, data_seed=4, data_kind="grf", pw="cic", bk_lmax=0,
+               bk_bins=bs.all_bins, bk_sym=bs.sym_factor, bk_num=_quiet(bs.Bk_numerator_ideal, data),
+               bk_fish=bs.fish_ideal)
+    for k, v in bk.items():
+        out["Bk_" + k] = v
+    return out
+
+
+@case
+def pk_windows(pb):
+    """32^3, L=400, lmax=4, tabulated fiducial P(k), CIC and interlaced-TSC windows."""
+    N, L = 32, 400.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.22, 6)
+    data = synthetic.lognormal(N, L, seed=7)
+    out = dict(N=N, L=L, edges=edges, data_seed=7, data_kind="lognormal", pk_lmax=4)
+    for pw in ["cic", "interlaced-tsc"]:
+        base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, Pk=synthetic.pk_table(1.0), pixel_window=pw, backend="mkl")
+        ps = _quiet(pb.PSpec, base, edges, lmax=4)
+        pk = _quiet(ps.Pk_ideal, data)
+        tag = pw.replace("-", "_")
+        out[tag + "_num"] = _quiet(ps.Pk_numerator_ideal, data)
+        out[tag + "_fish"] = ps.fish_ideal
+        for k, v in pk.items():
+            out[tag + "_Pk_" + k] = v
+        out[tag + "_fish_nodisc"] = _quiet(ps.compute_fisher_ideal, discreteness_correction=False)
+    return out
+
+
+@case
+def grf_noise(pb):
+    """generate_data(seed=5, fourier) at 16^3 with a tabulated P(k) and CIC window."""
+    N, L = 16, 300.0
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, Pk=synthetic.pk_table(1.0), pixel_window="cic", backend="mkl")
+    a = base.generate_data(seed=5, output_type="fourier")
+    return dict(N=N, L=L, seed=5, pw="cic", a=a)
+
+
+def _mask24(N, L):
+    return synthetic.shell_mask(N, L, r_in=L / 6, r_out=0.4667 * L, n_holes=10, hole_r=(10.0, 30.0),
+                                hole_box=0.4667 * L, seed=0)
+
+
+@case
+def pk_fisher_mask(pb):
+    """24^3, L=600, lmax=4, 4 bins, shell-sector mask; seeds 0,1; Q-maps of seed 0."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="none", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=4, mask=mask)
+    cap = _Capture(base.integrator)
+    base.integrator = cap
+    f0 = ps.compute_fisher_contribution(0)
+    q0 = np.asarray(cap.q_rows)
+    base.integrator = cap._inner
+    f1 = ps.compute_fisher_contribution(1)
+    fish = 0.5 * (f0 + f1)
+    data = (synthetic.lognormal(N, L, seed=11).astype(np.float64) * mask)
+    pk = _quiet(ps.Pk_unwindowed, data, fish=fish)
+    out = dict(N=N, L=L, edges=edges, pk_lmax=4, f0=f0, f1=f1, q0=q0, data_seed=11,
+               num=ps.Pk_numerator(data))
+    for k, v in pk.items():
+        out["Pk_" + k] = v
+    return out
+
+
+@case
+def pk_fisher_nomask(pb):
+    """24^3, L=600, lmax=2, 4 bins, no mask, TSC window; seed 2."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="tsc", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=2)
+    return dict(N=N, L=L, edges=edges, pk_lmax=2, pw="tsc", f2=ps.compute_fisher_contribution(2))
+
+
+@case
+def bk_fisher_mask(pb):
+    """24^3, L=600, lmax=0 and lmax=2, 4 bins, shell-sector mask; seed 0; Q_Ainv of lmax=0."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="none", backend="mkl")
+    bs = _quiet(pb.BSpec, base, edges, lmax=0, mask=mask)
+    cap = _Capture(base.integrator)
+    base.integrator = cap
+    f0 = _quiet(bs.compute_fisher_contribution, 0)
+    q0 = cap.q_array
+    base.integrator = cap._inner
+    data = (synthetic.lognormal(N, L, seed=12).astype(np.float64) * mask)
+    bk = _quiet(bs.Bk_unwindowed, data, fish=f0 + np.eye(len(f0)) * 0.0, include_linear_term=False)
+    bs2 = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask)
+    f2 = _quiet(bs2.compute_fisher_contribution, 0)
+    out = dict(N=N, L=L, edges=edges, bins0=bs.all_bins, sym0=bs.sym_factor, f0=f0, q0=q0,
+               bins2=bs2.all_bins, sym2=bs2.sym_factor, f2_l2=f2, data_seed=12,
+               num0=_quiet(bs.Bk_numerator, data, include_linear_term=False))
+    for k, v in bk.items():
+        out["Bk_" + k] = v
+    return out
+
+
+@case
+def bk_fisher_nomask(pb):
+    """24^3, L=600, lmax=2, 4 bins, no mask, CIC window; seed 3."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="mkl")
+    bs = _quiet(pb.BSpec, base, edges, lmax=2)
+    f3 = _quiet(bs.compute_fisher_contribution, 3)
+    return dict(N=N, L=L, edges=edges, bk_lmax=2, pw="cic", bins=bs.all_bins, sym=bs.sym_factor, f3=f3)
+
+
+def main(names=None):
+    pb = load_reference()
+    for name, fn in CASES.items():
+        if names and name not in names:
+            continue
+        t = time.time()
+        out = fn(pb)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **{k: np.asarray(v) for k, v in out.items()})
+        print("%-22s %6.1fs  %8.1f KB" % (name, time.time() - t, os.path.getsize(path) / 1024))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

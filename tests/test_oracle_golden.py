@@ -1,0 +1,145 @@
+"""Pin the oracle to the reference: every golden fixture (made by running the reference,
+tests/golden/make_golden.py) is reproduced by oracle/polybin_oracle.py."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import polybin_oracle as O
+from polybin3d_b200 import synthetic
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-11
+
+
+def gold(name):
+    return np.load(os.path.join(GOLD, name + ".npz"))
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+def field(g):
+    kind, seed, N, L = str(g["data_kind"]), int(g["data_seed"]), int(g["N"]), float(g["L"])
+    return synthetic.grf(N, L, seed) if kind == "grf" else synthetic.lognormal(N, L, seed)
+
+
+def mask24(N, L):
+    return synthetic.shell_mask(N, L, r_in=L / 6, r_out=0.4667 * L, n_holes=10, hole_r=(10.0, 30.0),
+                                hole_box=0.4667 * L, seed=0)
+
+
+def test_cfg1_pk_bk():
+    g = gold("cfg1")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3)
+    d = field(g)
+    ps = O.OraclePSpec(b, g["edges"], lmax=2)
+    assert rel(ps.numerator(d), g["pk_num"]) < TOL
+    assert rel(ps.fisher_ideal(), g["pk_fish"]) < TOL
+    pk = ps.Pk_ideal(d)
+    for k in pk:
+        assert rel(pk[k], g["Pk_" + k]) < TOL
+    bs = O.OracleBSpec(b, g["edges"], lmax=0)
+    assert np.array_equal(bs.all_bins, g["bk_bins"])
+    sym = bs.symmetry_factor()
+    assert np.array_equal(sym, g["bk_sym"])
+    assert rel(bs.numerator(d, sym=sym), g["bk_num"]) < TOL
+    assert rel(bs.fisher_ideal(sym=sym), g["bk_fish"]) < TOL
+    bk = bs.Bk_ideal(d, sym=sym)
+    assert rel(bk["b0"], g["Bk_b0"]) < TOL
+
+
+def test_bk_lmax2_tsc():
+    g = gold("bk_l2_tsc")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc")
+    bs = O.OracleBSpec(b, g["edges"], lmax=2)
+    assert np.array_equal(bs.all_bins, g["bk_bins"])
+    sym = bs.symmetry_factor()
+    assert rel(sym, g["bk_sym"]) < TOL
+    d = field(g)
+    assert rel(bs.numerator(d, sym=sym), g["bk_num"]) < TOL
+    assert rel(bs.fisher_ideal(sym=sym), g["bk_fish"]) < TOL
+    assert rel(bs.fisher_ideal(False, sym=sym), g["bk_fish_nodisc"]) < TOL
+    bk = bs.Bk_ideal(d, sym=sym)
+    for k in bk:
+        assert rel(bk[k], g["Bk_" + k]) < TOL
+
+
+def test_bk_squeezed_partial_triangles():
+    g = gold("bk_squeeze_partial")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic")
+    bs = O.OracleBSpec(b, g["edges"], lmax=0, k_bins_squeeze=g["edges_sq"], include_partial_triangles=True)
+    assert np.array_equal(bs.all_bins, g["bk_bins"])
+    d = field(g)
+    sym = bs.symmetry_factor()
+    assert rel(bs.numerator(d, sym=sym), g["bk_num"]) < TOL
+    bk = bs.Bk_ideal(d, sym=sym)
+    assert rel(bk["b0"], g["Bk_b0"]) < TOL
+
+
+@pytest.mark.parametrize("pw", ["cic", "interlaced-tsc"])
+def test_pk_windows_tabulated_pk(pw):
+    g = gold("pk_windows")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, Pk=synthetic.pk_table(1.0), pixel_window=pw)
+    ps = O.OraclePSpec(b, g["edges"], lmax=4)
+    d = field(g)
+    tag = pw.replace("-", "_")
+    assert rel(ps.numerator(d), g[tag + "_num"]) < TOL
+    assert rel(ps.fisher_ideal(), g[tag + "_fish"]) < TOL
+    assert rel(ps.fisher_ideal(False), g[tag + "_fish_nodisc"]) < TOL
+
+
+def test_grf_from_reference_noise():
+    g = gold("grf_noise")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, Pk=synthetic.pk_table(1.0), pixel_window="cic")
+    assert rel(b.grf_from_noise(*b.reference_noise(int(g["seed"]))), g["a"]) < 1e-14
+
+
+def test_pk_fisher_masked_and_qmaps():
+    g = gold("pk_fisher_mask")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3)
+    ps = O.OraclePSpec(b, g["edges"], lmax=4, mask=mask24(N, L))
+    f0 = ps.fisher_contribution(b.reference_noise(0 + 10 ** 7))
+    f1 = ps.fisher_contribution(b.reference_noise(1 + 10 ** 7))
+    assert rel(f0, g["f0"]) < TOL and rel(f1, g["f1"]) < TOL
+
+
+def test_pk_fisher_nomask():
+    g = gold("pk_fisher_nomask")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc")
+    ps = O.OraclePSpec(b, g["edges"], lmax=2)
+    assert rel(ps.fisher_contribution(b.reference_noise(2 + 10 ** 7)), g["f2"]) < TOL
+
+
+def test_bk_fisher_masked_and_qmaps():
+    g = gold("bk_fisher_mask")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3)
+    m = mask24(N, L)
+    bs = O.OracleBSpec(b, g["edges"], lmax=0, mask=m)
+    assert np.array_equal(bs.all_bins, g["bins0"])
+    f, Q = bs.fisher_contribution(b.reference_noise(10 ** 7), b.reference_noise(2 * 10 ** 7), return_Q=True)
+    assert rel(f, g["f0"]) < TOL
+    assert rel(Q, g["q0"]) < TOL
+    bs2 = O.OracleBSpec(b, g["edges"], lmax=2, mask=m)
+    f2 = bs2.fisher_contribution(b.reference_noise(10 ** 7), b.reference_noise(2 * 10 ** 7))
+    assert rel(f2, g["f2_l2"]) < TOL
+
+
+def test_bk_fisher_nomask_lmax2():
+    g = gold("bk_fisher_nomask")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic")
+    bs = O.OracleBSpec(b, g["edges"], lmax=2)
+    assert rel(bs.symmetry_factor(), g["sym"]) < TOL
+    f = bs.fisher_contribution(b.reference_noise(3 + 10 ** 7), b.reference_noise(3 + 2 * 10 ** 7))
+    assert rel(f, g["f3"]) < TOL
