@@ -1,0 +1,331 @@
+"""Benchmark: Bk_ideal fields/s at 256^3 (16 bins, lmax=2, TSC, mixed precision).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--contraction auto|tc|simt]
+
+One step = one float32 lognormal field through BSpec.Bk_ideal: r2c, one fused filter
+launch writing the 32 bin-filtered half spectra (Theta_b L_l / W_TSC), one batched c2r,
+the triplet contraction over 888 bin triplets, and the inverse ideal Fisher (cached, as
+the reference caches it).  `value` times that on device-resident fields; `e2e` times the
+public call Bk_ideal(field) on pinned host fields, H2D copy and result readback included.
+Under torchrun every rank runs independent fields (replicas: a 256^3 field does not
+shard), timing is the max over ranks and `value` counts all ranks' fields.
+
+--impl reference times the reference's own CPU implementation of the same step on the
+host cores: its compiled Cython assemble_b3 (oracle/_ref, built from the reference's
+utils.pyx) with FP64 scipy FFTs and the filter loop of bspec.py:912-956, on a bounded
+sample of each field's triplets when a whole field would take too long.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+N, L, LMAX, NK = 256, 2000.0, 2, 16
+EDGES = np.linspace(2 * np.pi / L, 0.2, NK + 1)
+METRIC = "Bk fields/s at 256^3 (16 bins, lmax=2, TSC, mixed precision)"
+WORKLOAD = "Bk_ideal 256^3 box 2000 Mpc/h, TSC, lmax=2, 16 linear bins 2pi/2000..0.2, 888 triangle bins"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--contraction", default="auto", choices=["auto", "tc", "simt"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+class Clocks:
+    """Sample nvidia-smi SM clocks and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 6:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[2 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference_step(bs, frac, field, nthreads, ref_utils):
+    """One (sampled) field of the reference's numerator on the host, FP64.
+    Filtering and FFTs follow bspec.py:912-956; the cubic sum is the reference's compiled
+    assemble_b3 when oracle/_ref is built, else the oracle's C loop."""
+    from oracle import polybin_oracle as O
+    x = bs.weighted_data(field, "ideal")
+    g = bs.g_maps(x)
+    ab = bs.all_bins
+    n = int(round(frac * len(ab)))
+    if n == 0:
+        return None
+    sub = np.ascontiguousarray(ab[:n])
+    if ref_utils is not None:
+        B3 = ref_utils.assemble_b3(np.ascontiguousarray(g), sub, nthreads)
+    else:
+        flat = g.reshape(bs.Nl * bs.Nk_squeeze, -1)
+        B3 = O.triplet_sum(flat, flat, flat, bs.triplet_index()[:n], nthreads)
+    return B3
+
+
+def load_ref_utils():
+    import importlib.util
+    d = os.path.join(REPO, "oracle", "_ref")
+    if not os.path.isdir(d):
+        return None
+    for f in os.listdir(d):
+        if f.startswith("pb_ref_utils") and f.endswith(".so"):
+            spec = importlib.util.spec_from_file_location("pb_ref_utils", os.path.join(d, f))
+            m = importlib.util.module_from_spec(spec)
+            try:
+                spec.loader.exec_module(m)
+                return m
+            except Exception:
+                return None
+    return None
+
+
+def cpu_baseline(fields, max_seconds=25.0, warmup=1, steps=2):
+    """Time the CPU path on a bounded sample; returns (fields/s, kind, cores, sample-note)."""
+    from oracle import polybin_oracle as O
+    nthreads = os.cpu_count()
+    ref_utils = load_ref_utils()
+    base = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc", nthreads=nthreads)
+    bs = O.OracleBSpec(base, EDGES, lmax=LMAX)
+    # probe: the per-field part (FFTs, filters) and the cost of 2% of the triplets
+    t = time.perf_counter()
+    cpu_reference_step(bs, 0.0, fields[0], nthreads, ref_utils)
+    t_field = time.perf_counter() - t
+    t = time.perf_counter()
+    cpu_reference_step(bs, 0.02, fields[0], nthreads, ref_utils)
+    t_trip = max(1e-6, time.perf_counter() - t - t_field) / 0.02
+    budget = max_seconds / (warmup + steps)
+    frac = 1.0
+    for f in (1.0, 0.5, 0.25, 0.125, 0.0625, 0.03125):
+        frac = f
+        if t_field + f * t_trip <= budget:
+            break
+    for i in range(warmup):
+        cpu_reference_step(bs, frac, fields[i % len(fields)], nthreads, ref_utils)
+    ts = []
+    for i in range(steps):
+        t = time.perf_counter()
+        cpu_reference_step(bs, frac, fields[i % len(fields)], nthreads, ref_utils)
+        ts.append(time.perf_counter() - t)
+    ts = float(np.median(ts))
+    # a field = the FFT/filter part once + all triplets; only the triplet sum is sampled
+    per_field = ts + (1.0 - frac) * t_trip
+    kind = "reference" if ref_utils is not None else "port"
+    note = ("one 256^3 field per step: 32 FP64 c2r (scipy) + %s over %.1f%% of the 888 triplets; "
+            "fields/s = 1 / (step time + unsampled triplets at the probed rate), median of %d after %d warm-up"
+            % ("reference assemble_b3 (oracle/_ref)" if ref_utils else "oracle C triplet loop",
+               100 * frac, steps, warmup))
+    return 1.0 / per_field, kind, nthreads, note
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from polybin3d_b200 import synthetic
+    fields = [synthetic.lognormal(N, L, seed=s) for s in range(2)]
+    v, kind, cores, note = cpu_baseline(fields, max_seconds=max(30.0, 4.0 * (args.steps + args.warmup)),
+                                        warmup=args.warmup, steps=args.steps)
+    line = {"metric": METRIC, "value": v, "unit": "fields/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded float32 lognormal fields)",
+            "config": {"workload": WORKLOAD}, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "fields/s", "cores": cores, "kind": kind, "sample": note},
+            "e2e": {"value": v, "unit": "fields/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local):
+    import contextlib
+    import io
+
+    import torch
+    import polybin3d_b200 as pb
+    from polybin3d_b200 import _native as nat
+    from polybin3d_b200 import synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    with contextlib.redirect_stdout(io.StringIO()):
+        base = pb.PolyBin3D([L] * 3, [N] * 3, pixel_window="tsc", backend="cuda", precision="mixed")
+        bs = pb.BSpec(base, EDGES, lmax=LMAX, contraction=args.contraction)
+        bs.compute_fisher_ideal()  # one-off, cached (as the reference caches it)
+    method = bs._method(torch.float32)
+    inv_fish = torch.as_tensor(bs.inv_fish_ideal, device=dev)
+    norm = torch.as_tensor(base.volume / float(N ** 3) / bs.sym_factor, device=dev)
+
+    n_pool = 4
+    host = [torch.from_numpy(synthetic.lognormal(N, L, seed=1000 * rank + s)).pin_memory() for s in range(n_pool)]
+    resident = [h.to(dev) for h in host]
+    torch.cuda.synchronize()
+
+    # device-resident step: the Bk_ideal numerator + F^-1, no host sync
+    cev = []
+
+    def step(i, record=False):
+        x = resident[i % n_pool]
+        xk = base.fft_r2c(x)
+        w = bs._data_weight(torch.float32)
+        G = bs._g_maps(xk, w, 1.0)
+        plan = bs._plan("b3", G.shape[0], G.shape[0], G.shape[0], bs._triplet_index())
+        out = torch.empty(plan.n_trip, dtype=torch.float64, device=dev)
+        if record:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        plan.contract(G, G, G, out, base.ws, method=method)
+        if record:
+            e1.record()
+            cev.append((e0, e1))
+        return inv_fish @ (out * norm)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = nat.LAUNCHES[0]
+    with Clocks(local) as clk:
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for i in range(args.steps):
+            res = step(i, record=True)
+        t1.record()
+        torch.cuda.synchronize()
+    launches = nat.LAUNCHES[0] - l0  # kernels of libpb_b200 (cuFFT and torch launches not counted)
+    ms = t0.elapsed_time(t1)
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in cev]))
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * args.steps / (ms / 1000.0)
+
+    # end-to-end through the public API from pinned host memory
+    for i in range(args.warmup):
+        with contextlib.redirect_stdout(io.StringIO()):
+            bs.Bk_ideal(host[i % n_pool])
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        with contextlib.redirect_stdout(io.StringIO()):
+            r = bs.Bk_ideal(host[i % n_pool])
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e = world * args.steps / (e2e_ms / 1000.0)
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        alg_bytes = bs.Nl * bs.Nk_squeeze * N ** 3 * 4  # every map read once
+        achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
+        traffic = None
+        try:
+            prof = json.load(open(os.path.join(REPO, "profiles", "triplet_traffic.json")))
+            traffic = prof.get("bytes_per_launch")
+        except Exception:
+            pass
+        line = {"metric": METRIC, "value": value, "unit": "fields/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 maps / fp64 sums",
+                "data": "synthetic (seeded float32 lognormal fields, pool of 4 per rank)",
+                "config": {"workload": WORKLOAD, "contraction": "tc" if method == nat.PB_TRIPLET_TC else "simt",
+                           "l2": "inputs+intermediates 4.4 GB/step >> 126 MB L2", "parallelism": "replicas"},
+                "e2e": {"value": e2e, "unit": "fields/s", "h2d_bytes_per_step": N ** 3 * 4,
+                        "d2h_bytes_per_step": bs.N_bins * 8},
+                "gpu_launches": launches,
+                "roofline": {"bound": "hbm", "kernel": "triplet contraction", "achieved": achieved,
+                             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                             "alg_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+                "clocks": clk.summary()}
+        if not args.no_cpu_baseline and world == 1:
+            from polybin3d_b200 import synthetic as S
+            v, kind, cores, note = cpu_baseline([host[0].numpy(), host[1].numpy()])
+            line["cpu_baseline"] = {"value": v, "unit": "fields/s", "cores": cores, "kind": kind, "sample": note}
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,197 @@
+/*
+ * polybin3d_b200 — C ABI of the B200-native binned-polyspectrum hot path.
+ *
+ * Every entry point takes raw device pointers, element counts, a `pb_grid_t` describing
+ * the Fourier grid, and a CUDA stream (as void*).  Nothing here allocates device memory:
+ * scratch comes from the caller, sized by the matching *_workspace_size query.  Calls
+ * are stream-ordered and never synchronise the host, so they can be captured in CUDA
+ * graphs.  Status: 0 = ok, negative = error; pb_last_error() gives the message of the
+ * last failure on the calling host thread.
+ *
+ * Layouts (C-contiguous, one "map" per slab):
+ *   real map      double|float [n0][n1][n2]
+ *   half spectrum complex      [n0][n1][n2/2+1], interleaved (re, im), numpy rfftn order:
+ *                 index i on axes 0,1 is frequency i for i < n/2 and i - n otherwise;
+ *                 index l on axis 2 is frequency l (0..n2/2).
+ * Mode geometry is recomputed on the device bit-exactly as the reference builds it in
+ * numpy (PolyBin3D/base.py:86-92, 111-116): k_i = (double)idx * kF_i,
+ * |k| = sqrt((kx*kx + ky*ky) + kz*kz), mu = kz/|k|, deg = 1 + (kz > 0).
+ * A mode is in bin [lo, hi) iff lo <= |k| && |k| < hi  (PolyBin3D/cython/utils.pyx:63).
+ */
+#ifndef POLYBIN3D_B200_H
+#define POLYBIN3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PB_API __attribute__((visibility("default")))
+#else
+#define PB_API
+#endif
+
+#define PB_ABI_VERSION 1
+
+#define PB_OK 0
+#define PB_ERR_INVALID (-1)     /* bad argument (shape, size, null pointer, range)      */
+#define PB_ERR_CUDA (-2)        /* CUDA runtime error                                    */
+#define PB_ERR_CUFFT (-3)       /* cuFFT error                                           */
+#define PB_ERR_WORKSPACE (-4)   /* caller workspace too small                            */
+#define PB_ERR_UNSUPPORTED (-5) /* configuration not built / device not sm_100           */
+#define PB_ERR_TIMEOUT (-6)     /* a bounded device wait expired                        */
+
+#define PB_F32 0
+#define PB_F64 1
+
+typedef struct pb_grid {
+    int32_t n[3];      /* real-space grid; n[2] even                                        */
+    int32_t reserved;  /* 0                                                                 */
+    double kf[3];      /* fundamental frequencies 2 pi / L_i                                */
+} pb_grid_t;
+
+/* Library identity and errors.  No reference counterpart (the reference raises Python
+ * exceptions: e.g. PolyBin3D/base.py:54, pspec.py:591). */
+PB_API int pb_abi_version(void);
+PB_API const char *pb_last_error(void);
+
+/* ---------------------------------------------------------------------------------- */
+/* 3-D real FFTs.  Replace PolyBin3D/base.py:176-229 (`to_fourier`, `to_real`) and the   */
+/* plan set-up of base.py:256-302 (`_fft_setup`).  Forward r2c is unnormalised; the c2r  */
+/* is unnormalised too (the 1/N^3 of numpy's irfftn is folded into the kernels that      */
+/* write its input).  The c2r overwrites its input.                                      */
+/* ---------------------------------------------------------------------------------- */
+typedef struct pb_fft_plan pb_fft_plan;
+#define PB_FFT_R2C 0
+#define PB_FFT_C2R 1
+PB_API int pb_fft_plan_create(const pb_grid_t *g, int batch, int precision, int direction,
+                       pb_fft_plan **plan, size_t *workspace_bytes);
+PB_API int pb_fft_exec(pb_fft_plan *plan, const void *in, void *out, void *workspace, void *stream);
+PB_API int pb_fft_plan_destroy(pb_fft_plan *plan);
+
+/* ---------------------------------------------------------------------------------- */
+/* Spectral filter: writes n_maps half spectra in one pass over the grid.               */
+/*   out[m](k) = [acc ? out[m](k) : 0] + scale[m] * w(k)^wpow[m] * src[src_idx[m]](k)    */
+/*               * Theta(lo[m] <= |k| < hi[m]) * L_{l1[m]}(mu) * L_{l2[m]}(mu)            */
+/* src == NULL means a source of 1 + 0i (used for binning functions of a weight grid).   */
+/* w (real, same precision as the spectra) may be NULL (= 1); wpow in {-1,0,1,2}, where  */
+/* -1 divides (0 where w == 0).  l1, l2 in {0,...,4}.  src and w live on grid g; out may */
+/* live on a smaller grid out_n[3] (NULL = g): each output mode reads the source mode of */
+/* the same frequency, so band-limited maps can be synthesised on a coarser grid.        */
+/* Replaces MapUtils.fourier_filter / fourier_filter_ll / prod_fourier / prod_fourier_  */
+/* filter / div_fourier (PolyBin3D/cython/utils.pyx:213-338) and jax_utils.py:97-100.    */
+/* ---------------------------------------------------------------------------------- */
+#define PB_FILTER_MAX_MAPS 128
+PB_API int pb_spectral_filter(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
+                              int64_t src_stride,
+                       void *out, int n_maps, const int32_t *src_idx, const double *lo,
+                       const double *hi, const int32_t *l1, const int32_t *l2,
+                       const double *scale, const int32_t *wpow, const void *w, int accumulate,
+                       void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* k-bin x Legendre reductions over the half spectrum, FP64 accumulation.                */
+/*   mode PB_RED_ABS2  : f_r = |a_r|^2                 (IntegrationUtils.integrate,       */
+/*                                                      utils.pyx:80-104)                 */
+/*   mode PB_RED_CROSS : f_r = Re(a * conj(b_r))       (cross_integrate, utils.pyx:51-75) */
+/*                       a is one spectrum, b holds n_rows spectra                        */
+/*   mode PB_RED_REAL2 : f = w^2, w = a real per mode  (real_integrate_double,           */
+/*                       (a == NULL: w = 1, mode counts) utils.pyx:109-134)              */
+/*   out[r][e][b] = scale * sum_{lo_b<=|k|<hi_b} deg * f_r * L_{ells[2e]}(mu) L_{ells[2e+1]}(mu)
+/* with lo_b = edges[b], hi_b = edges[b+1] (strictly increasing, host array, nk <= 64),  */
+/* n_ell <= 9 (pairs of Legendre orders, host array).  out is device FP64,              */
+/* accumulate != 0 adds into it.  Deterministic (fixed-order two-pass reduction).       */
+/* ---------------------------------------------------------------------------------- */
+#define PB_RED_ABS2 0
+#define PB_RED_CROSS 1
+#define PB_RED_REAL2 2
+#define PB_RED_MAX_BINS 64
+#define PB_RED_MAX_ELLS 9
+PB_API int pb_bin_reduce_workspace_size(const pb_grid_t *g, int n_rows, int nk, int n_ell, size_t *bytes);
+PB_API int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const void *a, const void *b,
+                  int n_rows, int64_t row_stride, const double *edges, int nk,
+                  const int32_t *ells, int n_ell, double scale, double *out, int accumulate,
+                  void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Triplet contraction over real maps (the bispectrum cubic sum):                        */
+/*   out[t] = scale * sum_x A[i1_t](x) * B[i2_t](x) * C[i3_t](x)                          */
+/* A, B, C: n_a / n_b / n_c maps of n_vox voxels each (may alias).  Replaces assemble_b3 */
+/* and sum_triplet (PolyBin3D/cython/utils.pyx:614-636, 357-366; jax_utils.py:279-291).  */
+/*                                                                                       */
+/* pb_triplet_plan (host only) tiles the host int32 list idx of n_trip (i1,i2,i3) rows   */
+/* into a table of work items; call with table == NULL to get its size and item count,  */
+/* then copy the table to device memory once and pass it to pb_triplet_contract.        */
+/* method PB_TRIPLET_SIMT: CUDA-core FMA form in the maps' precision, per-tile sums      */
+/*   folded into FP64 registers.                                                         */
+/* method PB_TRIPLET_TC: f32 maps; tcgen05 tensor cores on split-fp16 products (3 MMAs   */
+/*   per tile), FP32 accumulation in TMEM folded into FP64 after every tile.             */
+/* Output FP64 on the device, deterministic for a given device.                          */
+/* ---------------------------------------------------------------------------------- */
+#define PB_TRIPLET_SIMT 0
+#define PB_TRIPLET_TC 1
+PB_API int pb_triplet_plan(int n_a, int n_b, int n_c, const int32_t *idx, int n_trip, void *table,
+                    size_t *table_bytes, int *n_items);
+PB_API int pb_triplet_workspace_size(int precision, int method, int64_t n_vox, int n_items, int n_trip,
+                              size_t *bytes);
+PB_API int pb_triplet_contract(int precision, int method, const void *A, int n_a, const void *B, int n_b,
+                        const void *C, int n_c, int64_t n_vox, const void *table, int n_items,
+                        int n_trip, double scale, double *out, void *workspace,
+                        size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Real-space elementwise products.                                                      */
+/*   PB_EW_MUL      : out = s * x * y                  (prod_real, utils.pyx:248-260)     */
+/*   PB_EW_PRODDIFF : out = s * (x*y - z*u)            (prod_real_diff, utils.pyx:371-383)*/
+/* n elements; y is read at i % y_period when y_period > 0 (one mask over a batch of     */
+/* maps; MUL only); z/u may be NULL where unused; out may alias x.                       */
+/* ---------------------------------------------------------------------------------- */
+#define PB_EW_MUL 0
+#define PB_EW_PRODDIFF 1
+PB_API int pb_elementwise(int precision, int op, int64_t n, const void *x, const void *y, int64_t y_period,
+                          const void *z, const void *u, double s, void *out, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Gaussian random field from white noise (PolyBin3D/base.py:305-353):                   */
+/*   r = noise_re + i noise_im on the full grid, r[0,0,0] = 0,                            */
+/*   a(k) = 0.5 (r(k) + conj(r(-k))) on the half grid, times amp(k) * scale              */
+/* noise: FP64 [n_batch][n0][n1][n2] each; amp: FP64 half grid (sqrt(P) * W); out: half  */
+/* spectra [n_batch] in `precision`.                                                     */
+/* ---------------------------------------------------------------------------------- */
+PB_API int pb_grf_from_noise(const pb_grid_t *g, int precision, const double *noise_re,
+                      const double *noise_im, int n_batch, const double *amp, double scale,
+                      void *out, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Batched pair products of real maps:                                                   */
+/*   out[p] = s * (X[i_p] * Y[j_p] - Z[i_p] * U[j_p])   (Z = U = NULL: s * X[i_p] Y[j_p]) */
+/* pairs: host int32 (i_p, j_p) rows.  The g-map pair differences of the bispectrum      */
+/* Fisher (prod_real_diff, utils.pyx:371-383, called at PolyBin3D/bspec.py:591-613).     */
+/* ---------------------------------------------------------------------------------- */
+#define PB_PAIR_MAX 256
+PB_API int pb_pair_products(int precision, int64_t n_vox, const void *X, const void *Y, const void *Z,
+                            const void *U, const int32_t *pairs, int n_pairs, double s, void *out,
+                            void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Fisher rows over one k-shell (IntegrationUtils.integrate_row, utils.pyx:162-179,      */
+/* called per row at PolyBin3D/bspec.py:597):                                            */
+/*   out[out_row[r] * out_stride + j] = scale * sum_{i < n_modes} deg(m_i)               */
+/*                                      * Re(conj(F[row_key[r]](m_i)) * Q[j](m_i))        */
+/* for r < n_rows (<= 32), j < n_cols.  modes: device int64 list of the shell's half-    */
+/* grid indices (the modes with lo <= |k| < hi); F: n_f half spectra; Q: n_cols half     */
+/* spectra; row_key/out_row: host int32.  Deterministic chunked FP64 sums.               */
+/* ---------------------------------------------------------------------------------- */
+PB_API int pb_shell_rows_workspace_size(int64_t n_modes, int n_rows, int n_cols, size_t *bytes);
+PB_API int pb_shell_rows(const pb_grid_t *g, int precision, const void *F, int n_f, const void *Q,
+                         int n_cols, const int64_t *modes, int64_t n_modes, const int32_t *row_key,
+                         const int32_t *out_row, int n_rows, double scale, double *out,
+                         int64_t out_stride, void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POLYBIN3D_B200_H */

@@ -1,0 +1,301 @@
+"""ctypes binding of the C ABI (include/polybin3d_b200.h) on torch device tensors.
+
+Torch supplies device memory and the current CUDA stream; every computation is a call
+into libpb_b200.so.  There is no fallback: if the library or a CUDA device is missing,
+loading raises.
+"""
+import ctypes
+import os
+import threading
+
+import numpy as np
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpb_b200.so")
+
+PB_F32, PB_F64 = 0, 1
+PB_FFT_R2C, PB_FFT_C2R = 0, 1
+PB_RED_ABS2, PB_RED_CROSS, PB_RED_REAL2 = 0, 1, 2
+PB_TRIPLET_SIMT, PB_TRIPLET_TC = 0, 1
+PB_EW_MUL, PB_EW_PRODDIFF = 0, 1
+FILTER_MAX_MAPS = 128
+
+_ERRORS = {-1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: MemoryError, -5: NotImplementedError,
+           -6: TimeoutError}
+
+
+class PBGrid(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32 * 3), ("reserved", ctypes.c_int32), ("kf", ctypes.c_double * 3)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_SZ = ctypes.c_size_t
+_GP = ctypes.POINTER(PBGrid)
+
+SIGNATURES = {
+    "pb_abi_version": ([], _I),
+    "pb_last_error": ([], ctypes.c_char_p),
+    "pb_fft_plan_create": ([_GP, _I, _I, _I, ctypes.POINTER(_P), ctypes.POINTER(_SZ)], _I),
+    "pb_fft_exec": ([_P, _P, _P, _P, _P], _I),
+    "pb_fft_plan_destroy": ([_P], _I),
+    "pb_spectral_filter": ([_GP, _P, _I, _P, _I64, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P], _I),
+    "pb_bin_reduce_workspace_size": ([_GP, _I, _I, _I, ctypes.POINTER(_SZ)], _I),
+    "pb_bin_reduce": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P, _SZ, _P], _I),
+    "pb_triplet_plan": ([_I, _I, _I, _P, _I, _P, ctypes.POINTER(_SZ), ctypes.POINTER(_I)], _I),
+    "pb_triplet_workspace_size": ([_I, _I, _I64, _I, _I, ctypes.POINTER(_SZ)], _I),
+    "pb_triplet_contract": ([_I, _I, _P, _I, _P, _I, _P, _I, _I64, _P, _I, _I, _D, _P, _P, _SZ, _P], _I),
+    "pb_elementwise": ([_I, _I, _I64, _P, _P, _I64, _P, _P, _D, _P, _P], _I),
+    "pb_grf_from_noise": ([_GP, _I, _P, _P, _I, _P, _D, _P, _P], _I),
+    "pb_pair_products": ([_I, _I64, _P, _P, _P, _P, _P, _I, _D, _P, _P], _I),
+    "pb_shell_rows_workspace_size": ([_I64, _I, _I, ctypes.POINTER(_SZ)], _I),
+    "pb_shell_rows": ([_GP, _I, _P, _I, _P, _I, _P, _I64, _P, _P, _I, _D, _P, _I64, _P, _SZ, _P], _I),
+}
+
+
+def load(path=LIB_PATH):
+    """Load libpb_b200.so (raises if absent: there is no CPU fallback)."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise ImportError("polybin3d_b200: CUDA extension %s is not built "
+                              "(run `python -m polybin3d_b200.build`)" % path)
+        lib = ctypes.CDLL(path)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        if lib.pb_abi_version() != 1:
+            raise ImportError("polybin3d_b200: ABI version mismatch")
+        _lib = lib
+        return lib
+
+
+LAUNCHES = [0]  # kernels of this library launched through these wrappers (bench bookkeeping)
+
+
+def _count(n):
+    LAUNCHES[0] += n
+
+
+def check(status, what=""):
+    if status != 0:
+        msg = load().pb_last_error().decode(errors="replace")
+        raise _ERRORS.get(status, RuntimeError)("%s: %s" % (what, msg) if what else msg)
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("polybin3d_b200 backend='cuda' needs a CUDA device; there is no CPU fallback")
+    load()
+
+
+def stream_ptr():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def ptr(t):
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def hptr(a):
+    """Host numpy array -> void*."""
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def precision_of(dtype):
+    if dtype in (torch.float32, torch.complex64):
+        return PB_F32
+    if dtype in (torch.float64, torch.complex128):
+        return PB_F64
+    raise TypeError("unsupported dtype %s" % dtype)
+
+
+# --------------------------------------------------------------------------------------
+# workspace arena (torch-allocated scratch, reused across calls on the same stream)
+# --------------------------------------------------------------------------------------
+class Workspace:
+    def __init__(self, device):
+        self.device = device
+        self.bufs = {}
+
+    def get(self, nbytes, slot="default"):
+        nbytes = max(int(nbytes), 256)
+        b = self.bufs.get(slot)
+        if b is None or b.numel() < nbytes:
+            b = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self.bufs[slot] = b
+        return b
+
+
+# --------------------------------------------------------------------------------------
+# FFT plans
+# --------------------------------------------------------------------------------------
+class FFTPlan:
+    def __init__(self, grid, batch, precision, direction):
+        lib = load()
+        h = ctypes.c_void_p()
+        ws = ctypes.c_size_t()
+        check(lib.pb_fft_plan_create(ctypes.byref(grid), batch, precision, direction, ctypes.byref(h),
+                                     ctypes.byref(ws)), "pb_fft_plan_create")
+        self.h, self.ws_bytes = h, ws.value
+        self.batch, self.precision, self.direction = batch, precision, direction
+
+    def exec(self, inp, out, workspace):
+        check(load().pb_fft_exec(self.h, ptr(inp), ptr(out), ptr(workspace), stream_ptr()), "pb_fft_exec")
+
+    def __del__(self):
+        try:
+            if self.h:
+                load().pb_fft_plan_destroy(self.h)
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------------------
+# kernels
+# --------------------------------------------------------------------------------------
+def spectral_filter(grid, precision, src, out, maps, w=None, accumulate=False, src_stride=None, out_n=None):
+    """maps: list of (src_idx, lo, hi, l1, l2, scale, wpow) -> writes out[m] (torch, complex);
+    out_n: output grid dims (a smaller grid of the same frequencies), None = the input grid."""
+    lib = load()
+    on = None if out_n is None else np.ascontiguousarray(out_n, dtype=np.int32)
+    n = len(maps)
+    if n == 0:
+        return
+    for c0 in range(0, n, FILTER_MAX_MAPS):
+        chunk = maps[c0:c0 + FILTER_MAX_MAPS]
+        arr = np.asarray(chunk, dtype=np.float64)
+        si = np.ascontiguousarray(arr[:, 0].astype(np.int32))
+        lo = np.ascontiguousarray(arr[:, 1])
+        hi = np.ascontiguousarray(arr[:, 2])
+        l1 = np.ascontiguousarray(arr[:, 3].astype(np.int32))
+        l2 = np.ascontiguousarray(arr[:, 4].astype(np.int32))
+        sc = np.ascontiguousarray(arr[:, 5])
+        wp = np.ascontiguousarray(arr[:, 6].astype(np.int32))
+        o = out[c0:c0 + len(chunk)]
+        stride = src_stride if src_stride is not None else (src[0].numel() if src is not None and src.dim() == 4 else 0)
+        check(lib.pb_spectral_filter(ctypes.byref(grid), None if on is None else hptr(on), precision, ptr(src),
+                                     stride, ptr(o), len(chunk),
+                                     hptr(si), hptr(lo), hptr(hi), hptr(l1), hptr(l2), hptr(sc), hptr(wp),
+                                     ptr(w), int(bool(accumulate)), stream_ptr()), "pb_spectral_filter")
+        _count(1)
+
+
+def bin_reduce(grid, precision, mode, a, b, n_rows, edges, ells, scale, out, ws, accumulate=False, row_stride=0):
+    lib = load()
+    edges = np.ascontiguousarray(edges, dtype=np.float64)
+    nk = len(edges) - 1
+    ells = np.ascontiguousarray(np.asarray(ells, dtype=np.int32).reshape(-1))
+    n_ell = len(ells) // 2
+    nbytes = ctypes.c_size_t()
+    check(lib.pb_bin_reduce_workspace_size(ctypes.byref(grid), n_rows, nk, n_ell, ctypes.byref(nbytes)),
+          "pb_bin_reduce_workspace_size")
+    buf = ws.get(nbytes.value, "binred")
+    check(lib.pb_bin_reduce(ctypes.byref(grid), precision, mode, ptr(a), ptr(b), n_rows, row_stride, hptr(edges), nk,
+                            hptr(ells), n_ell, scale, ptr(out), int(bool(accumulate)), ptr(buf), buf.numel(),
+                            stream_ptr()), "pb_bin_reduce")
+    _count(2)
+
+
+def elementwise(op, x, y, z=None, u=None, s=1.0, out=None, y_period=0):
+    """out = s*x*y (MUL, y read at i % y_period if y_period) or s*(x*y - z*u) (PRODDIFF)."""
+    lib = load()
+    out = torch.empty_like(x) if out is None else out
+    check(lib.pb_elementwise(precision_of(x.dtype), op, x.numel(), ptr(x), ptr(y), int(y_period), ptr(z), ptr(u),
+                             float(s), ptr(out), stream_ptr()), "pb_elementwise")
+    _count(1)
+    return out
+
+
+def grf_from_noise(grid, precision, noise_re, noise_im, amp, scale, out):
+    lib = load()
+    nb = noise_re.shape[0] if noise_re.dim() == 4 else 1
+    check(lib.pb_grf_from_noise(ctypes.byref(grid), precision, ptr(noise_re), ptr(noise_im), nb, ptr(amp),
+                                float(scale), ptr(out), stream_ptr()), "pb_grf_from_noise")
+    _count(1)
+    return out
+
+
+class TripletPlan:
+    """Device work-item table for a fixed triplet list (pb_triplet_plan)."""
+
+    def __init__(self, n_a, n_b, n_c, idx, device):
+        lib = load()
+        idx = np.ascontiguousarray(np.asarray(idx, dtype=np.int32).reshape(-1, 3))
+        self.n_a, self.n_b, self.n_c, self.n_trip = n_a, n_b, n_c, len(idx)
+        nbytes = ctypes.c_size_t()
+        nitems = ctypes.c_int()
+        check(lib.pb_triplet_plan(n_a, n_b, n_c, hptr(idx), len(idx), None, ctypes.byref(nbytes),
+                                  ctypes.byref(nitems)), "pb_triplet_plan")
+        host = np.zeros(nbytes.value, dtype=np.uint8)
+        check(lib.pb_triplet_plan(n_a, n_b, n_c, hptr(idx), len(idx), hptr(host), ctypes.byref(nbytes),
+                                  ctypes.byref(nitems)), "pb_triplet_plan")
+        self.n_items = nitems.value
+        self.table = torch.from_numpy(host).to(device)
+
+    def workspace_bytes(self, precision, method, n_vox):
+        nbytes = ctypes.c_size_t()
+        check(load().pb_triplet_workspace_size(precision, method, n_vox, self.n_items, self.n_trip,
+                                               ctypes.byref(nbytes)), "pb_triplet_workspace_size")
+        return nbytes.value
+
+    def contract(self, A, B, C, out, ws, method=PB_TRIPLET_SIMT, scale=1.0):
+        """A, B, C: torch (n_maps, ...) real maps of one precision; out: float64 device (n_trip,)."""
+        prec = precision_of(A.dtype)
+        n_vox = A[0].numel()
+        buf = ws.get(self.workspace_bytes(prec, method, n_vox), "triplet")
+        check(load().pb_triplet_contract(prec, method, ptr(A), A.shape[0], ptr(B), B.shape[0], ptr(C), C.shape[0],
+                                         n_vox, ptr(self.table), self.n_items, self.n_trip, float(scale), ptr(out),
+                                         ptr(buf), buf.numel(), stream_ptr()), "pb_triplet_contract")
+        _count(2)
+        return out
+
+
+def pair_products(X, Y, pairs, Z=None, U=None, s=1.0, out=None):
+    """out[p] = s*(X[i]Y[j] - Z[i]U[j]) for host (i, j) pairs; X.. are (n, ...) real maps."""
+    pairs = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+    n_vox = X[0].numel()
+    if out is None:
+        out = torch.empty((len(pairs),) + tuple(X.shape[1:]), dtype=X.dtype, device=X.device)
+    check(load().pb_pair_products(precision_of(X.dtype), n_vox, ptr(X), ptr(Y), ptr(Z), ptr(U), hptr(pairs),
+                                  len(pairs), float(s), ptr(out), stream_ptr()), "pb_pair_products")
+    _count((len(pairs) + 255) // 256)
+    return out
+
+
+def shell_rows(grid, F, Q, modes, row_key, out_row, scale, out, ws):
+    """Rows of out (n, n_cols) FP64 for one shell; row_key/out_row host int lists (<= 32 each)."""
+    lib = load()
+    rk = np.ascontiguousarray(row_key, dtype=np.int32)
+    orow = np.ascontiguousarray(out_row, dtype=np.int32)
+    n_modes = modes.numel()
+    nbytes = ctypes.c_size_t()
+    check(lib.pb_shell_rows_workspace_size(n_modes, len(rk), Q.shape[0], ctypes.byref(nbytes)),
+          "pb_shell_rows_workspace_size")
+    buf = ws.get(nbytes.value, "shellrows")
+    check(lib.pb_shell_rows(ctypes.byref(grid), precision_of(F.dtype), ptr(F), F.shape[0], ptr(Q), Q.shape[0],
+                            ptr(modes), n_modes, hptr(rk), hptr(orow), len(rk), float(scale), ptr(out),
+                            out.shape[-1], ptr(buf), buf.numel(), stream_ptr()), "pb_shell_rows")
+    _count(2)
+
+
+_tc = None
+
+
+def tc_built():
+    """True when libpb_b200 carries the tcgen05 triplet contraction."""
+    global _tc
+    if _tc is None:
+        nbytes = ctypes.c_size_t()
+        st = load().pb_triplet_workspace_size(PB_F32, PB_TRIPLET_TC, 1 << 20, 1, 1, ctypes.byref(nbytes))
+        _tc = (st == 0)
+    return _tc

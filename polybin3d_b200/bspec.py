@@ -1,0 +1,653 @@
+"""Bispectrum estimators, backend='cuda' (mirrors PolyBin3D/bspec.py, global sightline).
+
+Numerator: one r2c, one filter launch writing all Nl x Nk bin-filtered half spectra
+(Theta_b L_l invP / W fused), one batched c2r, and the triplet contraction
+sum_x g_b1 g_b2 g_l,b3 for every bin triplet (pb_triplet_contract).  Ideal Fisher and
+symmetry factors reuse the same contraction on the binning functions (FP64).  The Monte
+Carlo Fisher builds every Q-map leg with batched pair products, batched FFTs and three
+accumulating filter launches, then forms Fisher rows per k-shell (pb_shell_rows), FP64.
+"""
+import numpy as np
+import torch
+from scipy.interpolate import interp1d
+
+from . import _native as nat
+
+
+def real_harmonics(k_grids, l):
+    """Real spherical harmonics of the unit vector for even l = 2, 4; the same functions and
+    normalisation as compute_real_harmonics (PolyBin3D/cython/utils.pyx:518-609), so that
+    sum_m Y_lm(k) Y_lm(k') = L_l(k.k')."""
+    kx, ky, kz = k_grids
+    norm = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    safe = np.where(norm == 0, 1.0, norm)
+    xh, yh, zh = [np.where(norm == 0, 0.0, c / safe) for c in (kx, ky, kz)]
+    if l == 2:
+        return [6.0 * xh * yh * np.sqrt(1.0 / 12.0),
+                3.0 * yh * zh * np.sqrt(1.0 / 3.0),
+                zh ** 2 - xh ** 2 / 2.0 - yh ** 2 / 2.0,
+                3.0 * xh * zh * np.sqrt(1.0 / 3.0),
+                (3 * xh ** 2 - 3 * yh ** 2) * np.sqrt(1.0 / 12.0)]
+    if l == 4:
+        x2, y2, z2 = xh * xh, yh * yh, zh * zh
+        return [(420.0 * x2 * xh * yh - 420.0 * xh * y2 * yh) * np.sqrt(1.0 / 20160.0),
+                (315.0 * x2 * yh * zh - 105.0 * y2 * yh * zh) * np.sqrt(1.0 / 2520.0),
+                (-15.0 * x2 * xh * yh - 15.0 * xh * y2 * yh + 90.0 * xh * yh * z2) * np.sqrt(1.0 / 180.0),
+                (-7.5 * x2 * yh * zh - 7.5 * y2 * yh * zh + 10.0 * yh * z2 * zh) * np.sqrt(1.0 / 10.0),
+                35.0 / 8.0 * z2 * z2 - 15.0 / 4.0 * z2 + 3.0 / 8.0,
+                (-7.5 * x2 * xh * zh - 7.5 * xh * y2 * zh + 10.0 * xh * z2 * zh) * np.sqrt(1.0 / 10.0),
+                (-7.5 * x2 * x2 + 45.0 * x2 * z2 + 7.5 * y2 * y2 - 45.0 * y2 * z2) * np.sqrt(1.0 / 180.0),
+                (105.0 * x2 * xh * zh - 315.0 * xh * y2 * zh) * np.sqrt(1.0 / 2520.0),
+                (105.0 * x2 * x2 - 630.0 * x2 * y2 + 105.0 * y2 * y2) * np.sqrt(1.0 / 20160.0)]
+    raise ValueError("l must be 2 or 4")
+
+
+class BSpec:
+    """Bispectrum estimators (bspec.py:12-30 for the inputs).  Keyword-only addition:
+    - contraction: 'auto' (tensor cores in precision='mixed' when built, else CUDA cores),
+      'tc' or 'simt'.
+    - dealias: synthesise the bin-filtered maps on the smallest FFT-friendly grid M with
+      M > 3 K per axis (K = largest binned frequency index); every product of three such
+      maps is then alias-free and sum_x over the M-grid equals (M/N)^3 times the sum over
+      the full grid exactly, so results are unchanged up to rounding.  Default True."""
+
+    def __init__(self, base, k_bins, lmax=0, mask=None, applySinv=None, k_bins_squeeze=None,
+                 include_partial_triangles=False, add_GIC=False, mask_IC=None, add_RIC=False, radial_bins_RIC=[],
+                 Pk_fid=None, mask_shot=None, applySinv_transpose=None, *, contraction='auto', dealias=True,
+                 verb=True):
+        self.base = base
+        self.applySinv = applySinv
+        self.k_bins = np.asarray(k_bins)
+        self.lmax = lmax
+        self.Nk = len(k_bins) - 1
+        self.Nl = self.lmax // 2 + 1
+        self.include_partial_triangles = include_partial_triangles
+        self.add_GIC = add_GIC
+        self.add_RIC = add_RIC
+        self.Pk_fid = Pk_fid
+        self.applySinv_transpose = applySinv_transpose
+        if contraction not in ('auto', 'tc', 'simt'):
+            raise ValueError("contraction must be 'auto', 'tc' or 'simt'")
+        self.contraction = contraction
+        self.verb = verb
+
+        if verb:
+            print("")
+        assert self.lmax % 2 == 0, "l-max must be even!"
+        assert np.max(self.k_bins) < np.min(base.kNy), "k_max must be less than k_Nyquist!"
+        assert np.min(self.k_bins) >= np.max(base.kF), "k_min must be at least the k_fundamental!"
+        assert np.max(self.k_bins) <= base.Pfid[0][-1], "Fiducial power spectrum should extend up to k_max!"
+        assert np.min(self.k_bins) >= base.Pfid[0][0], "Fiducial power spectrum should extend down to k_min!"
+        if verb:
+            print("Binning: %d bins in [%.3f, %.3f] h/Mpc" % (self.Nk, np.min(self.k_bins), np.max(self.k_bins)))
+
+        # squeezed binning (bspec.py:53-65)
+        if type(k_bins_squeeze) != type(None):
+            self.k_bins_squeeze = np.asarray(k_bins_squeeze)
+            self.Nk_squeeze = len(k_bins_squeeze) - 1
+            assert (self.k_bins_squeeze[:self.Nk + 1] == self.k_bins).all(), "k_bins_squeeze must contain all non-squeezed bins!"
+            assert np.max(self.k_bins_squeeze) < np.min(base.kNy), "k_max must be less than k_Nyquist!"
+            assert np.min(self.k_bins_squeeze) >= np.max(base.kF), "k_min must be at least the k_fundamental!"
+            assert np.max(self.k_bins_squeeze) <= base.Pfid[0][-1], "Fiducial power spectrum should extend up to k_max!"
+            assert np.min(self.k_bins_squeeze) >= base.Pfid[0][0], "Fiducial power spectrum should extend down to k_min!"
+            if verb:
+                print("Squezed binning: %d bins in [%.3f, %.3f] h/Mpc" % (self.Nk_squeeze, np.min(self.k_bins_squeeze),
+                                                                          np.max(self.k_bins_squeeze)))
+        else:
+            self.k_bins_squeeze = self.k_bins.copy()
+            self.Nk_squeeze = self.Nk
+        if not np.all(np.diff(self.k_bins_squeeze) > 0):
+            raise ValueError("k_bins must be strictly increasing")
+
+        # triangle bins (bspec.py:67-79)
+        all_bins = []
+        for l in range(0, self.lmax + 1, 2):
+            for bin1 in range(self.Nk):
+                for bin2 in range(bin1, self.Nk_squeeze):
+                    for bin3 in range(bin2, self.Nk_squeeze):
+                        if not self._check_bin(bin1, bin2, bin3):
+                            continue
+                        all_bins.append((bin1, bin2, bin3, l))
+        self.all_bins = np.asarray(all_bins, dtype=np.int64)
+        self.N_bins = len(self.all_bins)
+        self.N3 = self.N_bins // self.Nl
+        if verb:
+            print("l-max: %d" % (self.lmax))
+            print("N_bins: %d" % self.N_bins)
+        assert type(self.lmax) == int, "l-max must be an integer!"
+        assert self.lmax <= 4, "Only l-max<=4 is currently supported!"
+
+        # mask (bspec.py:86-110)
+        if type(mask) == type(None):
+            self.const_mask = True
+            self.mask_mean = 1.
+            self.cube_mask_mean = 1.
+            assert not self.add_GIC, "Global integral constraint cannot be used without a mask!"
+            assert not self.add_RIC, "Radial integral constraint cannot be used without a mask!"
+        else:
+            if type(mask) != np.ndarray:
+                mask = np.array(mask.cpu() if isinstance(mask, torch.Tensor) else mask)
+            self.mask = mask.astype(np.float64)
+            if type(mask_IC) != type(None):
+                self.mask_IC = mask_IC.astype(np.float64)
+            if np.std(self.mask) < 1e-12:
+                self.const_mask = True
+                self.mask_mean = np.mean(self.mask)
+            else:
+                self.const_mask = False
+            self.cube_mask_mean = np.mean(self.mask ** 3)
+        if verb:
+            print("Mask: constant" if self.const_mask else "Mask: spatially varying")
+        if type(mask_shot) != type(None):
+            self.mask_shot = mask_shot.astype(np.float64)
+
+        if self.applySinv is not None:
+            raise NotImplementedError("backend='cuda' implements the trivial S^-1 weighting (applySinv=None)")
+        if self.add_GIC or self.add_RIC:
+            raise NotImplementedError("backend='cuda' does not implement integral constraints")
+        self.applySinv = self.base.applySinv_trivial
+        self.applySinv_transpose = self.base.applySinv_trivial
+
+        # fiducial weighting 1/P_fid (bspec.py:138-156); None -> unit weight on every binned mode
+        self._unit_w = (type(self.Pk_fid) != str and (np.asarray(self.Pk_fid) == None).all()) or \
+                       (isinstance(self.Pk_fid, str) and self.Pk_fid == 'default' and base._unit_pk)  # noqa: E711
+        if not (isinstance(self.Pk_fid, str) and self.Pk_fid == 'default') and not self._unit_w:
+            assert len(self.Pk_fid) == 2, "Pk should contain k and P_0(k) columns"
+        self._plans = {}
+        self._shell_modes = None
+        self.map_grid = self._dealiased_grid() if dealias else tuple(int(n) for n in base.gridsize)
+        self.Ylm_real = None
+        self.Ylm_fourier = None
+
+    # ------------------------------------------------------------------------------
+    # binning helpers (bspec.py:171-220)
+    # ------------------------------------------------------------------------------
+    def _check_bin(self, bin1, bin2, bin3):
+        """Triangle condition on bin centres, or on edges for partial triangles (bspec.py:171-199)."""
+        if self.include_partial_triangles:
+            k3_hi = self.k_bins_squeeze[bin1 + 1] + self.k_bins_squeeze[bin2 + 1]
+            if bin1 > bin2:
+                k3_lo = self.k_bins_squeeze[bin1] - self.k_bins_squeeze[bin2 + 1]
+            elif bin1 == bin2:
+                k3_lo = 0.
+            else:
+                k3_lo = self.k_bins_squeeze[bin2] - self.k_bins_squeeze[bin1 + 1]
+            if self.k_bins_squeeze[bin3] >= k3_hi - 1e-10 or self.k_bins_squeeze[bin3 + 1] <= k3_lo + 1e-10:
+                return 0
+            return 1
+        k1 = 0.5 * (self.k_bins[bin1] + self.k_bins[bin1 + 1])
+        k2 = 0.5 * (self.k_bins_squeeze[bin2] + self.k_bins_squeeze[bin2 + 1])
+        k3 = 0.5 * (self.k_bins_squeeze[bin3] + self.k_bins_squeeze[bin3 + 1])
+        if k3 < abs(k1 - k2) or k3 > k1 + k2:
+            return 0
+        return 1
+
+    def get_ks(self):
+        """Central k1, k2, k3 of every triangle bin (bspec.py:201-220)."""
+        k1s, k2s, k3s = [], [], []
+        for bin1 in range(self.Nk):
+            k1 = 0.5 * (self.k_bins[bin1] + self.k_bins[bin1 + 1])
+            for bin2 in range(bin1, self.Nk_squeeze):
+                k2 = 0.5 * (self.k_bins_squeeze[bin2] + self.k_bins_squeeze[bin2 + 1])
+                for bin3 in range(bin2, self.Nk_squeeze):
+                    k3 = 0.5 * (self.k_bins_squeeze[bin3] + self.k_bins_squeeze[bin3 + 1])
+                    if not self._check_bin(bin1, bin2, bin3):
+                        continue
+                    k1s.append(k1)
+                    k2s.append(k2)
+                    k3s.append(k3)
+        return np.asarray([k1s, k2s, k3s])
+
+    def _dealiased_grid(self):
+        """Per axis, the smallest even 2^a 3^b 5^c 7^d size M > 3 K (K = floor(k_max / kF))
+        not above the data grid."""
+        b = self.base
+        kmax = float(np.max(self.k_bins_squeeze))
+        dims = []
+        for i in range(3):
+            K = int(np.floor(kmax / b.kF[i]))
+            m = 3 * K + 1
+            while True:
+                r = m
+                for f in (2, 3, 5, 7):
+                    while r % f == 0:
+                        r //= f
+                if r == 1 and m % 2 == 0:
+                    break
+                m += 1
+            dims.append(int(min(m, int(b.gridsize[i]))))
+        return tuple(dims)
+
+    @property
+    def map_scale(self):
+        """(N/M)^3: converts a sum over the map grid into the sum over the data grid."""
+        return float(np.prod(self.base.gridsize) / np.prod(self.map_grid))
+
+    # ------------------------------------------------------------------------------
+    # device helpers
+    # ------------------------------------------------------------------------------
+    @property
+    def invPk0(self):
+        """1/P_fid on the half grid (bspec.py:139-156), host FP64."""
+        b = self.base
+        if isinstance(self.Pk_fid, str) and self.Pk_fid == 'default':
+            return b.invPk0_grid
+        if self._unit_w:
+            k_tmp = np.arange(np.min(b.kF) / 10., np.max(b.kNy) * 2, np.min(b.kF) / 10.)
+            Pfid = np.asarray([k_tmp, 1. + 0. * k_tmp])
+        else:
+            Pfid = np.asarray(self.Pk_fid)
+        P = interp1d(Pfid[0], Pfid[1], bounds_error=False, fill_value=0.)(b.modk_grid)
+        inv = np.zeros(P.shape, dtype=np.float64)
+        inv[P != 0] = 1. / P[P != 0]
+        return inv
+
+    def _invp_device(self):
+        """Device 1/P_fid weight, or None when it is 1 on every binned mode."""
+        if self._unit_w:
+            return None
+        return self.base.to_device_grid(('bk_invp', id(self)), lambda: self.invPk0, torch.float64)
+
+    def _data_weight(self, dtype):
+        """invP / W on the half grid for the ideal numerator (None when identically 1)."""
+        b = self.base
+        if self._unit_w and b.pixel_window == 'none':
+            return None
+
+        def f():
+            w = np.ones(b.nhalf_shape) if self._unit_w else self.invPk0.copy()
+            if b.pixel_window != 'none':
+                W = b.pixel_window_grid
+                nz = W != 0
+                w = np.where(nz, w / np.where(nz, W, 1.), 0.)
+            return w
+        return b.to_device_grid(('bk_dataw', id(self)), f, dtype)
+
+    def _plan(self, key, n_a, n_b, n_c, idx):
+        if key is None:
+            return nat.TripletPlan(n_a, n_b, n_c, idx, self.base.device)
+        key = (key, n_a, n_b, n_c)
+        p = self._plans.get(key)
+        if p is None:
+            p = nat.TripletPlan(n_a, n_b, n_c, idx, self.base.device)
+            self._plans[key] = p
+        return p
+
+    def _method(self, dtype):
+        if dtype == torch.float64 or self.contraction == 'simt':
+            return nat.PB_TRIPLET_SIMT
+        if self.contraction == 'tc':
+            return nat.PB_TRIPLET_TC
+        return nat.PB_TRIPLET_TC if tc_available() else nat.PB_TRIPLET_SIMT
+
+    def _contract(self, key, A, B, C, idx, scale=1.0):
+        """FP64 triplet sums of maps A, B, C; maps on the dealiased grid are rescaled to
+        full-grid sums."""
+        b = self.base
+        plan = self._plan(key, A.shape[0], B.shape[0], C.shape[0], idx)
+        out = torch.empty(plan.n_trip, dtype=torch.float64, device=b.device)
+        if tuple(A.shape[1:]) != tuple(int(n) for n in b.gridsize):
+            scale = scale * float(np.prod(b.gridsize)) / float(np.prod(A.shape[1:]))
+        plan.contract(A, B, C, out, b.ws, method=self._method(A.dtype), scale=scale)
+        return out
+
+    def _binned_maps(self, src, specs, w, dtype, coarse=True):
+        """Real maps irfftn(Theta_b L_l1 L_l2 * w^wp * src) for specs [(b, l1, l2, scale)], batched.
+        coarse: synthesise them on the dealiased map grid (same 1/N^3 normalisation)."""
+        b = self.base
+        ks = self.k_bins_squeeze
+        cd = torch.complex128 if dtype == torch.float64 else torch.complex64
+        prec = nat.precision_of(dtype)
+        dims = self.map_grid if coarse else tuple(int(n) for n in b.gridsize)
+        hs = (dims[0], dims[1], dims[2] // 2 + 1)
+        half = torch.empty((len(specs),) + hs, dtype=cd, device=b.device)
+        wp = 0 if w is None else 1
+        maps = [(0, ks[bb], ks[bb + 1], l1, l2, sc / b.nreal, wp) for (bb, l1, l2, sc) in specs]
+        nat.spectral_filter(b.grid, prec, src, half, maps, w=w, src_stride=b.nhalf,
+                            out_n=None if coarse is False or dims == tuple(int(n) for n in b.gridsize) else dims)
+        b.n_FFTs_reverse += len(specs)
+        return b.fft_c2r(half)
+
+    # ------------------------------------------------------------------------------
+    # symmetry factors (bspec.py:222-279)
+    # ------------------------------------------------------------------------------
+    def _compute_symmetry_factor(self):
+        if self.verb:
+            print("Computing degeneracy factor")
+        sym = []
+        for (b1, b2, b3, l) in self.all_bins[:self.N3]:
+            if b1 == b2 and b1 == b3:
+                sym.append(6.)
+            elif b1 == b2 or b1 == b3 or b2 == b3:
+                sym.append(2.)
+            else:
+                sym.append(1.)
+        if self.lmax > 0:
+            b = self.base
+            nks = self.Nk_squeeze
+            w = self._invp_device()
+            bins = self._binned_maps(None, [(i, 0, 0, 1.0) for i in range(nks)], w, torch.float64)
+            kg = b.k_grids
+            invP = np.ones(b.nhalf_shape) if self._unit_w else self.invPk0
+            for l in range(2, self.lmax + 1, 2):
+                rows = self.all_bins[self.all_bins[:, 3] == l]
+                need = sorted({int(r[2]) for r in rows if (r[0] != r[1] and r[1] == r[2]) or (r[0] == r[1] == r[2])})
+                # sum over m of bins-weighted squares of the Y_lm-weighted binning functions
+                pair_idx = sorted({(int(r[0]), int(r[2])) for r in rows if r[0] != r[1] and r[1] == r[2]} |
+                                  {(int(r[2]), int(r[2])) for r in rows if r[0] == r[1] == r[2]})
+                num = {p: 0.0 for p in pair_idx}
+                if pair_idx:
+                    for y in real_harmonics(kg, l):
+                        wy = torch.as_tensor(invP * y, device=b.device)
+                        ym = self._binned_maps(None, [(i, 0, 0, 1.0) for i in need], wy, torch.float64)
+                        pos = {bb: i for i, bb in enumerate(need)}
+                        idx = np.asarray([(p[0], pos[p[1]], pos[p[1]]) for p in pair_idx], dtype=np.int32)
+                        vals = self._contract(None, bins, ym, ym, idx).cpu().numpy()
+                        for p, v in zip(pair_idx, vals):
+                            num[p] += v
+                    idx3 = np.asarray([(p[0], p[1], p[1]) for p in pair_idx], dtype=np.int32)
+                    den = dict(zip(pair_idx, self._contract(('sym_den', l), bins, bins, bins, idx3).cpu().numpy()))
+                for (b1, b2, b3, ll) in rows:
+                    if b1 != b2 and b2 != b3:
+                        sym.append(1.)
+                    elif b1 == b2 and b2 != b3:
+                        sym.append(2.)
+                    elif b1 != b2 and b2 == b3:
+                        sym.append(1. + num[(b1, b3)] / den[(b1, b3)])
+                    else:
+                        sym.append(2. * (1. + 2. * num[(b3, b3)] / den[(b3, b3)]))
+        self.sym_factor = np.asarray(sym)
+        assert len(self.sym_factor) == self.N_bins
+
+    # ------------------------------------------------------------------------------
+    # numerator (bspec.py:895-983)
+    # ------------------------------------------------------------------------------
+    def _triplet_index(self):
+        ab = self.all_bins
+        return np.stack([ab[:, 0], ab[:, 1], (ab[:, 3] // 2) * self.Nk_squeeze + ab[:, 2]], axis=1).astype(np.int32)
+
+    def _g_maps(self, xk, w, scale):
+        """All Nl x Nk_squeeze bin-filtered maps g[l/2, b] of one weighted spectrum."""
+        specs = [(bb, l, 0, scale) for l in range(0, self.lmax + 1, 2) for bb in range(self.Nk_squeeze)]
+        return self._binned_maps(xk, specs, w, xk.real.dtype)
+
+    def _compute_bk_numerator(self, data, include_linear_term=True, filtering='ideal', verb=False):
+        assert filtering in ['ideal', 'Sinv'], "Unknown filtering option supplied!"
+        if (not hasattr(self, 'preload')) and include_linear_term:
+            raise Exception("Need to generate or specify bias simulations!")
+        b = self.base
+        if not isinstance(data, torch.Tensor):
+            assert type(data[0, 0, 0]) in [np.float32, np.float64], "Data must be of type float32 or float64!"
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        B3 = self._bk_cubic(data, filtering)
+        norm = b.volume / float(b.gridsize.prod()) / self.sym_factor
+        return B3.cpu().numpy() * norm
+
+    def _bk_cubic(self, data, filtering):
+        """Device FP64 cubic sums B3[i] (assemble_b3 of the g-maps)."""
+        b = self.base
+        x = b.as_device(data)
+        xk = b.to_fourier(x)
+        rd = x.dtype
+        if filtering == 'ideal':
+            w = self._data_weight(rd)
+            scale = 1.0 / self.cube_mask_mean ** (1. / 3.)
+        else:
+            w = None
+            if b.pixel_window != 'none':
+                w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), rd)
+            scale = 1.0
+        G = self._g_maps(xk, w, scale)
+        return self._contract('b3', G, G, G, self._triplet_index())
+
+    def _inv_window(self):
+        W = self.base.pixel_window_grid
+        nz = W != 0
+        return np.where(nz, 1. / np.where(nz, W, 1.), 0.)
+
+    def Bk_numerator(self, data, include_linear_term=True, verb=False):
+        """Numerator of the unwindowed estimator (bspec.py:429-439); the linear term needs
+        bias simulations, which this backend does not generate."""
+        if not self.const_mask:
+            assert data.shape == self.mask.shape, "Data must have same shape as the mask!"
+        return self._compute_bk_numerator(data, include_linear_term=include_linear_term, filtering='Sinv', verb=verb)
+
+    def Bk_numerator_ideal(self, data, verb=False):
+        """Numerator of the ideal estimator (bspec.py:986-997)."""
+        if not self.const_mask:
+            assert data.shape == self.mask.shape, "Data must have same shape as the mask!"
+        return self._compute_bk_numerator(data, include_linear_term=False, filtering='ideal', verb=verb)
+
+    def load_sims(self, load_sim, N_sims, verb=False, input_type='real', preload=True):
+        raise NotImplementedError("the linear term (bias simulations) is not implemented in backend='cuda'")
+
+    def generate_sims(self, N_sim, Pk_input=[], verb=False, preload=True):
+        raise NotImplementedError("the linear term (bias simulations) is not implemented in backend='cuda'")
+
+    # ------------------------------------------------------------------------------
+    # ideal Fisher (bspec.py:999-1083)
+    # ------------------------------------------------------------------------------
+    def compute_fisher_ideal(self, discreteness_correction=True, verb=False):
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        if self.verb:
+            print("Computing ideal Fisher matrix")
+        nks = self.Nk_squeeze
+        w = self._invp_device()
+        idx3 = self.all_bins[:self.N3, :3].astype(np.int32)
+        b = self.base
+        if discreteness_correction:
+            fish = np.zeros((self.N_bins, self.N_bins))
+            u = self._binned_maps(None, [(bb, l, 0, 1.0) for l in range(0, self.lmax + 1, 2) for bb in range(nks)], w,
+                                  torch.float64)
+            u0 = u[:nks]
+            for l in range(0, self.lmax + 1, 2):
+                for lp in range(l, self.lmax + 1, 2):
+                    ull = self._binned_maps(None, [(bb, l, lp, 1.0) for bb in range(nks)], w, torch.float64)
+                    T1 = self._contract('fid', u0, u0, ull, idx3).cpu().numpy()
+                    T2 = self._contract('fid', u0, u[l // 2 * nks:(l // 2 + 1) * nks],
+                                        u[lp // 2 * nks:(lp // 2 + 1) * nks], idx3).cpu().numpy()
+                    for i in range(self.N3):
+                        b1, b2, b3 = idx3[i]
+                        if b1 != b2 and b2 != b3:
+                            v = T1[i]
+                        elif b1 == b2 and b2 != b3:
+                            v = 2. * T1[i]
+                        elif b1 != b2 and b2 == b3:
+                            v = T2[i] + T1[i]
+                        else:
+                            v = 4. * T2[i] + 2. * T1[i]
+                        fish[l // 2 * self.N3 + i, lp // 2 * self.N3 + i] = v
+            fish = fish + fish.T - np.diag(np.diag(fish))
+            scaling = b.gridsize.prod() ** 2 / b.volume
+            fish = fish / np.outer(self.sym_factor, self.sym_factor) * scaling
+        else:
+            u0 = self._binned_maps(None, [(bb, 0, 0, 1.0) for bb in range(nks)], w, torch.float64)
+            N_triangles = self._contract('fid', u0, u0, u0, idx3).cpu().numpy()
+            fish_diag = np.zeros(self.N_bins)
+            for l in range(0, self.lmax + 1, 2):
+                fish_diag[l // 2 * self.N3:(l // 2 + 1) * self.N3] = N_triangles / (2. * l + 1.)
+            fish = np.diag(fish_diag / self.sym_factor) * b.gridsize.prod() ** 2 / b.volume
+        self.fish_ideal = fish
+        self.inv_fish_ideal = np.linalg.inv(self.fish_ideal)
+        self.discreteness_correction = discreteness_correction
+        return fish
+
+    def Bk_ideal(self, data, fish_ideal=[], discreteness_correction=True, verb=False):
+        """Ideal estimator (bspec.py:1085-1118)."""
+        if len(fish_ideal) != 0:
+            self.fish_ideal = fish_ideal
+            self.inv_fish_ideal = np.linalg.inv(fish_ideal)
+        if not hasattr(self, 'inv_fish_ideal'):
+            self.compute_fisher_ideal(discreteness_correction=discreteness_correction, verb=verb)
+        elif getattr(self, 'discreteness_correction', discreteness_correction) != discreteness_correction:
+            self.compute_fisher_ideal(discreteness_correction=discreteness_correction, verb=verb)
+        Bk_num_ideal = self.Bk_numerator_ideal(data, verb=verb)
+        Bk_out = np.matmul(self.inv_fish_ideal, Bk_num_ideal)
+        Bk_dict = {}
+        index = 0
+        for l in range(0, self.lmax + 1, 2):
+            Bk_dict['b%s' % l] = Bk_out[index:index + self.N3]
+            index += self.N3
+        return Bk_dict
+
+    # ------------------------------------------------------------------------------
+    # Monte Carlo Fisher (bspec.py:473-693), FP64
+    # ------------------------------------------------------------------------------
+    def _mask_device(self):
+        return self.base.to_device_grid(('bk_mask', id(self)), lambda: self.mask, torch.float64)
+
+    def _modes_of_shell(self, s):
+        if self._shell_modes is None:
+            b = self.base
+            mk = b.modk_grid.reshape(-1)
+            ks = self.k_bins_squeeze
+            self._shell_modes = [torch.as_tensor(np.nonzero((mk >= ks[i]) & (mk < ks[i + 1]))[0].astype(np.int64),
+                                                 device=b.device) for i in range(self.Nk_squeeze)]
+        return self._shell_modes[s]
+
+    def _apply_filter_spectra(self, Q, prescaled):
+        """S^-1 P on a batch of half spectra: mask_mean * Q, or rfftn(mask * irfftn(Q)); in place.
+        `prescaled`: Q already carries mask_mean (constant mask) or 1/N^3 (varying mask)."""
+        b = self.base
+        if self.const_mask:
+            return Q
+        m = self._mask_device()
+        qr = b.fft_c2r(Q)
+        nat.elementwise(nat.PB_EW_MUL, qr, m, out=qr, y_period=b.nreal)
+        b.n_FFTs_reverse += Q.shape[0]
+        b.n_FFTs_forward += Q.shape[0]
+        return b.fft_r2c(qr, out=Q)
+
+    def _all_g(self, w1, w2):
+        nks = self.Nk_squeeze
+        specs = [(bb, l, 0, 1.0) for l in range(0, self.lmax + 1, 2) for bb in range(nks)]
+        G1 = self._binned_maps(w1, specs, None, torch.float64, coarse=False)
+        G2 = self._binned_maps(w2, specs, None, torch.float64, coarse=False)
+        return G1, G2
+
+    def _key_fts(self, G1, G2, keys):
+        """FT[g1_0,A g1_l,B - g2_0,A g2_l,B] for keys (A, B, l) as a batch of half spectra."""
+        b = self.base
+        nks = self.Nk_squeeze
+        pairs = [(A, (l // 2) * nks + B) for (A, B, l) in keys]
+        prods = nat.pair_products(G1, G1, pairs, Z=G2, U=G2)
+        b.n_FFTs_forward += len(keys)
+        return b.fft_r2c(prods)
+
+    def _fisher_from_fields(self, a1, a2):
+        b = self.base
+        ab = self.all_bins
+        ks = self.k_bins_squeeze
+        F64 = nat.PB_F64
+        nh = b.nhalf
+        invN = 1.0 / b.nreal
+        # --- Q[A^-1 a] (compute_Q 'Ainv', bspec.py:536-640)
+        ainv_w = b.to_device_grid('ainv', b._ainv_weight, torch.float64)
+        w = torch.empty((2,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+        nat.spectral_filter(b.grid, F64, a1, w[0:1], [(0, -1.0, np.inf, 0, 0, 1.0, 1)], w=ainv_w)
+        nat.spectral_filter(b.grid, F64, a2, w[1:2], [(0, -1.0, np.inf, 0, 0, 1.0, 1)], w=ainv_w)
+        G1, G2 = self._all_g(w[0], w[1])
+        keys = sorted({(int(r[0]), int(r[1]), 0) for r in ab} | {(int(r[1]), int(r[2]), int(r[3])) for r in ab} |
+                      {(int(r[0]), int(r[2]), int(r[3])) for r in ab})
+        kpos = {k: i for i, k in enumerate(keys)}
+        FT = self._key_fts(G1, G2, keys)
+        del G1, G2
+        qs = self.mask_mean if self.const_mask else invN
+        Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+        leg1 = [(kpos[(r[0], r[1], 0)], ks[r[2]], ks[r[2] + 1], r[3], 0, qs, 0) for r in ab.tolist()]
+        leg2 = [(kpos[(r[1], r[2], r[3])], ks[r[0]], ks[r[0] + 1], 0, 0, qs, 0) for r in ab.tolist()]
+        leg3 = [(kpos[(r[0], r[2], r[3])], ks[r[1]], ks[r[1] + 1], 0, 0, qs, 0) for r in ab.tolist()]
+        nat.spectral_filter(b.grid, F64, FT, Q, leg1, src_stride=nh)
+        nat.spectral_filter(b.grid, F64, FT, Q, leg2, src_stride=nh, accumulate=True)
+        nat.spectral_filter(b.grid, F64, FT, Q, leg3, src_stride=nh, accumulate=True)
+        del FT
+        Q = self._apply_filter_spectra(Q, True)
+        # --- rows from Q[S^-1 P a] (compute_Q 'Sinv', bspec.py:528-597)
+        if self.const_mask:
+            ws = torch.empty((2,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+            nat.spectral_filter(b.grid, F64, a1, ws[0:1], [(0, -1.0, np.inf, 0, 0, self.mask_mean, 0)])
+            nat.spectral_filter(b.grid, F64, a2, ws[1:2], [(0, -1.0, np.inf, 0, 0, self.mask_mean, 0)])
+        else:
+            ws = torch.empty((2,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+            nat.spectral_filter(b.grid, F64, a1, ws[0:1], [(0, -1.0, np.inf, 0, 0, invN, 0)])
+            nat.spectral_filter(b.grid, F64, a2, ws[1:2], [(0, -1.0, np.inf, 0, 0, invN, 0)])
+            b.n_FFTs_reverse += 2
+            ws = self._apply_filter_spectra(ws, True)
+        G1, G2 = self._all_g(ws[0], ws[1])
+        skeys = sorted({(int(r[0]), int(r[2]), int(r[3])) for r in ab})
+        spos = {k: i for i, k in enumerate(skeys)}
+        FTs = self._key_fts(G1, G2, skeys)
+        del G1, G2
+        fish = torch.zeros((self.N_bins, self.N_bins), dtype=torch.float64, device=b.device)
+        scale = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
+        for s in range(self.Nk_squeeze):
+            rows = np.nonzero(ab[:, 1] == s)[0]
+            if len(rows) == 0:
+                continue
+            modes = self._modes_of_shell(s)
+            for r0 in range(0, len(rows), 32):
+                rr = rows[r0:r0 + 32]
+                rk = [spos[(int(ab[i, 0]), int(ab[i, 2]), int(ab[i, 3]))] for i in rr]
+                nat.shell_rows(b.grid, FTs, Q, modes, rk, rr, scale, fish, b.ws)
+        return fish.cpu().numpy() / np.outer(self.sym_factor, self.sym_factor)
+
+    def compute_fisher_contribution(self, seed, verb=False):
+        """Fisher contribution of one GRF pair with the reference's noise draws (bspec.py:441-445)."""
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        b = self.base
+        r1 = b.reference_noise(seed + int(1e7))
+        r2 = b.reference_noise(seed + int(2e7))
+        a1 = b.grf_from_noise(torch.as_tensor(r1[0], device=b.device), torch.as_tensor(r1[1], device=b.device))
+        a2 = b.grf_from_noise(torch.as_tensor(r2[0], device=b.device), torch.as_tensor(r2[1], device=b.device))
+        return self._fisher_from_fields(a1, a2)
+
+    def compute_fisher(self, N_it, verb=False):
+        """Mean Fisher over seeds 0..N_it-1 (bspec.py:678-693)."""
+        fish = np.zeros((self.N_bins, self.N_bins))
+        for seed in range(N_it):
+            if seed % 5 == 0:
+                print("Computing Fisher contribution %d of %d" % (seed + 1, N_it))
+            fish += self.compute_fisher_contribution(seed, verb=verb) / N_it
+        self.fish = fish
+        self.inv_fish = np.linalg.inv(fish)
+        return fish
+
+    def Bk_unwindowed(self, data, fish=[], include_linear_term=True, verb=False):
+        """Unwindowed estimator (bspec.py:863-893)."""
+        if len(fish) != 0:
+            self.fish = fish
+            self.inv_fish = np.linalg.inv(fish)
+        if not hasattr(self, 'inv_fish'):
+            raise Exception("Need to compute Fisher matrix first!")
+        Bk_num = self.Bk_numerator(data, include_linear_term=include_linear_term, verb=verb)
+        Bk_out = np.matmul(self.inv_fish, Bk_num)
+        Bk_dict = {}
+        index = 0
+        for l in range(0, self.lmax + 1, 2):
+            Bk_dict['b%s' % l] = Bk_out[index:index + self.N3]
+            index += self.N3
+        return Bk_dict
+
+    def compute_shot_contribution(self, seed, verb=False, data=None, data2=None, cubic_only=False):
+        raise NotImplementedError("shot-noise Monte Carlo is not implemented in backend='cuda'")
+
+    def compute_covariance_contribution(self, seed, Pk_cov, verb=False, mask_shot_2pt=None):
+        raise NotImplementedError("covariance Monte Carlo is not implemented in backend='cuda'")
+
+
+_TC_OK = None
+
+
+def tc_available():
+    """True when the tensor-core contraction is built for this device (sm_100)."""
+    global _TC_OK
+    if _TC_OK is None:
+        try:
+            cap = torch.cuda.get_device_capability()
+            _TC_OK = cap[0] == 10 and nat.tc_built()
+        except Exception:
+            _TC_OK = False
+    return _TC_OK

@@ -1,0 +1,81 @@
+// Shared device helpers: exact k-grid geometry, Legendre polynomials, error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include "../../include/polybin3d_b200.h"
+
+namespace pb {
+
+// ---- error plumbing ---------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_check(cudaError_t e, const char *where);
+#define PB_CUDA(call)                                                   \
+    do {                                                                \
+        cudaError_t _e = (call);                                        \
+        if (_e != cudaSuccess) return ::pb::cuda_check(_e, #call);      \
+    } while (0)
+#define PB_LAUNCH_CHECK(where)                                          \
+    do {                                                                \
+        cudaError_t _e = cudaGetLastError();                            \
+        if (_e != cudaSuccess) return ::pb::cuda_check(_e, where);      \
+    } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int num_sms();
+
+// ---- grid geometry ----------------------------------------------------------------
+struct Grid {
+    int n0, n1, n2, nh2;     // real dims and half-axis length n2/2+1
+    double kf0, kf1, kf2;
+    int64_t nhalf;           // n0*n1*nh2
+    int64_t nreal;           // n0*n1*n2
+};
+
+int make_grid(const pb_grid_t *g, Grid *out);
+
+// frequency index of array position i on an axis of length n (numpy fftshift order)
+__device__ __forceinline__ int freq_index(int i, int n) { return i < (n >> 1) ? i : i - n; }
+
+struct Mode {
+    double k;    // |k|
+    double mu;   // kz/|k| (0 at k=0)
+    double deg;  // 1 + (kz > 0)
+};
+
+// |k| exactly as numpy: k_i = (double)idx*kF_i, sqrt((kx*kx + ky*ky) + kz*kz), no FMA.
+__device__ __forceinline__ Mode mode_of(const Grid &g, int64_t idx) {
+    int l = (int)(idx % g.nh2);
+    int64_t r = idx / g.nh2;
+    int j = (int)(r % g.n1);
+    int i = (int)(r / g.n1);
+    double kx = __dmul_rn((double)freq_index(i, g.n0), g.kf0);
+    double ky = __dmul_rn((double)freq_index(j, g.n1), g.kf1);
+    double kz = __dmul_rn((double)l, g.kf2);
+    double s = __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
+    Mode m;
+    m.k = __dsqrt_rn(s);
+    m.mu = (m.k != 0.0) ? __ddiv_rn(kz, m.k) : 0.0;
+    m.deg = (l > 0) ? 2.0 : 1.0;
+    return m;
+}
+
+// Legendre polynomials L_0..L_4 (PolyBin3D/cython/utils.pyx:385-400)
+__device__ __forceinline__ double legendre(int l, double mu) {
+    double m2 = mu * mu;
+    switch (l) {
+        case 0: return 1.0;
+        case 1: return mu;
+        case 2: return 0.5 * (3.0 * m2 - 1.0);
+        case 3: return 0.5 * mu * (5.0 * m2 - 3.0);
+        default: return (35.0 * m2 * m2 - 30.0 * m2 + 3.0) * 0.125;
+    }
+}
+
+template <typename T> struct cplx;
+template <> struct cplx<float> { using type = float2; };
+template <> struct cplx<double> { using type = double2; };
+
+}  // namespace pb

@@ -1,0 +1,442 @@
+// Core entry points: errors, cuFFT plans, the spectral filter, elementwise products
+// and the Gaussian-random-field kernel.
+#include <cufft.h>
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "pb_common.cuh"
+
+namespace pb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int code, const std::string &msg) {
+    set_error(msg);
+    return code;
+}
+
+int cuda_check(cudaError_t e, const char *where) {
+    return fail(PB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+int num_sms() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+    return n > 0 ? n : 148;
+}
+
+int make_grid(const pb_grid_t *g, Grid *out) {
+    if (!g) return fail(PB_ERR_INVALID, "grid is NULL");
+    for (int i = 0; i < 3; ++i) {
+        if (g->n[i] <= 0) return fail(PB_ERR_INVALID, "grid dimensions must be positive");
+        if (!(g->kf[i] > 0.0)) return fail(PB_ERR_INVALID, "fundamental frequencies must be positive");
+    }
+    if (g->n[2] % 2 != 0)
+        return fail(PB_ERR_INVALID, "Last dimension of grid must be even for real-to-complex FFTs.");
+    out->n0 = g->n[0];
+    out->n1 = g->n[1];
+    out->n2 = g->n[2];
+    out->nh2 = g->n[2] / 2 + 1;
+    out->kf0 = g->kf[0];
+    out->kf1 = g->kf[1];
+    out->kf2 = g->kf[2];
+    out->nhalf = (int64_t)out->n0 * out->n1 * out->nh2;
+    out->nreal = (int64_t)out->n0 * out->n1 * out->n2;
+    return PB_OK;
+}
+
+static int grid_blocks(int64_t work, int threads, int per_sm = 8) {
+    int64_t b = (work + threads - 1) / threads;
+    int64_t cap = (int64_t)num_sms() * per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// ------------------------------------------------------------------------------------
+// spectral filter
+// ------------------------------------------------------------------------------------
+struct FilterParams {
+    double lo[PB_FILTER_MAX_MAPS];
+    double hi[PB_FILTER_MAX_MAPS];
+    double scale[PB_FILTER_MAX_MAPS];
+    int32_t src[PB_FILTER_MAX_MAPS];
+    int8_t l1[PB_FILTER_MAX_MAPS];
+    int8_t l2[PB_FILTER_MAX_MAPS];
+    int8_t wpow[PB_FILTER_MAX_MAPS];
+    int32_t n_maps;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) filter_kernel(Grid g, Grid go, const typename cplx<T>::type *src,
+                                                     int64_t src_stride, typename cplx<T>::type *out, const T *w,
+                                                     int acc, FilterParams p) {
+    // iterate over the modes of the output grid `go`; each maps to the source mode of the
+    // same frequency on `g` (identical when the grids agree)
+    using C = typename cplx<T>::type;
+    const bool same = (go.n0 == g.n0 && go.n1 == g.n1 && go.n2 == g.n2);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < go.nhalf; idx += stride) {
+        Mode md = mode_of(go, idx);
+        int64_t sidx = idx;
+        if (!same) {
+            int l = (int)(idx % go.nh2);
+            int64_t r = idx / go.nh2;
+            int j = (int)(r % go.n1);
+            int i = (int)(r / go.n1);
+            int fi = freq_index(i, go.n0), fj = freq_index(j, go.n1);
+            int si = fi < 0 ? fi + g.n0 : fi, sj = fj < 0 ? fj + g.n1 : fj;
+            sidx = ((int64_t)si * g.n1 + sj) * g.nh2 + l;
+        }
+        double wv = w ? (double)w[sidx] : 1.0;
+        int cached = -1;
+        C s;
+        s.x = 1;
+        s.y = 0;
+        for (int m = 0; m < p.n_maps; ++m) {
+            C *o = out + (int64_t)m * go.nhalf + idx;
+            bool in = (p.lo[m] <= md.k) && (md.k < p.hi[m]);
+            if (!in) {
+                if (!acc) { C z; z.x = 0; z.y = 0; *o = z; }
+                continue;
+            }
+            if (src && p.src[m] != cached) {
+                s = src[(int64_t)p.src[m] * src_stride + sidx];
+                cached = p.src[m];
+            }
+            double f = p.scale[m] * legendre(p.l1[m], md.mu) * legendre(p.l2[m], md.mu);
+            if (p.wpow[m] == 1) f *= wv;
+            else if (p.wpow[m] == 2) f *= wv * wv;
+            else if (p.wpow[m] == -1) f = (wv != 0.0) ? f / wv : 0.0;
+            C v;
+            v.x = (T)((double)s.x * f);
+            v.y = (T)((double)s.y * f);
+            if (acc) {
+                C prev = *o;
+                v.x += prev.x;
+                v.y += prev.y;
+            }
+            *o = v;
+        }
+    }
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+// ------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------
+extern "C" int pb_abi_version(void) { return PB_ABI_VERSION; }
+
+extern "C" const char *pb_last_error(void) { return g_last_error.c_str(); }
+
+struct pb_fft_plan {
+    cufftHandle h;
+    int direction;
+    int precision;
+    size_t ws;
+};
+
+static const char *cufft_name(cufftResult r) {
+    switch (r) {
+        case CUFFT_SUCCESS: return "CUFFT_SUCCESS";
+        case CUFFT_INVALID_PLAN: return "CUFFT_INVALID_PLAN";
+        case CUFFT_ALLOC_FAILED: return "CUFFT_ALLOC_FAILED";
+        case CUFFT_INVALID_VALUE: return "CUFFT_INVALID_VALUE";
+        case CUFFT_INTERNAL_ERROR: return "CUFFT_INTERNAL_ERROR";
+        case CUFFT_EXEC_FAILED: return "CUFFT_EXEC_FAILED";
+        case CUFFT_SETUP_FAILED: return "CUFFT_SETUP_FAILED";
+        case CUFFT_INVALID_SIZE: return "CUFFT_INVALID_SIZE";
+        default: return "CUFFT_ERROR";
+    }
+}
+
+#define PB_CUFFT(call)                                                                 \
+    do {                                                                               \
+        cufftResult _r = (call);                                                       \
+        if (_r != CUFFT_SUCCESS) return fail(PB_ERR_CUFFT, std::string(#call ": ") + cufft_name(_r)); \
+    } while (0)
+
+extern "C" int pb_fft_plan_create(const pb_grid_t *g, int batch, int precision, int direction,
+                                  pb_fft_plan **plan, size_t *workspace_bytes) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (!plan) return fail(PB_ERR_INVALID, "plan out-pointer is NULL");
+    if (batch < 1) return fail(PB_ERR_INVALID, "batch must be >= 1");
+    if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
+    if (direction != PB_FFT_R2C && direction != PB_FFT_C2R) return fail(PB_ERR_INVALID, "bad direction");
+    cufftType type = direction == PB_FFT_R2C ? (precision == PB_F64 ? CUFFT_D2Z : CUFFT_R2C)
+                                             : (precision == PB_F64 ? CUFFT_Z2D : CUFFT_C2R);
+    long long n[3] = {G.n0, G.n1, G.n2};
+    long long rdist = G.nreal, cdist = G.nhalf;
+    long long idist = direction == PB_FFT_R2C ? rdist : cdist;
+    long long odist = direction == PB_FFT_R2C ? cdist : rdist;
+    pb_fft_plan *p = new pb_fft_plan();
+    p->direction = direction;
+    p->precision = precision;
+    cufftResult r = cufftCreate(&p->h);
+    if (r != CUFFT_SUCCESS) {
+        delete p;
+        return fail(PB_ERR_CUFFT, std::string("cufftCreate: ") + cufft_name(r));
+    }
+    r = cufftSetAutoAllocation(p->h, 0);
+    size_t ws = 0;
+    if (r == CUFFT_SUCCESS)
+        r = cufftMakePlanMany64(p->h, 3, n, nullptr, 1, idist, nullptr, 1, odist, type, batch, &ws);
+    if (r != CUFFT_SUCCESS) {
+        cufftDestroy(p->h);
+        delete p;
+        return fail(PB_ERR_CUFFT, std::string("cufftMakePlanMany64: ") + cufft_name(r));
+    }
+    p->ws = ws;
+    *plan = p;
+    if (workspace_bytes) *workspace_bytes = ws;
+    return PB_OK;
+}
+
+extern "C" int pb_fft_exec(pb_fft_plan *p, const void *in, void *out, void *workspace, void *stream) {
+    if (!p || !in || !out) return fail(PB_ERR_INVALID, "pb_fft_exec: NULL argument");
+    if (p->ws && !workspace) return fail(PB_ERR_WORKSPACE, "pb_fft_exec: plan needs a workspace");
+    PB_CUFFT(cufftSetStream(p->h, as_stream(stream)));
+    if (p->ws) PB_CUFFT(cufftSetWorkArea(p->h, workspace));
+    void *i = const_cast<void *>(in);
+    if (p->direction == PB_FFT_R2C) {
+        if (p->precision == PB_F64)
+            PB_CUFFT(cufftExecD2Z(p->h, (cufftDoubleReal *)i, (cufftDoubleComplex *)out));
+        else
+            PB_CUFFT(cufftExecR2C(p->h, (cufftReal *)i, (cufftComplex *)out));
+    } else {
+        if (p->precision == PB_F64)
+            PB_CUFFT(cufftExecZ2D(p->h, (cufftDoubleComplex *)i, (cufftDoubleReal *)out));
+        else
+            PB_CUFFT(cufftExecC2R(p->h, (cufftComplex *)i, (cufftReal *)out));
+    }
+    return PB_OK;
+}
+
+extern "C" int pb_fft_plan_destroy(pb_fft_plan *p) {
+    if (!p) return PB_OK;
+    cufftResult r = cufftDestroy(p->h);
+    delete p;
+    if (r != CUFFT_SUCCESS) return fail(PB_ERR_CUFFT, std::string("cufftDestroy: ") + cufft_name(r));
+    return PB_OK;
+}
+
+extern "C" int pb_spectral_filter(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
+                                  int64_t src_stride, void *out, int n_maps, const int32_t *src_idx,
+                                  const double *lo, const double *hi, const int32_t *l1, const int32_t *l2,
+                                  const double *scale, const int32_t *wpow, const void *w, int accumulate,
+                                  void *stream) {
+    Grid G, GO;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    GO = G;
+    if (out_n) {
+        pb_grid_t go = *g;
+        for (int i = 0; i < 3; ++i) go.n[i] = out_n[i];
+        st = make_grid(&go, &GO);
+        if (st) return st;
+        if (GO.n0 > G.n0 || GO.n1 > G.n1 || GO.n2 > G.n2)
+            return fail(PB_ERR_INVALID, "pb_spectral_filter: output grid larger than the input grid");
+    }
+    if (!out) return fail(PB_ERR_INVALID, "pb_spectral_filter: out is NULL");
+    if (n_maps < 1 || n_maps > PB_FILTER_MAX_MAPS)
+        return fail(PB_ERR_INVALID, "pb_spectral_filter: n_maps must be in [1, 128]");
+    if (!lo || !hi || !l1 || !l2 || !scale)
+        return fail(PB_ERR_INVALID, "pb_spectral_filter: NULL parameter array");
+    FilterParams p;
+    p.n_maps = n_maps;
+    for (int m = 0; m < n_maps; ++m) {
+        if (l1[m] < 0 || l1[m] > 4 || l2[m] < 0 || l2[m] > 4)
+            return fail(PB_ERR_INVALID, "pb_spectral_filter: Legendre order must be in [0, 4]");
+        int wp = wpow ? wpow[m] : 0;
+        if (wp < -1 || wp > 2) return fail(PB_ERR_INVALID, "pb_spectral_filter: wpow must be -1, 0, 1 or 2");
+        if (wp != 0 && !w) return fail(PB_ERR_INVALID, "pb_spectral_filter: wpow set but weight grid is NULL");
+        p.lo[m] = lo[m];
+        p.hi[m] = hi[m];
+        p.scale[m] = scale[m];
+        p.src[m] = src_idx ? src_idx[m] : 0;
+        if (p.src[m] < 0) return fail(PB_ERR_INVALID, "pb_spectral_filter: negative source index");
+        p.l1[m] = (int8_t)l1[m];
+        p.l2[m] = (int8_t)l2[m];
+        p.wpow[m] = (int8_t)wp;
+    }
+    int threads = 256;
+    int blocks = grid_blocks(GO.nhalf, threads);
+    if (precision == PB_F32)
+        filter_kernel<float><<<blocks, threads, 0, as_stream(stream)>>>(
+            G, GO, (const float2 *)src, src_stride, (float2 *)out, (const float *)w, accumulate, p);
+    else if (precision == PB_F64)
+        filter_kernel<double><<<blocks, threads, 0, as_stream(stream)>>>(
+            G, GO, (const double2 *)src, src_stride, (double2 *)out, (const double *)w, accumulate, p);
+    else
+        return fail(PB_ERR_INVALID, "bad precision");
+    PB_LAUNCH_CHECK("pb_spectral_filter");
+    return PB_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// elementwise
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void ew_kernel(int op, int64_t n, const T *x, const T *y, int64_t y_period, const T *z, const T *u, T s,
+                          T *out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        T v;
+        T yv = y[y_period ? i % y_period : i];
+        if (op == PB_EW_MUL) v = x[i] * yv;
+        else v = x[i] * yv - z[i] * u[i];
+        out[i] = s * v;
+    }
+}
+
+extern "C" int pb_elementwise(int precision, int op, int64_t n, const void *x, const void *y, int64_t y_period,
+                              const void *z, const void *u, double s, void *out, void *stream) {
+    if (n < 0) return fail(PB_ERR_INVALID, "pb_elementwise: negative size");
+    if (n == 0) return PB_OK;
+    if (!x || !y || !out) return fail(PB_ERR_INVALID, "pb_elementwise: NULL argument");
+    if (op == PB_EW_PRODDIFF && (!z || !u)) return fail(PB_ERR_INVALID, "pb_elementwise: PRODDIFF needs z, u");
+    if (op != PB_EW_MUL && op != PB_EW_PRODDIFF) return fail(PB_ERR_INVALID, "pb_elementwise: bad op");
+    if (y_period < 0 || (y_period > 0 && n % y_period != 0))
+        return fail(PB_ERR_INVALID, "pb_elementwise: y_period must divide n");
+    if (op == PB_EW_PRODDIFF && y_period != 0) return fail(PB_ERR_INVALID, "pb_elementwise: PRODDIFF takes no y_period");
+    int threads = 256;
+    int blocks = grid_blocks(n, threads, 16);
+    if (precision == PB_F32)
+        ew_kernel<float><<<blocks, threads, 0, as_stream(stream)>>>(op, n, (const float *)x, (const float *)y, y_period,
+                                                                   (const float *)z, (const float *)u,
+                                                                   (float)s, (float *)out);
+    else if (precision == PB_F64)
+        ew_kernel<double><<<blocks, threads, 0, as_stream(stream)>>>(op, n, (const double *)x, (const double *)y, y_period,
+                                                                    (const double *)z, (const double *)u, s,
+                                                                    (double *)out);
+    else
+        return fail(PB_ERR_INVALID, "bad precision");
+    PB_LAUNCH_CHECK("pb_elementwise");
+    return PB_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Gaussian random field from white noise
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void grf_kernel(Grid g, const double *nre, const double *nim, int n_batch, const double *amp,
+                           double scale, typename cplx<T>::type *out) {
+    using C = typename cplx<T>::type;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t total = g.nhalf * n_batch;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        int64_t bidx = t / g.nhalf;
+        int64_t idx = t - bidx * g.nhalf;
+        int l = (int)(idx % g.nh2);
+        int64_t r = idx / g.nh2;
+        int j = (int)(r % g.n1);
+        int i = (int)(r / g.n1);
+        int mi = (g.n0 - i) % g.n0, mj = (g.n1 - j) % g.n1, ml = (g.n2 - l) % g.n2;
+        const double *re = nre + bidx * g.nreal;
+        const double *im = nim + bidx * g.nreal;
+        int64_t p = ((int64_t)i * g.n1 + j) * g.n2 + l;
+        int64_t q = ((int64_t)mi * g.n1 + mj) * g.n2 + ml;
+        double ar = 0.0, ai = 0.0;
+        if (p != 0) {  // r[0,0,0] = 0 and its mirror is itself
+            ar = 0.5 * (re[p] + re[q]);
+            ai = 0.5 * (im[p] - im[q]);
+        }
+        double a = amp[idx];
+        C v;
+        v.x = (T)(ar * a * scale);
+        v.y = (T)(ai * a * scale);
+        out[t] = v;
+    }
+}
+
+extern "C" int pb_grf_from_noise(const pb_grid_t *g, int precision, const double *noise_re, const double *noise_im,
+                                 int n_batch, const double *amp, double scale, void *out, void *stream) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (!noise_re || !noise_im || !amp || !out) return fail(PB_ERR_INVALID, "pb_grf_from_noise: NULL argument");
+    if (n_batch < 1) return fail(PB_ERR_INVALID, "pb_grf_from_noise: n_batch must be >= 1");
+    int threads = 256;
+    int blocks = grid_blocks(G.nhalf * n_batch, threads, 16);
+    if (precision == PB_F32)
+        grf_kernel<float><<<blocks, threads, 0, as_stream(stream)>>>(G, noise_re, noise_im, n_batch, amp, scale,
+                                                                    (float2 *)out);
+    else if (precision == PB_F64)
+        grf_kernel<double><<<blocks, threads, 0, as_stream(stream)>>>(G, noise_re, noise_im, n_batch, amp, scale,
+                                                                     (double2 *)out);
+    else
+        return fail(PB_ERR_INVALID, "bad precision");
+    PB_LAUNCH_CHECK("pb_grf_from_noise");
+    return PB_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// batched pair products  out[p] = s * (X[i_p] * Y[j_p] - Z[i_p] * U[j_p])
+// ------------------------------------------------------------------------------------
+namespace pb {
+struct PairParams {
+    int32_t i[PB_PAIR_MAX];
+    int32_t j[PB_PAIR_MAX];
+    int32_t n;
+};
+
+template <typename T>
+__global__ void pair_kernel(int64_t n_vox, const T *X, const T *Y, const T *Z, const T *U, T s, T *out,
+                            PairParams p) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int pidx = blockIdx.y;
+    const T *x = X + (int64_t)p.i[pidx] * n_vox;
+    const T *y = Y + (int64_t)p.j[pidx] * n_vox;
+    const T *z = Z ? Z + (int64_t)p.i[pidx] * n_vox : nullptr;
+    const T *u = U ? U + (int64_t)p.j[pidx] * n_vox : nullptr;
+    T *o = out + (int64_t)pidx * n_vox;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_vox; v += stride) {
+        T r = x[v] * y[v];
+        if (z) r -= z[v] * u[v];
+        o[v] = s * r;
+    }
+}
+}  // namespace pb
+
+extern "C" int pb_pair_products(int precision, int64_t n_vox, const void *X, const void *Y, const void *Z,
+                                const void *U, const int32_t *pairs, int n_pairs, double s, void *out, void *stream) {
+    if (n_vox < 1 || n_pairs < 0) return fail(PB_ERR_INVALID, "pb_pair_products: bad sizes");
+    if (n_pairs == 0) return PB_OK;
+    if (!X || !Y || !pairs || !out) return fail(PB_ERR_INVALID, "pb_pair_products: NULL argument");
+    if ((Z == nullptr) != (U == nullptr)) return fail(PB_ERR_INVALID, "pb_pair_products: Z and U go together");
+    size_t esz = precision == PB_F64 ? 8 : 4;
+    if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
+    int threads = 256;
+    int bx = grid_blocks(n_vox, threads, 2);
+    for (int c0 = 0; c0 < n_pairs; c0 += PB_PAIR_MAX) {
+        PairParams p;
+        p.n = std::min(PB_PAIR_MAX, n_pairs - c0);
+        for (int k = 0; k < p.n; ++k) {
+            p.i[k] = pairs[2 * (c0 + k)];
+            p.j[k] = pairs[2 * (c0 + k) + 1];
+            if (p.i[k] < 0 || p.j[k] < 0) return fail(PB_ERR_INVALID, "pb_pair_products: negative map index");
+        }
+        dim3 grid(bx, p.n);
+        void *o = (char *)out + (size_t)c0 * n_vox * esz;
+        if (precision == PB_F32)
+            pair_kernel<float><<<grid, threads, 0, as_stream(stream)>>>(n_vox, (const float *)X, (const float *)Y,
+                                                                       (const float *)Z, (const float *)U, (float)s,
+                                                                       (float *)o, p);
+        else
+            pair_kernel<double><<<grid, threads, 0, as_stream(stream)>>>(n_vox, (const double *)X, (const double *)Y,
+                                                                        (const double *)Z, (const double *)U, s,
+                                                                        (double *)o, p);
+        PB_LAUNCH_CHECK("pb_pair_products");
+    }
+    return PB_OK;
+}

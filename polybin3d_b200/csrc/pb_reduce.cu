@@ -1,0 +1,316 @@
+// k-bin x Legendre reductions over half spectra (the power-spectrum binning pass) and
+// the per-shell Fisher-row contraction.  FP64 accumulation, deterministic two-pass sums.
+#include <algorithm>
+#include <string>
+#include <vector>
+#include "pb_common.cuh"
+
+namespace pb {
+
+struct RedParams {
+    double edges[PB_RED_MAX_BINS + 1];
+    int8_t la[PB_RED_MAX_ELLS];
+    int8_t lb[PB_RED_MAX_ELLS];
+    int32_t nk;
+    int32_t n_ell;
+};
+
+constexpr int RED_THREADS = 256;
+constexpr int RED_CHUNK = 4;  // consecutive modes per thread per step (same kz line, mostly same bin)
+
+static int red_blocks(const Grid &G) {
+    int64_t per_block = (int64_t)RED_THREADS * RED_CHUNK;
+    int64_t b = (G.nhalf + per_block - 1) / per_block;
+    int64_t cap = (int64_t)num_sms() * 2;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, cap));
+}
+
+// bin b with edges[b] <= k < edges[b+1], or -1
+__device__ __forceinline__ int find_bin(const double *edges, int nk, double k) {
+    if (!(edges[0] <= k) || !(k < edges[nk])) return -1;
+    int lo = 0, hi = nk;  // invariant: edges[lo] <= k < edges[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (edges[mid] <= k) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(RED_THREADS) binred_kernel(Grid g, const typename cplx<T>::type *a,
+                                                            const typename cplx<T>::type *b, const T *w,
+                                                            int64_t row_stride, RedParams p, double *partials) {
+    using C = typename cplx<T>::type;
+    __shared__ double acc[PB_RED_MAX_ELLS * PB_RED_MAX_BINS];
+    __shared__ double edges[PB_RED_MAX_BINS + 1];
+    const int nk = p.nk, ne = p.n_ell;
+    for (int i = threadIdx.x; i < ne * nk; i += blockDim.x) acc[i] = 0.0;
+    for (int i = threadIdx.x; i <= nk; i += blockDim.x) edges[i] = p.edges[i];
+    __syncthreads();
+    const int row = blockIdx.y;
+    const C *arow = (MODE == PB_RED_ABS2) ? a + (int64_t)row * row_stride : a;
+    const C *brow = (MODE == PB_RED_CROSS) ? b + (int64_t)row * row_stride : nullptr;
+    const int64_t step = (int64_t)gridDim.x * blockDim.x * RED_CHUNK;
+    for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * RED_CHUNK; base < g.nhalf;
+         base += step) {
+        int cur = -1;
+        double run[PB_RED_MAX_ELLS];
+#pragma unroll
+        for (int e = 0; e < PB_RED_MAX_ELLS; ++e) run[e] = 0.0;
+        const int64_t end = min(base + RED_CHUNK, g.nhalf);
+        for (int64_t idx = base; idx < end; ++idx) {
+            Mode md = mode_of(g, idx);
+            int bin = find_bin(edges, nk, md.k);
+            if (bin != cur) {
+                if (cur >= 0) {
+#pragma unroll
+                    for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                        if (e < ne) atomicAdd(&acc[e * nk + cur], run[e]);
+                }
+#pragma unroll
+                for (int e = 0; e < PB_RED_MAX_ELLS; ++e) run[e] = 0.0;
+                cur = bin;
+            }
+            if (bin < 0) continue;
+            double f;
+            if (MODE == PB_RED_ABS2) {
+                C v = arow[idx];
+                f = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+            } else if (MODE == PB_RED_CROSS) {
+                C u = arow[idx], v = brow[idx];
+                f = (double)u.x * (double)v.x + (double)u.y * (double)v.y;
+            } else {
+                double v = w ? (double)w[idx] : 1.0;
+                f = v * v;
+            }
+            f *= md.deg;
+#pragma unroll
+            for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                if (e < ne) run[e] += f * legendre(p.la[e], md.mu) * legendre(p.lb[e], md.mu);
+        }
+        if (cur >= 0) {
+#pragma unroll
+            for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                if (e < ne) atomicAdd(&acc[e * nk + cur], run[e]);
+        }
+    }
+    __syncthreads();
+    double *dst = partials + ((int64_t)row * gridDim.x + blockIdx.x) * (ne * nk);
+    for (int i = threadIdx.x; i < ne * nk; i += blockDim.x) dst[i] = acc[i];
+}
+
+__global__ void binred_finalize(const double *partials, int n_blocks, int per_row, int n_rows, double scale,
+                                double *out, int accumulate) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_rows * per_row) return;
+    int row = t / per_row, j = t - row * per_row;
+    const double *src = partials + (int64_t)row * n_blocks * per_row + j;
+    double s = 0.0;
+    for (int blk = 0; blk < n_blocks; ++blk) s += src[(int64_t)blk * per_row];
+    s *= scale;
+    out[t] = accumulate ? out[t] + s : s;
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" int pb_bin_reduce_workspace_size(const pb_grid_t *g, int n_rows, int nk, int n_ell, size_t *bytes) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (!bytes) return fail(PB_ERR_INVALID, "bytes is NULL");
+    if (n_rows < 1 || nk < 1 || n_ell < 1) return fail(PB_ERR_INVALID, "pb_bin_reduce: empty reduction");
+    *bytes = (size_t)n_rows * red_blocks(G) * nk * n_ell * sizeof(double);
+    return PB_OK;
+}
+
+extern "C" int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const void *a, const void *b,
+                             int n_rows, int64_t row_stride, const double *edges, int nk, const int32_t *ells,
+                             int n_ell, double scale, double *out, int accumulate, void *workspace,
+                             size_t workspace_bytes, void *stream) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (nk < 1 || nk > PB_RED_MAX_BINS) return fail(PB_ERR_INVALID, "pb_bin_reduce: nk must be in [1, 64]");
+    if (n_ell < 1 || n_ell > PB_RED_MAX_ELLS) return fail(PB_ERR_INVALID, "pb_bin_reduce: n_ell must be in [1, 9]");
+    if (n_rows < 1 || n_rows > 65535) return fail(PB_ERR_INVALID, "pb_bin_reduce: n_rows must be in [1, 65535]");
+    if (!edges || !ells || !out) return fail(PB_ERR_INVALID, "pb_bin_reduce: NULL argument");
+    if (mode == PB_RED_ABS2 && !a) return fail(PB_ERR_INVALID, "pb_bin_reduce: ABS2 needs a");
+    if (mode == PB_RED_CROSS && (!a || !b)) return fail(PB_ERR_INVALID, "pb_bin_reduce: CROSS needs a and b");
+    if (mode < 0 || mode > 2) return fail(PB_ERR_INVALID, "pb_bin_reduce: bad mode");
+    if (row_stride == 0) row_stride = G.nhalf;
+    RedParams p;
+    for (int i = 0; i <= nk; ++i) {
+        p.edges[i] = edges[i];
+        if (i > 0 && !(edges[i] > edges[i - 1]))
+            return fail(PB_ERR_INVALID, "pb_bin_reduce: bin edges must be strictly increasing");
+    }
+    for (int e = 0; e < n_ell; ++e) {
+        if (ells[2 * e] < 0 || ells[2 * e] > 4 || ells[2 * e + 1] < 0 || ells[2 * e + 1] > 4)
+            return fail(PB_ERR_INVALID, "pb_bin_reduce: Legendre order must be in [0, 4]");
+        p.la[e] = (int8_t)ells[2 * e];
+        p.lb[e] = (int8_t)ells[2 * e + 1];
+    }
+    p.nk = nk;
+    p.n_ell = n_ell;
+    int nb = red_blocks(G);
+    size_t need = (size_t)n_rows * nb * nk * n_ell * sizeof(double);
+    if (!workspace || workspace_bytes < need)
+        return fail(PB_ERR_WORKSPACE, "pb_bin_reduce: workspace too small (need " + std::to_string(need) + " bytes)");
+    double *partials = (double *)workspace;
+    dim3 grid(nb, n_rows);
+    cudaStream_t s = as_stream(stream);
+#define PB_RED_LAUNCH(T, M)                                                                        \
+    binred_kernel<T, M><<<grid, RED_THREADS, 0, s>>>(G, (const cplx<T>::type *)a, (const cplx<T>::type *)b, \
+                                                      (const T *)a, row_stride, p, partials)
+    if (precision == PB_F32) {
+        if (mode == PB_RED_ABS2) PB_RED_LAUNCH(float, PB_RED_ABS2);
+        else if (mode == PB_RED_CROSS) PB_RED_LAUNCH(float, PB_RED_CROSS);
+        else PB_RED_LAUNCH(float, PB_RED_REAL2);
+    } else if (precision == PB_F64) {
+        if (mode == PB_RED_ABS2) PB_RED_LAUNCH(double, PB_RED_ABS2);
+        else if (mode == PB_RED_CROSS) PB_RED_LAUNCH(double, PB_RED_CROSS);
+        else PB_RED_LAUNCH(double, PB_RED_REAL2);
+    } else {
+        return fail(PB_ERR_INVALID, "bad precision");
+    }
+#undef PB_RED_LAUNCH
+    PB_LAUNCH_CHECK("pb_bin_reduce");
+    int per_row = nk * n_ell;
+    int total = per_row * n_rows;
+    binred_finalize<<<(total + 255) / 256, 256, 0, s>>>(partials, nb, per_row, n_rows, scale, out, accumulate);
+    PB_LAUNCH_CHECK("pb_bin_reduce(finalize)");
+    return PB_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Fisher rows over one k-shell:  out[orow[r]][j] = scale * sum_{i} deg_i Re(conj(F[key_r](m_i)) Q_j(m_i))
+// over the shell's mode list m_i.  Chunked: each block stages SR_CH modes of <= SR_R rows
+// and SR_CT columns in shared memory, writes one partial per (chunk, row, column);
+// a second pass sums the chunks in order.
+// ------------------------------------------------------------------------------------
+namespace pb {
+constexpr int SR_THREADS = 256;
+constexpr int SR_CH = 32;   // modes per chunk
+constexpr int SR_R = 32;    // rows per launch
+constexpr int SR_CT = 32;   // columns per block
+
+struct ShellRowKeys {
+    int32_t key[SR_R];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(SR_THREADS) shell_rows_kernel(Grid g, const typename cplx<T>::type *F,
+                                                               const typename cplx<T>::type *Q, int n_rows,
+                                                               int n_cols, const int64_t *modes, int64_t n_modes,
+                                                               ShellRowKeys keys, double *partials) {
+    using C = typename cplx<T>::type;
+    __shared__ double2 Fs[SR_R][SR_CH + 1];
+    __shared__ double2 Qs[SR_CT][SR_CH + 1];
+    const int chunk = blockIdx.x;
+    const int j0 = blockIdx.y * SR_CT;
+    const int64_t m0 = (int64_t)chunk * SR_CH;
+    const int ncols_here = min(SR_CT, n_cols - j0);
+    for (int e = threadIdx.x; e < SR_R * SR_CH; e += SR_THREADS) {
+        int r = e / SR_CH, i = e - r * SR_CH;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < n_rows && m0 + i < n_modes) {
+            int64_t idx = modes[m0 + i];
+            double deg = ((idx % g.nh2) > 0) ? 2.0 : 1.0;
+            C f = F[(int64_t)keys.key[r] * g.nhalf + idx];
+            v = make_double2(deg * (double)f.x, deg * (double)f.y);
+        }
+        Fs[r][i] = v;
+    }
+    for (int e = threadIdx.x; e < SR_CT * SR_CH; e += SR_THREADS) {
+        int j = e / SR_CH, i = e - j * SR_CH;
+        double2 v = make_double2(0.0, 0.0);
+        if (j < ncols_here && m0 + i < n_modes) {
+            C q = Q[(int64_t)(j0 + j) * g.nhalf + modes[m0 + i]];
+            v = make_double2((double)q.x, (double)q.y);
+        }
+        Qs[j][i] = v;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < SR_R * SR_CT; o += SR_THREADS) {
+        int r = o / SR_CT, j = o - r * SR_CT;
+        if (r >= n_rows || j >= ncols_here) continue;
+        double s = 0.0;
+#pragma unroll 8
+        for (int i = 0; i < SR_CH; ++i) s += Fs[r][i].x * Qs[j][i].x + Fs[r][i].y * Qs[j][i].y;
+        partials[((int64_t)chunk * n_rows + r) * n_cols + j0 + j] = s;
+    }
+}
+
+struct ShellRowOut {
+    int32_t orow[SR_R];
+};
+
+__global__ void shell_rows_finalize(const double *partials, int n_chunks, int n_rows, int n_cols, double scale,
+                                    double *out, int64_t out_stride, ShellRowOut o) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_rows * n_cols) return;
+    int r = t / n_cols, j = t - r * n_cols;
+    double s = 0.0;
+    for (int c = 0; c < n_chunks; ++c) s += partials[((int64_t)c * n_rows + r) * n_cols + j];
+    out[(int64_t)o.orow[r] * out_stride + j] = s * scale;
+}
+}  // namespace pb
+
+extern "C" int pb_shell_rows_workspace_size(int64_t n_modes, int n_rows, int n_cols, size_t *bytes) {
+    if (!bytes) return fail(PB_ERR_INVALID, "bytes is NULL");
+    if (n_modes < 0 || n_rows < 1 || n_rows > SR_R || n_cols < 1)
+        return fail(PB_ERR_INVALID, "pb_shell_rows_workspace_size: bad sizes");
+    int64_t n_chunks = std::max<int64_t>(1, (n_modes + SR_CH - 1) / SR_CH);
+    *bytes = (size_t)n_chunks * n_rows * n_cols * sizeof(double);
+    return PB_OK;
+}
+
+extern "C" int pb_shell_rows(const pb_grid_t *g, int precision, const void *F, int n_f, const void *Q, int n_cols,
+                             const int64_t *modes, int64_t n_modes, const int32_t *row_key, const int32_t *out_row,
+                             int n_rows, double scale, double *out, int64_t out_stride, void *workspace,
+                             size_t workspace_bytes, void *stream) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (!F || !Q || !row_key || !out_row || !out) return fail(PB_ERR_INVALID, "pb_shell_rows: NULL argument");
+    if (n_rows < 1 || n_rows > SR_R) return fail(PB_ERR_INVALID, "pb_shell_rows: n_rows must be in [1, 32]");
+    if (n_cols < 1 || n_f < 1) return fail(PB_ERR_INVALID, "pb_shell_rows: empty input");
+    if (n_modes < 0 || (n_modes > 0 && !modes)) return fail(PB_ERR_INVALID, "pb_shell_rows: bad mode list");
+    ShellRowKeys keys;
+    ShellRowOut orow;
+    for (int r = 0; r < SR_R; ++r) {
+        keys.key[r] = r < n_rows ? row_key[r] : 0;
+        orow.orow[r] = r < n_rows ? out_row[r] : 0;
+        if (r < n_rows && (keys.key[r] < 0 || keys.key[r] >= n_f))
+            return fail(PB_ERR_INVALID, "pb_shell_rows: row key out of range");
+        if (r < n_rows && orow.orow[r] < 0) return fail(PB_ERR_INVALID, "pb_shell_rows: negative output row");
+    }
+    if (out_stride == 0) out_stride = n_cols;
+    int64_t n_chunks = std::max<int64_t>(1, (n_modes + SR_CH - 1) / SR_CH);
+    size_t need = (size_t)n_chunks * n_rows * n_cols * sizeof(double);
+    if (!workspace || workspace_bytes < need) return fail(PB_ERR_WORKSPACE, "pb_shell_rows: workspace too small");
+    if (n_chunks > 2147483647) return fail(PB_ERR_INVALID, "pb_shell_rows: too many modes");
+    cudaStream_t s = as_stream(stream);
+    dim3 grid((unsigned)n_chunks, (n_cols + SR_CT - 1) / SR_CT);
+    double *partials = (double *)workspace;
+    if (n_modes == 0) {
+        // empty shell: zero partials through a one-chunk launch with no modes
+    }
+    if (precision == PB_F64)
+        shell_rows_kernel<double><<<grid, SR_THREADS, 0, s>>>(G, (const double2 *)F, (const double2 *)Q, n_rows,
+                                                              n_cols, modes, n_modes, keys, partials);
+    else if (precision == PB_F32)
+        shell_rows_kernel<float><<<grid, SR_THREADS, 0, s>>>(G, (const float2 *)F, (const float2 *)Q, n_rows, n_cols,
+                                                             modes, n_modes, keys, partials);
+    else
+        return fail(PB_ERR_INVALID, "bad precision");
+    PB_LAUNCH_CHECK("pb_shell_rows");
+    int total = n_rows * n_cols;
+    shell_rows_finalize<<<(total + 255) / 256, 256, 0, s>>>(partials, (int)n_chunks, n_rows, n_cols, scale, out,
+                                                           out_stride, orow);
+    PB_LAUNCH_CHECK("pb_shell_rows(finalize)");
+    return PB_OK;
+}

@@ -1,0 +1,277 @@
+// Triplet contraction  out[t] = scale * sum_x A[i1](x) B[i2](x) C[i3](x)  on CUDA cores.
+//
+// The triplet list is tiled on the host into "items": one A map, up to TB B maps and up
+// to TC C maps, so one thread forms TB pair products and TB x TC FMAs per voxel from
+// 1 + TB + TC shared-memory loads.  A CTA stages a tile of TV voxels of every map in
+// shared memory, P threads share an item (voxels strided by P), per-tile sums are kept in
+// the maps' precision and folded into FP64 registers after each tile.  Per-CTA FP64
+// partials go to the caller's workspace and a second kernel sums them in a fixed order,
+// so results are deterministic.
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+#include "pb_common.cuh"
+#include "pb_triplet.cuh"
+
+namespace pb {
+
+int triplet_build_items(int n_a, int n_b, int n_c, const int32_t *idx, int n_trip, std::vector<TripletItem> &items) {
+    items.clear();
+    if (n_trip < 1) return fail(PB_ERR_INVALID, "triplet list is empty");
+    if (!idx) return fail(PB_ERR_INVALID, "triplet index array is NULL");
+    // a -> list of (b, c, t)
+    std::map<int, std::vector<std::array<int, 3>>> by_a;
+    for (int t = 0; t < n_trip; ++t) {
+        int a = idx[3 * t], b = idx[3 * t + 1], c = idx[3 * t + 2];
+        if (a < 0 || a >= n_a || b < 0 || b >= n_b || c < 0 || c >= n_c)
+            return fail(PB_ERR_INVALID, "triplet index out of range at row " + std::to_string(t));
+        by_a[a].push_back({b, c, t});
+    }
+    for (auto &kv : by_a) {
+        std::vector<int> bs;
+        for (auto &e : kv.second) bs.push_back(e[0]);
+        std::sort(bs.begin(), bs.end());
+        bs.erase(std::unique(bs.begin(), bs.end()), bs.end());
+        for (size_t b0 = 0; b0 < bs.size(); b0 += TRIP_TB) {
+            size_t nb = std::min<size_t>(TRIP_TB, bs.size() - b0);
+            std::vector<int> cs;
+            for (auto &e : kv.second)
+                for (size_t i = 0; i < nb; ++i)
+                    if (e[0] == bs[b0 + i]) cs.push_back(e[1]);
+            std::sort(cs.begin(), cs.end());
+            cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+            for (size_t c0 = 0; c0 < cs.size(); c0 += TRIP_TC) {
+                size_t nc = std::min<size_t>(TRIP_TC, cs.size() - c0);
+                TripletItem it;
+                it.a = kv.first;
+                for (int i = 0; i < TRIP_TB; ++i) it.b[i] = bs[b0 + std::min<size_t>(i, nb - 1)];
+                for (int j = 0; j < TRIP_TC; ++j) it.c[j] = cs[c0 + std::min<size_t>(j, nc - 1)];
+                for (int i = 0; i < TRIP_TB; ++i)
+                    for (int j = 0; j < TRIP_TC; ++j) it.out[i][j] = -1;
+                int filled = 0;
+                for (auto &e : kv.second) {
+                    for (size_t i = 0; i < nb; ++i) {
+                        if (e[0] != bs[b0 + i]) continue;
+                        for (size_t j = 0; j < nc; ++j)
+                            if (e[1] == cs[c0 + j]) {
+                                it.out[i][j] = e[2];
+                                ++filled;
+                            }
+                    }
+                }
+                if (filled) items.push_back(it);
+            }
+        }
+    }
+    return PB_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// SIMT kernel
+// ------------------------------------------------------------------------------------
+constexpr int SIMT_THREADS = 256;
+constexpr int SIMT_TV = 128;       // voxels per tile
+constexpr int SIMT_PAD = 4;        // row padding (floats/doubles) against bank conflicts
+
+template <typename T>
+__global__ void __launch_bounds__(SIMT_THREADS) triplet_simt_kernel(const T *A, int n_a, const T *B, int n_b,
+                                                                   int off_b, const T *C, int n_c, int off_c,
+                                                                   int n_rows, int64_t n_vox,
+                                                                   const TripletItem *items, int n_items,
+                                                                   int group_p, double *partials, int n_trip) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *tile = reinterpret_cast<T *>(smem_raw);
+    constexpr int LD = SIMT_TV + SIMT_PAD;
+    const int slots = SIMT_THREADS / group_p;
+    const int item_id = blockIdx.y * slots + threadIdx.x / group_p;
+    const int p = threadIdx.x % group_p;
+    const bool active = item_id < n_items;
+    int ra = 0, rb[TRIP_TB], rc[TRIP_TC];
+    if (active) {
+        // rows clamped into the staged tile: a table built for other map counts cannot
+        // index outside shared memory
+        const TripletItem &it = items[item_id];
+        ra = min(max(it.a, 0), n_rows - 1);
+#pragma unroll
+        for (int i = 0; i < TRIP_TB; ++i) rb[i] = min(max(off_b + it.b[i], 0), n_rows - 1);
+#pragma unroll
+        for (int j = 0; j < TRIP_TC; ++j) rc[j] = min(max(off_c + it.c[j], 0), n_rows - 1);
+    } else {
+#pragma unroll
+        for (int i = 0; i < TRIP_TB; ++i) rb[i] = 0;
+#pragma unroll
+        for (int j = 0; j < TRIP_TC; ++j) rc[j] = 0;
+    }
+    double accd[TRIP_TB][TRIP_TC];
+#pragma unroll
+    for (int i = 0; i < TRIP_TB; ++i)
+#pragma unroll
+        for (int j = 0; j < TRIP_TC; ++j) accd[i][j] = 0.0;
+
+    const int64_t n_tiles = (n_vox + SIMT_TV - 1) / SIMT_TV;
+    for (int64_t tt = blockIdx.x; tt < n_tiles; tt += gridDim.x) {
+        const int64_t v0 = tt * SIMT_TV;
+        // stage rows: [0,n_a) from A, then B (if distinct), then C (if distinct)
+        for (int e = threadIdx.x; e < n_rows * SIMT_TV; e += SIMT_THREADS) {
+            int r = e / SIMT_TV, v = e - r * SIMT_TV;
+            const T *src;
+            int m;
+            if (r < n_a) { src = A; m = r; }
+            else if (off_b > 0 && r < off_b + n_b) { src = B; m = r - off_b; }
+            else { src = C; m = r - off_c; }
+            int64_t x = v0 + v;
+            tile[r * LD + v] = (x < n_vox) ? src[(int64_t)m * n_vox + x] : (T)0;
+        }
+        __syncthreads();
+        if (active) {
+            T acc[TRIP_TB][TRIP_TC];
+#pragma unroll
+            for (int i = 0; i < TRIP_TB; ++i)
+#pragma unroll
+                for (int j = 0; j < TRIP_TC; ++j) acc[i][j] = (T)0;
+            for (int v = p; v < SIMT_TV; v += group_p) {
+                T av = tile[ra * LD + v];
+                T cv[TRIP_TC];
+#pragma unroll
+                for (int j = 0; j < TRIP_TC; ++j) cv[j] = tile[rc[j] * LD + v];
+#pragma unroll
+                for (int i = 0; i < TRIP_TB; ++i) {
+                    T pv = av * tile[rb[i] * LD + v];
+#pragma unroll
+                    for (int j = 0; j < TRIP_TC; ++j) acc[i][j] = fma(pv, cv[j], acc[i][j]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < TRIP_TB; ++i)
+#pragma unroll
+                for (int j = 0; j < TRIP_TC; ++j) accd[i][j] += (double)acc[i][j];
+        }
+        __syncthreads();
+    }
+    // reduce over the group_p lanes of an item (consecutive lanes, group_p <= 32)
+#pragma unroll
+    for (int i = 0; i < TRIP_TB; ++i)
+#pragma unroll
+        for (int j = 0; j < TRIP_TC; ++j)
+            for (int o = group_p >> 1; o > 0; o >>= 1) accd[i][j] += __shfl_xor_sync(0xffffffffu, accd[i][j], o);
+    if (active && p == 0) {
+        const TripletItem &it = items[item_id];
+        double *dst = partials + (int64_t)blockIdx.x * n_trip;
+#pragma unroll
+        for (int i = 0; i < TRIP_TB; ++i)
+#pragma unroll
+            for (int j = 0; j < TRIP_TC; ++j)
+                if (it.out[i][j] >= 0 && it.out[i][j] < n_trip) dst[it.out[i][j]] = accd[i][j];
+    }
+}
+
+__global__ void triplet_finalize(const double *partials, int n_parts, int n_trip, double scale, double *out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_trip) return;
+    double s = 0.0;
+    for (int c = 0; c < n_parts; ++c) s += partials[(int64_t)c * n_trip + t];
+    out[t] = s * scale;
+}
+
+int simt_geometry(int64_t n_vox, int n_items, int *grid_x, int *grid_y, int *group_p) {
+    int slots_needed = n_items;
+    // threads per item: spread voxels when there are few items
+    int p = 1;
+    while (p < 32 && (SIMT_THREADS / (p * 2)) >= slots_needed) p *= 2;
+    int slots = SIMT_THREADS / p;
+    *group_p = p;
+    *grid_y = (n_items + slots - 1) / slots;
+    int64_t n_tiles = (n_vox + SIMT_TV - 1) / SIMT_TV;
+    int64_t gx = std::min<int64_t>(n_tiles, (int64_t)num_sms() * 2);
+    *grid_x = (int)std::max<int64_t>(1, gx);
+    return PB_OK;
+}
+
+int launch_triplet_simt(int precision, const void *A, int n_a, const void *B, int n_b, const void *C, int n_c,
+                        int64_t n_vox, const TripletItem *items_dev, int n_items, int n_trip, double scale,
+                        double *out, void *workspace, size_t workspace_bytes, cudaStream_t s) {
+    int gx, gy, gp;
+    simt_geometry(n_vox, n_items, &gx, &gy, &gp);
+    size_t need = (size_t)gx * n_trip * sizeof(double);
+    if (!workspace || workspace_bytes < need)
+        return fail(PB_ERR_WORKSPACE, "pb_triplet_contract: workspace too small (need " + std::to_string(need) + ")");
+    int off_b = (B == A && n_b == n_a) ? 0 : n_a;
+    int after_b = off_b > 0 ? off_b + n_b : n_a;
+    int off_c;
+    if (C == A && n_c == n_a) off_c = 0;
+    else if (C == B && n_c == n_b) off_c = off_b;
+    else off_c = after_b;
+    int n_rows = (off_c == after_b) ? after_b + n_c : after_b;
+    size_t esz = precision == PB_F64 ? 8 : 4;
+    size_t smem = (size_t)n_rows * (SIMT_TV + SIMT_PAD) * esz;
+    if (smem > 227 * 1024) return fail(PB_ERR_UNSUPPORTED, "pb_triplet_contract: too many maps for one tile");
+    dim3 grid(gx, gy);
+    double *partials = (double *)workspace;
+    if (precision == PB_F32) {
+        PB_CUDA(cudaFuncSetAttribute(triplet_simt_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        triplet_simt_kernel<float><<<grid, SIMT_THREADS, smem, s>>>(
+            (const float *)A, n_a, (const float *)B, n_b, off_b, (const float *)C, n_c, off_c, n_rows, n_vox,
+            items_dev, n_items, gp, partials, n_trip);
+    } else {
+        PB_CUDA(cudaFuncSetAttribute(triplet_simt_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        triplet_simt_kernel<double><<<grid, SIMT_THREADS, smem, s>>>(
+            (const double *)A, n_a, (const double *)B, n_b, off_b, (const double *)C, n_c, off_c, n_rows, n_vox,
+            items_dev, n_items, gp, partials, n_trip);
+    }
+    PB_LAUNCH_CHECK("pb_triplet_contract(simt)");
+    triplet_finalize<<<(n_trip + 255) / 256, 256, 0, s>>>(partials, gx, n_trip, scale, out);
+    PB_LAUNCH_CHECK("pb_triplet_contract(finalize)");
+    return PB_OK;
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" int pb_triplet_plan(int n_a, int n_b, int n_c, const int32_t *idx, int n_trip, void *table,
+                               size_t *table_bytes, int *n_items) {
+    std::vector<TripletItem> items;
+    int st = triplet_build_items(n_a, n_b, n_c, idx, n_trip, items);
+    if (st) return st;
+    size_t bytes = items.size() * sizeof(TripletItem);
+    if (n_items) *n_items = (int)items.size();
+    if (!table) {
+        if (table_bytes) *table_bytes = bytes;
+        return PB_OK;
+    }
+    if (!table_bytes || *table_bytes < bytes) return fail(PB_ERR_INVALID, "pb_triplet_plan: table buffer too small");
+    memcpy(table, items.data(), bytes);
+    *table_bytes = bytes;
+    return PB_OK;
+}
+
+extern "C" int pb_triplet_workspace_size(int precision, int method, int64_t n_vox, int n_items, int n_trip,
+                                         size_t *bytes) {
+    if (!bytes) return fail(PB_ERR_INVALID, "bytes is NULL");
+    if (n_vox < 1 || n_items < 1 || n_trip < 1) return fail(PB_ERR_INVALID, "pb_triplet_workspace_size: empty");
+    if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
+    if (method == PB_TRIPLET_TC) return triplet_tc_workspace_size(n_vox, n_items, n_trip, bytes);
+    int gx, gy, gp;
+    simt_geometry(n_vox, n_items, &gx, &gy, &gp);
+    *bytes = (size_t)gx * n_trip * sizeof(double);
+    return PB_OK;
+}
+
+extern "C" int pb_triplet_contract(int precision, int method, const void *A, int n_a, const void *B, int n_b,
+                                   const void *C, int n_c, int64_t n_vox, const void *table, int n_items, int n_trip,
+                                   double scale, double *out, void *workspace, size_t workspace_bytes, void *stream) {
+    if (!A || !B || !C || !table || !out) return fail(PB_ERR_INVALID, "pb_triplet_contract: NULL argument");
+    if (n_vox < 1 || n_items < 1 || n_trip < 1) return fail(PB_ERR_INVALID, "pb_triplet_contract: empty contraction");
+    if (n_a < 1 || n_b < 1 || n_c < 1) return fail(PB_ERR_INVALID, "pb_triplet_contract: empty map set");
+    if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
+    const TripletItem *items = (const TripletItem *)table;
+    if (method == PB_TRIPLET_TC) {
+        if (precision != PB_F32) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction takes f32 maps");
+        return launch_triplet_tc(A, n_a, B, n_b, C, n_c, n_vox, items, n_items, n_trip, scale, out, workspace,
+                                 workspace_bytes, as_stream(stream));
+    }
+    if (method != PB_TRIPLET_SIMT) return fail(PB_ERR_INVALID, "bad method");
+    return launch_triplet_simt(precision, A, n_a, B, n_b, C, n_c, n_vox, items, n_items, n_trip, scale, out,
+                               workspace, workspace_bytes, as_stream(stream));
+}

@@ -1,0 +1,318 @@
+"""Power-spectrum estimators, backend='cuda' (mirrors PolyBin3D/pspec.py, global sightline).
+
+Numerators: one r2c, an optional weighting pass, and one k-bin x Legendre reduction
+for all multipoles at once (pb_bin_reduce).  Monte Carlo Fisher: GRF from the reference's
+own noise draw, the N_bins Q-maps batched through one filter launch and batched FFTs,
+and every Fisher row from one CROSS reduction (FP64 throughout).
+"""
+import numpy as np
+import torch
+
+from . import _native as nat
+
+
+class PSpec:
+    """Power spectrum estimators (pspec.py:10-26 for the inputs)."""
+
+    def __init__(self, base, k_bins, lmax=2, mask=None, applySinv=None, odd_l=False, add_GIC=False, mask_IC=None,
+                 add_RIC=False, radial_bins_RIC=[], mask_shot=None, applySinv_transpose=None, verb=True):
+        self.base = base
+        self.applySinv = applySinv
+        self.k_bins = np.asarray(k_bins)
+        self.lmax = lmax
+        self.Nk = len(k_bins) - 1
+        self.odd_l = odd_l
+        self.Nl = self.lmax + 1 if self.odd_l else self.lmax // 2 + 1
+        self.Nl_even = self.lmax // 2 + 1
+        self.N_bins = self.Nk * self.Nl
+        self.add_GIC = add_GIC
+        self.add_RIC = add_RIC
+        self.applySinv_transpose = applySinv_transpose
+
+        if verb:
+            print("")
+        # range checks (pspec.py:46-59)
+        assert np.max(self.k_bins) < np.min(base.kNy), "k_max must be less than k_Nyquist!"
+        assert np.min(self.k_bins) >= np.max(base.kF), "k_min must be at least the k_fundamental!"
+        assert np.max(self.k_bins) <= base.Pfid[0][-1], "Fiducial power spectrum should extend up to k_max!"
+        assert np.min(self.k_bins) >= base.Pfid[0][0], "Fiducial power spectrum should extend down to k_min!"
+        if verb:
+            print("Binning: %d bins in [%.3f, %.3f] h/Mpc" % (self.Nk, np.min(self.k_bins), np.max(self.k_bins)))
+            print("l-max: %d" % (self.lmax))
+        if self.odd_l:
+            assert self.lmax > 0, "lmax must be greater than 0 to use odd harmonics!"
+            assert self.base.sightline == 'local', "Odd spherical harmonics should only be used for local line-of-sight!"
+        assert type(self.lmax) == int, "l-max must be an integer!"
+        assert self.lmax <= 4, "Only l-max<=4 is currently supported!"
+        if not np.all(np.diff(self.k_bins) > 0):
+            raise ValueError("k_bins must be strictly increasing")
+
+        # mask (pspec.py:62-85)
+        if type(mask) == type(None):
+            self.const_mask = True
+            self.mask_mean = 1.
+            self.sq_mask_mean = 1.
+            assert not self.add_GIC, "Global integral constraint cannot be used without a mask!"
+            assert not self.add_RIC, "Radial integral constraint cannot be used without a mask!"
+        else:
+            if type(mask) != np.ndarray:
+                mask = np.array(mask.cpu() if isinstance(mask, torch.Tensor) else mask)
+            self.mask = mask.astype(np.float64)
+            if type(mask_IC) != type(None):
+                self.mask_IC = mask_IC.astype(np.float64)
+            if np.std(self.mask) < 1e-12:
+                self.const_mask = True
+                self.mask_mean = np.mean(self.mask)
+            else:
+                self.const_mask = False
+            self.sq_mask_mean = np.mean(self.mask ** 2)
+        if verb:
+            print("Mask: constant" if self.const_mask else "Mask: spatially varying")
+        if type(mask_shot) != type(None):
+            self.mask_shot = mask_shot.astype(np.float64)
+
+        if self.applySinv is not None:
+            raise NotImplementedError("backend='cuda' implements the trivial S^-1 weighting (applySinv=None)")
+        if self.add_GIC or self.add_RIC:
+            raise NotImplementedError("backend='cuda' does not implement integral constraints")
+        self.applySinv = self.base.applySinv_trivial
+        self.applySinv_transpose = self.base.applySinv_trivial
+        self.Ylm_real = None
+        self.Ylm_fourier = None
+
+    def get_ks(self):
+        """Central k of each bin (pspec.py:122-128)."""
+        return np.asarray([0.5 * (self.k_bins[b] + self.k_bins[b + 1]) for b in range(self.Nk)])
+
+    # ------------------------------------------------------------------------------
+    # helpers
+    # ------------------------------------------------------------------------------
+    def _ells(self, Nl):
+        return [(2 * li, 0) for li in range(Nl)]
+
+    def _data_device(self, data, dtype=None):
+        if not isinstance(data, torch.Tensor):
+            assert type(data[0, 0, 0]) in [np.float32, np.float64], "Data must be of type float32 or float64!"
+        else:
+            assert data.dtype in (torch.float32, torch.float64), "Data must be of type float32 or float64!"
+        return self.base.as_device(data, dtype)
+
+    def _weighted_spectrum(self, data, filtering, dtype=None):
+        """x(k) = rfftn(d) / W [* invP / sqrt(<m^2>)] on the device (pspec.py:617-640)."""
+        b = self.base
+        x = self._data_device(data, dtype)
+        xk = b.to_fourier(x)
+        prec = nat.precision_of(xk.dtype)
+        rd = torch.float64 if prec == nat.PB_F64 else torch.float32
+        if filtering == 'ideal':
+            unit = b._unit_pk and b.pixel_window == 'none'
+            if not unit:
+                w = b.to_device_grid('pk_ideal_w', lambda: self._ideal_weight(), rd)
+                nat.spectral_filter(b.grid, prec, xk, xk, [(0, -1.0, np.inf, 0, 0, 1.0, 1)], w=w)
+            scale = 1.0 / self.sq_mask_mean
+        else:
+            if b.pixel_window != 'none':
+                w = b.to_device_grid('window', lambda: b.pixel_window_grid, rd)
+                nat.spectral_filter(b.grid, prec, xk, xk, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
+            scale = 1.0
+        return xk, scale
+
+    def _ideal_weight(self):
+        b = self.base
+        w = b.invPk0_grid.copy()
+        if b.pixel_window != 'none':
+            W = b.pixel_window_grid
+            nz = W != 0
+            w[nz] = w[nz] / W[nz]
+            w[~nz] = 0.
+        return w
+
+    def _compute_pk_numerator(self, data, filtering='ideal'):
+        """Numerator, global sightline (pspec.py:613-686)."""
+        assert filtering in ['ideal', 'Sinv'], "Unknown filtering option supplied!"
+        b = self.base
+        xk, s2 = self._weighted_spectrum(data, filtering)
+        Nl = self.Nl if filtering == 'Sinv' else self.Nl_even
+        out = torch.empty(Nl * self.Nk, dtype=torch.float64, device=b.device)
+        scale = 0.5 * s2 * b.volume / float(b.gridsize.prod()) ** 2
+        nat.bin_reduce(b.grid, nat.precision_of(xk.dtype), nat.PB_RED_ABS2, xk, None, 1, self.k_bins,
+                       self._ells(Nl), scale, out, b.ws)
+        return out.cpu().numpy()
+
+    # ------------------------------------------------------------------------------
+    # unwindowed estimator
+    # ------------------------------------------------------------------------------
+    def Pk_numerator(self, data):
+        """Numerator of the unwindowed estimator, trivial S^-1 (pspec.py:131-139)."""
+        if not self.const_mask:
+            assert data.shape == self.mask.shape, "Data must have same shape as the mask!"
+        return self._compute_pk_numerator(data, filtering='Sinv')
+
+    def _mask_device(self):
+        return self.base.to_device_grid(('pk_mask', id(self)), lambda: self.mask, torch.float64)
+
+    def _fisher_from_fields(self, a):
+        """Fisher contributions of a batch of GRFs a (B, half) complex128 (pspec.py:264-456)."""
+        b = self.base
+        B = a.shape[0]
+        nh = b.nhalf
+        grid = b.grid
+        F64 = nat.PB_F64
+        invN = 1.0 / b.nreal
+        ainv_w = b.to_device_grid('ainv', b._ainv_weight, torch.float64)
+        Ainv = torch.empty_like(a)
+        nat.spectral_filter(grid, F64, a, Ainv, [(i, -1.0, np.inf, 0, 0, 1.0, 1) for i in range(B)], w=ainv_w,
+                            src_stride=nh)
+        if self.const_mask:
+            SinvP = a
+            qscale = self.mask_mean * self.mask_mean
+        else:
+            m = self._mask_device()
+            ar = a.clone()
+            nat.spectral_filter(grid, F64, ar, ar, [(i, -1.0, np.inf, 0, 0, invN, 0) for i in range(B)],
+                                src_stride=nh)
+            ar = b.fft_c2r(ar)
+            b.n_FFTs_reverse += B
+            nat.elementwise(nat.PB_EW_MUL, ar, m, out=ar, y_period=b.nreal)
+            SinvP = b.fft_r2c(ar)
+            b.n_FFTs_forward += B
+            qscale = 1.0
+        fish = torch.empty((B, self.N_bins, self.N_bins), dtype=torch.float64, device=b.device)
+        scaling = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
+        rows = [(li, ki) for li in range(self.Nl) for ki in range(self.Nk)]
+        for i in range(B):
+            Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+            maps = [(i, self.k_bins[ki], self.k_bins[ki + 1], 2 * li, 0, qscale if self.const_mask else invN, 0)
+                    for (li, ki) in rows]
+            nat.spectral_filter(grid, F64, SinvP, Q, maps, src_stride=nh)
+            if not self.const_mask:
+                qr = b.fft_c2r(Q)
+                b.n_FFTs_reverse += self.N_bins
+                nat.elementwise(nat.PB_EW_MUL, qr, m, out=qr, y_period=b.nreal)
+                Q = b.fft_r2c(qr, out=Q)
+                b.n_FFTs_forward += self.N_bins
+            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, self.k_bins, self._ells(self.Nl),
+                           scaling, fish[i], b.ws)
+        return fish
+
+    def compute_fisher_contribution(self, seed, verb=False):
+        """Fisher contribution of one GRF with the reference's noise for this seed (pspec.py:141-147)."""
+        b = self.base
+        re, im = b.reference_noise(seed + int(1e7))
+        a = b.grf_from_noise(torch.as_tensor(re, device=b.device)[None], torch.as_tensor(im, device=b.device)[None])
+        return self._fisher_from_fields(a)[0].cpu().numpy()
+
+    def compute_fisher(self, N_it, verb=False, *, batch=4):
+        """Mean Fisher over seeds 0..N_it-1 (pspec.py:553-569); `batch` GRFs per device pass."""
+        b = self.base
+        fish = torch.zeros((self.N_bins, self.N_bins), dtype=torch.float64, device=b.device)
+        for s0 in range(0, N_it, batch):
+            seeds = list(range(s0, min(N_it, s0 + batch)))
+            if s0 % 5 == 0 or verb:
+                print("Computing Fisher contribution %d of %d" % (s0 + 1, N_it))
+            noise = [b.reference_noise(s + int(1e7)) for s in seeds]
+            nre = torch.as_tensor(np.stack([n[0] for n in noise]), device=b.device)
+            nim = torch.as_tensor(np.stack([n[1] for n in noise]), device=b.device)
+            f = self._fisher_from_fields(b.grf_from_noise(nre, nim))
+            for i in range(len(seeds)):
+                fish += f[i] / N_it
+        fish = fish.cpu().numpy()
+        self.fish = fish
+        self.inv_fish = np.linalg.inv(fish)
+        return fish
+
+    def Pk_unwindowed(self, data, fish=[], shot_num=[], subtract_shotnoise=False):
+        """Unwindowed estimator (pspec.py:571-611)."""
+        if len(fish) != 0:
+            self.fish = fish
+            self.inv_fish = np.linalg.inv(fish)
+        if len(shot_num) != 0 or subtract_shotnoise:
+            self.shot_num = shot_num
+            self.shot = np.matmul(self.inv_fish, self.shot_num)
+        if not hasattr(self, 'inv_fish'):
+            raise Exception("Need to compute Fisher matrix first!")
+        if not hasattr(self, 'shot') and subtract_shotnoise:
+            raise Exception("Need to compute shot-noise first!")
+        Pk_num = self.Pk_numerator(data)
+        Pk_out = np.matmul(self.inv_fish, Pk_num)
+        if subtract_shotnoise:
+            Pk_out -= self.shot
+        Pk_dict = {}
+        index = 0
+        for l in range(0, self.lmax + 1, 2 - self.odd_l):
+            Pk_dict['p%s' % l] = Pk_out[index:index + self.Nk]
+            index += self.Nk
+        return Pk_dict
+
+    # ------------------------------------------------------------------------------
+    # ideal estimator
+    # ------------------------------------------------------------------------------
+    def Pk_numerator_ideal(self, data):
+        """Numerator of the ideal estimator (pspec.py:689-700)."""
+        if not self.const_mask:
+            assert data.shape == self.mask.shape, "Data must have same shape as the mask!"
+        return self._compute_pk_numerator(data, filtering='ideal')
+
+    def compute_fisher_ideal(self, discreteness_correction=True, Pk_fid='default'):
+        """Ideal Fisher matrix (pspec.py:702-752), FP64 reductions on the device."""
+        b = self.base
+        print("Computing ideal Fisher matrix")
+        fish = np.zeros((self.Nl_even * self.Nk, self.Nl_even * self.Nk))
+        if Pk_fid != 'default':
+            if (np.asarray(Pk_fid) == None).all() or (Pk_fid == 'none'):  # noqa: E711
+                k_tmp = np.arange(np.min(b.kF) / 10., np.max(b.kNy) * 2, np.min(b.kF) / 10.)
+                Pfid = np.asarray([k_tmp, 1. + 0. * k_tmp])
+            else:
+                assert len(Pk_fid) == 2, "Pk should contain k and P_0(k) columns"
+                Pfid = np.asarray(Pk_fid)
+            from scipy.interpolate import interp1d
+            Pk0 = interp1d(Pfid[0], Pfid[1], bounds_error=False, fill_value=0.)(b.modk_grid)
+            inv = np.zeros(b.modk_grid.shape)
+            good = (Pk0 != 0) & np.isfinite(Pk0)
+            inv[good] = 1. / Pk0[good]
+            w = torch.as_tensor(inv, device=b.device)
+        else:
+            w = None if b._unit_pk else b.to_device_grid('invPk0', lambda: b.invPk0_grid, torch.float64)
+        if discreteness_correction:
+            pairs = [(2 * la, 2 * lb) for la in range(self.Nl_even) for lb in range(self.Nl_even)]
+        else:
+            pairs = [(0, 0)]
+        out = torch.empty(len(pairs) * self.Nk, dtype=torch.float64, device=b.device)
+        nat.bin_reduce(b.grid, nat.PB_F64, nat.PB_RED_REAL2, w, None, 1, self.k_bins, pairs, 0.5, out, b.ws)
+        vals = out.cpu().numpy().reshape(len(pairs), self.Nk)
+        if discreteness_correction:
+            for e, (la2, lb2) in enumerate(pairs):
+                la, lb = la2 // 2, lb2 // 2
+                fish[la * self.Nk:(la + 1) * self.Nk, lb * self.Nk:(lb + 1) * self.Nk] = np.diag(vals[e])
+        else:
+            for la in range(self.Nl_even):
+                fish[la * self.Nk:(la + 1) * self.Nk, la * self.Nk:(la + 1) * self.Nk] = np.diag(vals[0]) / (4. * la + 1.)
+        self.fish_ideal = fish
+        self.inv_fish_ideal = np.linalg.inv(self.fish_ideal)
+        return fish
+
+    def Pk_ideal(self, data, fish_ideal=[], discreteness_correction=True):
+        """Ideal estimator (pspec.py:754-784)."""
+        if len(fish_ideal) != 0:
+            self.fish_ideal = fish_ideal
+            self.inv_fish_ideal = np.linalg.inv(fish_ideal)
+        if not hasattr(self, 'inv_fish_ideal'):
+            self.compute_fisher_ideal(discreteness_correction=discreteness_correction)
+        Pk_num_ideal = self.Pk_numerator_ideal(data)
+        Pk_out = np.matmul(self.inv_fish_ideal, Pk_num_ideal)
+        Pk_dict = {}
+        index = 0
+        for l in range(0, self.lmax + 1, 2):
+            Pk_dict['p%s' % l] = Pk_out[index:index + self.Nk]
+            index += self.Nk
+        return Pk_dict
+
+    def compute_shot_contribution(self, seed):
+        raise NotImplementedError("shot-noise Monte Carlo is not implemented in backend='cuda'")
+
+    def compute_covariance_contribution(self, seed, Pk_cov, verb=False):
+        raise NotImplementedError("covariance Monte Carlo is not implemented in backend='cuda'")
+
+    def compute_theory_contribution(self, seed, k_bins_theory, lmax_theory=None, include_wideangle=False,
+                                    verb=False):
+        raise NotImplementedError("theory matrices are not implemented in backend='cuda'")
