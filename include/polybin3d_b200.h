@@ -191,6 +191,23 @@ PB_API int pb_shell_rows(const pb_grid_t *g, int precision, const void *F, int n
                          const int32_t *out_row, int n_rows, double scale, double *out,
                          int64_t out_stride, void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---------------------------------------------------------------------------------- */
+/* pb_bin_reduce_noalloc: pb_bin_reduce for callers that cannot allocate device memory   */
+/* (a binding that only forwards the pointers it was given, or a process whose GPU       */
+/* memory belongs to another framework's pool).  No counterpart in the reference.        */
+/* Same arguments and results as pb_bin_reduce minus the workspace: the partial sums go  */
+/* to a fixed 2 MiB device array inside the library (PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES   */
+/* doubles, held on every GPU that loads the library until exit).  Fails with           */
+/* PB_ERR_INVALID when n_rows * nk * n_ell exceeds it.  The first call on a device looks */
+/* up the array's device address and should come before any stream capture.  All calls  */
+/* share the array: calls that overlap on the GPU race and must be serialised.           */
+/* ---------------------------------------------------------------------------------- */
+#define PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES 262144
+PB_API int pb_bin_reduce_noalloc(const pb_grid_t *g, int precision, int mode, const void *a,
+                                 const void *b, int n_rows, int64_t row_stride, const double *edges,
+                                 int nk, const int32_t *ells, int n_ell, double scale, double *out,
+                                 int accumulate, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -314,3 +314,114 @@ extern "C" int pb_shell_rows(const pb_grid_t *g, int precision, const void *F, i
     PB_LAUNCH_CHECK("pb_shell_rows(finalize)");
     return PB_OK;
 }
+
+// ------------------------------------------------------------------------------------
+// pb_bin_reduce_noalloc: the k-bin reduction with its scratch in a fixed device array.
+//
+// Some callers cannot hand this library a workspace: a binding that only forwards the
+// input and output pointers it was given and owns no device allocator, or a host program
+// whose GPU memory is entirely reserved by another framework's pool, where a cudaMalloc
+// (which may also synchronise the device) is not acceptable.  For them the per-block
+// partial sums live in the file-scope array below, PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES
+// doubles (2 MiB); every GPU that loads the library keeps it until the process exits.
+//
+// The array's host-side name is only a stand-in for the device symbol, so its device
+// address is looked up once per device with cudaGetSymbolAddress, with that device
+// current, on the first call made on that device; make that first call before any stream
+// capture.  All calls share the one array: calls whose kernels overlap on the GPU (other
+// streams, other host threads) race on it and must be serialised by the caller.  Each call
+// writes every partial it later reads, so nothing is carried over from the previous call.
+// ------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace pb {
+static __device__ __align__(256) double g_binred_scratch[PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES];
+
+static std::mutex g_binred_scratch_mu;
+static double *g_binred_scratch_dev[64];  // device address per device ordinal, looked up once
+
+static int binred_scratch_address(double **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_check(e, "pb_bin_reduce_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= 64) return fail(PB_ERR_UNSUPPORTED, "pb_bin_reduce_noalloc: device ordinal >= 64");
+    std::lock_guard<std::mutex> lock(g_binred_scratch_mu);
+    if (!g_binred_scratch_dev[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_binred_scratch);
+        if (e != cudaSuccess) return cuda_check(e, "pb_bin_reduce_noalloc: cudaGetSymbolAddress");
+        g_binred_scratch_dev[dev] = (double *)p;
+    }
+    *out = g_binred_scratch_dev[dev];
+    return PB_OK;
+}
+}  // namespace pb
+
+extern "C" int pb_bin_reduce_noalloc(const pb_grid_t *g, int precision, int mode, const void *a, const void *b,
+                                     int n_rows, int64_t row_stride, const double *edges, int nk,
+                                     const int32_t *ells, int n_ell, double scale, double *out, int accumulate,
+                                     void *stream) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (nk < 1 || nk > PB_RED_MAX_BINS) return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: nk must be in [1, 64]");
+    if (n_ell < 1 || n_ell > PB_RED_MAX_ELLS)
+        return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: n_ell must be in [1, 9]");
+    if (n_rows < 1 || n_rows > 65535)
+        return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: n_rows must be in [1, 65535]");
+    if (!edges || !ells || !out) return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: NULL argument");
+    if (mode == PB_RED_ABS2 && !a) return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: ABS2 needs a");
+    if (mode == PB_RED_CROSS && (!a || !b)) return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: CROSS needs a and b");
+    if (mode < 0 || mode > 2) return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: bad mode");
+    if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
+    // partial sums: one slot of n_ell*nk doubles per (row, block); shrink the block count
+    // to fit the fixed array, down to one block per row
+    const int64_t per_row_block = (int64_t)nk * n_ell;
+    const int64_t fit = PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES / ((int64_t)n_rows * per_row_block);
+    if (fit < 1)
+        return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: n_rows * nk * n_ell = " +
+                                        std::to_string((int64_t)n_rows * per_row_block) +
+                                        " doubles exceeds the fixed scratch of " +
+                                        std::to_string((int64_t)PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES) +
+                                        "; use pb_bin_reduce with a workspace");
+    if (row_stride == 0) row_stride = G.nhalf;
+    RedParams p;
+    for (int i = 0; i <= nk; ++i) {
+        p.edges[i] = edges[i];
+        if (i > 0 && !(edges[i] > edges[i - 1]))
+            return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: bin edges must be strictly increasing");
+    }
+    for (int e = 0; e < n_ell; ++e) {
+        if (ells[2 * e] < 0 || ells[2 * e] > 4 || ells[2 * e + 1] < 0 || ells[2 * e + 1] > 4)
+            return fail(PB_ERR_INVALID, "pb_bin_reduce_noalloc: Legendre order must be in [0, 4]");
+        p.la[e] = (int8_t)ells[2 * e];
+        p.lb[e] = (int8_t)ells[2 * e + 1];
+    }
+    p.nk = nk;
+    p.n_ell = n_ell;
+    double *partials = nullptr;
+    st = binred_scratch_address(&partials);
+    if (st) return st;
+    int nb = (int)std::min<int64_t>(red_blocks(G), fit);
+    dim3 grid(nb, n_rows);
+    cudaStream_t s = as_stream(stream);
+#define PB_RED_LAUNCH(T, M)                                                                        \
+    binred_kernel<T, M><<<grid, RED_THREADS, 0, s>>>(G, (const cplx<T>::type *)a, (const cplx<T>::type *)b, \
+                                                      (const T *)a, row_stride, p, partials)
+    if (precision == PB_F32) {
+        if (mode == PB_RED_ABS2) PB_RED_LAUNCH(float, PB_RED_ABS2);
+        else if (mode == PB_RED_CROSS) PB_RED_LAUNCH(float, PB_RED_CROSS);
+        else PB_RED_LAUNCH(float, PB_RED_REAL2);
+    } else {
+        if (mode == PB_RED_ABS2) PB_RED_LAUNCH(double, PB_RED_ABS2);
+        else if (mode == PB_RED_CROSS) PB_RED_LAUNCH(double, PB_RED_CROSS);
+        else PB_RED_LAUNCH(double, PB_RED_REAL2);
+    }
+#undef PB_RED_LAUNCH
+    PB_LAUNCH_CHECK("pb_bin_reduce_noalloc");
+    int per_row = nk * n_ell;
+    int total = per_row * n_rows;
+    binred_finalize<<<(total + 255) / 256, 256, 0, s>>>(partials, nb, per_row, n_rows, scale, out, accumulate);
+    PB_LAUNCH_CHECK("pb_bin_reduce_noalloc(finalize)");
+    return PB_OK;
+}
