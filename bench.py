@@ -37,7 +37,7 @@ WORKLOAD = "Bk_ideal 256^3 box 2000 Mpc/h, TSC, lmax=2, 16 linear bins 2pi/2000.
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--contraction", default="auto", choices=["auto", "tc", "simt"])
@@ -56,7 +56,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -287,7 +287,7 @@ def run_ours(args, rank, world, local):
         except Exception:
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
-        alg_bytes = bs.Nl * bs.Nk_squeeze * N ** 3 * 4  # every map read once
+        alg_bytes = bs.Nl * bs.Nk_squeeze * int(np.prod(bs.map_grid)) * 4  # every map read once
         achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
         traffic = None
         try:
@@ -300,6 +300,7 @@ def run_ours(args, rank, world, local):
                 "vs_baseline": None, "dtype": "f32 maps / fp64 sums",
                 "data": "synthetic (seeded float32 lognormal fields, pool of 4 per rank)",
                 "config": {"workload": WORKLOAD, "contraction": "tc" if method == nat.PB_TRIPLET_TC else "simt",
+                           "map_grid": list(bs.map_grid),
                            "l2": "inputs+intermediates 4.4 GB/step >> 126 MB L2", "parallelism": "replicas"},
                 "e2e": {"value": e2e, "unit": "fields/s", "h2d_bytes_per_step": N ** 3 * 4,
                         "d2h_bytes_per_step": bs.N_bins * 8},

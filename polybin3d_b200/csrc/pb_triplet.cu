@@ -69,20 +69,83 @@ int triplet_build_items(int n_a, int n_b, int n_c, const int32_t *idx, int n_tri
 
 // ------------------------------------------------------------------------------------
 // SIMT kernel
+//
+// Tiles of SIMT_TV voxels of every map are staged in shared memory with cp.async, double
+// buffered so the next tile's copy overlaps this tile's FMAs.  Per-thread sums stay in
+// the maps' precision for SIMT_FLUSH tiles and are then folded into this CTA's FP64
+// partial row in global memory (each slot has a single writer, so the order is fixed).
 // ------------------------------------------------------------------------------------
 constexpr int SIMT_THREADS = 256;
 constexpr int SIMT_TV = 128;       // voxels per tile
-constexpr int SIMT_PAD = 4;        // row padding (floats/doubles) against bank conflicts
+constexpr int SIMT_PAD = 4;        // row padding (elements) against bank conflicts
+constexpr int SIMT_FLUSH = 8;      // tiles between FP64 folds
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int valid_bytes) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
 template <typename T>
-__global__ void __launch_bounds__(SIMT_THREADS) triplet_simt_kernel(const T *A, int n_a, const T *B, int n_b,
-                                                                   int off_b, const T *C, int n_c, int off_c,
-                                                                   int n_rows, int64_t n_vox,
-                                                                   const TripletItem *items, int n_items,
-                                                                   int group_p, double *partials, int n_trip) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *tile = reinterpret_cast<T *>(smem_raw);
+__device__ __forceinline__ void simt_stage(T *buf, const T *A, int n_a, const T *B, int n_b, int off_b, const T *C,
+                                           int off_c, int n_rows, int64_t n_vox, int64_t v0, bool vec) {
     constexpr int LD = SIMT_TV + SIMT_PAD;
+    constexpr int EPV = 16 / sizeof(T);  // elements per 16-byte copy
+    if (vec) {
+        const int per_row = SIMT_TV / EPV;
+        for (int e = threadIdx.x; e < n_rows * per_row; e += SIMT_THREADS) {
+            int r = e / per_row, c = e - r * per_row;
+            const T *src;
+            int m;
+            if (r < n_a) { src = A; m = r; }
+            else if (off_b > 0 && r < off_b + n_b) { src = B; m = r - off_b; }
+            else { src = C; m = r - off_c; }
+            int64_t x = v0 + (int64_t)c * EPV;
+            int64_t left = n_vox - x;
+            int bytes = left >= EPV ? 16 : (left > 0 ? (int)left * (int)sizeof(T) : 0);
+            const T *g = src + (int64_t)m * n_vox + (bytes > 0 ? x : 0);
+            cp_async16(buf + r * LD + c * EPV, g, bytes);
+        }
+    } else {
+        for (int e = threadIdx.x; e < n_rows * SIMT_TV; e += SIMT_THREADS) {
+            int r = e / SIMT_TV, v = e - r * SIMT_TV;
+            const T *src;
+            int m;
+            if (r < n_a) { src = A; m = r; }
+            else if (off_b > 0 && r < off_b + n_b) { src = B; m = r - off_b; }
+            else { src = C; m = r - off_c; }
+            int64_t x = v0 + v;
+            bool ok = x < n_vox;
+            if (sizeof(T) == 4) {
+                cp_async4(buf + r * LD + v, src + (int64_t)m * n_vox + (ok ? x : 0), ok);
+            } else {
+                cp_async4(buf + r * LD + v, src + (int64_t)m * n_vox + (ok ? x : 0), ok);
+                cp_async4(reinterpret_cast<char *>(buf + r * LD + v) + 4,
+                          reinterpret_cast<const char *>(src + (int64_t)m * n_vox + (ok ? x : 0)) + 4, ok);
+            }
+        }
+    }
+    cp_async_commit();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SIMT_THREADS, sizeof(T) == 4 ? 3 : 1) triplet_simt_kernel(const T *A, int n_a, const T *B, int n_b,
+                                                                      int off_b, const T *C, int n_c, int off_c,
+                                                                      int n_rows, int64_t n_vox,
+                                                                      const TripletItem *items, int n_items,
+                                                                      int group_p, double *partials, int n_trip,
+                                                                      int vec) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LD = SIMT_TV + SIMT_PAD;
+    T *buf0 = reinterpret_cast<T *>(smem_raw);
+    T *buf1 = buf0 + n_rows * LD;
     const int slots = SIMT_THREADS / group_p;
     const int item_id = blockIdx.y * slots + threadIdx.x / group_p;
     const int p = threadIdx.x % group_p;
@@ -103,33 +166,37 @@ __global__ void __launch_bounds__(SIMT_THREADS) triplet_simt_kernel(const T *A, 
 #pragma unroll
         for (int j = 0; j < TRIP_TC; ++j) rc[j] = 0;
     }
-    double accd[TRIP_TB][TRIP_TC];
+    // output slot of (i, j) in this CTA's partial row, or -1 (read from the table when used)
+    const int32_t *outs = active ? &items[item_id].out[0][0] : nullptr;
+    double *dst = partials + (int64_t)blockIdx.x * n_trip;
+    // this CTA's slots start at zero (single writer per slot: the lane p == 0 of the item)
+    if (active && p == 0) {
+        for (int q = 0; q < TRIP_TB * TRIP_TC; ++q) {
+            int o = outs[q];
+            if (o >= 0 && o < n_trip) dst[o] = 0.0;
+        }
+    }
+    T acc[TRIP_TB][TRIP_TC];
 #pragma unroll
     for (int i = 0; i < TRIP_TB; ++i)
 #pragma unroll
-        for (int j = 0; j < TRIP_TC; ++j) accd[i][j] = 0.0;
+        for (int j = 0; j < TRIP_TC; ++j) acc[i][j] = (T)0;
 
     const int64_t n_tiles = (n_vox + SIMT_TV - 1) / SIMT_TV;
-    for (int64_t tt = blockIdx.x; tt < n_tiles; tt += gridDim.x) {
-        const int64_t v0 = tt * SIMT_TV;
-        // stage rows: [0,n_a) from A, then B (if distinct), then C (if distinct)
-        for (int e = threadIdx.x; e < n_rows * SIMT_TV; e += SIMT_THREADS) {
-            int r = e / SIMT_TV, v = e - r * SIMT_TV;
-            const T *src;
-            int m;
-            if (r < n_a) { src = A; m = r; }
-            else if (off_b > 0 && r < off_b + n_b) { src = B; m = r - off_b; }
-            else { src = C; m = r - off_c; }
-            int64_t x = v0 + v;
-            tile[r * LD + v] = (x < n_vox) ? src[(int64_t)m * n_vox + x] : (T)0;
+    int64_t tt = blockIdx.x;
+    if (tt < n_tiles) simt_stage<T>(buf0, A, n_a, B, n_b, off_b, C, off_c, n_rows, n_vox, tt * SIMT_TV, vec);
+    int cur = 0, since_flush = 0;
+    for (; tt < n_tiles; tt += gridDim.x) {
+        T *tile = cur ? buf1 : buf0;
+        const int64_t nxt = tt + gridDim.x;
+        if (nxt < n_tiles) {
+            simt_stage<T>(cur ? buf0 : buf1, A, n_a, B, n_b, off_b, C, off_c, n_rows, n_vox, nxt * SIMT_TV, vec);
+            cp_async_wait1();
+        } else {
+            cp_async_wait0();
         }
         __syncthreads();
         if (active) {
-            T acc[TRIP_TB][TRIP_TC];
-#pragma unroll
-            for (int i = 0; i < TRIP_TB; ++i)
-#pragma unroll
-                for (int j = 0; j < TRIP_TC; ++j) acc[i][j] = (T)0;
             for (int v = p; v < SIMT_TV; v += group_p) {
                 T av = tile[ra * LD + v];
                 T cv[TRIP_TC];
@@ -142,27 +209,25 @@ __global__ void __launch_bounds__(SIMT_THREADS) triplet_simt_kernel(const T *A, 
                     for (int j = 0; j < TRIP_TC; ++j) acc[i][j] = fma(pv, cv[j], acc[i][j]);
                 }
             }
+        }
+        __syncthreads();
+        cur ^= 1;
+        if (++since_flush == SIMT_FLUSH || tt + gridDim.x >= n_tiles) {
+            since_flush = 0;
+            // reduce over the group_p lanes of an item (consecutive lanes) and fold into FP64
 #pragma unroll
             for (int i = 0; i < TRIP_TB; ++i)
 #pragma unroll
-                for (int j = 0; j < TRIP_TC; ++j) accd[i][j] += (double)acc[i][j];
+                for (int j = 0; j < TRIP_TC; ++j) {
+                    double s = (double)acc[i][j];
+                    for (int o = group_p >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                    if (active && p == 0) {
+                        int o = outs[i * TRIP_TC + j];
+                        if (o >= 0 && o < n_trip) dst[o] += s;
+                    }
+                    acc[i][j] = (T)0;
+                }
         }
-        __syncthreads();
-    }
-    // reduce over the group_p lanes of an item (consecutive lanes, group_p <= 32)
-#pragma unroll
-    for (int i = 0; i < TRIP_TB; ++i)
-#pragma unroll
-        for (int j = 0; j < TRIP_TC; ++j)
-            for (int o = group_p >> 1; o > 0; o >>= 1) accd[i][j] += __shfl_xor_sync(0xffffffffu, accd[i][j], o);
-    if (active && p == 0) {
-        const TripletItem &it = items[item_id];
-        double *dst = partials + (int64_t)blockIdx.x * n_trip;
-#pragma unroll
-        for (int i = 0; i < TRIP_TB; ++i)
-#pragma unroll
-            for (int j = 0; j < TRIP_TC; ++j)
-                if (it.out[i][j] >= 0 && it.out[i][j] < n_trip) dst[it.out[i][j]] = accd[i][j];
     }
 }
 
@@ -183,7 +248,7 @@ int simt_geometry(int64_t n_vox, int n_items, int *grid_x, int *grid_y, int *gro
     *group_p = p;
     *grid_y = (n_items + slots - 1) / slots;
     int64_t n_tiles = (n_vox + SIMT_TV - 1) / SIMT_TV;
-    int64_t gx = std::min<int64_t>(n_tiles, (int64_t)num_sms() * 2);
+    int64_t gx = std::min<int64_t>(n_tiles, (int64_t)num_sms() * 3);
     *grid_x = (int)std::max<int64_t>(1, gx);
     return PB_OK;
 }
@@ -204,20 +269,24 @@ int launch_triplet_simt(int precision, const void *A, int n_a, const void *B, in
     else off_c = after_b;
     int n_rows = (off_c == after_b) ? after_b + n_c : after_b;
     size_t esz = precision == PB_F64 ? 8 : 4;
-    size_t smem = (size_t)n_rows * (SIMT_TV + SIMT_PAD) * esz;
+    size_t smem = 2 * (size_t)n_rows * (SIMT_TV + SIMT_PAD) * esz;
     if (smem > 227 * 1024) return fail(PB_ERR_UNSUPPORTED, "pb_triplet_contract: too many maps for one tile");
+    // 16-byte copies need every map row 16-byte aligned
+    size_t align_mask = 15;
+    int vec = ((n_vox * (int64_t)esz) % 16 == 0) && (((uintptr_t)A & align_mask) == 0) &&
+              (((uintptr_t)B & align_mask) == 0) && (((uintptr_t)C & align_mask) == 0);
     dim3 grid(gx, gy);
     double *partials = (double *)workspace;
     if (precision == PB_F32) {
         PB_CUDA(cudaFuncSetAttribute(triplet_simt_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         triplet_simt_kernel<float><<<grid, SIMT_THREADS, smem, s>>>(
             (const float *)A, n_a, (const float *)B, n_b, off_b, (const float *)C, n_c, off_c, n_rows, n_vox,
-            items_dev, n_items, gp, partials, n_trip);
+            items_dev, n_items, gp, partials, n_trip, vec);
     } else {
         PB_CUDA(cudaFuncSetAttribute(triplet_simt_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         triplet_simt_kernel<double><<<grid, SIMT_THREADS, smem, s>>>(
             (const double *)A, n_a, (const double *)B, n_b, off_b, (const double *)C, n_c, off_c, n_rows, n_vox,
-            items_dev, n_items, gp, partials, n_trip);
+            items_dev, n_items, gp, partials, n_trip, vec);
     }
     PB_LAUNCH_CHECK("pb_triplet_contract(simt)");
     triplet_finalize<<<(n_trip + 255) / 256, 256, 0, s>>>(partials, gx, n_trip, scale, out);
