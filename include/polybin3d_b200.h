@@ -122,25 +122,30 @@ PB_API int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const void
 /* A, B, C: n_a / n_b / n_c maps of n_vox voxels each (may alias).  Replaces assemble_b3 */
 /* and sum_triplet (PolyBin3D/cython/utils.pyx:614-636, 357-366; jax_utils.py:279-291).  */
 /*                                                                                       */
-/* pb_triplet_plan (host only) tiles the host int32 list idx of n_trip (i1,i2,i3) rows   */
-/* into a table of work items; call with table == NULL to get its size and item count,  */
-/* then copy the table to device memory once and pass it to pb_triplet_contract.        */
+/* pb_triplet_plan (host only) turns the host int32 list idx of n_trip (i1,i2,i3) rows   */
+/* into a table (work items of the CUDA-core form, the pair rows and the triplet ->      */
+/* (pair, i3) map of the tensor-core form) and its counts; call with table == NULL to    */
+/* get its size, then copy the table to device memory once and pass it with the counts  */
+/* to pb_triplet_contract.                                                              */
 /* method PB_TRIPLET_SIMT: CUDA-core FMA form in the maps' precision, per-tile sums      */
 /*   folded into FP64 registers.                                                         */
-/* method PB_TRIPLET_TC: f32 maps; tcgen05 tensor cores on split-fp16 products (3 MMAs   */
-/*   per tile), FP32 accumulation in TMEM folded into FP64 after every tile.             */
+/* method PB_TRIPLET_TC: f32 maps; tcgen05 tensor cores (sm_100a).  Pair products        */
+/*   A = A[i1]*B[i2] and the C maps are split into bf16 hi + lo; per 16 voxels two MMAs   */
+/*   (A_hi and A_lo against [C_hi | C_lo]) accumulate all four terms in FP32 in TMEM,    */
+/*   folded into FP64 every 16 tiles.  At most 512 pairs and 128 C maps.                 */
 /* Output FP64 on the device, deterministic for a given device.                          */
 /* ---------------------------------------------------------------------------------- */
 #define PB_TRIPLET_SIMT 0
 #define PB_TRIPLET_TC 1
+/* counts[4]: n_items (CUDA-core work items), n_pairs (distinct (i1,i2)), n_groups, n_trip */
 PB_API int pb_triplet_plan(int n_a, int n_b, int n_c, const int32_t *idx, int n_trip, void *table,
-                    size_t *table_bytes, int *n_items);
-PB_API int pb_triplet_workspace_size(int precision, int method, int64_t n_vox, int n_items, int n_trip,
-                              size_t *bytes);
+                           size_t *table_bytes, int32_t *counts);
+PB_API int pb_triplet_workspace_size(int precision, int method, int64_t n_vox, const int32_t *counts,
+                                     int n_c, size_t *bytes);
 PB_API int pb_triplet_contract(int precision, int method, const void *A, int n_a, const void *B, int n_b,
-                        const void *C, int n_c, int64_t n_vox, const void *table, int n_items,
-                        int n_trip, double scale, double *out, void *workspace,
-                        size_t workspace_bytes, void *stream);
+                               const void *C, int n_c, int64_t n_vox, const void *table,
+                               const int32_t *counts, double scale, double *out, void *workspace,
+                               size_t workspace_bytes, void *stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Real-space elementwise products.                                                      */

@@ -49,9 +49,9 @@ SIGNATURES = {
     "pb_bin_reduce_workspace_size": ([_GP, _I, _I, _I, ctypes.POINTER(_SZ)], _I),
     "pb_bin_reduce": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P, _SZ, _P], _I),
     "pb_bin_reduce_noalloc": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P], _I),
-    "pb_triplet_plan": ([_I, _I, _I, _P, _I, _P, ctypes.POINTER(_SZ), ctypes.POINTER(_I)], _I),
-    "pb_triplet_workspace_size": ([_I, _I, _I64, _I, _I, ctypes.POINTER(_SZ)], _I),
-    "pb_triplet_contract": ([_I, _I, _P, _I, _P, _I, _P, _I, _I64, _P, _I, _I, _D, _P, _P, _SZ, _P], _I),
+    "pb_triplet_plan": ([_I, _I, _I, _P, _I, _P, ctypes.POINTER(_SZ), _P], _I),
+    "pb_triplet_workspace_size": ([_I, _I, _I64, _P, _I, ctypes.POINTER(_SZ)], _I),
+    "pb_triplet_contract": ([_I, _I, _P, _I, _P, _I, _P, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
     "pb_elementwise": ([_I, _I, _I64, _P, _P, _I64, _P, _P, _D, _P, _P], _I),
     "pb_grf_from_noise": ([_GP, _I, _P, _P, _I, _P, _D, _P, _P], _I),
     "pb_pair_products": ([_I, _I64, _P, _P, _P, _P, _P, _I, _D, _P, _P], _I),
@@ -234,18 +234,19 @@ class TripletPlan:
         idx = np.ascontiguousarray(np.asarray(idx, dtype=np.int32).reshape(-1, 3))
         self.n_a, self.n_b, self.n_c, self.n_trip = n_a, n_b, n_c, len(idx)
         nbytes = ctypes.c_size_t()
-        nitems = ctypes.c_int()
+        self.counts = np.zeros(4, dtype=np.int32)
         check(lib.pb_triplet_plan(n_a, n_b, n_c, hptr(idx), len(idx), None, ctypes.byref(nbytes),
-                                  ctypes.byref(nitems)), "pb_triplet_plan")
+                                  hptr(self.counts)), "pb_triplet_plan")
         host = np.zeros(nbytes.value, dtype=np.uint8)
         check(lib.pb_triplet_plan(n_a, n_b, n_c, hptr(idx), len(idx), hptr(host), ctypes.byref(nbytes),
-                                  ctypes.byref(nitems)), "pb_triplet_plan")
-        self.n_items = nitems.value
+                                  hptr(self.counts)), "pb_triplet_plan")
+        self.host_table = host
+        self.n_items, self.n_pairs = int(self.counts[0]), int(self.counts[1])
         self.table = torch.from_numpy(host).to(device)
 
     def workspace_bytes(self, precision, method, n_vox):
         nbytes = ctypes.c_size_t()
-        check(load().pb_triplet_workspace_size(precision, method, n_vox, self.n_items, self.n_trip,
+        check(load().pb_triplet_workspace_size(precision, method, n_vox, hptr(self.counts), self.n_c,
                                                ctypes.byref(nbytes)), "pb_triplet_workspace_size")
         return nbytes.value
 
@@ -255,7 +256,7 @@ class TripletPlan:
         n_vox = A[0].numel()
         buf = ws.get(self.workspace_bytes(prec, method, n_vox), "triplet")
         check(load().pb_triplet_contract(prec, method, ptr(A), A.shape[0], ptr(B), B.shape[0], ptr(C), C.shape[0],
-                                         n_vox, ptr(self.table), self.n_items, self.n_trip, float(scale), ptr(out),
+                                         n_vox, ptr(self.table), hptr(self.counts), float(scale), ptr(out),
                                          ptr(buf), buf.numel(), stream_ptr()), "pb_triplet_contract")
         _count(2)
         return out
@@ -297,6 +298,7 @@ def tc_built():
     global _tc
     if _tc is None:
         nbytes = ctypes.c_size_t()
-        st = load().pb_triplet_workspace_size(PB_F32, PB_TRIPLET_TC, 1 << 20, 1, 1, ctypes.byref(nbytes))
+        counts = np.ones(4, dtype=np.int32)
+        st = load().pb_triplet_workspace_size(PB_F32, PB_TRIPLET_TC, 1 << 20, hptr(counts), 1, ctypes.byref(nbytes))
         _tc = (st == 0)
     return _tc

@@ -288,7 +288,18 @@ class BSpec:
         out = torch.empty(plan.n_trip, dtype=torch.float64, device=b.device)
         if tuple(A.shape[1:]) != tuple(int(n) for n in b.gridsize):
             scale = scale * float(np.prod(b.gridsize)) / float(np.prod(A.shape[1:]))
-        plan.contract(A, B, C, out, b.ws, method=self._method(A.dtype), scale=scale)
+        method = self._method(A.dtype)
+        if method == nat.PB_TRIPLET_TC and getattr(plan, "tc_unsupported", False):
+            method = nat.PB_TRIPLET_SIMT
+        try:
+            plan.contract(A, B, C, out, b.ws, method=method, scale=scale)
+        except NotImplementedError:
+            # the tensor-core tiling does not fit this shape (too many pair rows or maps
+            # for shared memory / TMEM): the CUDA-core kernel takes it
+            if method != nat.PB_TRIPLET_TC or self.contraction == 'tc':
+                raise
+            plan.tc_unsupported = True
+            plan.contract(A, B, C, out, b.ws, method=nat.PB_TRIPLET_SIMT, scale=scale)
         return out
 
     def _binned_maps(self, src, specs, w, dtype, coarse=True):

@@ -8,6 +8,7 @@
 // partials go to the caller's workspace and a second kernel sums them in a fixed order,
 // so results are deterministic.
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <string>
 #include <vector>
@@ -294,53 +295,111 @@ int launch_triplet_simt(int precision, const void *A, int n_a, const void *B, in
     return PB_OK;
 }
 
+static size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+TableLayout table_layout(const int32_t *counts) {
+    TableLayout L;
+    L.off_items = 0;
+    L.off_pairs = align16(L.off_items + (size_t)counts[0] * sizeof(TripletItem));
+    L.off_groups = align16(L.off_pairs + (size_t)counts[1] * 2 * sizeof(int32_t));
+    L.off_tmap = align16(L.off_groups + (size_t)counts[2] * sizeof(TcGroup));
+    L.bytes = align16(L.off_tmap + (size_t)counts[3] * 2 * sizeof(int32_t));
+    return L;
+}
+
 }  // namespace pb
 
 using namespace pb;
 
 extern "C" int pb_triplet_plan(int n_a, int n_b, int n_c, const int32_t *idx, int n_trip, void *table,
-                               size_t *table_bytes, int *n_items) {
+                               size_t *table_bytes, int32_t *counts) {
     std::vector<TripletItem> items;
     int st = triplet_build_items(n_a, n_b, n_c, idx, n_trip, items);
     if (st) return st;
-    size_t bytes = items.size() * sizeof(TripletItem);
-    if (n_items) *n_items = (int)items.size();
+    // pair rows (i1, i2) in lexicographic order, groups sharing i1, and triplet -> (row, col)
+    std::map<std::pair<int, int>, int> pair_row;
+    for (int t = 0; t < n_trip; ++t) pair_row[{idx[3 * t], idx[3 * t + 1]}] = 0;
+    std::vector<int32_t> pairs;
+    int r = 0;
+    for (auto &kv : pair_row) {
+        kv.second = r++;
+        pairs.push_back(kv.first.first);
+        pairs.push_back(kv.first.second);
+    }
+    std::vector<TcGroup> groups;
+    for (int row = 0; row < r;) {
+        TcGroup g;
+        g.a = pairs[2 * row];
+        g.row0 = row;
+        g.count = 0;
+        g.pad = 0;
+        while (row < r && g.count < TC_GROUP && pairs[2 * row] == g.a) {
+            ++g.count;
+            ++row;
+        }
+        groups.push_back(g);
+    }
+    std::vector<int32_t> tmap(2 * (size_t)n_trip);
+    for (int t = 0; t < n_trip; ++t) {
+        tmap[2 * t] = pair_row[{idx[3 * t], idx[3 * t + 1]}];
+        tmap[2 * t + 1] = idx[3 * t + 2];
+    }
+    int32_t c[4] = {(int32_t)items.size(), (int32_t)r, (int32_t)groups.size(), (int32_t)n_trip};
+    if (counts) memcpy(counts, c, sizeof(c));
+    TableLayout L = table_layout(c);
     if (!table) {
-        if (table_bytes) *table_bytes = bytes;
+        if (table_bytes) *table_bytes = L.bytes;
         return PB_OK;
     }
-    if (!table_bytes || *table_bytes < bytes) return fail(PB_ERR_INVALID, "pb_triplet_plan: table buffer too small");
-    memcpy(table, items.data(), bytes);
-    *table_bytes = bytes;
+    if (!table_bytes || *table_bytes < L.bytes) return fail(PB_ERR_INVALID, "pb_triplet_plan: table buffer too small");
+    unsigned char *T = (unsigned char *)table;
+    memset(T, 0, L.bytes);
+    memcpy(T + L.off_items, items.data(), items.size() * sizeof(TripletItem));
+    memcpy(T + L.off_pairs, pairs.data(), pairs.size() * sizeof(int32_t));
+    memcpy(T + L.off_groups, groups.data(), groups.size() * sizeof(TcGroup));
+    memcpy(T + L.off_tmap, tmap.data(), tmap.size() * sizeof(int32_t));
+    *table_bytes = L.bytes;
     return PB_OK;
 }
 
-extern "C" int pb_triplet_workspace_size(int precision, int method, int64_t n_vox, int n_items, int n_trip,
+static int check_counts(const int32_t *counts) {
+    if (!counts) return fail(PB_ERR_INVALID, "triplet counts are NULL");
+    if (counts[0] < 1 || counts[1] < 1 || counts[2] < 1 || counts[3] < 1)
+        return fail(PB_ERR_INVALID, "triplet plan is empty");
+    return PB_OK;
+}
+
+extern "C" int pb_triplet_workspace_size(int precision, int method, int64_t n_vox, const int32_t *counts, int n_c,
                                          size_t *bytes) {
     if (!bytes) return fail(PB_ERR_INVALID, "bytes is NULL");
-    if (n_vox < 1 || n_items < 1 || n_trip < 1) return fail(PB_ERR_INVALID, "pb_triplet_workspace_size: empty");
+    int st = check_counts(counts);
+    if (st) return st;
+    if (n_vox < 1) return fail(PB_ERR_INVALID, "pb_triplet_workspace_size: empty");
     if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
-    if (method == PB_TRIPLET_TC) return triplet_tc_workspace_size(n_vox, n_items, n_trip, bytes);
+    if (method == PB_TRIPLET_TC) return triplet_tc_workspace_size(n_vox, counts, n_c, bytes);
     int gx, gy, gp;
-    simt_geometry(n_vox, n_items, &gx, &gy, &gp);
-    *bytes = (size_t)gx * n_trip * sizeof(double);
+    simt_geometry(n_vox, counts[0], &gx, &gy, &gp);
+    *bytes = (size_t)gx * counts[3] * sizeof(double);
     return PB_OK;
 }
 
 extern "C" int pb_triplet_contract(int precision, int method, const void *A, int n_a, const void *B, int n_b,
-                                   const void *C, int n_c, int64_t n_vox, const void *table, int n_items, int n_trip,
+                                   const void *C, int n_c, int64_t n_vox, const void *table, const int32_t *counts,
                                    double scale, double *out, void *workspace, size_t workspace_bytes, void *stream) {
     if (!A || !B || !C || !table || !out) return fail(PB_ERR_INVALID, "pb_triplet_contract: NULL argument");
-    if (n_vox < 1 || n_items < 1 || n_trip < 1) return fail(PB_ERR_INVALID, "pb_triplet_contract: empty contraction");
+    int st = check_counts(counts);
+    if (st) return st;
+    if (n_vox < 1) return fail(PB_ERR_INVALID, "pb_triplet_contract: empty contraction");
     if (n_a < 1 || n_b < 1 || n_c < 1) return fail(PB_ERR_INVALID, "pb_triplet_contract: empty map set");
     if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
-    const TripletItem *items = (const TripletItem *)table;
+    const unsigned char *T = (const unsigned char *)table;
     if (method == PB_TRIPLET_TC) {
         if (precision != PB_F32) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction takes f32 maps");
-        return launch_triplet_tc(A, n_a, B, n_b, C, n_c, n_vox, items, n_items, n_trip, scale, out, workspace,
-                                 workspace_bytes, as_stream(stream));
+        return launch_triplet_tc(A, n_a, B, n_b, C, n_c, n_vox, T, counts, scale, out, workspace, workspace_bytes,
+                                 as_stream(stream));
     }
     if (method != PB_TRIPLET_SIMT) return fail(PB_ERR_INVALID, "bad method");
-    return launch_triplet_simt(precision, A, n_a, B, n_b, C, n_c, n_vox, items, n_items, n_trip, scale, out,
-                               workspace, workspace_bytes, as_stream(stream));
+    TableLayout L = table_layout(counts);
+    return launch_triplet_simt(precision, A, n_a, B, n_b, C, n_c, n_vox, (const TripletItem *)(T + L.off_items),
+                               counts[0], counts[3], scale, out, workspace, workspace_bytes, as_stream(stream));
 }

@@ -17,10 +17,26 @@ struct TripletItem {
     int32_t out[TRIP_TB][TRIP_TC];  // triplet index or -1
 };
 
+// Pair rows of the tensor-core form: the distinct (i1, i2) of the triplet list in
+// lexicographic order; groups of up to TC_GROUP consecutive pairs share i1.
+constexpr int TC_GROUP = 4;
+struct TcGroup {
+    int32_t a;      // map index of the shared first factor
+    int32_t row0;   // first pair row
+    int32_t count;  // pairs in the group (<= TC_GROUP)
+    int32_t pad;
+};
+
+// Device table: [items][pairs (i1,i2)][groups][tmap (row, col) per triplet], 16-byte aligned
+struct TableLayout {
+    size_t off_items, off_pairs, off_groups, off_tmap, bytes;
+};
+TableLayout table_layout(const int32_t *counts);  // counts = {n_items, n_pairs, n_groups, n_trip}
+
 int triplet_build_items(int n_a, int n_b, int n_c, const int32_t *idx, int n_trip, std::vector<TripletItem> &items);
-int triplet_tc_workspace_size(int64_t n_vox, int n_items, int n_trip, size_t *bytes);
+int triplet_tc_workspace_size(int64_t n_vox, const int32_t *counts, int n_c, size_t *bytes);
 int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void *C, int n_c, int64_t n_vox,
-                      const TripletItem *items, int n_items, int n_trip, double scale, double *out,
-                      void *workspace, size_t workspace_bytes, cudaStream_t s);
+                      const unsigned char *table, const int32_t *counts, double scale, double *out, void *workspace,
+                      size_t workspace_bytes, cudaStream_t s);
 
 }  // namespace pb

@@ -70,13 +70,15 @@ def test_triplet_plan_covers_each_triplet_once():
         idx = np.asarray(idx, dtype=np.int32)
         lib = nat.load()
         nb = ctypes.c_size_t()
-        ni = ctypes.c_int()
+        counts = np.zeros(4, dtype=np.int32)
         nat.check(lib.pb_triplet_plan(n_maps, n_maps, n_maps, nat.hptr(idx), n_trip, None, ctypes.byref(nb),
-                                      ctypes.byref(ni)))
+                                      nat.hptr(counts)))
         host = np.zeros(nb.value, dtype=np.uint8)
         nat.check(lib.pb_triplet_plan(n_maps, n_maps, n_maps, nat.hptr(idx), n_trip, nat.hptr(host),
-                                      ctypes.byref(nb), ctypes.byref(ni)))
-        rec = host.view(np.int32).reshape(ni.value, -1)   # a, b[4], c[8], out[4][8]
+                                      ctypes.byref(nb), nat.hptr(counts)))
+        n_items, n_pairs, n_groups = int(counts[0]), int(counts[1]), int(counts[2])
+        assert counts[3] == n_trip
+        rec = host[:n_items * 180].view(np.int32).reshape(n_items, -1)   # a, b[4], c[8], out[4][8]
         got = {}
         for r in rec:
             a, bs, cs, out = r[0], r[1:5], r[5:13], r[13:45].reshape(4, 8)
@@ -88,12 +90,30 @@ def test_triplet_plan_covers_each_triplet_once():
         assert len(got) == n_trip
         for t, v in got.items():
             assert tuple(idx[t]) == tuple(int(x) for x in v)
+        # tensor-core section: pairs sorted, groups cover every pair row, tmap consistent
+        a16 = lambda x: (x + 15) // 16 * 16
+        off_p = a16(n_items * 180)
+        off_g = a16(off_p + n_pairs * 8)
+        off_t = a16(off_g + n_groups * 16)
+        pairs = host[off_p:off_p + n_pairs * 8].view(np.int32).reshape(-1, 2)
+        assert [tuple(p) for p in pairs] == sorted({(int(a), int(b)) for a, b, _ in idx})
+        groups = host[off_g:off_g + n_groups * 16].view(np.int32).reshape(-1, 4)
+        covered = []
+        for a, row0, cnt, _ in groups:
+            assert 1 <= cnt <= 4
+            for r in range(row0, row0 + cnt):
+                assert pairs[r][0] == a
+                covered.append(r)
+        assert covered == list(range(n_pairs))
+        tmap = host[off_t:off_t + n_trip * 8].view(np.int32).reshape(-1, 2)
+        for t in range(n_trip):
+            assert tuple(pairs[tmap[t, 0]]) == (idx[t, 0], idx[t, 1]) and tmap[t, 1] == idx[t, 2]
 
 
 def test_triplet_plan_rejects_out_of_range():
     lib = nat.load()
     idx = np.array([[0, 1, 5]], dtype=np.int32)
     nb = ctypes.c_size_t()
-    ni = ctypes.c_int()
-    st = lib.pb_triplet_plan(4, 4, 4, nat.hptr(idx), 1, None, ctypes.byref(nb), ctypes.byref(ni))
+    counts = np.zeros(4, dtype=np.int32)
+    st = lib.pb_triplet_plan(4, 4, 4, nat.hptr(idx), 1, None, ctypes.byref(nb), nat.hptr(counts))
     assert st == -1 and b"out of range" in lib.pb_last_error()
