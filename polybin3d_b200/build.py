@@ -65,7 +65,7 @@ def build(verbose=False, force=False, extra=()):
             if r.returncode != 0:
                 raise RuntimeError("nvcc failed for " + cmd[-3])
     if force or jobs or _stale(LIB, objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcufft", "-lcuda"]
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcufft"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or r.returncode != 0:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)

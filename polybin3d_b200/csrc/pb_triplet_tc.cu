@@ -542,6 +542,25 @@ static int tc_geometry(int n_rows, int off_b, int off_c, const int32_t *counts, 
     return PB_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so the library has no
+// link-time dependency on the driver library (it loads on machines without a GPU)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+        looked = true;
+    }
+    return fn;
+}
+
 static int tc_grid(int64_t n_vox) {
     int64_t n_tiles = (n_vox + TC_KT - 1) / TC_KT;
     return (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, num_sms()));
@@ -581,6 +600,8 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
                   (((uintptr_t)C & 15) == 0) && n_a <= 256 && n_b <= 256 && n_c <= 256 && n_vox < (1LL << 31);
     CUtensorMap maps[3];
     memset(maps, 0, sizeof(maps));
+    EncodeTiledFn enc = use_tma ? encode_tiled() : nullptr;
+    if (!enc) use_tma = 0;
     if (use_tma) {
         const void *bases[3] = {A, B, C};
         const int rows[3] = {n_a, n_b, n_c};
@@ -589,7 +610,7 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
             cuuint64_t strides[1] = {(cuuint64_t)n_vox * 4};
             cuuint32_t box[2] = {(cuuint32_t)TC_KT, (cuuint32_t)rows[k]};
             cuuint32_t estr[2] = {1, 1};
-            CUresult r = cuTensorMapEncodeTiled(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(bases[k]),
+            CUresult r = enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(bases[k]),
                                                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
