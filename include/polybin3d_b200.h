@@ -79,18 +79,29 @@ PB_API int pb_fft_plan_destroy(pb_fft_plan *plan);
 /* src == NULL means a source of 1 + 0i (used for binning functions of a weight grid).   */
 /* w (real, same precision as the spectra) may be NULL (= 1); wpow in {-1,0,1,2}, where  */
 /* -1 divides (0 where w == 0).  l1, l2 in {0,...,4}.  src and w live on grid g; out may */
-/* live on a smaller grid out_n[3] (NULL = g): each output mode reads the source mode of */
-/* the same frequency, so band-limited maps can be synthesised on a coarser grid.        */
+/* live on another grid out_n[3] (NULL = g): each output mode reads the source mode of   */
+/* the same frequency (0 if the source grid lacks it), so band-limited maps can move     */
+/* between the data grid and a coarser map grid.  dst_idx (host, may be NULL = identity) */
+/* sends entry m to output dst_idx[m]; outputs may repeat, which requires accumulate.    */
 /* Replaces MapUtils.fourier_filter / fourier_filter_ll / prod_fourier / prod_fourier_  */
 /* filter / div_fourier (PolyBin3D/cython/utils.pyx:213-338) and jax_utils.py:97-100.    */
 /* ---------------------------------------------------------------------------------- */
 #define PB_FILTER_MAX_MAPS 128
 PB_API int pb_spectral_filter(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
-                              int64_t src_stride,
-                       void *out, int n_maps, const int32_t *src_idx, const double *lo,
-                       const double *hi, const int32_t *l1, const int32_t *l2,
-                       const double *scale, const int32_t *wpow, const void *w, int accumulate,
-                       void *stream);
+                              int64_t src_stride, void *out, int n_maps, const int32_t *src_idx,
+                              const int32_t *dst_idx, const double *lo, const double *hi,
+                              const int32_t *l1, const int32_t *l2, const double *scale,
+                              const int32_t *wpow, const void *w, int accumulate, void *stream);
+
+/* Binned-weight filter (the backward of the k-bin reduction):                           */
+/*   out(k) = scale * src(k) * w(k)^wpow * sum_e coef[e][b(k)] L_{ells[e]}(mu),           */
+/* b(k) the bin of |k| in `edges` (host, nk bins), 0 outside all bins; coef is a device  */
+/* FP64 array [n_ell][nk] (so it can be an autograd cotangent); wpow in [-2, 2] (negative */
+/* divides, 0 where w == 0).  The vector-Jacobian product of the power-spectrum         */
+/* numerator, whose rows are the Q-maps of PolyBin3D/pspec.py:443-456.                    */
+PB_API int pb_binned_filter(const pb_grid_t *g, int precision, const void *src, void *out,
+                            const double *edges, int nk, const int32_t *ells, int n_ell,
+                            const double *coef, const void *w, int wpow, double scale, void *stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* k-bin x Legendre reductions over the half spectrum, FP64 accumulation.                */
@@ -129,10 +140,11 @@ PB_API int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const void
 /* to pb_triplet_contract.                                                              */
 /* method PB_TRIPLET_SIMT: CUDA-core FMA form in the maps' precision, per-tile sums      */
 /*   folded into FP64 registers.                                                         */
-/* method PB_TRIPLET_TC: f32 maps; tcgen05 tensor cores (sm_100a).  Pair products        */
-/*   A = A[i1]*B[i2] and the C maps are split into bf16 hi + lo; per 16 voxels two MMAs   */
-/*   (A_hi and A_lo against [C_hi | C_lo]) accumulate all four terms in FP32 in TMEM,    */
-/*   folded into FP64 every 16 tiles.  At most 512 pairs and 128 C maps.                 */
+/* method PB_TRIPLET_TC: f32 maps; tcgen05 tensor cores (sm_100a).  The C maps (rows hi  */
+/*   and lo interleaved, MMA M = 2 n_c) and the pair products A[i1]*B[i2] (MMA N, up to   */
+/*   256 pairs per tile) are split into bf16 hi + lo; per 64 voxels two MMAs (C x P_hi,    */
+/*   C x P_lo) accumulate all four terms in FP32 in TMEM, folded into FP64 every 16 voxel */
+/*   tiles.  At most 1024 distinct pairs and 64 C maps (else PB_ERR_UNSUPPORTED).         */
 /* Output FP64 on the device, deterministic for a given device.                          */
 /* ---------------------------------------------------------------------------------- */
 #define PB_TRIPLET_SIMT 0

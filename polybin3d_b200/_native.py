@@ -45,7 +45,8 @@ SIGNATURES = {
     "pb_fft_plan_create": ([_GP, _I, _I, _I, ctypes.POINTER(_P), ctypes.POINTER(_SZ)], _I),
     "pb_fft_exec": ([_P, _P, _P, _P, _P], _I),
     "pb_fft_plan_destroy": ([_P], _I),
-    "pb_spectral_filter": ([_GP, _P, _I, _P, _I64, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P], _I),
+    "pb_spectral_filter": ([_GP, _P, _I, _P, _I64, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P], _I),
+    "pb_binned_filter": ([_GP, _I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _D, _P], _I),
     "pb_bin_reduce_workspace_size": ([_GP, _I, _I, _I, ctypes.POINTER(_SZ)], _I),
     "pb_bin_reduce": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P, _SZ, _P], _I),
     "pb_bin_reduce_noalloc": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P], _I),
@@ -164,9 +165,11 @@ class FFTPlan:
 # --------------------------------------------------------------------------------------
 # kernels
 # --------------------------------------------------------------------------------------
-def spectral_filter(grid, precision, src, out, maps, w=None, accumulate=False, src_stride=None, out_n=None):
+def spectral_filter(grid, precision, src, out, maps, w=None, accumulate=False, src_stride=None, out_n=None,
+                    dst=None):
     """maps: list of (src_idx, lo, hi, l1, l2, scale, wpow) -> writes out[m] (torch, complex);
-    out_n: output grid dims (a smaller grid of the same frequencies), None = the input grid."""
+    out_n: output grid dims (same frequencies on another grid), None = the input grid;
+    dst: output index per entry (outputs may repeat; needs accumulate)."""
     lib = load()
     on = None if out_n is None else np.ascontiguousarray(out_n, dtype=np.int32)
     n = len(maps)
@@ -182,11 +185,16 @@ def spectral_filter(grid, precision, src, out, maps, w=None, accumulate=False, s
         l2 = np.ascontiguousarray(arr[:, 4].astype(np.int32))
         sc = np.ascontiguousarray(arr[:, 5])
         wp = np.ascontiguousarray(arr[:, 6].astype(np.int32))
-        o = out[c0:c0 + len(chunk)]
+        if dst is None:
+            o = out[c0:c0 + len(chunk)]
+            di = None
+        else:
+            o = out
+            di = np.ascontiguousarray(np.asarray(dst[c0:c0 + len(chunk)], dtype=np.int32))
         stride = src_stride if src_stride is not None else (src[0].numel() if src is not None and src.dim() == 4 else 0)
         check(lib.pb_spectral_filter(ctypes.byref(grid), None if on is None else hptr(on), precision, ptr(src),
-                                     stride, ptr(o), len(chunk),
-                                     hptr(si), hptr(lo), hptr(hi), hptr(l1), hptr(l2), hptr(sc), hptr(wp),
+                                     stride, ptr(o), len(chunk), hptr(si), None if di is None else hptr(di),
+                                     hptr(lo), hptr(hi), hptr(l1), hptr(l2), hptr(sc), hptr(wp),
                                      ptr(w), int(bool(accumulate)), stream_ptr()), "pb_spectral_filter")
         _count(1)
 
@@ -302,3 +310,15 @@ def tc_built():
         st = load().pb_triplet_workspace_size(PB_F32, PB_TRIPLET_TC, 1 << 20, hptr(counts), 1, ctypes.byref(nbytes))
         _tc = (st == 0)
     return _tc
+
+
+def binned_filter(grid, src, out, edges, ells, coef, w=None, wpow=0, scale=1.0):
+    """out(k) = scale * src(k) * w^wpow * sum_e coef[e, bin(k)] L_ells[e](mu); coef device FP64 (n_ell, nk)."""
+    edges = np.ascontiguousarray(edges, dtype=np.float64)
+    ells = np.ascontiguousarray(np.asarray(ells, dtype=np.int32).reshape(-1))
+    coef = coef.to(torch.float64).contiguous()
+    check(load().pb_binned_filter(ctypes.byref(grid), precision_of(src.dtype), ptr(src), ptr(out), hptr(edges),
+                                  len(edges) - 1, hptr(ells), len(ells), ptr(coef), ptr(w), int(wpow), float(scale),
+                                  stream_ptr()), "pb_binned_filter")
+    _count(1)
+    return out

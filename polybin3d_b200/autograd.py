@@ -1,0 +1,177 @@
+"""Differentiable estimator numerators: the Q-maps of the Monte Carlo Fisher matrices are
+vector-Jacobian products of these functions.
+
+For the power spectrum (PolyBin3D/pspec.py:613-686, trivial S^-1, data = m * d)
+
+    num_{l b}(d) = 1/2 V/N^6 sum_k deg Theta_b L_{2l} |rfftn(m d) / W|^2
+    d num_{l b} / d d = V/N^3 * m * irfftn(Theta_b L_{2l} rfftn(m d) / W^2)
+
+so the reference's Q_{l b} = rfftn(m irfftn(Theta_b L_{2l} rfftn(m a)))  (pspec.py:443-456)
+is (N^3/V) rfftn(d num_{l b}/d d) at d = a.  The backward is one pass of the binned-weight
+filter kernel (pb_binned_filter) with the cotangent as per-bin weights, one c2r and one mask
+product.
+
+For the bispectrum (PolyBin3D/bspec.py:895-983, no linear term) the numerator is
+V/(N^3 sym_i) sum_x g_b1 g_b2 g_{l,b3} with g_{l,b} = irfftn(Theta_b L_l rfftn(m d) / W);
+its derivative is the sum over the three legs of irfftn(Theta_leg L_leg / W FT[product of the
+other two maps]) times m, the same construction as the reference's Q-maps (bspec.py:600-640).
+The backward recomputes the bin-filtered maps (nothing is stored by the forward), forms the
+pair products with pb_pair_products, transforms them, and gathers every leg into one
+spectrum with the accumulating spectral filter.  Maps, products and their transforms live
+on the dealiased map grid, which is exact for every frequency inside the bins.
+"""
+import numpy as np
+import torch
+
+from . import _native as nat
+
+
+def _mask_of(est):
+    if est.const_mask:
+        return None
+    return est._mask_device()
+
+
+class PkNumerator(torch.autograd.Function):
+    """num = PkNumerator.apply(d, pspec): the unwindowed numerator of data m*d as a
+    differentiable FP64 device tensor (N_bins,)."""
+
+    @staticmethod
+    def forward(ctx, d, ps):
+        b = ps.base
+        d = d.to(torch.float64).contiguous()
+        ctx.ps = ps
+        ctx.save_for_backward(d)
+        y = d
+        m = _mask_of(ps)
+        if m is not None:
+            y = nat.elementwise(nat.PB_EW_MUL, d, m)
+        xk = b.fft_r2c(y)
+        b.n_FFTs_forward += 1
+        if b.pixel_window != 'none':
+            w = b.to_device_grid('window', lambda: b.pixel_window_grid, torch.float64)
+            nat.spectral_filter(b.grid, nat.PB_F64, xk, xk, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
+        out = torch.empty(ps.N_bins, dtype=torch.float64, device=b.device)
+        nat.bin_reduce(b.grid, nat.PB_F64, nat.PB_RED_ABS2, xk, None, 1, ps.k_bins, ps._ells(ps.Nl),
+                       0.5 * b.volume / float(b.gridsize.prod()) ** 2, out, b.ws)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        ps = ctx.ps
+        b = ps.base
+        (d,) = ctx.saved_tensors
+        m = _mask_of(ps)
+        y = d if m is None else nat.elementwise(nat.PB_EW_MUL, d, m)
+        xk = b.fft_r2c(y)
+        b.n_FFTs_forward += 1
+        coef = g.to(torch.float64).reshape(ps.Nl, ps.Nk).contiguous()
+        w = None
+        if b.pixel_window != 'none':
+            w = b.to_device_grid('window', lambda: b.pixel_window_grid, torch.float64)
+        spec = torch.empty_like(xk)
+        nat.binned_filter(b.grid, xk, spec, ps.k_bins, [2 * li for li in range(ps.Nl)], coef, w=w,
+                          wpow=-2 if w is not None else 0, scale=b.volume / float(b.gridsize.prod()) ** 2)
+        grad = b.fft_c2r(spec)
+        b.n_FFTs_reverse += 1
+        if m is not None:
+            grad = nat.elementwise(nat.PB_EW_MUL, grad, m, out=grad)
+        return grad, None
+
+
+class BkNumerator(torch.autograd.Function):
+    """num = BkNumerator.apply(d, bspec): the unwindowed numerator (no linear term) of data
+    m*d as a differentiable FP64 device tensor (N_bins,)."""
+
+    @staticmethod
+    def _maps(bs, d):
+        b = bs.base
+        m = _mask_of(bs)
+        y = d if m is None else nat.elementwise(nat.PB_EW_MUL, d, m)
+        xk = b.fft_r2c(y)
+        b.n_FFTs_forward += 1
+        w = None
+        if b.pixel_window != 'none':
+            w = b.to_device_grid(('bk_invwin', id(bs)), lambda: bs._inv_window(), torch.float64)
+        return bs._g_maps(xk, w, 1.0)
+
+    @staticmethod
+    def forward(ctx, d, bs):
+        if not hasattr(bs, 'sym_factor'):
+            bs._compute_symmetry_factor()
+        d = d.to(torch.float64).contiguous()
+        ctx.bs = bs
+        ctx.save_for_backward(d)
+        G = BkNumerator._maps(bs, d)
+        B3 = bs._contract('b3', G, G, G, bs._triplet_index())
+        norm = torch.as_tensor(bs.base.volume / float(bs.base.gridsize.prod()) / bs.sym_factor, device=d.device)
+        return B3 * norm
+
+    @staticmethod
+    def backward(ctx, g):
+        bs = ctx.bs
+        b = bs.base
+        (d,) = ctx.saved_tensors
+        G = BkNumerator._maps(bs, d)  # recomputed, not stored
+        Mdims = tuple(int(n) for n in G.shape[1:])
+        nks = bs.Nk_squeeze
+        ks = bs.k_bins_squeeze
+        ab = bs.all_bins
+        gam = g.to(torch.float64).cpu().numpy()
+        N3 = float(b.gridsize.prod())
+        M3 = float(np.prod(Mdims))
+        # coefficient of triplet i: V / (sym_i N^3) * (N^3/M^3) [map-grid transform] / N^3 [c2r]
+        coef = gam * b.volume / (bs.sym_factor * N3 * M3)
+        legs = {}
+        keys = {}
+
+        def key_of(i, j):
+            return keys.setdefault((i, j), len(keys))
+
+        for t, (b1, b2, b3, l) in enumerate(ab.tolist()):
+            if coef[t] == 0.0:
+                continue
+            c3 = (l // 2) * nks + b3
+            for (kk, C, lc) in ((key_of(b2, c3), b1, 0), (key_of(b1, c3), b2, 0), (key_of(b1, b2), b3, l)):
+                legs[(kk, C, lc)] = legs.get((kk, C, lc), 0.0) + coef[t]
+        grad_spec = torch.zeros((1,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+        if keys:
+            pairs = sorted(keys, key=keys.get)
+            prods = nat.pair_products(G, G, pairs)
+            FT = b.fft_r2c(prods)
+            b.n_FFTs_forward += len(pairs)
+            entries = [(kk, ks[C], ks[C + 1], lc, 0, v, 0) for (kk, C, lc), v in legs.items()]
+            nat.spectral_filter(b.grid_of(Mdims), nat.PB_F64, FT, grad_spec, entries, accumulate=True,
+                                src_stride=FT[0].numel(), out_n=[int(n) for n in b.gridsize], dst=[0] * len(entries))
+        if b.pixel_window != 'none':
+            w = b.to_device_grid('window', lambda: b.pixel_window_grid, torch.float64)
+            nat.spectral_filter(b.grid, nat.PB_F64, grad_spec, grad_spec, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
+        grad = b.fft_c2r(grad_spec)[0]
+        b.n_FFTs_reverse += 1
+        m = _mask_of(bs)
+        if m is not None:
+            grad = nat.elementwise(nat.PB_EW_MUL, grad, m, out=grad)
+        return grad, None
+
+
+def pk_numerator(ps, d):
+    """Differentiable unwindowed power-spectrum numerator of data m*d (FP64 device tensor)."""
+    return PkNumerator.apply(d, ps)
+
+
+def bk_numerator(bs, d):
+    """Differentiable unwindowed bispectrum numerator (no linear term) of data m*d."""
+    return BkNumerator.apply(d, bs)
+
+
+def q_maps_pk(ps, d):
+    """All N_bins Q-maps (N^3/V) rfftn(d num_i/d d) at d, as rows of a complex128 tensor;
+    equal to the reference's Q_{l b} of pspec.py:443-456 when d is the GRF in real space."""
+    b = ps.base
+    d = d.to(torch.float64).contiguous().requires_grad_(True)
+    out = torch.empty((ps.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+    num = pk_numerator(ps, d)
+    for i in range(ps.N_bins):
+        (gi,) = torch.autograd.grad(num[i], d, retain_graph=i + 1 < ps.N_bins)
+        out[i] = b.fft_r2c(gi.contiguous()) * (float(b.gridsize.prod()) / b.volume)
+    return out

@@ -66,6 +66,7 @@ struct FilterParams {
     double hi[PB_FILTER_MAX_MAPS];
     double scale[PB_FILTER_MAX_MAPS];
     int32_t src[PB_FILTER_MAX_MAPS];
+    int16_t dst[PB_FILTER_MAX_MAPS];
     int8_t l1[PB_FILTER_MAX_MAPS];
     int8_t l2[PB_FILTER_MAX_MAPS];
     int8_t wpow[PB_FILTER_MAX_MAPS];
@@ -76,37 +77,45 @@ template <typename T>
 __global__ void __launch_bounds__(256) filter_kernel(Grid g, Grid go, const typename cplx<T>::type *src,
                                                      int64_t src_stride, typename cplx<T>::type *out, const T *w,
                                                      int acc, FilterParams p) {
-    // iterate over the modes of the output grid `go`; each maps to the source mode of the
-    // same frequency on `g` (identical when the grids agree)
+    // iterate over the modes of the output grid `go`; each reads the source mode of the
+    // same frequency on `g` (identical when the grids agree; a frequency the source grid
+    // does not hold reads 0)
     using C = typename cplx<T>::type;
     const bool same = (go.n0 == g.n0 && go.n1 == g.n1 && go.n2 == g.n2);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < go.nhalf; idx += stride) {
         Mode md = mode_of(go, idx);
         int64_t sidx = idx;
+        bool have = true;
         if (!same) {
             int l = (int)(idx % go.nh2);
             int64_t r = idx / go.nh2;
             int j = (int)(r % go.n1);
             int i = (int)(r / go.n1);
             int fi = freq_index(i, go.n0), fj = freq_index(j, go.n1);
+            have = (2 * fi >= -g.n0) && (2 * fi < g.n0) && (2 * fj >= -g.n1) && (2 * fj < g.n1) && (l < g.nh2);
             int si = fi < 0 ? fi + g.n0 : fi, sj = fj < 0 ? fj + g.n1 : fj;
-            sidx = ((int64_t)si * g.n1 + sj) * g.nh2 + l;
+            sidx = have ? ((int64_t)si * g.n1 + sj) * g.nh2 + l : 0;
         }
-        double wv = w ? (double)w[sidx] : 1.0;
+        double wv = (w && have) ? (double)w[sidx] : 1.0;
         int cached = -1;
         C s;
         s.x = 1;
         s.y = 0;
         for (int m = 0; m < p.n_maps; ++m) {
-            C *o = out + (int64_t)m * go.nhalf + idx;
+            C *o = out + (int64_t)p.dst[m] * go.nhalf + idx;
             bool in = (p.lo[m] <= md.k) && (md.k < p.hi[m]);
             if (!in) {
                 if (!acc) { C z; z.x = 0; z.y = 0; *o = z; }
                 continue;
             }
             if (src && p.src[m] != cached) {
-                s = src[(int64_t)p.src[m] * src_stride + sidx];
+                if (have) {
+                    s = src[(int64_t)p.src[m] * src_stride + sidx];
+                } else {
+                    s.x = 0;
+                    s.y = 0;
+                }
                 cached = p.src[m];
             }
             double f = p.scale[m] * legendre(p.l1[m], md.mu) * legendre(p.l2[m], md.mu);
@@ -123,6 +132,55 @@ __global__ void __launch_bounds__(256) filter_kernel(Grid g, Grid go, const type
             }
             *o = v;
         }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// binned-weight filter: out(k) = scale * src(k) * w(k)^wpow * sum_e coef[e][bin(k)] L_{ells[e]}(mu)
+// ------------------------------------------------------------------------------------
+struct BinWParams {
+    double edges[PB_RED_MAX_BINS + 1];
+    int8_t ell[PB_RED_MAX_ELLS];
+    int32_t nk, n_ell, wpow;
+    double scale;
+};
+
+template <typename T>
+__global__ void binned_filter_kernel(Grid g, const typename cplx<T>::type *src, typename cplx<T>::type *out,
+                                     const double *coef, const T *w, BinWParams p) {
+    using C = typename cplx<T>::type;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < g.nhalf; idx += stride) {
+        Mode md = mode_of(g, idx);
+        int b = -1;
+        if (p.edges[0] <= md.k && md.k < p.edges[p.nk]) {
+            int lo = 0, hi = p.nk;
+            while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                if (p.edges[mid] <= md.k) lo = mid;
+                else hi = mid;
+            }
+            b = lo;
+        }
+        C v;
+        v.x = 0;
+        v.y = 0;
+        if (b >= 0) {
+            double f = 0.0;
+            for (int e = 0; e < p.n_ell; ++e) f += coef[e * p.nk + b] * legendre(p.ell[e], md.mu);
+            f *= p.scale;
+            if (w) {
+                double wv = (double)w[idx];
+                if (p.wpow == 1) f *= wv;
+                else if (p.wpow == 2) f *= wv * wv;
+                else if (p.wpow == -1) f = wv != 0.0 ? f / wv : 0.0;
+                else if (p.wpow == -2) f = wv != 0.0 ? f / (wv * wv) : 0.0;
+            }
+            C s = src[idx];
+            v.x = (T)((double)s.x * f);
+            v.y = (T)((double)s.y * f);
+        }
+        out[idx] = v;
     }
 }
 
@@ -232,9 +290,9 @@ extern "C" int pb_fft_plan_destroy(pb_fft_plan *p) {
 
 extern "C" int pb_spectral_filter(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
                                   int64_t src_stride, void *out, int n_maps, const int32_t *src_idx,
-                                  const double *lo, const double *hi, const int32_t *l1, const int32_t *l2,
-                                  const double *scale, const int32_t *wpow, const void *w, int accumulate,
-                                  void *stream) {
+                                  const int32_t *dst_idx, const double *lo, const double *hi, const int32_t *l1,
+                                  const int32_t *l2, const double *scale, const int32_t *wpow, const void *w,
+                                  int accumulate, void *stream) {
     Grid G, GO;
     int st = make_grid(g, &G);
     if (st) return st;
@@ -244,8 +302,8 @@ extern "C" int pb_spectral_filter(const pb_grid_t *g, const int32_t *out_n, int 
         for (int i = 0; i < 3; ++i) go.n[i] = out_n[i];
         st = make_grid(&go, &GO);
         if (st) return st;
-        if (GO.n0 > G.n0 || GO.n1 > G.n1 || GO.n2 > G.n2)
-            return fail(PB_ERR_INVALID, "pb_spectral_filter: output grid larger than the input grid");
+        if (w && (GO.n0 > G.n0 || GO.n1 > G.n1 || GO.n2 > G.n2))
+            return fail(PB_ERR_INVALID, "pb_spectral_filter: a weight grid needs an output grid no larger than the input");
     }
     if (!out) return fail(PB_ERR_INVALID, "pb_spectral_filter: out is NULL");
     if (n_maps < 1 || n_maps > PB_FILTER_MAX_MAPS)
@@ -265,6 +323,11 @@ extern "C" int pb_spectral_filter(const pb_grid_t *g, const int32_t *out_n, int 
         p.scale[m] = scale[m];
         p.src[m] = src_idx ? src_idx[m] : 0;
         if (p.src[m] < 0) return fail(PB_ERR_INVALID, "pb_spectral_filter: negative source index");
+        int d = dst_idx ? dst_idx[m] : m;
+        if (d < 0 || d > 32767) return fail(PB_ERR_INVALID, "pb_spectral_filter: output index out of range");
+        if (dst_idx && !accumulate)
+            return fail(PB_ERR_INVALID, "pb_spectral_filter: an output index map needs accumulate (outputs may repeat)");
+        p.dst[m] = (int16_t)d;
         p.l1[m] = (int8_t)l1[m];
         p.l2[m] = (int8_t)l2[m];
         p.wpow[m] = (int8_t)wp;
@@ -438,5 +501,42 @@ extern "C" int pb_pair_products(int precision, int64_t n_vox, const void *X, con
                                                                         (double *)o, p);
         PB_LAUNCH_CHECK("pb_pair_products");
     }
+    return PB_OK;
+}
+
+extern "C" int pb_binned_filter(const pb_grid_t *g, int precision, const void *src, void *out, const double *edges,
+                                int nk, const int32_t *ells, int n_ell, const double *coef, const void *w, int wpow,
+                                double scale, void *stream) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (!src || !out || !edges || !ells || !coef) return fail(PB_ERR_INVALID, "pb_binned_filter: NULL argument");
+    if (nk < 1 || nk > PB_RED_MAX_BINS) return fail(PB_ERR_INVALID, "pb_binned_filter: nk must be in [1, 64]");
+    if (n_ell < 1 || n_ell > PB_RED_MAX_ELLS) return fail(PB_ERR_INVALID, "pb_binned_filter: n_ell must be in [1, 9]");
+    if (wpow < -2 || wpow > 2) return fail(PB_ERR_INVALID, "pb_binned_filter: wpow must be in [-2, 2]");
+    BinWParams p;
+    for (int i = 0; i <= nk; ++i) {
+        p.edges[i] = edges[i];
+        if (i > 0 && !(edges[i] > edges[i - 1])) return fail(PB_ERR_INVALID, "pb_binned_filter: edges must increase");
+    }
+    for (int e = 0; e < n_ell; ++e) {
+        if (ells[e] < 0 || ells[e] > 4) return fail(PB_ERR_INVALID, "pb_binned_filter: Legendre order must be in [0, 4]");
+        p.ell[e] = (int8_t)ells[e];
+    }
+    p.nk = nk;
+    p.n_ell = n_ell;
+    p.wpow = w ? wpow : 0;
+    p.scale = scale;
+    int threads = 256;
+    int blocks = grid_blocks(G.nhalf, threads);
+    if (precision == PB_F32)
+        binned_filter_kernel<float><<<blocks, threads, 0, as_stream(stream)>>>(G, (const float2 *)src, (float2 *)out,
+                                                                               coef, (const float *)w, p);
+    else if (precision == PB_F64)
+        binned_filter_kernel<double><<<blocks, threads, 0, as_stream(stream)>>>(G, (const double2 *)src,
+                                                                                (double2 *)out, coef, (const double *)w, p);
+    else
+        return fail(PB_ERR_INVALID, "bad precision");
+    PB_LAUNCH_CHECK("pb_binned_filter");
     return PB_OK;
 }
