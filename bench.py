@@ -34,15 +34,41 @@ METRIC = "Bk fields/s at 256^3 (16 bins, lmax=2, TSC, mixed precision)"
 WORKLOAD = "Bk_ideal 256^3 box 2000 Mpc/h, TSC, lmax=2, 16 linear bins 2pi/2000..0.2, 888 triangle bins"
 
 
+FISHER = {
+    # Pk_unwindowed + PSpec.compute_fisher: 128^3, box 1500, lmax=4, 20 bins to 0.25, shell-sector mask
+    "fisher_pk128": dict(N=128, L=1500.0, lmax=4, edges=np.linspace(2 * np.pi / 1500.0, 0.25, 21), batch=8,
+                         metric="Pk Fisher MC sims/s at 128^3 (60 bins, lmax=4, masked)",
+                         workload="PSpec.compute_fisher 128^3 box 1500 Mpc/h, lmax=4, 20 linear bins 2pi/1500..0.25, "
+                                  "shell-sector mask with 200 holes"),
+    # Bk_unwindowed + BSpec.compute_fisher: 128^3, box 1500, lmax=0, 12 bins to 0.2, same mask
+    "fisher_bk128": dict(N=128, L=1500.0, lmax=0, edges=np.linspace(2 * np.pi / 1500.0, 0.2, 13), batch=1,
+                         metric="Bk Fisher MC sims/s at 128^3 (203 bins, lmax=0, masked)",
+                         workload="BSpec.compute_fisher 128^3 box 1500 Mpc/h, lmax=0, 12 linear bins 2pi/1500..0.2, "
+                                  "shell-sector mask with 200 holes"),
+}
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=None)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="bk256", choices=["bk256"] + sorted(FISHER))
     p.add_argument("--contraction", default="auto", choices=["auto", "tc", "simt"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.steps is None:
+        a.steps = 50 if a.workload == "bk256" else 6
+    return a
+
+
+def fisher_mask(N, L):
+    """Shell 250 < r < 700 Mpc/h about the box centre, octant x,y,z > 0, 200 seeded holes of
+    radius 5-20 Mpc/h (float32)."""
+    from polybin3d_b200 import synthetic
+    return synthetic.shell_mask(N, L, r_in=250.0, r_out=700.0, n_holes=200, hole_r=(5.0, 20.0), hole_box=700.0,
+                                seed=0)
 
 
 class Clocks:
@@ -319,10 +345,176 @@ def run_ours(args, rank, world, local):
         torch.distributed.destroy_process_group()
 
 
+def fisher_alg_bytes(kind, N, n_bins):
+    """Compulsory HBM bytes of one FP64 Monte Carlo realisation, each kernel reading its
+    inputs and writing its outputs once and each 3D FFT counted as one read + one write
+    (N^3 voxels of 8 B, N^3/2 half modes of 16 B).
+    Pk, per Fisher row: Q spectrum write (8 N^3), c2r (8 + 8), mask product (24), r2c (8 + 8),
+    CROSS reduction read (8): 72 N^3.
+    Bk, per bin: three accumulating leg passes (3 x 16 N^3), the S^-1 P mask filter of its
+    Q (c2r 16, mask 24, r2c 16) and its rows' read (8): 112 N^3."""
+    per = 72 if kind == "pk" else 112
+    return float(per) * N ** 3 * n_bins
+
+
+def fisher_cpu_baseline(cfg, kind):
+    """The oracle port of the reference's Monte Carlo Fisher contribution (FP64, scipy FFTs
+    with all host threads) for one realisation on the reference's MT19937 noise."""
+    from oracle import polybin_oracle as O
+    nthreads = os.cpu_count()
+    N, L = cfg["N"], cfg["L"]
+    ref_utils = load_ref_utils()
+    ob = O.OracleBase([L] * 3, [N] * 3, nthreads=nthreads, kernels=ref_utils)
+    m = fisher_mask(N, L).astype(np.float64)
+    if kind == "pk":
+        est = O.OraclePSpec(ob, cfg["edges"], lmax=cfg["lmax"], mask=m)
+        est.fisher_contribution(ob.reference_noise(int(1e7)))  # warm-up
+        ts = []
+        for s in (1, 2):
+            t = time.perf_counter()
+            est.fisher_contribution(ob.reference_noise(s + int(1e7)))
+            ts.append(time.perf_counter() - t)
+        note = ("seeds 1, 2 after one warm-up, median, (the reference's MT19937 noise) through the "
+                "compute_fisher_contribution flow restated in the oracle")
+        return 1.0 / float(np.median(ts)), "reference" if ref_utils is not None else "port", nthreads, (
+            note + (", with the reference's compiled filter / integration kernels (oracle/_ref)" if ref_utils
+                    is not None else ", numpy kernels") + ", scipy FFT workers=%d" % nthreads)
+    else:
+        est = O.OracleBSpec(ob, cfg["edges"], lmax=cfg["lmax"], mask=m)
+        sym = est.symmetry_factor()  # cached once, as the reference caches it
+        t = time.perf_counter()
+        est.fisher_contribution(ob.reference_noise(int(1e7)), ob.reference_noise(int(2e7)), sym=sym)
+    dt = time.perf_counter() - t
+    note = ("one realisation (seed 0, the reference's MT19937 noise): the compute_fisher_contribution flow "
+            "restated in the oracle, %s, scipy FFT workers=%d; single timing"
+            % ("with the reference's compiled filter / integration kernels (oracle/_ref)" if ref_utils is not None
+               else "numpy kernels", nthreads))
+    return 1.0 / dt, "reference" if ref_utils is not None else "port", nthreads, note
+
+
+def run_fisher(args, rank, world, local):
+    import contextlib
+    import io
+
+    import torch
+    import polybin3d_b200 as pb
+    from polybin3d_b200 import _native as nat
+
+    cfg = FISHER[args.workload]
+    kind = "pk" if args.workload.startswith("fisher_pk") else "bk"
+    if args.impl == "reference":
+        if rank == 0:
+            v, k, cores, note = fisher_cpu_baseline(cfg, kind)
+            print(json.dumps({"metric": cfg["metric"], "value": v, "unit": "sims/s", "n_gpus": args.gpus,
+                              "steps": 1, "warmup": 0, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic (Gaussian random fields, shell-sector mask)",
+                              "config": {"workload": cfg["workload"]}, "impl": "reference",
+                              "cpu_baseline": {"value": v, "unit": "sims/s", "cores": cores, "kind": k,
+                                               "sample": note},
+                              "e2e": {"value": v, "unit": "sims/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    group = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    N, L, B = cfg["N"], cfg["L"], cfg["batch"]
+    with contextlib.redirect_stdout(io.StringIO()):
+        base = pb.PolyBin3D([L] * 3, [N] * 3, backend="cuda")
+        m = fisher_mask(N, L)
+        if kind == "pk":
+            est = pb.PSpec(base, cfg["edges"], lmax=cfg["lmax"], mask=m)
+        else:
+            est = pb.BSpec(base, cfg["edges"], lmax=cfg["lmax"], mask=m)
+
+    def fisher(n_it, noise):
+        with contextlib.redirect_stdout(io.StringIO()):
+            if kind == "pk":
+                return est.compute_fisher(n_it, batch=B, noise=noise)
+            return est.compute_fisher(n_it, noise=noise)
+
+    per_step = B * world  # realisations per step over all ranks
+    fisher(args.warmup * per_step, "philox")  # capture + warm-up replays
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = nat.LAUNCHES[0]
+    with Clocks(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fisher(args.steps * per_step, "philox")
+        e1.record()
+        torch.cuda.synchronize()
+    launches = nat.LAUNCHES[0] - l0
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = args.steps * per_step / (ms / 1000.0)
+
+    # end to end: the reference-identical path (MT19937 noise drawn on the host, copied in)
+    n_e2e = max(1, min(args.steps, 2)) * per_step
+    fisher(per_step, "reference")
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    fisher(n_e2e, "reference")
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = n_e2e / e2e_s
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        alg = fisher_alg_bytes(kind, N, est.N_bins)
+        achieved = alg / (ms / 1000.0 / (args.steps * B)) / 1e9
+        fields = 1 if kind == "pk" else 2
+        line = {"metric": cfg["metric"], "value": value, "unit": "sims/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (Gaussian random fields drawn on the device, shell-sector mask)",
+                "config": {"workload": cfg["workload"], "n_bins": est.N_bins, "realisations_per_step": per_step,
+                           "graph": "one captured CUDA graph per batch of %d" % B,
+                           "l2": "per-realisation working set > 3 GB >> 126 MB L2",
+                           "parallelism": "seeds round-robin over ranks" if world > 1 else "single GPU"},
+                "e2e": {"value": e2e, "unit": "sims/s",
+                        "h2d_bytes_per_step": per_step * fields * 2 * N ** 3 * 8,
+                        "d2h_bytes_per_step": est.N_bins ** 2 * 8,
+                        "path": "compute_fisher(noise='reference'): the reference's MT19937 draw on the host"},
+                "gpu_launches": launches,
+                "roofline": {"bound": "hbm", "kernel": "whole realisation (FFTs, filters, reductions)",
+                             "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                             "traffic": None, "alg_bytes_per_realisation": alg,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+                "clocks": clk.summary()}
+        if not args.no_cpu_baseline and world == 1:
+            v, k, cores, note = fisher_cpu_baseline(cfg, kind)
+            line["cpu_baseline"] = {"value": v, "unit": "sims/s", "cores": cores, "kind": k, "sample": note}
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args)
-    if args.impl == "reference":
+    if args.workload != "bk256":
+        run_fisher(args, rank, world, local)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_ours(args, rank, world, local)

@@ -182,6 +182,16 @@ PB_API int pb_grf_from_noise(const pb_grid_t *g, int precision, const double *no
                       const double *noise_im, int n_batch, const double *amp, double scale,
                       void *out, void *stream);
 
+/* The same field with the white noise drawn on the device: for field b with seed       */
+/* seeds[b] (device int64 array, so a captured graph can be replayed with new seeds) the */
+/* noise at full-grid voxel p is a Box-Muller pair (re, im) of the first two words of    */
+/* Philox4x32-10 (Salmon et al., SC'11) with key = seed and counter = (p, 0x5A17, 0).   */
+/* Deterministic per (seed, voxel), independent of the batch it is drawn in; it is NOT   */
+/* the reference's MT19937 stream (use pb_grf_from_noise for reference-identical noise). */
+#define PB_PHILOX_DOMAIN 0x5A17u
+PB_API int pb_grf_philox(const pb_grid_t *g, int precision, const int64_t *seeds, int n_batch,
+                         const double *amp, double scale, void *out, void *stream);
+
 /* ---------------------------------------------------------------------------------- */
 /* Batched pair products of real maps:                                                   */
 /*   out[p] = s * (X[i_p] * Y[j_p] - Z[i_p] * U[j_p])   (Z = U = NULL: s * X[i_p] Y[j_p]) */

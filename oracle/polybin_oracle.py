@@ -83,6 +83,24 @@ def pair_sum(A, B, idx, nthreads=None):
 # --------------------------------------------------------------------------------------
 # small helpers
 # --------------------------------------------------------------------------------------
+def philox4x32_10(c0, c1, c2, c3, k0, k1):
+    """Philox4x32-10 (Salmon et al., SC'11) on uint64 numpy arrays holding 32-bit words;
+    returns the four output words.  Pinned to the published known-answer vectors in the
+    CPU tests."""
+    m32 = np.uint64(0xFFFFFFFF)
+    M0, M1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
+    c = [np.asarray(v, dtype=np.uint64) & m32 for v in (c0, c1, c2, c3)]
+    k0, k1 = int(k0) & 0xFFFFFFFF, int(k1) & 0xFFFFFFFF
+    for _ in range(10):
+        p0 = M0 * c[0]
+        p1 = M1 * c[2]
+        c = [(p1 >> np.uint64(32)) ^ c[1] ^ np.uint64(k0), p1 & m32, (p0 >> np.uint64(32)) ^ c[3] ^ np.uint64(k1),
+             p0 & m32]
+        k0 = (k0 + 0x9E3779B9) & 0xFFFFFFFF
+        k1 = (k1 + 0xBB67AE85) & 0xFFFFFFFF
+    return c
+
+
 def legendre(l, mu):
     """Explicit Legendre polynomials, as utils.pyx:385-400."""
     if l == 0:
@@ -157,7 +175,11 @@ def pixel_window_1d(kind, x):
 class OracleBase:
     """Grids and FFTs of the reference base class, global sightline, real FFTs."""
 
-    def __init__(self, boxsize, gridsize, Pk=None, pixel_window="none", nthreads=None):
+    def __init__(self, boxsize, gridsize, Pk=None, pixel_window="none", nthreads=None, kernels=None):
+        """kernels: optionally the reference's compiled Cython module (oracle/_ref, built from
+        utils.pyx); its IntegrationUtils / MapUtils then run fourier_filter, cross_integrate,
+        integrate_row and prod_real_diff (same results, multithreaded): the CPU-baseline
+        timing mode.  Default: the numpy restatement."""
         self.boxsize = np.asarray(boxsize, dtype=np.float64)
         self.gridsize = np.asarray(gridsize, dtype=int)
         self.nthreads = nthreads or os.cpu_count()
@@ -193,6 +215,11 @@ class OracleBase:
         self.Pk0_grid[~np.isfinite(self.Pk0_grid)] = 0.0
         self.invPk0_grid[self.modk_grid == 0] = 1.0
         self.Pk0_grid[self.modk_grid == 0] = 1.0
+        self._iu = self._mu = None
+        if kernels is not None:                                         # base.py:138-144
+            self._iu = kernels.IntegrationUtils(self.modk_grid, True, self.nthreads, self.degeneracy_factor,
+                                                self.muk_grid)
+            self._mu = kernels.MapUtils(self.modk_grid, self.gridsize, self.nthreads, self.muk_grid)
 
     # FFTs, numpy normalisation (base.py:176-229)
     def to_fourier(self, x):
@@ -207,6 +234,8 @@ class OracleBase:
 
     def fourier_filter(self, kmap, l, kmin, kmax, l2=0):
         """Theta_b(k) L_l(mu) [L_l2(mu)] kmap  (fourier_filter / fourier_filter_ll, utils.pyx:283-320)."""
+        if self._mu is not None and l2 == 0:
+            return self._mu.fourier_filter(np.ascontiguousarray(kmap, dtype=np.complex128), l, kmin, kmax)
         out = np.zeros(self.modk_grid.shape, dtype=np.complex128)
         m = self.in_bin(kmin, kmax)
         leg = legendre(l, self.muk_grid[m]) * legendre(l2, self.muk_grid[m])
@@ -227,6 +256,9 @@ class OracleBase:
                            for b in range(len(k_edges) - 1)])
 
     def cross_integrate(self, s1, s2, k_edges, l):
+        if self._iu is not None:
+            return self._iu.cross_integrate(np.ascontiguousarray(s1), np.ascontiguousarray(s2),
+                                            np.ascontiguousarray(k_edges, dtype=np.float64), l)
         vals = self.degeneracy_factor * (s1 * np.conj(s2)).real * legendre(l, self.muk_grid)
         return np.asarray([vals[self.in_bin(k_edges[b], k_edges[b + 1])].sum()
                            for b in range(len(k_edges) - 1)])
@@ -238,9 +270,18 @@ class OracleBase:
 
     def integrate_row(self, input_map, input_array, kmin, kmax):
         """out[j] = sum_{k in [kmin,kmax)} deg Re(conj(map) * array[j])  (utils.pyx:162-179)."""
+        if self._iu is not None:
+            return self._iu.integrate_row(np.ascontiguousarray(input_map), np.ascontiguousarray(input_array),
+                                          kmin, kmax)
         m = self.in_bin(kmin, kmax)
         w = self.degeneracy_factor[m] * np.conj(input_map[m])
         return (input_array[:, m] * w[None, :]).real.sum(axis=1)
+
+    def prod_real_diff(self, a, b, c, d):
+        """a b - c d of real maps (prod_real_diff, utils.pyx:371-383)."""
+        if self._mu is not None:
+            return self._mu.prod_real_diff(a, b, c, d)
+        return a * b - c * d
 
     # Gaussian random field from supplied white noise (base.py:305-353)
     def grf_from_noise(self, noise_re, noise_im, Pk_grid=None, include_pixel_window=True):
@@ -263,6 +304,21 @@ class OracleBase:
         rs = np.random.RandomState(seed)
         re = rs.randn(*self.gridsize)
         im = rs.randn(*self.gridsize)
+        return re, im
+
+    def philox_noise(self, seed):
+        """White noise of the on-device Philox GRF (not a reference function: the CUDA
+        path's throughput mode draws its noise on the GPU).  Voxel p of the full grid:
+        Box-Muller on the first two words of Philox4x32-10(counter=(p, 0x5A17, 0),
+        key=seed)."""
+        p = np.arange(int(np.prod(self.gridsize)), dtype=np.uint64)
+        x = philox4x32_10(p & 0xFFFFFFFF, p >> np.uint64(32), np.full_like(p, 0x5A17), np.zeros_like(p),
+                          int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF)
+        u1 = (x[0].astype(np.float64) + 0.5) * 2.0 ** -32
+        u2 = (x[1].astype(np.float64) + 0.5) * 2.0 ** -32
+        rad = np.sqrt(-2.0 * np.log(u1))
+        re = (rad * np.cos(2 * np.pi * u2)).reshape(tuple(self.gridsize))
+        im = (rad * np.sin(2 * np.pi * u2)).reshape(tuple(self.gridsize))
         return re, im
 
     def applyAinv_fourier(self, a):
@@ -575,9 +631,9 @@ class OracleBSpec:
                 i3 = np.where((ab[:, 2] == B) & (ab[:, 0] == A))[0]
                 if len(i1) + len(i2) + len(i3) == 0:
                     continue
-                ft = [b.to_fourier(g1[A] * g1[B] - g2[A] * g2[B])]
+                ft = [b.to_fourier(b.prod_real_diff(g1[A], g1[B], g2[A], g2[B]))]
                 for l in range(2, self.lmax + 1, 2):
-                    ft.append(b.to_fourier(g1[A] * gl1[l // 2 - 1] - g2[A] * gl2[l // 2 - 1]))
+                    ft.append(b.to_fourier(b.prod_real_diff(g1[A], gl1[l // 2 - 1], g2[A], gl2[l // 2 - 1])))
                 for ii in i1:                                            # leg b3, L_l on it
                     C, l = ab[ii, 2], ab[ii, 3]
                     Q[ii] += b.fourier_filter(ft[0], l, ks[C], ks[C + 1])
@@ -604,9 +660,9 @@ class OracleBSpec:
                     continue
                 for l in range(0, self.lmax + 1, 2):
                     if l == 0:
-                        ft = b.to_fourier(g1[A] * g1[B] - g2[A] * g2[B])
+                        ft = b.to_fourier(b.prod_real_diff(g1[A], g1[B], g2[A], g2[B]))
                     else:
-                        ft = b.to_fourier(g1[A] * gl1[l // 2 - 1] - g2[A] * gl2[l // 2 - 1])
+                        ft = b.to_fourier(b.prod_real_diff(g1[A], gl1[l // 2 - 1], g2[A], gl2[l // 2 - 1]))
                     for ii in these[ab[these, 3] == l]:
                         s = ab[ii, 1]
                         fish[ii] = b.integrate_row(ft, Q, ks[s], ks[s + 1])

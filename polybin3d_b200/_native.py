@@ -55,6 +55,7 @@ SIGNATURES = {
     "pb_triplet_contract": ([_I, _I, _P, _I, _P, _I, _P, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
     "pb_elementwise": ([_I, _I, _I64, _P, _P, _I64, _P, _P, _D, _P, _P], _I),
     "pb_grf_from_noise": ([_GP, _I, _P, _P, _I, _P, _D, _P, _P], _I),
+    "pb_grf_philox": ([_GP, _I, _P, _I, _P, _D, _P, _P], _I),
     "pb_pair_products": ([_I, _I64, _P, _P, _P, _P, _P, _I, _D, _P, _P], _I),
     "pb_shell_rows_workspace_size": ([_I64, _I, _I, ctypes.POINTER(_SZ)], _I),
     "pb_shell_rows": ([_GP, _I, _P, _I, _P, _I, _P, _I64, _P, _P, _I, _D, _P, _I64, _P, _SZ, _P], _I),
@@ -221,6 +222,14 @@ def elementwise(op, x, y, z=None, u=None, s=1.0, out=None, y_period=0):
     out = torch.empty_like(x) if out is None else out
     check(lib.pb_elementwise(precision_of(x.dtype), op, x.numel(), ptr(x), ptr(y), int(y_period), ptr(z), ptr(u),
                              float(s), ptr(out), stream_ptr()), "pb_elementwise")
+    _count(1)
+    return out
+
+
+def grf_philox(grid, precision, seeds, amp, scale, out):
+    """Half-spectrum GRFs from on-device Philox noise; seeds: device int64 (n_batch,)."""
+    check(load().pb_grf_philox(ctypes.byref(grid), precision, ptr(seeds), seeds.numel(), ptr(amp), float(scale),
+                               ptr(out), stream_ptr()), "pb_grf_philox")
     _count(1)
     return out
 

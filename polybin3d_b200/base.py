@@ -347,6 +347,22 @@ class PolyBin3D:
                            float(self.gridsize.prod() / np.sqrt(self.volume)), out)
         return out
 
+    def grf_philox(self, seeds, out=None, include_pixel_window=True, dtype=torch.float64):
+        """Half-spectrum GRFs (n_seeds, half) from white noise drawn on the device
+        (Philox4x32-10 keyed by each seed): the distribution of generate_data (base.py:305-353),
+        not the reference's MT19937 stream.  `seeds`: host ints or a device int64 tensor
+        (a captured graph replays with whatever that tensor holds)."""
+        if not isinstance(seeds, torch.Tensor):
+            seeds = torch.as_tensor(np.asarray(seeds, dtype=np.int64), device=self.device)
+        amp = self.to_device_grid(('amp', include_pixel_window), lambda: self._grf_amp(None, include_pixel_window),
+                                  torch.float64)
+        cd = torch.complex128 if dtype == torch.float64 else torch.complex64
+        if out is None:
+            out = torch.empty((seeds.numel(),) + self.nhalf_shape, dtype=cd, device=self.device)
+        nat.grf_philox(self.grid, nat.precision_of(dtype), seeds, amp, float(self.gridsize.prod() / np.sqrt(self.volume)),
+                       out)
+        return out
+
     def reference_noise(self, seed):
         """White noise exactly as the reference draws it: np.random.seed(seed), then
         randn(*gridsize) for the real and the imaginary parts (base.py:315-316, 332)."""

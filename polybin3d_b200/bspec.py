@@ -12,6 +12,7 @@ import torch
 from scipy.interpolate import interp1d
 
 from . import _native as nat
+from . import realisations
 
 
 def real_harmonics(k_grids, l):
@@ -154,6 +155,7 @@ class BSpec:
         if not (isinstance(self.Pk_fid, str) and self.Pk_fid == 'default') and not self._unit_w:
             assert len(self.Pk_fid) == 2, "Pk should contain k and P_0(k) columns"
         self._plans = {}
+        self._captured = None
         self._shell_modes = None
         self.map_grid = self._dealiased_grid() if dealias else tuple(int(n) for n in base.gridsize)
         self.Ylm_real = None
@@ -602,7 +604,9 @@ class BSpec:
                 rr = rows[r0:r0 + 32]
                 rk = [spos[(int(ab[i, 0]), int(ab[i, 2]), int(ab[i, 3]))] for i in rr]
                 nat.shell_rows(b.grid, FTs, Q, modes, rk, rr, scale, fish, b.ws)
-        return fish.cpu().numpy() / np.outer(self.sym_factor, self.sym_factor)
+        sym = self.base.to_device_grid(('bk_sym2', id(self)), lambda: np.outer(self.sym_factor, self.sym_factor),
+                                       torch.float64)
+        return fish / sym
 
     def compute_fisher_contribution(self, seed, verb=False):
         """Fisher contribution of one GRF pair with the reference's noise draws (bspec.py:441-445)."""
@@ -613,15 +617,37 @@ class BSpec:
         r2 = b.reference_noise(seed + int(2e7))
         a1 = b.grf_from_noise(torch.as_tensor(r1[0], device=b.device), torch.as_tensor(r1[1], device=b.device))
         a2 = b.grf_from_noise(torch.as_tensor(r2[0], device=b.device), torch.as_tensor(r2[1], device=b.device))
-        return self._fisher_from_fields(a1, a2)
+        return self._fisher_from_fields(a1, a2).cpu().numpy()
 
-    def compute_fisher(self, N_it, verb=False):
-        """Mean Fisher over seeds 0..N_it-1 (bspec.py:678-693)."""
-        fish = np.zeros((self.N_bins, self.N_bins))
-        for seed in range(N_it):
-            if seed % 5 == 0:
-                print("Computing Fisher contribution %d of %d" % (seed + 1, N_it))
-            fish += self.compute_fisher_contribution(seed, verb=verb) / N_it
+    def compute_fisher(self, N_it, verb=False, *, group=None, noise='reference'):
+        """Mean Fisher over seeds 0..N_it-1 (bspec.py:678-693).  Under an initialised
+        torch.distributed process group (`group`, default the world) the seeds are shared
+        round-robin over the ranks; every rank returns the same matrix, summed in seed
+        order exactly as the one-process loop sums it.
+        noise='reference': the reference's own MT19937 draws per seed (identical inputs);
+        noise='philox': white noise drawn on the device (Philox, keyed by seed + 1e7 and
+        seed + 2e7) and each realisation replayed from one captured CUDA graph."""
+        assert noise in ('reference', 'philox'), "noise must be 'reference' or 'philox'"
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        b = self.base
+
+        def contrib(seeds):
+            if noise == 'philox':
+                if self._captured is None:
+                    self._captured = realisations.CapturedBatch(
+                        lambda sd: self._fisher_from_fields(b.grf_philox(sd + int(1e7)),
+                                                            b.grf_philox(sd + int(2e7)))[None], 1, b)
+                return torch.cat([self._captured.run([s]) for s in seeds])
+            return np.stack([self.compute_fisher_contribution(s, verb=verb) for s in seeds])
+
+        def progress(seeds):
+            for s in seeds:
+                if s % 5 == 0:
+                    print("Computing Fisher contribution %d of %d" % (s + 1, N_it))
+
+        fish = realisations.mc_mean(contrib, N_it, (self.N_bins, self.N_bins), self.base.device, group=group,
+                                    progress=progress).cpu().numpy()
         self.fish = fish
         self.inv_fish = np.linalg.inv(fish)
         return fish

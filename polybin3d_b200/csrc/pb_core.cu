@@ -422,6 +422,104 @@ __global__ void grf_kernel(Grid g, const double *nre, const double *nim, int n_b
     }
 }
 
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11): ten rounds of two 32x32->64 multiplies with the published multipliers, the key
+// bumped by the Weyl constants between rounds.
+struct Philox4 {
+    uint32_t x[4];
+};
+
+__device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                                 uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = M0 * c0, hi0 = __umulhi(M0, c0);
+        const uint32_t lo1 = M1 * c2, hi1 = __umulhi(M1, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0;
+        c1 = n1;
+        c2 = n2;
+        c3 = n3;
+        k0 += W0;
+        k1 += W1;
+    }
+    Philox4 o;
+    o.x[0] = c0;
+    o.x[1] = c1;
+    o.x[2] = c2;
+    o.x[3] = c3;
+    return o;
+}
+
+// (re, im) white noise at full-grid voxel p of the field with this seed: Box-Muller on
+// u1 = (x0 + 1/2) 2^-32, u2 = (x1 + 1/2) 2^-32 (both in (0, 1))
+__device__ __forceinline__ void philox_noise(int64_t seed, int64_t p, double &re, double &im) {
+    Philox4 r = philox4x32_10((uint32_t)p, (uint32_t)((uint64_t)p >> 32), PB_PHILOX_DOMAIN, 0u, (uint32_t)seed,
+                              (uint32_t)((uint64_t)seed >> 32));
+    const double u1 = ((double)r.x[0] + 0.5) * 2.3283064365386963e-10;
+    const double u2 = ((double)r.x[1] + 0.5) * 2.3283064365386963e-10;
+    const double rad = sqrt(-2.0 * log(u1));
+    double s, c;
+    sincospi(2.0 * u2, &s, &c);
+    re = rad * c;
+    im = rad * s;
+}
+
+template <typename T>
+__global__ void grf_philox_kernel(Grid g, const int64_t *seeds, int n_batch, const double *amp, double scale,
+                                  typename cplx<T>::type *out) {
+    using C = typename cplx<T>::type;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t total = g.nhalf * n_batch;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        int64_t bidx = t / g.nhalf;
+        int64_t idx = t - bidx * g.nhalf;
+        int l = (int)(idx % g.nh2);
+        int64_t r = idx / g.nh2;
+        int j = (int)(r % g.n1);
+        int i = (int)(r / g.n1);
+        int mi = (g.n0 - i) % g.n0, mj = (g.n1 - j) % g.n1, ml = (g.n2 - l) % g.n2;
+        int64_t p = ((int64_t)i * g.n1 + j) * g.n2 + l;
+        int64_t q = ((int64_t)mi * g.n1 + mj) * g.n2 + ml;
+        double ar = 0.0, ai = 0.0;
+        if (p != 0) {
+            const int64_t seed = seeds[bidx];
+            double pr, pi, qr, qi;
+            philox_noise(seed, p, pr, pi);
+            philox_noise(seed, q, qr, qi);
+            ar = 0.5 * (pr + qr);
+            ai = 0.5 * (pi - qi);
+        }
+        double a = amp[idx];
+        C v;
+        v.x = (T)(ar * a * scale);
+        v.y = (T)(ai * a * scale);
+        out[t] = v;
+    }
+}
+
+extern "C" int pb_grf_philox(const pb_grid_t *g, int precision, const int64_t *seeds, int n_batch, const double *amp,
+                             double scale, void *out, void *stream) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (!seeds || !amp || !out) return fail(PB_ERR_INVALID, "pb_grf_philox: NULL argument");
+    if (n_batch < 1) return fail(PB_ERR_INVALID, "pb_grf_philox: n_batch must be >= 1");
+    int threads = 256;
+    int blocks = grid_blocks(G.nhalf * n_batch, threads, 16);
+    if (precision == PB_F32)
+        grf_philox_kernel<float><<<blocks, threads, 0, as_stream(stream)>>>(G, seeds, n_batch, amp, scale,
+                                                                           (float2 *)out);
+    else if (precision == PB_F64)
+        grf_philox_kernel<double><<<blocks, threads, 0, as_stream(stream)>>>(G, seeds, n_batch, amp, scale,
+                                                                            (double2 *)out);
+    else
+        return fail(PB_ERR_INVALID, "bad precision");
+    PB_LAUNCH_CHECK("pb_grf_philox");
+    return PB_OK;
+}
+
 extern "C" int pb_grf_from_noise(const pb_grid_t *g, int precision, const double *noise_re, const double *noise_im,
                                  int n_batch, const double *amp, double scale, void *out, void *stream) {
     Grid G;

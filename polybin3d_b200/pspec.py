@@ -9,6 +9,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
+from . import realisations
 
 
 class PSpec:
@@ -79,6 +80,7 @@ class PSpec:
         self.applySinv_transpose = self.base.applySinv_trivial
         self.Ylm_real = None
         self.Ylm_fourier = None
+        self._captured = {}
 
     def get_ks(self):
         """Central k of each bin (pspec.py:122-128)."""
@@ -202,20 +204,37 @@ class PSpec:
         a = b.grf_from_noise(torch.as_tensor(re, device=b.device)[None], torch.as_tensor(im, device=b.device)[None])
         return self._fisher_from_fields(a)[0].cpu().numpy()
 
-    def compute_fisher(self, N_it, verb=False, *, batch=4):
-        """Mean Fisher over seeds 0..N_it-1 (pspec.py:553-569); `batch` GRFs per device pass."""
+    def compute_fisher(self, N_it, verb=False, *, batch=4, group=None, noise='reference'):
+        """Mean Fisher over seeds 0..N_it-1 (pspec.py:553-569); `batch` GRFs per device pass.
+        Under an initialised torch.distributed process group (`group`, default the world)
+        the seeds are shared round-robin over the ranks; every rank returns the same
+        matrix, summed in seed order exactly as the one-process loop sums it.
+        noise='reference': the reference's own MT19937 draw per seed (identical inputs);
+        noise='philox': white noise drawn on the device (Philox, keyed by seed + 1e7) and
+        each batch of realisations replayed from one captured CUDA graph."""
+        assert noise in ('reference', 'philox'), "noise must be 'reference' or 'philox'"
         b = self.base
-        fish = torch.zeros((self.N_bins, self.N_bins), dtype=torch.float64, device=b.device)
-        for s0 in range(0, N_it, batch):
-            seeds = list(range(s0, min(N_it, s0 + batch)))
-            if s0 % 5 == 0 or verb:
-                print("Computing Fisher contribution %d of %d" % (s0 + 1, N_it))
-            noise = [b.reference_noise(s + int(1e7)) for s in seeds]
-            nre = torch.as_tensor(np.stack([n[0] for n in noise]), device=b.device)
-            nim = torch.as_tensor(np.stack([n[1] for n in noise]), device=b.device)
-            f = self._fisher_from_fields(b.grf_from_noise(nre, nim))
-            for i in range(len(seeds)):
-                fish += f[i] / N_it
+
+        def contrib(seeds):
+            if noise == 'philox':
+                cap = self._captured.get(batch)
+                if cap is None:
+                    cap = realisations.CapturedBatch(
+                        lambda sd: self._fisher_from_fields(b.grf_philox(sd + int(1e7))), batch, b)
+                    self._captured[batch] = cap
+                return cap.run(seeds)
+            noise_ = [b.reference_noise(s + int(1e7)) for s in seeds]
+            nre = torch.as_tensor(np.stack([n[0] for n in noise_]), device=b.device)
+            nim = torch.as_tensor(np.stack([n[1] for n in noise_]), device=b.device)
+            return self._fisher_from_fields(b.grf_from_noise(nre, nim))
+
+        def progress(seeds):
+            for s in seeds:
+                if s % 5 == 0 or verb:
+                    print("Computing Fisher contribution %d of %d" % (s + 1, N_it))
+
+        fish = realisations.mc_mean(contrib, N_it, (self.N_bins, self.N_bins), b.device, batch=batch, group=group,
+                                    progress=progress)
         fish = fish.cpu().numpy()
         self.fish = fish
         self.inv_fish = np.linalg.inv(fish)

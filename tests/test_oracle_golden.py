@@ -143,3 +143,23 @@ def test_bk_fisher_nomask_lmax2():
     assert rel(bs.symmetry_factor(), g["sym"]) < TOL
     f = bs.fisher_contribution(b.reference_noise(3 + 10 ** 7), b.reference_noise(3 + 2 * 10 ** 7))
     assert rel(f, g["f3"]) < TOL
+
+
+def test_philox_known_answers():
+    """Philox4x32-10 known-answer vectors of the Random123 distribution (kat_vectors)."""
+    cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+             ((0xffffffff,) * 4, (0xffffffff,) * 2, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+             ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+              (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for c, k, want in cases:
+        got = O.philox4x32_10(*[np.array([v], dtype=np.uint64) for v in c], *k)
+        assert [int(g[0]) for g in got] == list(want)
+
+
+def test_philox_noise_is_gaussian():
+    b = O.OracleBase([500.0] * 3, [32] * 3)
+    re, im = b.philox_noise(12345)
+    x = np.concatenate([re.ravel(), im.ravel()])
+    assert abs(x.mean()) < 5e-3 and abs(x.std() - 1) < 5e-3
+    re2, _ = b.philox_noise(12346)
+    assert abs(np.corrcoef(re.ravel(), re2.ravel())[0, 1]) < 5e-3
