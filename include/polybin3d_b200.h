@@ -93,6 +93,28 @@ PB_API int pb_spectral_filter(const pb_grid_t *g, const int32_t *out_n, int prec
                               const int32_t *l1, const int32_t *l2, const double *scale,
                               const int32_t *wpow, const void *w, int accumulate, void *stream);
 
+/* ---------------------------------------------------------------------------------- */
+/* Band-limited map synthesis: pb_spectral_filter onto the output grid out_n followed by */
+/* the unnormalised C2R transform of every output spectrum, in one call:                 */
+/*   out[m](x) = sum_k F_m(k) e^{+2 pi i k.x / M},  F_m as in pb_spectral_filter          */
+/* Replaces fourier_filter + to_real per bin (utils.pyx:283-320, base.py:199-229; the    */
+/* g-maps of bspec.py:936-956).  F_m vanishes outside |k| < hi_m, so only those planes,  */
+/* columns and rows are transformed (pruned Stockham transforms in shared memory; two    */
+/* real output lines share one complex transform along z).  out: real [n_maps][M0][M1][M2] */
+/* in `precision`; src == NULL stands for a unit spectrum (the binning functions).       */
+/* At most 64 maps per call.  PB_ERR_UNSUPPORTED (use the filter + FFT                  */
+/* pair) when a band reaches a grid's Nyquist frequency, an upper edge is infinite, or an */
+/* output length has a prime factor other than 2, 3, 5.  Workspace from                 */
+/* pb_shell_synth_workspace_size (same grids, precision and upper edges).                */
+/* ---------------------------------------------------------------------------------- */
+PB_API int pb_shell_synth_workspace_size(const pb_grid_t *g, const int32_t *out_n, int precision, int n_maps,
+                                         const double *hi, size_t *bytes);
+PB_API int pb_shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
+                          int64_t src_stride, int n_maps, const int32_t *src_idx, const double *lo,
+                          const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
+                          const int32_t *wpow, const void *w, void *out, void *workspace,
+                          size_t workspace_bytes, void *stream);
+
 /* Binned-weight filter (the backward of the k-bin reduction):                           */
 /*   out(k) = scale * src(k) * w(k)^wpow * sum_e coef[e][b(k)] L_{ells[e]}(mu),           */
 /* b(k) the bin of |k| in `edges` (host, nk bins), 0 outside all bins; coef is a device  */

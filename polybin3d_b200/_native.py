@@ -20,6 +20,7 @@ PB_RED_ABS2, PB_RED_CROSS, PB_RED_REAL2 = 0, 1, 2
 PB_TRIPLET_SIMT, PB_TRIPLET_TC = 0, 1
 PB_EW_MUL, PB_EW_PRODDIFF = 0, 1
 FILTER_MAX_MAPS = 128
+SYNTH_MAX_MAPS = 64
 
 _ERRORS = {-1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: MemoryError, -5: NotImplementedError,
            -6: TimeoutError}
@@ -47,6 +48,8 @@ SIGNATURES = {
     "pb_fft_plan_destroy": ([_P], _I),
     "pb_spectral_filter": ([_GP, _P, _I, _P, _I64, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P], _I),
     "pb_binned_filter": ([_GP, _I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _D, _P], _I),
+    "pb_shell_synth_workspace_size": ([_GP, _P, _I, _I, _P, ctypes.POINTER(_SZ)], _I),
+    "pb_shell_synth": ([_GP, _P, _I, _P, _I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P], _I),
     "pb_bin_reduce_workspace_size": ([_GP, _I, _I, _I, ctypes.POINTER(_SZ)], _I),
     "pb_bin_reduce": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P, _SZ, _P], _I),
     "pb_bin_reduce_noalloc": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P], _I),
@@ -330,4 +333,32 @@ def binned_filter(grid, src, out, edges, ells, coef, w=None, wpow=0, scale=1.0):
                                   len(edges) - 1, hptr(ells), len(ells), ptr(coef), ptr(w), int(wpow), float(scale),
                                   stream_ptr()), "pb_binned_filter")
     _count(1)
+    return out
+
+
+def shell_synth(grid, precision, src, out, maps, out_n, ws, w=None, src_stride=None):
+    """Real maps out[m] = unnormalised c2r on grid out_n of the filter `maps` (entries
+    (src_idx, lo, hi, l1, l2, scale, wpow) as spectral_filter) in one pruned pass per chunk
+    of 64 maps.  Raises NotImplementedError when the band limits do not allow it."""
+    lib = load()
+    on = np.ascontiguousarray(out_n, dtype=np.int32)
+    stride = src_stride if src_stride is not None else (src[0].numel() if src is not None and src.dim() == 4 else 0)
+    for c0 in range(0, len(maps), SYNTH_MAX_MAPS):
+        chunk = maps[c0:c0 + SYNTH_MAX_MAPS]
+        arr = np.asarray(chunk, dtype=np.float64)
+        si = np.ascontiguousarray(arr[:, 0].astype(np.int32))
+        lo = np.ascontiguousarray(arr[:, 1])
+        hi = np.ascontiguousarray(arr[:, 2])
+        l1 = np.ascontiguousarray(arr[:, 3].astype(np.int32))
+        l2 = np.ascontiguousarray(arr[:, 4].astype(np.int32))
+        sc = np.ascontiguousarray(arr[:, 5])
+        wp = np.ascontiguousarray(arr[:, 6].astype(np.int32))
+        nbytes = ctypes.c_size_t()
+        check(lib.pb_shell_synth_workspace_size(ctypes.byref(grid), hptr(on), precision, len(chunk), hptr(hi),
+                                                ctypes.byref(nbytes)), "pb_shell_synth_workspace_size")
+        buf = ws.get(nbytes.value, "synth")
+        check(lib.pb_shell_synth(ctypes.byref(grid), hptr(on), precision, ptr(src), stride, len(chunk), hptr(si),
+                                 hptr(lo), hptr(hi), hptr(l1), hptr(l2), hptr(sc), hptr(wp), ptr(w),
+                                 ptr(out[c0:c0 + len(chunk)]), ptr(buf), buf.numel(), stream_ptr()), "pb_shell_synth")
+        _count(3)
     return out

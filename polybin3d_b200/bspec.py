@@ -50,12 +50,15 @@ class BSpec:
     - dealias: synthesise the bin-filtered maps on the smallest FFT-friendly grid M with
       M > 3 K per axis (K = largest binned frequency index); every product of three such
       maps is then alias-free and sum_x over the M-grid equals (M/N)^3 times the sum over
-      the full grid exactly, so results are unchanged up to rounding.  Default True."""
+      the full grid exactly, so results are unchanged up to rounding.  Default True.
+    - synthesis: how bin-filtered maps are made: 'pruned' (pb_shell_synth: filter and
+      inverse transform in one band-limited pass), 'cufft' (filter, then a cuFFT C2R of the
+      whole grid) or 'auto' (pruned where the band limits allow it)."""
 
     def __init__(self, base, k_bins, lmax=0, mask=None, applySinv=None, k_bins_squeeze=None,
                  include_partial_triangles=False, add_GIC=False, mask_IC=None, add_RIC=False, radial_bins_RIC=[],
                  Pk_fid=None, mask_shot=None, applySinv_transpose=None, *, contraction='auto', dealias=True,
-                 verb=True):
+                 synthesis='auto', verb=True):
         self.base = base
         self.applySinv = applySinv
         self.k_bins = np.asarray(k_bins)
@@ -70,6 +73,10 @@ class BSpec:
         if contraction not in ('auto', 'tc', 'simt'):
             raise ValueError("contraction must be 'auto', 'tc' or 'simt'")
         self.contraction = contraction
+        if synthesis not in ('auto', 'pruned', 'cufft'):
+            raise ValueError("synthesis must be 'auto', 'pruned' or 'cufft'")
+        self.synthesis = synthesis
+        self._synth_ok = {}
         self.verb = verb
 
         if verb:
@@ -312,10 +319,20 @@ class BSpec:
         cd = torch.complex128 if dtype == torch.float64 else torch.complex64
         prec = nat.precision_of(dtype)
         dims = self.map_grid if coarse else tuple(int(n) for n in b.gridsize)
-        hs = (dims[0], dims[1], dims[2] // 2 + 1)
-        half = torch.empty((len(specs),) + hs, dtype=cd, device=b.device)
         wp = 0 if w is None else 1
         maps = [(0, ks[bb], ks[bb + 1], l1, l2, sc / b.nreal, wp) for (bb, l1, l2, sc) in specs]
+        if self.synthesis != 'cufft' and self._synth_ok.get(dims, True):
+            out = torch.empty((len(specs),) + tuple(dims), dtype=dtype, device=b.device)
+            try:
+                nat.shell_synth(b.grid, prec, src, out, maps, dims, b.ws, w=w, src_stride=b.nhalf)
+                b.n_FFTs_reverse += len(specs)
+                return out
+            except NotImplementedError:
+                if self.synthesis == 'pruned':
+                    raise
+                self._synth_ok[dims] = False
+        hs = (dims[0], dims[1], dims[2] // 2 + 1)
+        half = torch.empty((len(specs),) + hs, dtype=cd, device=b.device)
         nat.spectral_filter(b.grid, prec, src, half, maps, w=w, src_stride=b.nhalf,
                             out_n=None if coarse is False or dims == tuple(int(n) for n in b.gridsize) else dims)
         b.n_FFTs_reverse += len(specs)

@@ -1,0 +1,742 @@
+// Band-limited map synthesis: the spectral filter followed by the inverse real 3D transform,
+// computed as a pruned transform.
+//
+//   out[m](x) = sum_k F_m(k) e^{+2 pi i k.x / M}   (unnormalised, numpy irfftn x M^3 convention)
+//   F_m(k)    = scale_m * src[src_m](k) * w(k)^wpow_m * Theta(lo_m <= |k| < hi_m) L_l1(mu) L_l2(mu)
+//
+// F_m vanishes outside the ball |k| < hi_m, so only the planes kz <= hi_m / kF_z, and in each
+// plane only the columns and rows inside the band limit, carry data.  Three passes of
+// batched 1D transforms (Stockham, mixed radix 2/3/4/5/8, in shared memory):
+//   S1  per (map, kz plane, chunk of ky columns): gather + filter the source modes of each
+//       column (kx inside the band), inverse transform along x -> U[m][kz][x][ky]
+//   S2  per (map, kz plane, chunk of x rows): ky inside the band -> inverse transform along
+//       y -> H[m][kz][x][y]
+//   S3  per (map, x, chunk of y lines): the Hermitian half-line kz in [0, Kz] of two real
+//       output lines packed into one complex transform along z -> out[m][x][y][z]
+// U and H live in the caller's workspace.  The passes agree on which columns carry data
+// through one device function (plane_radius), so S2 reads exactly what S1 wrote.
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+#include <vector>
+#include "pb_common.cuh"
+
+namespace pb {
+
+constexpr int SY_MAX_MAPS = 64;
+constexpr int SY_MAXF = 12;
+constexpr int SY_THREADS = 512;
+constexpr int SY_SMEM_BUDGET = 100 * 1024;
+
+struct FftAxis {
+    int n, np, lshift;  // length, number of radix passes, log2(lines per block)
+    int rad[SY_MAXF];
+};
+
+struct SynthMap {
+    double lo, hi, scale;
+    int src, l1, l2, wpow;
+    int kz_max;       // planes 0..kz_max
+    int rx, ry;       // band half-widths in x and y (index units)
+    int wu;           // U row width = 2 ry + 1
+    int64_t u_off;    // complex offset of this map's U block
+    int64_t h_off;    // complex offset of this map's H block
+    int b1, b2, b3;   // first block of this map in S1, S2, S3
+};
+
+struct SynthParams {
+    int n_maps;
+    int n0, n1, n2, nh2;        // source grid
+    int m0, m1, m2;             // output grid
+    double kf0, kf1, kf2;
+    int64_t src_stride;
+    FftAxis ax, ay, az;
+    int c1;                     // S1 column chunks per plane (max over maps)
+    SynthMap maps[SY_MAX_MAPS];
+};
+
+// ---- complex helpers ----------------------------------------------------------------
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cmuli(float2 a) { return make_float2(-a.y, a.x); }  // i * a
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cmuli(double2 a) { return make_double2(-a.y, a.x); }
+
+template <typename T> __device__ __forceinline__ typename cplx<T>::type cmake(double x, double y);
+template <> __device__ __forceinline__ float2 cmake<float>(double x, double y) { return make_float2((float)x, (float)y); }
+template <> __device__ __forceinline__ double2 cmake<double>(double x, double y) { return make_double2(x, y); }
+
+// ---- small inverse DFTs (sign +) in registers -----------------------------------------
+template <typename T, typename C>
+__device__ __forceinline__ void idft2(C &a, C &b) {
+    C t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <typename T, typename C>
+__device__ __forceinline__ void idft3(C *v) {
+    const T h = (T)0.86602540378443864676;  // sqrt(3) / 2
+    C s = cadd(v[1], v[2]);
+    C d = cscale(cmuli(csub(v[1], v[2])), h);
+    C t = csub(v[0], cscale(s, (T)0.5));
+    v[0] = cadd(v[0], s);
+    v[1] = cadd(t, d);
+    v[2] = csub(t, d);
+}
+
+template <typename T, typename C>
+__device__ __forceinline__ void idft4(C &v0, C &v1, C &v2, C &v3) {
+    C t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = cmuli(csub(v1, v3));
+    v0 = cadd(t0, t2);
+    v2 = csub(t0, t2);
+    v1 = cadd(t1, t3);
+    v3 = csub(t1, t3);
+}
+
+template <typename T, typename C>
+__device__ __forceinline__ void idft5(C *v) {
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+    C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    C a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    C x0 = v[0];
+    C r1 = cadd(x0, cadd(cscale(a1, c1), cscale(a2, c2)));
+    C r2 = cadd(x0, cadd(cscale(a1, c2), cscale(a2, c1)));
+    C i1 = cmuli(cadd(cscale(b1, s1), cscale(b2, s2)));
+    C i2 = cmuli(csub(cscale(b1, s2), cscale(b2, s1)));
+    v[0] = cadd(x0, cadd(a1, a2));
+    v[1] = cadd(r1, i1);
+    v[4] = csub(r1, i1);
+    v[2] = cadd(r2, i2);
+    v[3] = csub(r2, i2);
+}
+
+template <typename T, typename C>
+__device__ __forceinline__ void idft8(C *v) {
+    const T r = (T)0.70710678118654752440;
+    // even / odd halves
+    idft4<T, C>(v[0], v[2], v[4], v[6]);
+    idft4<T, C>(v[1], v[3], v[5], v[7]);
+    // twiddles e^{+i pi k / 4} on the odd half
+    C o1 = cscale(cadd(v[3], cmuli(v[3])), r);           // (1 + i)/sqrt2
+    C o2 = cmuli(v[5]);                                   // i
+    C o3 = cscale(csub(cmuli(v[7]), v[7]), r);            // (-1 + i)/sqrt2
+    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1];
+    v[0] = cadd(e0, o0);
+    v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1);
+    v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2);
+    v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3);
+    v[7] = csub(e3, o3);
+}
+
+// One Stockham pass of radix R over `lines` lines stored at stride ld in `src`, written to
+// `dst` (same layout); Ns = product of the radices of the previous passes; tw[t] =
+// e^{+2 pi i t / n}.  Threads run line-fastest: thread t takes line t mod L (L = 2^lshift
+// lines per block) and butterflies j = t / L, t / L + NG, ... (NG = blockDim / L), so a
+// warp touches 32 different lines at the same position and the line stride ld = n + 1
+// keeps those accesses on distinct banks.  j / Ns and j mod Ns are carried incrementally.
+template <int R, typename T>
+__device__ __forceinline__ void stockham_pass(const typename cplx<T>::type *src, typename cplx<T>::type *dst,
+                                              int ld, int lines, int lshift, int n, int Ns,
+                                              const typename cplx<T>::type *tw) {
+    using C = typename cplx<T>::type;
+    const int nb = n / R;
+    const int line = threadIdx.x & ((1 << lshift) - 1);
+    const int NG = blockDim.x >> lshift;
+    if (line >= lines) return;
+    const int tstep = n / (Ns * R);
+    int j = threadIdx.x >> lshift;
+    int jq = j / Ns, jm = j - jq * Ns;
+    const int sq = NG / Ns, sm = NG - sq * Ns;
+    const C *s = src + (int64_t)line * ld;
+    C *d = dst + (int64_t)line * ld;
+    for (; j < nb; j += NG) {
+        C v[R];
+        v[0] = s[j];
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            C x = s[j + r * nb];
+            if (jm > 0) x = cmul(x, tw[r * jm * tstep]);
+            v[r] = x;
+        }
+        if (R == 2) idft2<T, C>(v[0], v[1]);
+        else if (R == 3) idft3<T, C>(v);
+        else if (R == 4) idft4<T, C>(v[0], v[1], v[2], v[3]);
+        else if (R == 5) idft5<T, C>(v);
+        else idft8<T, C>(v);
+        const int o = jq * Ns * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[o + r * Ns] = v[r];
+        jq += sq;
+        jm += sm;
+        if (jm >= Ns) {
+            jm -= Ns;
+            ++jq;
+        }
+    }
+}
+
+// Radix plan of a length: 8s first, then 4, 2, 3, 5 (so Ns stays a power of two through the
+// radix-2^k passes).  Shared by the compile-time and the run-time forms.
+__host__ __device__ constexpr int radix_of(int n) {
+    return n % 8 == 0 ? 8 : n % 4 == 0 ? 4 : n % 2 == 0 ? 2 : n % 3 == 0 ? 3 : n % 5 == 0 ? 5 : 0;
+}
+__host__ __device__ constexpr int radix_at(int n, int q) {
+    for (int i = 0; i < q; ++i) n /= radix_of(n);
+    return radix_of(n);
+}
+__host__ __device__ constexpr int pass_count(int n) {
+    int c = 0;
+    while (n > 1) {
+        const int f = radix_of(n);
+        if (f == 0) return -1;
+        n /= f;
+        ++c;
+    }
+    return c;
+}
+
+// Compile-time-length pass: nb, Ns, the twiddle stride and the line stride are constants,
+// so the index arithmetic folds away.
+template <int R, typename T, int N, int NS>
+__device__ __forceinline__ void stockham_pass_ct(const typename cplx<T>::type *src, typename cplx<T>::type *dst,
+                                                 int lines, int lshift, const typename cplx<T>::type *tw) {
+    using C = typename cplx<T>::type;
+    constexpr int nb = N / R;
+    constexpr int tstep = N / (NS * R);
+    constexpr int ld = N + 1;
+    const int line = threadIdx.x & ((1 << lshift) - 1);
+    const int NG = blockDim.x >> lshift;
+    if (line >= lines) return;
+    const C *s = src + line * ld;
+    C *d = dst + line * ld;
+    for (int j = threadIdx.x >> lshift; j < nb; j += NG) {
+        const int jm = j % NS, jq = j / NS;
+        C v[R];
+        v[0] = s[j];
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            C x = s[j + r * nb];
+            if (NS > 1) x = cmul(x, tw[r * jm * tstep]);
+            v[r] = x;
+        }
+        if (R == 2) idft2<T, C>(v[0], v[1]);
+        else if (R == 3) idft3<T, C>(v);
+        else if (R == 4) idft4<T, C>(v[0], v[1], v[2], v[3]);
+        else if (R == 5) idft5<T, C>(v);
+        else idft8<T, C>(v);
+        const int o = jq * (NS * R) + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[o + r * NS] = v[r];
+    }
+}
+
+template <typename T, int N, int Q, int NS>
+__device__ __forceinline__ void passes_ct(typename cplx<T>::type *&src, typename cplx<T>::type *&dst, int lines,
+                                          int lshift, const typename cplx<T>::type *tw) {
+    if constexpr (Q < pass_count(N)) {
+        constexpr int R = radix_at(N, Q);
+        stockham_pass_ct<R, T, N, NS>(src, dst, lines, lshift, tw);
+        __syncthreads();
+        typename cplx<T>::type *t = src;
+        src = dst;
+        dst = t;
+        passes_ct<T, N, Q + 1, NS * R>(src, dst, lines, lshift, tw);
+    }
+}
+
+// All passes of one axis; data starts in b0, returns the buffer holding the result.
+// N > 0: compile-time length; N == 0: the length and radices of `ax` at run time.
+template <typename T, int N>
+__device__ typename cplx<T>::type *line_ifft(typename cplx<T>::type *b0, typename cplx<T>::type *b1, int ld,
+                                             int lines, const FftAxis &ax, const typename cplx<T>::type *tw) {
+    using C = typename cplx<T>::type;
+    C *src = b0, *dst = b1;
+    if constexpr (N > 0) {
+        passes_ct<T, N, 0, 1>(src, dst, lines, ax.lshift, tw);
+        return src;
+    }
+    int Ns = 1;
+    for (int q = 0; q < ax.np; ++q) {
+        const int R = ax.rad[q];
+        switch (R) {
+            case 2: stockham_pass<2, T>(src, dst, ld, lines, ax.lshift, ax.n, Ns, tw); break;
+            case 3: stockham_pass<3, T>(src, dst, ld, lines, ax.lshift, ax.n, Ns, tw); break;
+            case 4: stockham_pass<4, T>(src, dst, ld, lines, ax.lshift, ax.n, Ns, tw); break;
+            case 5: stockham_pass<5, T>(src, dst, ld, lines, ax.lshift, ax.n, Ns, tw); break;
+            default: stockham_pass<8, T>(src, dst, ld, lines, ax.lshift, ax.n, Ns, tw); break;
+        }
+        __syncthreads();
+        Ns *= R;
+        C *t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+template <typename T>
+__device__ __forceinline__ void make_twiddles(typename cplx<T>::type *tw, int n) {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        if (sizeof(T) == 4) {
+            // 2t/n is exact in FP32 for n <= 2^23
+            float sf, cf;
+            sincospif(2.0f * (float)t / (float)n, &sf, &cf);
+            tw[t] = cmake<T>(cf, sf);
+        } else {
+            double sd, cd;
+            sincospi(2.0 * (double)t / (double)n, &sd, &cd);
+            tw[t] = cmake<T>(cd, sd);
+        }
+    }
+}
+
+// |ky| bound of plane kz for a map of upper edge hi (one extra column of margin; the exact
+// membership test happens per mode).  -1: the plane is empty.
+__device__ __forceinline__ int plane_radius(const SynthParams &p, const SynthMap &mp, int kz) {
+    const double kzv = (double)kz * p.kf2;
+    const double r2 = mp.hi * mp.hi - kzv * kzv;
+    if (r2 < 0.0) return -1;
+    int r = (int)floor(sqrt(r2) / p.kf1) + 1;
+    return r < mp.ry ? r : mp.ry;
+}
+
+__device__ __forceinline__ int find_map(const SynthParams &p, int b, int which) {
+    int m = 0;
+    for (int i = 1; i < p.n_maps; ++i) {
+        const int first = which == 1 ? p.maps[i].b1 : (which == 2 ? p.maps[i].b2 : p.maps[i].b3);
+        if (b >= first) m = i;
+    }
+    return m;
+}
+
+// ---- S1: gather + filter + transform along x ------------------------------------------
+template <typename T, int N>
+__global__ void __launch_bounds__(SY_THREADS) synth_x_kernel(SynthParams p, const typename cplx<T>::type *src,
+                                                             const T *w, typename cplx<T>::type *U) {
+    using C = typename cplx<T>::type;
+    extern __shared__ __align__(16) unsigned char sy_smem[];
+    const FftAxis &ax = p.ax;
+    const int n = N > 0 ? N : ax.n, ld = n + 1, L = 1 << ax.lshift;
+    C *tw = reinterpret_cast<C *>(sy_smem);
+    C *b0 = tw + n;
+    C *b1 = b0 + L * ld;
+    const int m = find_map(p, blockIdx.x, 1);
+    const SynthMap mp = p.maps[m];
+    const int local = blockIdx.x - mp.b1;
+    const int kz = local / p.c1;
+    const int chunk = local - kz * p.c1;
+    const int R = plane_radius(p, mp, kz);
+    const int c0 = chunk * L;  // first column index (ky = c - ry)
+    const int col_first = max(c0, mp.ry - R), col_last = min(c0 + L - 1, mp.ry + R);
+    if (R < 0 || col_first > col_last) return;
+    const int lines = col_last - c0 + 1;  // lines below col_first stay 0
+    make_twiddles<T>(tw, n);
+    const C *s = src ? src + (int64_t)mp.src * p.src_stride : nullptr;  // NULL: unit spectrum
+    const double kzz = __dmul_rn((double)kz, p.kf2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int line = warp; line < lines; line += nw) {
+        const int c = c0 + line;
+        const int ky = c - mp.ry;
+        const double kyv = __dmul_rn((double)ky, p.kf1);
+        const int sj = ky < 0 ? ky + p.n1 : ky;
+        C *row = b0 + (int64_t)line * ld;
+        for (int e = lane; e < n; e += 32) {
+            const int kx = e < (n >> 1) ? e : e - n;
+            C v = cmake<T>(0.0, 0.0);
+            if (c >= col_first && kx >= -mp.rx && kx <= mp.rx) {
+                const double kxv = __dmul_rn((double)kx, p.kf0);
+                const double kk = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(kxv, kxv), __dmul_rn(kyv, kyv)),
+                                                       __dmul_rn(kzz, kzz)));
+                if (mp.lo <= kk && kk < mp.hi) {
+                    const double mu = kk != 0.0 ? __ddiv_rn(kzz, kk) : 0.0;
+                    const int si = kx < 0 ? kx + p.n0 : kx;
+                    const int64_t sidx = ((int64_t)si * p.n1 + sj) * p.nh2 + kz;
+                    double f = mp.scale * legendre(mp.l1, mu) * legendre(mp.l2, mu);
+                    if (mp.wpow != 0) {
+                        const double wv = (double)w[sidx];
+                        if (mp.wpow == 1) f *= wv;
+                        else if (mp.wpow == 2) f *= wv * wv;
+                        else f = wv != 0.0 ? f / wv : 0.0;
+                    }
+                    if (s) {
+                        const C x = s[sidx];
+                        v = cmake<T>((double)x.x * f, (double)x.y * f);
+                    } else {
+                        v = cmake<T>(f, 0.0);
+                    }
+                }
+            }
+            row[e] = v;
+        }
+    }
+    __syncthreads();
+    C *res = line_ifft<T, N>(b0, b1, ld, lines, ax, tw);
+    // U[m][kz][x][c]: consecutive threads take consecutive columns
+    C *u = U + mp.u_off + (int64_t)kz * n * mp.wu;
+    const int line = threadIdx.x & (L - 1), NG = blockDim.x >> ax.lshift;
+    const int c = c0 + line;
+    if (line < lines && c >= col_first)
+        for (int x = threadIdx.x >> ax.lshift; x < n; x += NG) u[(int64_t)x * mp.wu + c] = res[(int64_t)line * ld + x];
+}
+
+// ---- S2: transform along y --------------------------------------------------------------
+template <typename T, int N>
+__global__ void __launch_bounds__(SY_THREADS) synth_y_kernel(SynthParams p, const typename cplx<T>::type *U,
+                                                             typename cplx<T>::type *H) {
+    using C = typename cplx<T>::type;
+    extern __shared__ __align__(16) unsigned char sy_smem[];
+    const FftAxis &ay = p.ay;
+    const int n = N > 0 ? N : ay.n, ld = n + 1, L = 1 << ay.lshift;
+    C *tw = reinterpret_cast<C *>(sy_smem);
+    C *b0 = tw + n;
+    C *b1 = b0 + L * ld;
+    const int m = find_map(p, blockIdx.x, 2);
+    const SynthMap mp = p.maps[m];
+    const int local = blockIdx.x - mp.b2;
+    const int xchunks = (p.m0 + L - 1) >> ay.lshift;
+    const int kz = local / xchunks;
+    const int x0 = (local - kz * xchunks) * L;
+    const int lines = min(L, p.m0 - x0);
+    const int R = plane_radius(p, mp, kz);
+    make_twiddles<T>(tw, n);
+    const C *u = U + mp.u_off + (int64_t)kz * p.m0 * mp.wu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    // loads of a batch are issued before any of them is stored, so each thread keeps
+    // several global reads in flight
+    constexpr int UB = 8;
+    for (int line = warp; line < lines; line += nw) {
+        const C *urow = u + (int64_t)(x0 + line) * mp.wu + mp.ry;
+        C *row = b0 + (int64_t)line * ld;
+        for (int e0 = lane; e0 < n; e0 += 32 * UB) {
+            C v[UB];
+#pragma unroll
+            for (int q = 0; q < UB; ++q) {
+                const int e = e0 + 32 * q;
+                const int ky = e < (n >> 1) ? e : e - n;
+                v[q] = (e < n && ky >= -R && ky <= R) ? urow[ky] : cmake<T>(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < UB; ++q)
+                if (e0 + 32 * q < n) row[e0 + 32 * q] = v[q];
+        }
+    }
+    __syncthreads();
+    C *res = line_ifft<T, N>(b0, b1, ld, lines, ay, tw);
+    C *h = H + mp.h_off + ((int64_t)kz * p.m0 + x0) * p.m1;
+    for (int line = warp; line < lines; line += nw) {
+        const C *row = res + (int64_t)line * ld;
+        C *hrow = h + (int64_t)line * p.m1;
+        for (int y = lane; y < n; y += 32) hrow[y] = row[y];
+    }
+}
+
+// ---- S3: real transform along z, two output lines per complex transform -----------------
+template <typename T, int N>
+__global__ void __launch_bounds__(SY_THREADS) synth_z_kernel(SynthParams p, const typename cplx<T>::type *H,
+                                                             T *out) {
+    using C = typename cplx<T>::type;
+    extern __shared__ __align__(16) unsigned char sy_smem[];
+    const FftAxis &az = p.az;
+    const int n = N > 0 ? N : az.n, ld = n + 1, L = 1 << az.lshift;
+    C *tw = reinterpret_cast<C *>(sy_smem);
+    C *b0 = tw + n;
+    C *b1 = b0 + L * ld;
+    const int m = find_map(p, blockIdx.x, 3);
+    const SynthMap mp = p.maps[m];
+    const int local = blockIdx.x - mp.b3;
+    const int ychunks = (p.m1 + 2 * L - 1) / (2 * L);
+    const int x = local / ychunks;
+    const int y0 = (local - x * ychunks) * 2 * L;
+    const int ny = min(2 * L, p.m1 - y0);
+    const int lines = (ny + 1) >> 1;
+    const int K = mp.kz_max;
+    make_twiddles<T>(tw, n);
+    // line-fastest: consecutive threads read consecutive (y, y+1) pairs of one kz row
+    const int line = threadIdx.x & (L - 1), NG = blockDim.x >> az.lshift;
+    if (line < lines) {
+        C *d = b0 + (int64_t)line * ld;
+        for (int e = (threadIdx.x >> az.lshift) + K + 1; e < n - K; e += NG) d[e] = cmake<T>(0.0, 0.0);
+        const C *h = H + mp.h_off + (int64_t)x * p.m1 + y0 + 2 * line;
+        const int64_t plane = (int64_t)p.m0 * p.m1;
+        const bool has_b = 2 * line + 1 < ny;
+        constexpr int UB = 4;  // loads in flight per thread
+        for (int kz0 = threadIdx.x >> az.lshift; kz0 <= K; kz0 += UB * NG) {
+            C a[UB], b[UB];
+#pragma unroll
+            for (int q = 0; q < UB; ++q) {
+                const int kz = kz0 + q * NG;
+                a[q] = kz <= K ? h[kz * plane] : cmake<T>(0.0, 0.0);
+                b[q] = (kz <= K && has_b) ? h[kz * plane + 1] : cmake<T>(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < UB; ++q) {
+                const int kz = kz0 + q * NG;
+                if (kz > K) break;
+                if (kz == 0) {
+                    d[0] = cmake<T>((double)a[q].x, (double)b[q].x);
+                } else {
+                    C dp, dm;
+                    dp.x = a[q].x - b[q].y;
+                    dp.y = a[q].y + b[q].x;
+                    dm.x = a[q].x + b[q].y;
+                    dm.y = b[q].x - a[q].y;
+                    d[kz] = dp;
+                    d[n - kz] = dm;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    C *res = line_ifft<T, N>(b0, b1, ld, lines, az, tw);
+    T *o = out + (int64_t)m * p.m0 * p.m1 * p.m2 + ((int64_t)x * p.m1 + y0) * p.m2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int yy = warp; yy < ny; yy += nw) {
+        const C *row = res + (int64_t)(yy >> 1) * ld;
+        T *orow = o + (int64_t)yy * p.m2;
+        if (yy & 1)
+            for (int z = lane; z < n; z += 32) orow[z] = row[z].y;
+        else
+            for (int z = lane; z < n; z += 32) orow[z] = row[z].x;
+    }
+}
+
+// ---- host side ----------------------------------------------------------------------------
+static bool factor_axis(int n, FftAxis &ax) {
+    ax.n = n;
+    ax.np = 0;
+    int r = n;
+    while (r > 1 && ax.np < SY_MAXF) {
+        int f = 0;
+        if (r % 8 == 0) f = 8;
+        else if (r % 4 == 0) f = 4;
+        else if (r % 2 == 0) f = 2;
+        else if (r % 3 == 0) f = 3;
+        else if (r % 5 == 0) f = 5;
+        else return false;
+        ax.rad[ax.np++] = f;
+        r /= f;
+    }
+    return r == 1;
+}
+
+template <typename C>
+static int lines_for(int n, int cap) {
+    int L = 32;
+    while (L > 1 && (int64_t)(2 * L * (n + 1) + n) * (int64_t)sizeof(C) > SY_SMEM_BUDGET) L >>= 1;
+    return std::min(L, cap);
+}
+
+struct SynthLayout {
+    SynthParams p;
+    int64_t u_elems, h_elems;
+    int nb1, nb2, nb3;
+};
+
+static int synth_layout(const pb_grid_t *g, const int32_t *out_n, int precision, int n_maps, const double *lo,
+                        const double *hi, const int32_t *src_idx, const int32_t *l1, const int32_t *l2,
+                        const double *scale, const int32_t *wpow, int64_t src_stride, SynthLayout *L) {
+    Grid G;
+    int st = make_grid(g, &G);
+    if (st) return st;
+    if (!out_n) return fail(PB_ERR_INVALID, "pb_shell_synth: out_n is NULL");
+    if (n_maps < 1 || n_maps > SY_MAX_MAPS) return fail(PB_ERR_INVALID, "pb_shell_synth: n_maps must be in [1, 64]");
+    if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "pb_shell_synth: bad precision");
+    SynthParams &p = L->p;
+    memset(&p, 0, sizeof(p));
+    p.n_maps = n_maps;
+    p.n0 = G.n0;
+    p.n1 = G.n1;
+    p.n2 = G.n2;
+    p.nh2 = G.nh2;
+    p.m0 = out_n[0];
+    p.m1 = out_n[1];
+    p.m2 = out_n[2];
+    p.kf0 = G.kf0;
+    p.kf1 = G.kf1;
+    p.kf2 = G.kf2;
+    p.src_stride = src_stride;
+    for (int i = 0; i < 3; ++i)
+        if (out_n[i] < 2 || (out_n[i] & 1)) return fail(PB_ERR_INVALID, "pb_shell_synth: output dims must be even");
+    if (!factor_axis(p.m0, p.ax) || !factor_axis(p.m1, p.ay) || !factor_axis(p.m2, p.az))
+        return fail(PB_ERR_UNSUPPORTED, "pb_shell_synth: output dims must be products of 2, 3 and 5");
+    const bool f64 = precision == PB_F64;
+    const int lx = f64 ? lines_for<double2>(p.m0, 32) : lines_for<float2>(p.m0, 32);
+    const int ly = f64 ? lines_for<double2>(p.m1, 32) : lines_for<float2>(p.m1, 32);
+    const int lz = f64 ? lines_for<double2>(p.m2, 32) : lines_for<float2>(p.m2, 32);
+    auto lg = [](int v) { int k = 0; while ((1 << k) < v) ++k; return k; };
+    p.ax.lshift = lg(lx);
+    p.ay.lshift = lg(ly);
+    p.az.lshift = lg(lz);
+    int max_wu = 1;
+    for (int m = 0; m < n_maps; ++m) {
+        SynthMap &mp = p.maps[m];
+        if (!(hi[m] > 0.0) || !std::isfinite(hi[m]))
+            return fail(PB_ERR_UNSUPPORTED, "pb_shell_synth: every map needs a finite upper edge");
+        if (l1[m] < 0 || l1[m] > 4 || l2[m] < 0 || l2[m] > 4)
+            return fail(PB_ERR_INVALID, "pb_shell_synth: Legendre order must be in [0, 4]");
+        const int wp = wpow ? wpow[m] : 0;
+        if (wp < -1 || wp > 2) return fail(PB_ERR_INVALID, "pb_shell_synth: wpow must be -1, 0, 1 or 2");
+        mp.lo = lo[m];
+        mp.hi = hi[m];
+        mp.scale = scale[m];
+        mp.src = src_idx ? src_idx[m] : 0;
+        if (mp.src < 0) return fail(PB_ERR_INVALID, "pb_shell_synth: negative source index");
+        mp.l1 = l1[m];
+        mp.l2 = l2[m];
+        mp.wpow = wp;
+        // band half-widths with one index of margin (the exact membership test is per mode)
+        mp.rx = (int)std::floor(hi[m] / G.kf0) + 1;
+        mp.ry = (int)std::floor(hi[m] / G.kf1) + 1;
+        mp.kz_max = (int)std::floor(hi[m] / G.kf2) + 1;
+        // the band must sit strictly inside the output grid and inside the source grid
+        if (2 * mp.rx >= p.m0 || 2 * mp.ry >= p.m1 || 2 * mp.kz_max >= p.m2 || 2 * mp.rx >= G.n0 ||
+            2 * mp.ry >= G.n1 || mp.kz_max >= G.nh2 - 1)
+            return fail(PB_ERR_UNSUPPORTED, "pb_shell_synth: band limit reaches the Nyquist frequency of a grid");
+        mp.wu = 2 * mp.ry + 1;
+        max_wu = std::max(max_wu, mp.wu);
+    }
+    p.c1 = (max_wu + lx - 1) / lx;
+    int64_t u = 0, h = 0;
+    int b1 = 0, b2 = 0, b3 = 0;
+    const int xch = (p.m0 + ly - 1) / ly;
+    const int ych = (p.m1 + 2 * lz - 1) / (2 * lz);
+    for (int m = 0; m < n_maps; ++m) {
+        SynthMap &mp = p.maps[m];
+        const int planes = mp.kz_max + 1;
+        mp.u_off = u;
+        mp.h_off = h;
+        u += (int64_t)planes * p.m0 * mp.wu;
+        h += (int64_t)planes * p.m0 * p.m1;
+        mp.b1 = b1;
+        mp.b2 = b2;
+        mp.b3 = b3;
+        b1 += planes * p.c1;
+        b2 += planes * xch;
+        b3 += p.m0 * ych;
+    }
+    L->u_elems = u;
+    L->h_elems = h;
+    L->nb1 = b1;
+    L->nb2 = b2;
+    L->nb3 = b3;
+    return PB_OK;
+}
+
+
+// Lengths with a compile-time kernel; any other supported length runs the run-time form.
+template <typename F>
+static void with_length(int n, F &&f) {
+    switch (n) {
+        case 24: f(std::integral_constant<int, 24>()); break;
+        case 32: f(std::integral_constant<int, 32>()); break;
+        case 48: f(std::integral_constant<int, 48>()); break;
+        case 64: f(std::integral_constant<int, 64>()); break;
+        case 96: f(std::integral_constant<int, 96>()); break;
+        case 128: f(std::integral_constant<int, 128>()); break;
+        case 192: f(std::integral_constant<int, 192>()); break;
+        case 256: f(std::integral_constant<int, 256>()); break;
+        case 384: f(std::integral_constant<int, 384>()); break;
+        case 512: f(std::integral_constant<int, 512>()); break;
+        default: f(std::integral_constant<int, 0>()); break;
+    }
+}
+
+template <typename T>
+static int launch_synth(const SynthLayout &L, const typename cplx<T>::type *src, const T *w,
+                        typename cplx<T>::type *U, typename cplx<T>::type *H, T *out, cudaStream_t s) {
+    const SynthParams &p = L.p;
+    const size_t c = sizeof(typename cplx<T>::type);
+    auto smem = [&](const FftAxis &a) { return (size_t)(2 * (1 << a.lshift) * (a.n + 1) + a.n) * c; };
+    cudaError_t e = cudaSuccess;
+    with_length(p.ax.n, [&](auto NC) {
+        constexpr int N = decltype(NC)::value;
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(synth_x_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem(p.ax));
+        if (e == cudaSuccess) {
+            synth_x_kernel<T, N><<<L.nb1, SY_THREADS, smem(p.ax), s>>>(p, src, w, U);
+            e = cudaGetLastError();
+        }
+    });
+    if (e != cudaSuccess) return cuda_check(e, "pb_shell_synth (x)");
+    with_length(p.ay.n, [&](auto NC) {
+        constexpr int N = decltype(NC)::value;
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(synth_y_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem(p.ay));
+        if (e == cudaSuccess) {
+            synth_y_kernel<T, N><<<L.nb2, SY_THREADS, smem(p.ay), s>>>(p, U, H);
+            e = cudaGetLastError();
+        }
+    });
+    if (e != cudaSuccess) return cuda_check(e, "pb_shell_synth (y)");
+    with_length(p.az.n, [&](auto NC) {
+        constexpr int N = decltype(NC)::value;
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(synth_z_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem(p.az));
+        if (e == cudaSuccess) {
+            synth_z_kernel<T, N><<<L.nb3, SY_THREADS, smem(p.az), s>>>(p, H, out);
+            e = cudaGetLastError();
+        }
+    });
+    if (e != cudaSuccess) return cuda_check(e, "pb_shell_synth (z)");
+    return PB_OK;
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" int pb_shell_synth_workspace_size(const pb_grid_t *g, const int32_t *out_n, int precision, int n_maps,
+                                             const double *hi, size_t *bytes) {
+    if (!bytes || !hi) return fail(PB_ERR_INVALID, "pb_shell_synth_workspace_size: NULL argument");
+    if (n_maps < 1 || n_maps > SY_MAX_MAPS)
+        return fail(PB_ERR_INVALID, "pb_shell_synth_workspace_size: n_maps must be in [1, 64]");
+    std::vector<double> lo(n_maps, 0.0), sc(n_maps, 1.0);
+    std::vector<int32_t> zero(n_maps, 0);
+    SynthLayout L;
+    int st = synth_layout(g, out_n, precision, n_maps, lo.data(), hi, nullptr, zero.data(), zero.data(), sc.data(),
+                          nullptr, 0, &L);
+    if (st) return st;
+    const size_t c = precision == PB_F64 ? 16 : 8;
+    *bytes = (size_t)(L.u_elems + L.h_elems) * c + 256;
+    return PB_OK;
+}
+
+extern "C" int pb_shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
+                              int64_t src_stride, int n_maps, const int32_t *src_idx, const double *lo,
+                              const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
+                              const int32_t *wpow, const void *w, void *out, void *workspace, size_t workspace_bytes,
+                              void *stream) {
+    if (!out || !lo || !hi || !l1 || !l2 || !scale) return fail(PB_ERR_INVALID, "pb_shell_synth: NULL argument");
+    SynthLayout L;
+    int st = synth_layout(g, out_n, precision, n_maps, lo, hi, src_idx, l1, l2, scale, wpow, src_stride, &L);
+    if (st) return st;
+    for (int m = 0; m < n_maps; ++m)
+        if (L.p.maps[m].wpow != 0 && !w) return fail(PB_ERR_INVALID, "pb_shell_synth: wpow set but weight grid is NULL");
+    const size_t c = precision == PB_F64 ? 16 : 8;
+    const size_t need = (size_t)(L.u_elems + L.h_elems) * c + 256;
+    if (!workspace || workspace_bytes < need) return fail(PB_ERR_INVALID, "pb_shell_synth: workspace too small");
+    cudaStream_t s = as_stream(stream);
+    char *ws = (char *)(((uintptr_t)workspace + 255) & ~(uintptr_t)255);
+    if (precision == PB_F32) {
+        float2 *U = (float2 *)ws;
+        st = launch_synth<float>(L, (const float2 *)src, (const float *)w, U, U + L.u_elems, (float *)out, s);
+    } else {
+        double2 *U = (double2 *)ws;
+        st = launch_synth<double>(L, (const double2 *)src, (const double *)w, U, U + L.u_elems, (double *)out, s);
+    }
+    return st;
+}
