@@ -284,19 +284,18 @@ def run_ours(args, rank, world, local):
         ms = float(tt.item())
     value = world * args.steps / (ms / 1000.0)
 
-    # end-to-end through the public API from pinned host memory
-    for i in range(args.warmup):
-        with contextlib.redirect_stdout(io.StringIO()):
-            bs.Bk_ideal(host[i % n_pool])
+    # end-to-end through the public API from pinned host memory: Bk_ideal on the list of
+    # the step's fields (each field's H2D copy and result read-back inside the timed region;
+    # copies overlap the previous field's estimator)
+    with contextlib.redirect_stdout(io.StringIO()):
+        bs.Bk_ideal([host[i % n_pool] for i in range(args.warmup)])
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    t = time.perf_counter()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for i in range(args.steps):
-        with contextlib.redirect_stdout(io.StringIO()):
-            r = bs.Bk_ideal(host[i % n_pool])
+    with contextlib.redirect_stdout(io.StringIO()):
+        r = bs.Bk_ideal([host[i % n_pool] for i in range(args.steps)])
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)

@@ -505,7 +505,10 @@ class BSpec:
         return fish
 
     def Bk_ideal(self, data, fish_ideal=[], discreteness_correction=True, verb=False):
-        """Ideal estimator (bspec.py:1085-1118)."""
+        """Ideal estimator (bspec.py:1085-1118).  `data` may also be a list of fields: they
+        are streamed (the host-to-device copy of field i+1 overlaps the estimator of field i,
+        on its own stream, when the fields are pinned torch tensors) and a list of dicts is
+        returned."""
         if len(fish_ideal) != 0:
             self.fish_ideal = fish_ideal
             self.inv_fish_ideal = np.linalg.inv(fish_ideal)
@@ -513,14 +516,61 @@ class BSpec:
             self.compute_fisher_ideal(discreteness_correction=discreteness_correction, verb=verb)
         elif getattr(self, 'discreteness_correction', discreteness_correction) != discreteness_correction:
             self.compute_fisher_ideal(discreteness_correction=discreteness_correction, verb=verb)
+        if isinstance(data, (list, tuple)):
+            return [self._bk_dict(r) for r in self._bk_ideal_stream(data)]
         Bk_num_ideal = self.Bk_numerator_ideal(data, verb=verb)
-        Bk_out = np.matmul(self.inv_fish_ideal, Bk_num_ideal)
+        return self._bk_dict(np.matmul(self.inv_fish_ideal, Bk_num_ideal))
+
+    def _bk_dict(self, Bk_out):
         Bk_dict = {}
         index = 0
         for l in range(0, self.lmax + 1, 2):
             Bk_dict['b%s' % l] = Bk_out[index:index + self.N3]
             index += self.N3
         return Bk_dict
+
+    def _bk_ideal_stream(self, fields):
+        """F^-1 B_num for each field; two device field buffers, copies on a side stream."""
+        b = self.base
+        for f in fields:
+            if not isinstance(f, torch.Tensor):
+                assert type(f[0, 0, 0]) in [np.float32, np.float64], "Data must be of type float32 or float64!"
+            if not self.const_mask:
+                assert tuple(f.shape) == self.mask.shape, "Data must have same shape as the mask!"
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        dev = b.device
+        inv_fish = torch.as_tensor(self.inv_fish_ideal, device=dev)
+        norm = torch.as_tensor(b.volume / float(b.gridsize.prod()) / self.sym_factor, device=dev)
+        main = torch.cuda.current_stream(dev)
+        side = torch.cuda.Stream(device=dev)
+        rd = b.real_dtype
+        bufs = [torch.empty(tuple(int(n) for n in b.gridsize), dtype=rd, device=dev) for _ in range(2)]
+        ready = [torch.cuda.Event() for _ in range(2)]
+        free = [torch.cuda.Event() for _ in range(2)]
+        out = torch.empty((len(fields), self.N_bins), dtype=torch.float64).pin_memory()
+
+        def upload(i):
+            s = i % 2
+            with torch.cuda.stream(side):
+                if i >= 2:
+                    side.wait_event(free[s])
+                src = fields[i] if isinstance(fields[i], torch.Tensor) else torch.from_numpy(np.ascontiguousarray(fields[i]))
+                bufs[s].copy_(src, non_blocking=True)
+                ready[s].record(side)
+
+        if fields:
+            upload(0)
+        for i in range(len(fields)):
+            if i + 1 < len(fields):
+                upload(i + 1)
+            s = i % 2
+            main.wait_event(ready[s])
+            B3 = self._bk_cubic(bufs[s], 'ideal')
+            free[s].record(main)
+            out[i].copy_(inv_fish @ (B3 * norm), non_blocking=True)
+        main.synchronize()
+        return out.numpy()
 
     # ------------------------------------------------------------------------------
     # Monte Carlo Fisher (bspec.py:473-693), FP64

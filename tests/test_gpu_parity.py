@@ -245,3 +245,18 @@ def test_dealiased_map_grid_is_exact(pb):
         assert rel(r1[k], ref[k]) < 1e-10
         assert rel(r2[k], ref[k]) < 1e-10
     assert rel(bs.sym_factor, bs_full.sym_factor) < 1e-10
+
+
+def test_bk_ideal_streamed_list(pb):
+    """Bk_ideal on a list of fields (copies overlapped on a side stream) equals field-by-field."""
+    N, L = 48, 600.0
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="tsc", backend="cuda", precision="mixed")
+    bs = quiet(pb.BSpec, b, np.linspace(2 * np.pi / L, 0.11, 6), lmax=2)
+    fields = [torch.from_numpy(synthetic.lognormal(N, L, seed=s)).pin_memory() for s in range(3)]
+    fields.append(synthetic.lognormal(N, L, seed=7))  # a numpy field in the same list
+    one = [quiet(bs.Bk_ideal, f if isinstance(f, np.ndarray) else f.numpy()) for f in fields]
+    many = quiet(bs.Bk_ideal, fields)
+    assert len(many) == len(fields)
+    for a, r in zip(many, one):
+        for k in r:
+            assert rel(a[k], r[k]) < 1e-12
