@@ -208,8 +208,8 @@ class BSpec:
         return np.asarray([k1s, k2s, k3s])
 
     def _dealiased_grid(self):
-        """Per axis, the smallest even 2^a 3^b 5^c 7^d size M > 3 K (K = floor(k_max / kF))
-        not above the data grid."""
+        """Per axis, the smallest even 2^a 3^b 5^c size M > 3 K (K = floor(k_max / kF)) not
+        above the data grid (the lengths the pruned synthesis transforms)."""
         b = self.base
         kmax = float(np.max(self.k_bins_squeeze))
         dims = []
@@ -218,7 +218,7 @@ class BSpec:
             m = 3 * K + 1
             while True:
                 r = m
-                for f in (2, 3, 5, 7):
+                for f in (2, 3, 5):
                     while r % f == 0:
                         r //= f
                 if r == 1 and m % 2 == 0:
