@@ -125,6 +125,17 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                  : "memory");
 }
 
+// 32 lanes x 8 columns of 32-bit accumulators; tmem_ld_wait() before the values are used
+__device__ __forceinline__ void tmem_ld8_issue(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     uint32_t r[8];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
@@ -441,22 +452,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     // D row held by this lane: M = 64 -> rows 16q..16q+15 in lanes 0..15
                     const int m = geo.M == 64 ? (lane < 16 ? 16 * q + lane : -1) : 32 * q + lane;
                     const int j = m >= 0 ? (m >> 1) : -1;
-                    const bool writer = m >= 0 && (m & 1) == 0 && j < n_c;
+                    // after the hi + lo shuffle both lanes of a map hold its sums: the hi lane
+                    // adds columns 0..3 of each group of 8, the lo lane columns 4..7
+                    const bool writer = m >= 0 && j < n_c;
+                    const int half = m & 1;
                     const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(dset * geo.ntot);
-                    for (int cc = h; cc < geo.ntot / 8; cc += TC_EPI / 4) {
-                        float v[8];
-                        tmem_ld8(tbase + cc * 8, v);
+                    const int ngrp = geo.ntot / 8;
+                    for (int cc = h; cc < ngrp; cc += 2 * (TC_EPI / 4)) {
+                        // two column groups per TMEM wait
+                        const int cc2 = cc + TC_EPI / 4;
+                        float v[2][8];
+                        tmem_ld8_issue(tbase + cc * 8, v[0]);
+                        if (cc2 < ngrp) tmem_ld8_issue(tbase + cc2 * 8, v[1]);
+                        tmem_ld_wait();
 #pragma unroll
-                        for (int k = 0; k < 8; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], 1);
-                        if (writer) {
-                            const int col0 = cc * 8;
-                            int t = 0;
-                            while (t + 1 < geo.n_nt && col0 >= geo.nt_col[t + 1]) ++t;
-                            const int pend = (t + 1 < geo.n_nt) ? geo.nt_start[t + 1] : geo.n_pairs;
+                        for (int g2 = 0; g2 < 2; ++g2) {
+                            const int c8 = g2 == 0 ? cc : cc2;
+                            if (c8 >= ngrp) break;
 #pragma unroll
-                            for (int k = 0; k < 8; ++k) {
-                                const int p = geo.nt_start[t] + (col0 + k - geo.nt_col[t]);
-                                if (p < pend) acc[p * n_c + j] += (double)v[k];
+                            for (int k = 0; k < 8; ++k) v[g2][k] += __shfl_xor_sync(0xffffffffu, v[g2][k], 1);
+                            if (writer) {
+                                const int col0 = c8 * 8;
+                                int t = 0;
+                                while (t + 1 < geo.n_nt && col0 >= geo.nt_col[t + 1]) ++t;
+                                const int pend = (t + 1 < geo.n_nt) ? geo.nt_start[t + 1] : geo.n_pairs;
+#pragma unroll
+                                for (int k = 0; k < 4; ++k) {
+                                    const float val = half ? v[g2][4 + k] : v[g2][k];
+                                    const int p = geo.nt_start[t] + (col0 + 4 * half + k - geo.nt_col[t]);
+                                    if (p < pend) acc[p * n_c + j] += (double)val;
+                                }
                             }
                         }
                     }
