@@ -258,6 +258,98 @@ __device__ __forceinline__ void passes_ct(typename cplx<T>::type *&src, typename
     }
 }
 
+__host__ __device__ constexpr int ns_at(int n, int q) {
+    int ns = 1;
+    for (int i = 0; i < q; ++i) ns *= radix_at(n, i);
+    return ns;
+}
+
+// A compile-time pass whose operands come from and go to functors: v[r] = ldf(line, j + r nb)
+// (twiddled), stf(line, o + r Ns, v[r]).  ELEM: threads run j-fastest along a line (for
+// loads or stores that are contiguous along the line in global memory); otherwise
+// line-fastest as in stockham_pass_ct.
+template <int R, typename T, int N, int NS, bool ELEM, typename LD, typename ST>
+__device__ __forceinline__ void io_pass(int lines, int lshift, const typename cplx<T>::type *tw, LD &&ldf,
+                                        ST &&stf) {
+    using C = typename cplx<T>::type;
+    constexpr int nb = N / R;
+    constexpr int tstep = N / (NS * R);
+    auto body = [&](int line, int j) {
+        const int jm = j % NS, jq = j / NS;
+        C v[R];
+        v[0] = ldf(line, j);
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            C x = ldf(line, j + r * nb);
+            if (NS > 1) x = cmul(x, tw[r * jm * tstep]);
+            v[r] = x;
+        }
+        if (R == 2) idft2<T, C>(v[0], v[1]);
+        else if (R == 3) idft3<T, C>(v);
+        else if (R == 4) idft4<T, C>(v[0], v[1], v[2], v[3]);
+        else if (R == 5) idft5<T, C>(v);
+        else idft8<T, C>(v);
+        const int o = jq * (NS * R) + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) stf(line, o + r * NS, v[r]);
+    };
+    if (ELEM) {
+        for (int it = threadIdx.x; it < lines * nb; it += blockDim.x) {
+            const int line = it / nb;
+            body(line, it - line * nb);
+        }
+    } else {
+        const int line = threadIdx.x & ((1 << lshift) - 1);
+        if (line >= lines) return;
+        for (int j = threadIdx.x >> lshift; j < nb; j += blockDim.x >> lshift) body(line, j);
+    }
+}
+
+template <typename T, int N, int Q, int QEND>
+__device__ __forceinline__ void smem_passes(typename cplx<T>::type *&src, typename cplx<T>::type *&dst, int lines,
+                                            int lshift, const typename cplx<T>::type *tw) {
+    if constexpr (Q < QEND) {
+        stockham_pass_ct<radix_at(N, Q), T, N, ns_at(N, Q)>(src, dst, lines, lshift, tw);
+        __syncthreads();
+        typename cplx<T>::type *t = src;
+        src = dst;
+        dst = t;
+        smem_passes<T, N, Q + 1, QEND>(src, dst, lines, lshift, tw);
+    }
+}
+
+// Compile-time length, data in b0 (line stride N + 1): every pass but the last in shared
+// memory, the last one straight to stf(line, element, value).
+template <typename T, int N, bool LAST_ELEM, typename ST>
+__device__ __forceinline__ void line_ifft_tail(typename cplx<T>::type *b0, typename cplx<T>::type *b1, int lines,
+                                               int lshift, const typename cplx<T>::type *tw, ST &&stf) {
+    using C = typename cplx<T>::type;
+    constexpr int P = pass_count(N);
+    C *src = b0, *dst = b1;
+    smem_passes<T, N, 0, P - 1>(src, dst, lines, lshift, tw);
+    const C *s = src;
+    io_pass<radix_at(N, P - 1), T, N, ns_at(N, P - 1), LAST_ELEM>(
+        lines, lshift, tw, [&](int line, int e) { return s[line * (N + 1) + e]; }, stf);
+}
+
+// Compile-time length, first pass straight from ldf(line, element) (line-fastest), last pass
+// straight to stf; needs at least two passes.
+template <typename T, int N, bool LAST_ELEM, typename LD, typename ST>
+__device__ __forceinline__ void line_ifft_io(typename cplx<T>::type *b0, typename cplx<T>::type *b1, int lines,
+                                             int lshift, const typename cplx<T>::type *tw, LD &&ldf, ST &&stf) {
+    using C = typename cplx<T>::type;
+    constexpr int P = pass_count(N);
+    static_assert(P >= 2, "line_ifft_io needs two passes");
+    io_pass<radix_at(N, 0), T, N, 1, false>(lines, lshift, tw, ldf,
+                                            [&](int line, int e, C v) { b0[line * (N + 1) + e] = v; });
+    __syncthreads();
+    C *src = b0, *dst = b1;
+    smem_passes<T, N, 1, P - 1>(src, dst, lines, lshift, tw);
+    const C *s = src;
+    io_pass<radix_at(N, P - 1), T, N, ns_at(N, P - 1), LAST_ELEM>(
+        lines, lshift, tw, [&](int line, int e) { return s[line * (N + 1) + e]; }, stf);
+}
+
 // All passes of one axis; data starts in b0, returns the buffer holding the result.
 // N > 0: compile-time length; N == 0: the length and radices of `ax` at run time.
 template <typename T, int N>
@@ -384,13 +476,21 @@ __global__ void __launch_bounds__(SY_THREADS) synth_x_kernel(SynthParams p, cons
         }
     }
     __syncthreads();
-    C *res = line_ifft<T, N>(b0, b1, ld, lines, ax, tw);
     // U[m][kz][x][c]: consecutive threads take consecutive columns
     C *u = U + mp.u_off + (int64_t)kz * n * mp.wu;
-    const int line = threadIdx.x & (L - 1), NG = blockDim.x >> ax.lshift;
-    const int c = c0 + line;
-    if (line < lines && c >= col_first)
-        for (int x = threadIdx.x >> ax.lshift; x < n; x += NG) u[(int64_t)x * mp.wu + c] = res[(int64_t)line * ld + x];
+    if constexpr (N > 0) {
+        line_ifft_tail<T, N, false>(b0, b1, lines, ax.lshift, tw, [&](int line, int x, C v) {
+            const int c = c0 + line;
+            if (c >= col_first) u[(int64_t)x * mp.wu + c] = v;
+        });
+    } else {
+        C *res = line_ifft<T, N>(b0, b1, ld, lines, ax, tw);
+        const int line = threadIdx.x & (L - 1), NG = blockDim.x >> ax.lshift;
+        const int c = c0 + line;
+        if (line < lines && c >= col_first)
+            for (int x = threadIdx.x >> ax.lshift; x < n; x += NG)
+                u[(int64_t)x * mp.wu + c] = res[(int64_t)line * ld + x];
+    }
 }
 
 // ---- S2: transform along y --------------------------------------------------------------
@@ -435,12 +535,17 @@ __global__ void __launch_bounds__(SY_THREADS) synth_y_kernel(SynthParams p, cons
         }
     }
     __syncthreads();
-    C *res = line_ifft<T, N>(b0, b1, ld, lines, ay, tw);
     C *h = H + mp.h_off + ((int64_t)kz * p.m0 + x0) * p.m1;
-    for (int line = warp; line < lines; line += nw) {
-        const C *row = res + (int64_t)line * ld;
-        C *hrow = h + (int64_t)line * p.m1;
-        for (int y = lane; y < n; y += 32) hrow[y] = row[y];
+    if constexpr (N > 0) {
+        line_ifft_tail<T, N, true>(b0, b1, lines, ay.lshift, tw,
+                                   [&](int line, int y, C v) { h[(int64_t)line * p.m1 + y] = v; });
+    } else {
+        C *res = line_ifft<T, N>(b0, b1, ld, lines, ay, tw);
+        for (int line = warp; line < lines; line += nw) {
+            const C *row = res + (int64_t)line * ld;
+            C *hrow = h + (int64_t)line * p.m1;
+            for (int y = lane; y < n; y += 32) hrow[y] = row[y];
+        }
     }
 }
 
@@ -464,14 +569,59 @@ __global__ void __launch_bounds__(SY_THREADS) synth_z_kernel(SynthParams p, cons
     const int ny = min(2 * L, p.m1 - y0);
     const int lines = (ny + 1) >> 1;
     const int K = mp.kz_max;
-    make_twiddles<T>(tw, n);
+    make_twiddles<T>(tw, n);  // made visible by the barrier after the first pass
+    const int64_t plane = (int64_t)p.m0 * p.m1;
+    T *o = out + (int64_t)m * p.m0 * p.m1 * p.m2 + ((int64_t)x * p.m1 + y0) * p.m2;
+    if constexpr (N > 0 && pass_count(N) >= 2) {
+        // first pass straight from H (a warp reads the (y, y+1) pairs of 32 lines at one kz:
+        // 512 contiguous bytes; it needs no twiddles), last pass straight to the real rows
+        const C *hb = H + mp.h_off + (int64_t)x * p.m1 + y0;
+        line_ifft_io<T, N, true>(
+            b0, b1, lines, az.lshift, tw,
+            [&](int line, int e) -> C {
+                int kz;
+                bool mirror = false;
+                if (e <= K) {
+                    kz = e;
+                } else if (e >= N - K) {
+                    kz = N - e;
+                    mirror = true;
+                } else {
+                    return cmake<T>(0.0, 0.0);
+                }
+                const C *hl = hb + 2 * line + kz * plane;
+                C a, b;
+                if constexpr (std::is_same<T, float>::value) {
+                    const float4 q = *reinterpret_cast<const float4 *>(hl);
+                    a = make_float2(q.x, q.y);
+                    b = make_float2(q.z, q.w);
+                } else {
+                    a = hl[0];
+                    b = hl[1];
+                }
+                if (kz == 0) return cmake<T>((double)a.x, (double)b.x);
+                C r;
+                if (!mirror) {
+                    r.x = a.x - b.y;
+                    r.y = a.y + b.x;
+                } else {
+                    r.x = a.x + b.y;
+                    r.y = b.x - a.y;
+                }
+                return r;
+            },
+            [&](int line, int z, C v) {
+                o[(int64_t)(2 * line) * p.m2 + z] = v.x;
+                o[(int64_t)(2 * line + 1) * p.m2 + z] = v.y;
+            });
+        return;
+    }
     // line-fastest: consecutive threads read consecutive (y, y+1) pairs of one kz row
     const int line = threadIdx.x & (L - 1), NG = blockDim.x >> az.lshift;
     if (line < lines) {
         C *d = b0 + (int64_t)line * ld;
         for (int e = (threadIdx.x >> az.lshift) + K + 1; e < n - K; e += NG) d[e] = cmake<T>(0.0, 0.0);
         const C *h = H + mp.h_off + (int64_t)x * p.m1 + y0 + 2 * line;
-        const int64_t plane = (int64_t)p.m0 * p.m1;
         const bool has_b = 2 * line + 1 < ny;
         constexpr int UB = 4;  // loads in flight per thread
         for (int kz0 = threadIdx.x >> az.lshift; kz0 <= K; kz0 += UB * NG) {
@@ -502,7 +652,6 @@ __global__ void __launch_bounds__(SY_THREADS) synth_z_kernel(SynthParams p, cons
     }
     __syncthreads();
     C *res = line_ifft<T, N>(b0, b1, ld, lines, az, tw);
-    T *o = out + (int64_t)m * p.m0 * p.m1 * p.m2 + ((int64_t)x * p.m1 + y0) * p.m2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int yy = warp; yy < ny; yy += nw) {
         const C *row = res + (int64_t)(yy >> 1) * ld;
