@@ -26,6 +26,7 @@ namespace pb {
 constexpr int SY_MAX_MAPS = 64;
 constexpr int SY_MAXF = 12;
 constexpr int SY_THREADS = 512;
+constexpr int SY_THREADS_Z = 768;  // 24 line groups: the radix-8 passes of 192 take one butterfly per thread
 constexpr int SY_SMEM_BUDGET = 100 * 1024;
 
 struct FftAxis {
@@ -551,7 +552,7 @@ __global__ void __launch_bounds__(SY_THREADS) synth_y_kernel(SynthParams p, cons
 
 // ---- S3: real transform along z, two output lines per complex transform -----------------
 template <typename T, int N>
-__global__ void __launch_bounds__(SY_THREADS) synth_z_kernel(SynthParams p, const typename cplx<T>::type *H,
+__global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, const typename cplx<T>::type *H,
                                                              T *out) {
     using C = typename cplx<T>::type;
     extern __shared__ __align__(16) unsigned char sy_smem[];
@@ -836,7 +837,7 @@ static int launch_synth(const SynthLayout &L, const typename cplx<T>::type *src,
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(synth_z_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem(p.az));
         if (e == cudaSuccess) {
-            synth_z_kernel<T, N><<<L.nb3, SY_THREADS, smem(p.az), s>>>(p, H, out);
+            synth_z_kernel<T, N><<<L.nb3, SY_THREADS_Z, smem(p.az), s>>>(p, H, out);
             e = cudaGetLastError();
         }
     });
