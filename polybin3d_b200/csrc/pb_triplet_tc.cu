@@ -510,19 +510,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(geo.tmem_cols));
 }
 
+// one warp per triplet: lanes stride over the CTA partials, then a fixed-order warp sum
+// (deterministic for a given grid)
 __global__ void triplet_tc_finalize(const double *partials, int n_cta, int n_pairs, int n_c, const int32_t *tmap,
                                     int n_trip, double scale, double *out, const int *err) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     if (t >= n_trip) return;
     if (*err) {
-        out[t] = __longlong_as_double(0x7ff8000000000000LL);  // NaN: the contraction timed out
+        if (lane == 0) out[t] = __longlong_as_double(0x7ff8000000000000LL);  // NaN: the contraction timed out
         return;
     }
     const int row = tmap[2 * t], col = tmap[2 * t + 1];
     const double *p = partials + (size_t)row * n_c + col;
     double s = 0.0;
-    for (int c = 0; c < n_cta; ++c) s += p[(size_t)c * n_pairs * n_c];
-    out[t] = s * scale;
+    for (int c = lane; c < n_cta; c += 32) s += p[(size_t)c * n_pairs * n_c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[t] = s * scale;
 }
 
 static int tc_geometry(int n_rows, int off_b, int off_c, const int32_t *counts, int n_c, TcGeom *g) {
@@ -649,7 +654,7 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
         (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
         maps[2], (const int32_t *)(table + L.off_pairs), g, partials, err);
     PB_LAUNCH_CHECK("pb_triplet_contract(tc)");
-    triplet_tc_finalize<<<(counts[3] + 255) / 256, 256, 0, s>>>(partials, gx, g.n_pairs, n_c,
+    triplet_tc_finalize<<<(counts[3] + 7) / 8, 256, 0, s>>>(partials, gx, g.n_pairs, n_c,
                                                                (const int32_t *)(table + L.off_tmap), counts[3],
                                                                scale, out, err);
     PB_LAUNCH_CHECK("pb_triplet_contract(tc finalize)");
