@@ -48,18 +48,25 @@ FISHER = {
 }
 
 
+# Bk_ideal + its gradient at 512^3: 24 bins to 0.35, lmax=2, TSC, mixed precision, streamed fields
+BK512 = dict(N=512, L=4000.0, lmax=2, edges=np.linspace(2 * np.pi / 4000.0, 0.35, 25),
+             metric="Bk_ideal + dBk/ddelta fields/s at 512^3 (24 bins, lmax=2, TSC, mixed precision)",
+             workload="Bk_ideal and its vector-Jacobian product dBk/ddelta^T v, 512^3 box 4000 Mpc/h, TSC, lmax=2, "
+                      "24 linear bins 2pi/4000..0.35, 2756 triangle bins; g-maps recomputed in the backward")
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=None)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="bk256", choices=["bk256"] + sorted(FISHER))
+    p.add_argument("--workload", default="bk256", choices=["bk256", "bk512grad"] + sorted(FISHER))
     p.add_argument("--contraction", default="auto", choices=["auto", "tc", "simt"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     a = p.parse_args()
     if a.steps is None:
-        a.steps = 50 if a.workload == "bk256" else 6
+        a.steps = {"bk256": 50, "bk512grad": 16}.get(a.workload, 6)
     return a
 
 
@@ -508,10 +515,109 @@ def run_fisher(args, rank, world, local):
         torch.distributed.destroy_process_group()
 
 
+def run_bk512(args, rank, world, local):
+    """Forward + gradient at 512^3: per field, Bk = F_ideal^-1 num(d) and the VJP J^T v
+    (v a fixed random cotangent) through polybin3d_b200.autograd.BkNumerator."""
+    import contextlib
+    import io
+
+    import torch
+    import polybin3d_b200 as pb
+    from polybin3d_b200 import _native as nat
+    from polybin3d_b200 import synthetic
+    from polybin3d_b200.autograd import bk_numerator
+
+    cfg = BK512
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient path; its 512^3 "
+                              "numerator needs 48 FP64 maps (48 GB of host memory) per field"}))
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    N, L = cfg["N"], cfg["L"]
+    with contextlib.redirect_stdout(io.StringIO()):
+        base = pb.PolyBin3D([L] * 3, [N] * 3, pixel_window="tsc", backend="cuda", precision="mixed")
+        bs = pb.BSpec(base, cfg["edges"], lmax=cfg["lmax"], contraction=args.contraction)
+        t0 = time.perf_counter()
+        bs.compute_fisher_ideal()  # one-off, cached (as the reference caches it)
+        t_fisher = time.perf_counter() - t0
+    inv_fish = torch.as_tensor(bs.inv_fish_ideal, device=dev)
+    n_pool = 2
+    host = [torch.from_numpy(synthetic.lognormal(N, L, seed=1000 * rank + s)).pin_memory() for s in range(n_pool)]
+    resident = [h.to(dev) for h in host]
+    v = torch.as_tensor(np.random.default_rng(0).standard_normal(bs.N_bins), device=dev)
+
+    def step(x):
+        x = x.detach().requires_grad_(True)
+        bk = inv_fish @ bk_numerator(bs, x)
+        (g,) = torch.autograd.grad(bk, x, grad_outputs=v)
+        return bk.detach(), g
+
+    for i in range(args.warmup):
+        step(resident[i % n_pool])
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = nat.LAUNCHES[0]
+    with Clocks(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(args.steps):
+            step(resident[i % n_pool])
+        e1.record()
+        torch.cuda.synchronize()
+    launches = nat.LAUNCHES[0] - l0
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * args.steps / (ms / 1000.0)
+    # end to end: pinned host field in, Bk and the gradient map back to pinned host memory
+    g_host = torch.empty((N, N, N), dtype=torch.float32).pin_memory()
+    bk_host = torch.empty(bs.N_bins, dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(args.steps):
+        x = host[i % n_pool].to(dev, non_blocking=True)
+        bk, g = step(x)
+        bk_host.copy_(bk, non_blocking=True)
+        g_host.copy_(g, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    if rank == 0:
+        print(json.dumps({"metric": cfg["metric"], "value": value, "unit": "fields/s", "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f32 maps / fp64 sums", "data": "synthetic (seeded float32 lognormal fields)",
+                          "config": {"workload": cfg["workload"], "n_bins": bs.N_bins, "maps": bs.Nl * bs.Nk_squeeze,
+                                     "map_grid": list(bs.map_grid), "ideal_fisher_setup_s": t_fisher,
+                                     "l2": "inputs+intermediates > 40 GB/step >> 126 MB L2",
+                                     "parallelism": "replicas" if world > 1 else "single GPU"},
+                          "e2e": {"value": world * args.steps / (e2e_ms / 1000.0), "unit": "fields/s",
+                                  "h2d_bytes_per_step": N ** 3 * 4, "d2h_bytes_per_step": N ** 3 * 4 + bs.N_bins * 8},
+                          "gpu_launches": launches, "clocks": clk.summary()}))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args)
-    if args.workload != "bk256":
+    if args.workload == "bk512grad":
+        run_bk512(args, rank, world, local)
+    elif args.workload != "bk256":
         run_fisher(args, rank, world, local)
     elif args.impl == "reference":
         run_reference(args, rank, world)

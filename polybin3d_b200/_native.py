@@ -21,6 +21,7 @@ PB_TRIPLET_SIMT, PB_TRIPLET_TC = 0, 1
 PB_EW_MUL, PB_EW_PRODDIFF = 0, 1
 FILTER_MAX_MAPS = 128
 SYNTH_MAX_MAPS = 64
+SYNTH_WS_BYTES = 8 << 30  # transform workspace per pb_shell_synth call
 
 _ERRORS = {-1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: MemoryError, -5: NotImplementedError,
            -6: TimeoutError}
@@ -343,8 +344,19 @@ def shell_synth(grid, precision, src, out, maps, out_n, ws, w=None, src_stride=N
     lib = load()
     on = np.ascontiguousarray(out_n, dtype=np.int32)
     stride = src_stride if src_stride is not None else (src[0].numel() if src is not None and src.dim() == 4 else 0)
-    for c0 in range(0, len(maps), SYNTH_MAX_MAPS):
-        chunk = maps[c0:c0 + SYNTH_MAX_MAPS]
+    c0 = 0
+    while c0 < len(maps):
+        # at most 64 maps, and fewer while the transform workspace would exceed SYNTH_WS_BYTES
+        nc = min(SYNTH_MAX_MAPS, len(maps) - c0)
+        while True:
+            hi_c = np.ascontiguousarray(np.asarray(maps[c0:c0 + nc], dtype=np.float64)[:, 2])
+            nbytes = ctypes.c_size_t()
+            check(lib.pb_shell_synth_workspace_size(ctypes.byref(grid), hptr(on), precision, nc, hptr(hi_c),
+                                                    ctypes.byref(nbytes)), "pb_shell_synth_workspace_size")
+            if nbytes.value <= SYNTH_WS_BYTES or nc == 1:
+                break
+            nc = (nc + 1) // 2
+        chunk = maps[c0:c0 + nc]
         arr = np.asarray(chunk, dtype=np.float64)
         si = np.ascontiguousarray(arr[:, 0].astype(np.int32))
         lo = np.ascontiguousarray(arr[:, 1])
@@ -361,4 +373,5 @@ def shell_synth(grid, precision, src, out, maps, out_n, ws, w=None, src_stride=N
                                  hptr(lo), hptr(hi), hptr(l1), hptr(l2), hptr(sc), hptr(wp), ptr(w),
                                  ptr(out[c0:c0 + len(chunk)]), ptr(buf), buf.numel(), stream_ptr()), "pb_shell_synth")
         _count(3)
+        c0 += nc
     return out

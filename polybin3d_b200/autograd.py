@@ -26,10 +26,16 @@ import torch
 from . import _native as nat
 
 
-def _mask_of(est):
+def _mask_of(est, dtype=torch.float64):
     if est.const_mask:
         return None
-    return est._mask_device()
+    if dtype == torch.float64:
+        return est._mask_device()
+    return est.base.to_device_grid(('mask', id(est)), lambda: est.mask, dtype)
+
+
+# device bytes the Bk backward may hold in pair products and their spectra at once
+KEY_CHUNK_BYTES = 16 << 30
 
 
 class PkNumerator(torch.autograd.Function):
@@ -81,25 +87,28 @@ class PkNumerator(torch.autograd.Function):
 
 class BkNumerator(torch.autograd.Function):
     """num = BkNumerator.apply(d, bspec): the unwindowed numerator (no linear term) of data
-    m*d as a differentiable FP64 device tensor (N_bins,)."""
+    m*d as a differentiable FP64 device tensor (N_bins,).  Maps, transforms and the gradient
+    run in the base's precision (FP64, or FP32 with precision='mixed'); the cubic sums are
+    FP64 either way."""
 
     @staticmethod
     def _maps(bs, d):
         b = bs.base
-        m = _mask_of(bs)
+        m = _mask_of(bs, d.dtype)
         y = d if m is None else nat.elementwise(nat.PB_EW_MUL, d, m)
         xk = b.fft_r2c(y)
         b.n_FFTs_forward += 1
         w = None
         if b.pixel_window != 'none':
-            w = b.to_device_grid(('bk_invwin', id(bs)), lambda: bs._inv_window(), torch.float64)
+            w = b.to_device_grid(('bk_invwin', id(bs)), lambda: bs._inv_window(), d.dtype)
         return bs._g_maps(xk, w, 1.0)
 
     @staticmethod
     def forward(ctx, d, bs):
         if not hasattr(bs, 'sym_factor'):
             bs._compute_symmetry_factor()
-        d = d.to(torch.float64).contiguous()
+        ctx.in_dtype = d.dtype
+        d = d.to(bs.base.real_dtype).contiguous()
         ctx.bs = bs
         ctx.save_for_backward(d)
         G = BkNumerator._maps(bs, d)
@@ -112,6 +121,9 @@ class BkNumerator(torch.autograd.Function):
         bs = ctx.bs
         b = bs.base
         (d,) = ctx.saved_tensors
+        rd = d.dtype
+        prec = nat.precision_of(rd)
+        cd = torch.complex128 if rd == torch.float64 else torch.complex64
         G = BkNumerator._maps(bs, d)  # recomputed, not stored
         Mdims = tuple(int(n) for n in G.shape[1:])
         nks = bs.Nk_squeeze
@@ -134,24 +146,35 @@ class BkNumerator(torch.autograd.Function):
             c3 = (l // 2) * nks + b3
             for (kk, C, lc) in ((key_of(b2, c3), b1, 0), (key_of(b1, c3), b2, 0), (key_of(b1, b2), b3, l)):
                 legs[(kk, C, lc)] = legs.get((kk, C, lc), 0.0) + coef[t]
-        grad_spec = torch.zeros((1,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+        grad_spec = torch.zeros((1,) + b.nhalf_shape, dtype=cd, device=b.device)
         if keys:
             pairs = sorted(keys, key=keys.get)
-            prods = nat.pair_products(G, G, pairs)
-            FT = b.fft_r2c(prods)
-            b.n_FFTs_forward += len(pairs)
-            entries = [(kk, ks[C], ks[C + 1], lc, 0, v, 0) for (kk, C, lc), v in legs.items()]
-            nat.spectral_filter(b.grid_of(Mdims), nat.PB_F64, FT, grad_spec, entries, accumulate=True,
-                                src_stride=FT[0].numel(), out_n=[int(n) for n in b.gridsize], dst=[0] * len(entries))
+            by_key = {}
+            for (kk, C, lc), v in legs.items():
+                by_key.setdefault(kk, []).append((ks[C], ks[C + 1], lc, v))
+            # pair products and their spectra in chunks of keys (bounded device memory)
+            per_key = G[0].numel() * G.element_size() * 2
+            chunk = int(max(1, min(len(pairs), KEY_CHUNK_BYTES // per_key)))
+            for k0 in range(0, len(pairs), chunk):
+                k1 = min(len(pairs), k0 + chunk)
+                prods = nat.pair_products(G, G, pairs[k0:k1])
+                FT = b.fft_r2c(prods)
+                del prods
+                b.n_FFTs_forward += k1 - k0
+                entries = [(kk - k0, lo, hi, lc, 0, v, 0) for kk in range(k0, k1) for (lo, hi, lc, v) in by_key[kk]]
+                nat.spectral_filter(b.grid_of(Mdims), prec, FT, grad_spec, entries, accumulate=True,
+                                    src_stride=FT[0].numel(), out_n=[int(n) for n in b.gridsize],
+                                    dst=[0] * len(entries))
+                del FT
         if b.pixel_window != 'none':
-            w = b.to_device_grid('window', lambda: b.pixel_window_grid, torch.float64)
-            nat.spectral_filter(b.grid, nat.PB_F64, grad_spec, grad_spec, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
+            w = b.to_device_grid('window', lambda: b.pixel_window_grid, rd)
+            nat.spectral_filter(b.grid, prec, grad_spec, grad_spec, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
         grad = b.fft_c2r(grad_spec)[0]
         b.n_FFTs_reverse += 1
-        m = _mask_of(bs)
+        m = _mask_of(bs, rd)
         if m is not None:
             grad = nat.elementwise(nat.PB_EW_MUL, grad, m, out=grad)
-        return grad, None
+        return grad.to(ctx.in_dtype), None
 
 
 def pk_numerator(ps, d):

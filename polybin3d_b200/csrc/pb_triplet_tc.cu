@@ -511,9 +511,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // one warp per triplet: lanes stride over the CTA partials, then a fixed-order warp sum
-// (deterministic for a given grid)
-__global__ void triplet_tc_finalize(const double *partials, int n_cta, int n_pairs, int n_c, const int32_t *tmap,
-                                    int n_trip, double scale, double *out, const int *err) {
+// (deterministic for a given grid).  Pairs were contracted in chunks of `chunk` pairs: the
+// partials of chunk k start at n_cta * k * chunk * n_c, one [pairs of the chunk][n_c] block
+// per CTA.
+__global__ void triplet_tc_finalize(const double *partials, int n_cta, int n_pairs, int chunk, int n_c,
+                                    const int32_t *tmap, int n_trip, double scale, double *out, const int *err) {
     const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (t >= n_trip) return;
@@ -522,20 +524,22 @@ __global__ void triplet_tc_finalize(const double *partials, int n_cta, int n_pai
         return;
     }
     const int row = tmap[2 * t], col = tmap[2 * t + 1];
-    const double *p = partials + (size_t)row * n_c + col;
+    const int k = row / chunk, p_lo = k * chunk;
+    const int pk = min(chunk, n_pairs - p_lo);
+    const double *p = partials + (size_t)n_cta * p_lo * n_c + (size_t)(row - p_lo) * n_c + col;
     double s = 0.0;
-    for (int c = lane; c < n_cta; c += 32) s += p[(size_t)c * n_pairs * n_c];
+    for (int c = lane; c < n_cta; c += 32) s += p[(size_t)c * pk * n_c];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) out[t] = s * scale;
 }
 
-static int tc_geometry(int n_rows, int off_b, int off_c, const int32_t *counts, int n_c, TcGeom *g) {
+static int tc_geometry(int n_rows, int off_b, int off_c, int n_pairs, int n_c, TcGeom *g) {
     memset(g, 0, sizeof(*g));
     g->n_rows = n_rows;
     g->off_b = off_b;
     g->off_c = off_c;
-    g->n_pairs = counts[1];
+    g->n_pairs = n_pairs;
     g->n_c = n_c;
     if (n_c > TC_MAX_NC) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 64 C maps");
     g->M = (2 * n_c <= 64) ? 64 : 128;
@@ -616,11 +620,19 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
     else if (C == B && n_c == n_b) off_c = off_b;
     else off_c = after_b;
     int n_rows = (off_c == after_b) ? after_b + n_c : after_b;
+    // pairs go through in chunks small enough for shared memory and TMEM (the FP64
+    // accumulators and the pair operands grow with the pair count)
+    const int n_pairs = counts[1];
     TcGeom g;
-    int st = tc_geometry(n_rows, off_b, off_c, counts, n_c, &g);
+    int chunk = std::min(n_pairs, 512);
+    int st = tc_geometry(n_rows, off_b, off_c, chunk, n_c, &g);
+    while (st == PB_ERR_UNSUPPORTED && chunk > 16 && n_c <= TC_MAX_NC) {
+        chunk = (chunk + 1) / 2;
+        st = tc_geometry(n_rows, off_b, off_c, chunk, n_c, &g);
+    }
     if (st) return st;
     int gx = tc_grid(n_vox);
-    size_t need = 256 + (size_t)gx * g.n_pairs * n_c * sizeof(double);
+    size_t need = 256 + (size_t)gx * n_pairs * n_c * sizeof(double);
     if (!workspace || workspace_bytes < need)
         return fail(PB_ERR_WORKSPACE, "pb_triplet_contract(tc): workspace too small (need " + std::to_string(need) + ")");
     int *err = (int *)workspace;
@@ -649,12 +661,23 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
     }
     TableLayout L = table_layout(counts);
     PB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-    PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g.smem_bytes));
-    triplet_tc_kernel<<<gx, TC_THREADS, g.smem_bytes, s>>>(
-        (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
-        maps[2], (const int32_t *)(table + L.off_pairs), g, partials, err);
-    PB_LAUNCH_CHECK("pb_triplet_contract(tc)");
-    triplet_tc_finalize<<<(counts[3] + 7) / 8, 256, 0, s>>>(partials, gx, g.n_pairs, n_c,
+    const int32_t *pairs = (const int32_t *)(table + L.off_pairs);
+    int smem_max = 0;
+    for (int p_lo = 0; p_lo < n_pairs; p_lo += chunk) {
+        const int pk = std::min(chunk, n_pairs - p_lo);
+        TcGeom gk;
+        st = tc_geometry(n_rows, off_b, off_c, pk, n_c, &gk);
+        if (st) return st;
+        if (gk.smem_bytes > smem_max) {
+            PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, gk.smem_bytes));
+            smem_max = gk.smem_bytes;
+        }
+        triplet_tc_kernel<<<gx, TC_THREADS, gk.smem_bytes, s>>>(
+            (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
+            maps[2], pairs + 2 * p_lo, gk, partials + (size_t)gx * p_lo * n_c, err);
+        PB_LAUNCH_CHECK("pb_triplet_contract(tc)");
+    }
+    triplet_tc_finalize<<<(counts[3] + 7) / 8, 256, 0, s>>>(partials, gx, n_pairs, chunk, n_c,
                                                                (const int32_t *)(table + L.off_tmap), counts[3],
                                                                scale, out, err);
     PB_LAUNCH_CHECK("pb_triplet_contract(tc finalize)");

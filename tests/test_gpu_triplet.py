@@ -71,3 +71,24 @@ def test_distinct_map_sets():
     if nat.tc_built() and torch.cuda.get_device_capability()[0] == 10:
         plan.contract(A, B, C, out, ws, method=nat.PB_TRIPLET_TC)
         assert np.max(np.abs(out.cpu().numpy() - ref)) / scale < 2e-5
+
+
+def test_tc_pair_chunks():
+    """300 (b1, b2) pairs x 48 maps (24 bins, lmax=2): the FP64 accumulators and pair operands
+    exceed shared memory in one launch, so the tensor-core form runs the pairs in chunks."""
+    torch.manual_seed(2)
+    idx = bk_like_triplets(nk=24, lmax=2)
+    n_vox = 48 ** 3
+    G = torch.randn(48, n_vox, device="cuda", dtype=torch.float32)
+    ref = reference(G, G, G, torch.as_tensor(idx, device="cuda").long()).cpu().numpy()
+    ws = nat.Workspace(torch.device("cuda"))
+    plan = nat.TripletPlan(48, 48, 48, idx, torch.device("cuda"))
+    assert plan.n_pairs == 300
+    out = torch.empty(len(idx), dtype=torch.float64, device="cuda")
+    scale = np.max(np.abs(ref))
+    if nat.tc_built() and torch.cuda.get_device_capability()[0] == 10:
+        for _ in range(2):
+            plan.contract(G, G, G, out, ws, method=nat.PB_TRIPLET_TC)
+            got = out.cpu().numpy()
+            assert np.all(np.isfinite(got))
+            assert np.max(np.abs(got - ref)) / scale < 2e-5
