@@ -34,6 +34,14 @@ def _mask_of(est, dtype=torch.float64):
     return est.base.to_device_grid(('mask', id(est)), lambda: est.mask, dtype)
 
 
+def _settle():
+    """Backward runs on autograd's device thread.  On B200 a cuFFT transform issued from that
+    thread while the forward's kernels were still running returned CUFFT_EXEC_FAILED (seen at
+    512^3, where the forward's contraction runs for tens of ms); waiting for the stream first
+    avoids it.  The wait costs nothing measurable next to a backward pass."""
+    torch.cuda.current_stream().synchronize()
+
+
 # device bytes the Bk backward may hold in pair products and their spectra at once
 KEY_CHUNK_BYTES = 16 << 30
 
@@ -64,6 +72,7 @@ class PkNumerator(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
+        _settle()
         ps = ctx.ps
         b = ps.base
         (d,) = ctx.saved_tensors
@@ -118,6 +127,7 @@ class BkNumerator(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
+        _settle()
         bs = ctx.bs
         b = bs.base
         (d,) = ctx.saved_tensors

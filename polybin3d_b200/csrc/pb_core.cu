@@ -216,10 +216,17 @@ static const char *cufft_name(cufftResult r) {
     }
 }
 
+// a failed cuFFT call reports the CUDA runtime's pending error too (a launch failure such as
+// out-of-resources shows up there)
 #define PB_CUFFT(call)                                                                 \
     do {                                                                               \
         cufftResult _r = (call);                                                       \
-        if (_r != CUFFT_SUCCESS) return fail(PB_ERR_CUFFT, std::string(#call ": ") + cufft_name(_r)); \
+        if (_r != CUFFT_SUCCESS) {                                                     \
+            cudaError_t _e = cudaGetLastError();                                       \
+            return fail(PB_ERR_CUFFT, std::string(#call ": ") + cufft_name(_r) +      \
+                                          (_e != cudaSuccess ? std::string(" (CUDA: ") + cudaGetErrorString(_e) + ")" \
+                                                             : std::string()));        \
+        }                                                                              \
     } while (0)
 
 extern "C" int pb_fft_plan_create(const pb_grid_t *g, int batch, int precision, int direction,
@@ -263,6 +270,12 @@ extern "C" int pb_fft_plan_create(const pb_grid_t *g, int batch, int precision, 
 extern "C" int pb_fft_exec(pb_fft_plan *p, const void *in, void *out, void *workspace, void *stream) {
     if (!p || !in || !out) return fail(PB_ERR_INVALID, "pb_fft_exec: NULL argument");
     if (p->ws && !workspace) return fail(PB_ERR_WORKSPACE, "pb_fft_exec: plan needs a workspace");
+    {
+        // an error left pending by earlier work on this thread would otherwise surface as a
+        // failure of this transform
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_check(e, "pb_fft_exec (error pending before the transform)");
+    }
     PB_CUFFT(cufftSetStream(p->h, as_stream(stream)));
     if (p->ws) PB_CUFFT(cufftSetWorkArea(p->h, workspace));
     void *i = const_cast<void *>(in);
