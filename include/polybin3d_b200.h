@@ -182,6 +182,26 @@ PB_API int pb_triplet_contract(int precision, int method, const void *A, int n_a
                                size_t workspace_bytes, void *stream);
 
 /* ---------------------------------------------------------------------------------- */
+/* Bilinear maps (the adjoint of the triplet contraction with respect to its maps):       */
+/*   out[o](x) = sum_t [o_t == o] c_t G[i_t](x) G[j_t](x)                                  */
+/* The derivative of sum_t gamma_t sum_x G_a G_b G_c with respect to map G_o gathers, per */
+/* output map, every leg ending on it: one map per leg instead of one product map per pair */
+/* of maps, so the bispectrum gradient needs one forward transform per (bin, multipole)    */
+/* leg instead of one per pair (the per-pair Q-map construction of PolyBin3D/bspec.py:     */
+/* 600-640, as used for the autograd backward).                                           */
+/* pb_bilinear_plan (host only) validates the host term lists (o < n_out, i, j < n_g),     */
+/* merges duplicates and writes a table (call with table == NULL for its size and term    */
+/* count n_table); copy it to 16-byte aligned device memory and pass it with n_table and   */
+/* the same n_g and n_out to pb_bilinear_maps.  G: n_g real maps of n_vox voxels; out:     */
+/* n_out maps, every one written (zeros where an output has no term).  At most 128 maps    */
+/* and 4096 outputs.                                                                       */
+/* ---------------------------------------------------------------------------------- */
+PB_API int pb_bilinear_plan(int n_g, int n_out, const int32_t *o, const int32_t *i, const int32_t *j,
+                            const double *c, int n_terms, void *table, size_t *table_bytes, int32_t *n_table);
+PB_API int pb_bilinear_maps(int precision, int64_t n_vox, const void *G, int n_g, const void *table, int n_table,
+                            int n_out, void *out, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
 /* Real-space elementwise products.                                                      */
 /*   PB_EW_MUL      : out = s * x * y                  (prod_real, utils.pyx:248-260)     */
 /*   PB_EW_PRODDIFF : out = s * (x*y - z*u)            (prod_real_diff, utils.pyx:371-383)*/

@@ -49,6 +49,8 @@ SIGNATURES = {
     "pb_fft_plan_destroy": ([_P], _I),
     "pb_spectral_filter": ([_GP, _P, _I, _P, _I64, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P], _I),
     "pb_binned_filter": ([_GP, _I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _D, _P], _I),
+    "pb_bilinear_plan": ([_I, _I, _P, _P, _P, _P, _I, _P, ctypes.POINTER(_SZ), _P], _I),
+    "pb_bilinear_maps": ([_I, _I64, _P, _I, _P, _I, _I, _P, _P], _I),
     "pb_shell_synth_workspace_size": ([_GP, _P, _I, _I, _P, ctypes.POINTER(_SZ)], _I),
     "pb_shell_synth": ([_GP, _P, _I, _P, _I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P], _I),
     "pb_bin_reduce_workspace_size": ([_GP, _I, _I, _I, ctypes.POINTER(_SZ)], _I),
@@ -375,3 +377,34 @@ def shell_synth(grid, precision, src, out, maps, out_n, ws, w=None, src_stride=N
         _count(3)
         c0 += nc
     return out
+
+
+class BilinearPlan:
+    """Device table of pb_bilinear_plan for host terms (o, i, j, c)."""
+
+    def __init__(self, n_g, n_out, o, i, j, c, device):
+        lib = load()
+        o = np.ascontiguousarray(o, dtype=np.int32)
+        i = np.ascontiguousarray(i, dtype=np.int32)
+        j = np.ascontiguousarray(j, dtype=np.int32)
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        nbytes = ctypes.c_size_t()
+        n = np.zeros(1, dtype=np.int32)
+        check(lib.pb_bilinear_plan(n_g, n_out, hptr(o), hptr(i), hptr(j), hptr(c), len(o), None, ctypes.byref(nbytes),
+                                   hptr(n)), "pb_bilinear_plan")
+        host = np.zeros(nbytes.value, dtype=np.uint8)
+        check(lib.pb_bilinear_plan(n_g, n_out, hptr(o), hptr(i), hptr(j), hptr(c), len(o), hptr(host),
+                                   ctypes.byref(nbytes), hptr(n)), "pb_bilinear_plan")
+        self.n_g, self.n_out, self.n_table = n_g, n_out, int(n[0])
+        self.table = torch.from_numpy(host).to(device)
+
+    def maps(self, G, out=None):
+        """out[o] = sum_t c_t G[i_t] G[j_t]; G (n_g, ...) real maps."""
+        if G.shape[0] != self.n_g:
+            raise ValueError("BilinearPlan.maps: the plan was built for %d maps" % self.n_g)
+        if out is None:
+            out = torch.empty((self.n_out,) + tuple(G.shape[1:]), dtype=G.dtype, device=G.device)
+        check(load().pb_bilinear_maps(precision_of(G.dtype), G[0].numel(), ptr(G), self.n_g, ptr(self.table),
+                                      self.n_table, self.n_out, ptr(out), stream_ptr()), "pb_bilinear_maps")
+        _count(1)
+        return out

@@ -15,9 +15,10 @@ For the bispectrum (PolyBin3D/bspec.py:895-983, no linear term) the numerator is
 V/(N^3 sym_i) sum_x g_b1 g_b2 g_{l,b3} with g_{l,b} = irfftn(Theta_b L_l rfftn(m d) / W);
 its derivative is the sum over the three legs of irfftn(Theta_leg L_leg / W FT[product of the
 other two maps]) times m, the same construction as the reference's Q-maps (bspec.py:600-640).
-The backward recomputes the bin-filtered maps (nothing is stored by the forward), forms the
-pair products with pb_pair_products, transforms them, and gathers every leg into one
-spectrum with the accumulating spectral filter.  Maps, products and their transforms live
+The backward recomputes the bin-filtered maps (nothing is stored by the forward), sums, in
+real space, the products of the other two maps of every leg that ends on the same (bin,
+multipole) with pb_bilinear_maps (one map per leg instead of one per pair of maps),
+transforms those, and gathers them into one spectrum with the accumulating spectral filter.  Maps, products and their transforms live
 on the dealiased map grid, which is exact for every frequency inside the bins.
 """
 import numpy as np
@@ -158,20 +159,24 @@ class BkNumerator(torch.autograd.Function):
                 legs[(kk, C, lc)] = legs.get((kk, C, lc), 0.0) + coef[t]
         grad_spec = torch.zeros((1,) + b.nhalf_shape, dtype=cd, device=b.device)
         if keys:
+            # one real-space map per leg (bin C, multipole lc): the coefficient-weighted sum of
+            # the products of the other two maps of every triplet ending on it (pb_bilinear_maps);
+            # then one forward transform per leg and one accumulating filter into the gradient
             pairs = sorted(keys, key=keys.get)
-            by_key = {}
-            for (kk, C, lc), v in legs.items():
-                by_key.setdefault(kk, []).append((ks[C], ks[C + 1], lc, v))
-            # pair products and their spectra in chunks of keys (bounded device memory)
-            per_key = G[0].numel() * G.element_size() * 2
-            chunk = int(max(1, min(len(pairs), KEY_CHUNK_BYTES // per_key)))
-            for k0 in range(0, len(pairs), chunk):
-                k1 = min(len(pairs), k0 + chunk)
-                prods = nat.pair_products(G, G, pairs[k0:k1])
-                FT = b.fft_r2c(prods)
-                del prods
-                b.n_FFTs_forward += k1 - k0
-                entries = [(kk - k0, lo, hi, lc, 0, v, 0) for kk in range(k0, k1) for (lo, hi, lc, v) in by_key[kk]]
+            outs = sorted({(C, lc) for (kk, C, lc) in legs})
+            opos = {oc: n for n, oc in enumerate(outs)}
+            tl = [(opos[(C, lc)], pairs[kk][0], pairs[kk][1], v) for (kk, C, lc), v in legs.items()]
+            plan = nat.BilinearPlan(G.shape[0], len(outs), [t[0] for t in tl], [t[1] for t in tl],
+                                    [t[2] for t in tl], [t[3] for t in tl], b.device)
+            R = plan.maps(G)
+            del G
+            per_out = R[0].numel() * R.element_size() * 2
+            chunk = int(max(1, min(len(outs), KEY_CHUNK_BYTES // per_out)))
+            for o0 in range(0, len(outs), chunk):
+                o1 = min(len(outs), o0 + chunk)
+                FT = b.fft_r2c(R[o0:o1])
+                b.n_FFTs_forward += o1 - o0
+                entries = [(n - o0, ks[C], ks[C + 1], lc, 0, 1.0, 0) for n, (C, lc) in enumerate(outs[o0:o1], o0)]
                 nat.spectral_filter(b.grid_of(Mdims), prec, FT, grad_spec, entries, accumulate=True,
                                     src_stride=FT[0].numel(), out_n=[int(n) for n in b.gridsize],
                                     dst=[0] * len(entries))

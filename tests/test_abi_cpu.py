@@ -117,3 +117,35 @@ def test_triplet_plan_rejects_out_of_range():
     counts = np.zeros(4, dtype=np.int32)
     st = lib.pb_triplet_plan(4, 4, 4, nat.hptr(idx), 1, None, ctypes.byref(nb), nat.hptr(counts))
     assert st == -1 and b"out of range" in lib.pb_last_error()
+
+
+def test_bilinear_plan_host_logic():
+    """pb_bilinear_plan: i <= j canonical order, duplicates merged, empty outputs get a zero
+    term, out-of-range indices refused (host only)."""
+    import ctypes
+    from polybin3d_b200 import _native as nat
+    lib = nat.load()
+    o = np.array([1, 1, 0, 1], dtype=np.int32)
+    i = np.array([3, 0, 2, 3], dtype=np.int32)
+    j = np.array([0, 3, 2, 0], dtype=np.int32)
+    c = np.array([1.0, 2.0, 0.5, 4.0])
+    nb = ctypes.c_size_t()
+    n = np.zeros(1, dtype=np.int32)
+    assert lib.pb_bilinear_plan(4, 3, nat.hptr(o), nat.hptr(i), nat.hptr(j), nat.hptr(c), 4, None,
+                                ctypes.byref(nb), nat.hptr(n)) == 0
+    buf = np.zeros(nb.value, dtype=np.uint8)
+    assert lib.pb_bilinear_plan(4, 3, nat.hptr(o), nat.hptr(i), nat.hptr(j), nat.hptr(c), 4, nat.hptr(buf),
+                                ctypes.byref(nb), nat.hptr(n)) == 0
+    k = int(n[0])
+    head = ((3 + 1) * 4 + 15) // 16 * 16
+    offs = buf[:16].view(np.int32)[:4]
+    assert list(offs) == [0, 1, 2, 2]                     # output 2 has no term
+    rec = buf[head:].reshape(k, 16)
+    code = rec[:, :4].copy().view(np.uint32)[:, 0]
+    coef = rec[:, 8:].copy().view(np.float64)[:, 0]
+    rows = [(int((x >> 8) & 0xFF), int(x & 0xFF), float(e)) for x, e in zip(code, coef)]
+    assert rows == [(2, 2, 0.5), (0, 3, 7.0)]
+    assert [int((x >> 16) & 1) for x in code] == [1, 1]
+    bad = np.array([5], dtype=np.int32)
+    assert lib.pb_bilinear_plan(4, 3, nat.hptr(o[:1]), nat.hptr(bad), nat.hptr(j[:1]), nat.hptr(c[:1]), 1, None,
+                                ctypes.byref(nb), nat.hptr(n)) != 0

@@ -92,3 +92,26 @@ def test_tc_pair_chunks():
             got = out.cpu().numpy()
             assert np.all(np.isfinite(got))
             assert np.max(np.abs(got - ref)) / scale < 2e-5
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 1e-5)])
+def test_bilinear_maps(dtype, tol):
+    """pb_bilinear_maps against a torch sum of products (ragged voxel count, repeated and
+    reversed pairs, an output with no terms)."""
+    torch.manual_seed(3)
+    n_g, n_out, n_vox = 20, 6, 33_333
+    G = torch.randn(n_g, n_vox, device="cuda", dtype=torch.float64)
+    rng = np.random.default_rng(3)
+    n_t = 300
+    o = rng.integers(0, n_out - 1, n_t)          # output n_out-1 gets no term
+    i = rng.integers(0, n_g, n_t)
+    j = rng.integers(0, n_g, n_t)
+    c = rng.standard_normal(n_t)
+    ref = torch.zeros(n_out, n_vox, dtype=torch.float64, device="cuda")
+    for a, b, d, e in zip(o, i, j, c):
+        ref[a] += e * G[b] * G[d]
+    plan = nat.BilinearPlan(n_g, n_out, o, i, j, c, torch.device("cuda"))
+    out = plan.maps(G.to(dtype)).double()
+    scale = ref.abs().max()
+    assert float((out - ref).abs().max() / scale) < tol
+    assert float(out[n_out - 1].abs().max()) == 0.0
