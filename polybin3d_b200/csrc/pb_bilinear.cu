@@ -5,9 +5,9 @@
 // the other two maps; gathering all legs that end on the same output into one real-space
 // map leaves one forward transform per output instead of one per (pair of maps).
 //
-// A block stages a tile of BL_TILE voxels of every input map in shared memory as
+// A block stages a tile of 32 BL_V voxels of every input map in shared memory as
 // [map][voxel]; its warps take the outputs round-robin, lane l owning tile voxels l, l+32,
-// l+64 and l+96 (a warp reads one map at 32 consecutive voxels: one wavefront).  An
+// ..., l+32(BL_V-1) (a warp reads one map at 32 consecutive voxels: one wavefront).  An
 // output's terms are sorted by (i, j): per i-group a lane accumulates s = sum_j c G_j, then
 // acc += G_i s.  Term records are read by the whole warp at once (a broadcast load) and stay
 // in L1 across tiles; four blocks per SM keep enough warps in flight to cover their latency.
@@ -19,7 +19,6 @@
 namespace pb {
 
 constexpr int BL_THREADS = 256;
-constexpr int BL_TILE = 128;      // voxels per tile (4 per lane)
 constexpr int BL_MAXG = 128;      // input maps
 constexpr int BL_MAXOUT = 4096;   // outputs
 
@@ -38,11 +37,13 @@ __device__ __forceinline__ float term_coef<float>(const BlTerm &r) { return r.cf
 template <>
 __device__ __forceinline__ double term_coef<double>(const BlTerm &r) { return r.c; }
 
-template <typename T>
+// BL_V voxels per lane (8 in FP32, 4 in FP64: the same registers), tile = 32 BL_V voxels
+template <typename T, int BL_V>
 __global__ void __launch_bounds__(BL_THREADS, 4) bilinear_kernel(const T *G, int n_g, int64_t n_vox,
                                                                  const int32_t *offs, const BlTerm *rec, int n_out,
                                                                  T *out) {
     extern __shared__ __align__(16) unsigned char bl_smem[];
+    constexpr int BL_TILE = 32 * BL_V;
     T *sg = reinterpret_cast<T *>(bl_smem);  // [map][BL_TILE]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = BL_THREADS >> 5;
     for (int64_t v0 = (int64_t)blockIdx.x * BL_TILE; v0 < n_vox; v0 += (int64_t)gridDim.x * BL_TILE) {
@@ -53,29 +54,29 @@ __global__ void __launch_bounds__(BL_THREADS, 4) bilinear_kernel(const T *G, int
         }
         __syncthreads();
         for (int o = warp; o < n_out; o += nw) {
-            T acc[4], s[4], gi[4];
+            T acc[BL_V], s[BL_V], gi[BL_V];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) acc[u] = s[u] = gi[u] = (T)0;
+            for (int u = 0; u < BL_V; ++u) acc[u] = s[u] = gi[u] = (T)0;
             const int r1 = offs[o + 1];
             for (int r = offs[o]; r < r1; ++r) {
                 const BlTerm t = rec[r];
                 if (t.code & (1u << 16)) {
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
+                    for (int u = 0; u < BL_V; ++u) {
                         acc[u] += gi[u] * s[u];
                         s[u] = (T)0;
                     }
                     const T *gr = sg + ((t.code >> 8) & 0xFF) * BL_TILE + lane;
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) gi[u] = gr[32 * u];
+                    for (int u = 0; u < BL_V; ++u) gi[u] = gr[32 * u];
                 }
                 const T c = term_coef<T>(t);
                 const T *gr = sg + (t.code & 0xFF) * BL_TILE + lane;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) s[u] += c * gr[32 * u];
+                for (int u = 0; u < BL_V; ++u) s[u] += c * gr[32 * u];
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < BL_V; ++u) {
                 acc[u] += gi[u] * s[u];
                 const int64_t x = v0 + lane + 32 * u;
                 if (x < n_vox) out[(int64_t)o * n_vox + x] = acc[u];
@@ -147,22 +148,23 @@ extern "C" int pb_bilinear_maps(int precision, int64_t n_vox, const void *G, int
     if (n_out < 1 || n_out > BL_MAXOUT || n_table < 0)
         return fail(PB_ERR_INVALID, "pb_bilinear_maps: bad output or term count");
     if (((uintptr_t)table & 15) != 0) return fail(PB_ERR_INVALID, "pb_bilinear_maps: table must be 16-byte aligned");
-    const size_t c = precision == PB_F64 ? 8 : 4;
-    const size_t smem = (size_t)n_g * BL_TILE * c;
+    const bool f64 = precision == PB_F64;
+    const int tile = f64 ? 32 * 4 : 32 * 8;
+    const size_t smem = (size_t)n_g * tile * (f64 ? 8 : 4);
     const size_t head = ((size_t)(n_out + 1) * 4 + 15) / 16 * 16;
     const int32_t *offs = (const int32_t *)table;
     const BlTerm *rec = (const BlTerm *)((const char *)table + head);
-    const int64_t tiles = (n_vox + BL_TILE - 1) / BL_TILE;
+    const int64_t tiles = (n_vox + tile - 1) / tile;
     const int blocks = (int)std::min<int64_t>(tiles, (int64_t)num_sms() * 4 * 8);
     cudaStream_t s = as_stream(stream);
     if (precision == PB_F32) {
-        PB_CUDA(cudaFuncSetAttribute(bilinear_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        bilinear_kernel<float><<<blocks, BL_THREADS, smem, s>>>((const float *)G, n_g, n_vox, offs, rec, n_out,
-                                                                (float *)out);
+        PB_CUDA(cudaFuncSetAttribute(bilinear_kernel<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        bilinear_kernel<float, 8><<<blocks, BL_THREADS, smem, s>>>((const float *)G, n_g, n_vox, offs, rec, n_out,
+                                                                   (float *)out);
     } else if (precision == PB_F64) {
-        PB_CUDA(cudaFuncSetAttribute(bilinear_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        bilinear_kernel<double><<<blocks, BL_THREADS, smem, s>>>((const double *)G, n_g, n_vox, offs, rec, n_out,
-                                                                 (double *)out);
+        PB_CUDA(cudaFuncSetAttribute(bilinear_kernel<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        bilinear_kernel<double, 4><<<blocks, BL_THREADS, smem, s>>>((const double *)G, n_g, n_vox, offs, rec, n_out,
+                                                                    (double *)out);
     } else {
         return fail(PB_ERR_INVALID, "pb_bilinear_maps: bad precision");
     }
