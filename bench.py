@@ -32,6 +32,9 @@ N, L, LMAX, NK = 256, 2000.0, 2, 16
 EDGES = np.linspace(2 * np.pi / L, 0.2, NK + 1)
 METRIC = "Bk fields/s at 256^3 (16 bins, lmax=2, TSC, mixed precision)"
 WORKLOAD = "Bk_ideal 256^3 box 2000 Mpc/h, TSC, lmax=2, 16 linear bins 2pi/2000..0.2, 888 triangle bins"
+# DRAM bytes (read + write) of one contraction launch of this workload, from one ncu capture
+# (profiles/triplet_tc_bk256.md)
+TC_TRAFFIC_BYTES = 912_700_000
 
 
 FISHER = {
@@ -251,6 +254,7 @@ def run_ours(args, rank, world, local):
 
     # device-resident step: the Bk_ideal numerator + F^-1, no host sync
     cev = []
+    used = {}
 
     def step(i, record=False):
         x = resident[i % n_pool]
@@ -258,6 +262,7 @@ def run_ours(args, rank, world, local):
         w = bs._data_weight(torch.float32)
         G = bs._g_maps(xk, w, 1.0)
         plan = bs._plan("b3", G.shape[0], G.shape[0], G.shape[0], bs._triplet_index())
+        used["plan"] = plan
         out = torch.empty(plan.n_trip, dtype=torch.float64, device=dev)
         if record:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -319,14 +324,16 @@ def run_ours(args, rank, world, local):
         except Exception:
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
-        alg_bytes = bs.Nl * bs.Nk_squeeze * int(np.prod(bs.map_grid)) * 4  # every map read once
-        achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
-        traffic = None
-        try:
-            prof = json.load(open(os.path.join(REPO, "profiles", "triplet_traffic.json")))
-            traffic = prof.get("bytes_per_launch")
-        except Exception:
-            pass
+        bf16 = float(peaks.get("bf16_tflops", 1590.0))
+        n_vox = int(np.prod(bs.map_grid))
+        alg_bytes = bs.Nl * bs.Nk_squeeze * n_vox * 4  # every map read once
+        plan = used["plan"]
+        # GEMM form D[c, pair] = sum_x C_c(x) (A B)_pair(x) on the map grid, and the useful
+        # triple products (3 flops per voxel and triplet)
+        gemm_flops = 2.0 * plan.n_c * plan.n_pairs * n_vox
+        useful_flops = 3.0 * n_vox * plan.n_trip
+        achieved = gemm_flops / (kern_ms / 1000.0) / 1e12
+        achieved_hbm = alg_bytes / (kern_ms / 1000.0) / 1e9
         line = {"metric": METRIC, "value": value, "unit": "fields/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 maps / fp64 sums",
@@ -337,10 +344,15 @@ def run_ours(args, rank, world, local):
                 "e2e": {"value": e2e, "unit": "fields/s", "h2d_bytes_per_step": N ** 3 * 4,
                         "d2h_bytes_per_step": bs.N_bins * 8},
                 "gpu_launches": launches,
-                "roofline": {"bound": "hbm", "kernel": "triplet contraction", "achieved": achieved,
-                             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                             "alg_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms,
-                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+                "roofline": {"bound": "tensor", "kernel": "triplet contraction (tcgen05)", "achieved": achieved,
+                             "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+                             "traffic": TC_TRAFFIC_BYTES, "gemm_flops_per_launch": gemm_flops,
+                             "useful_flops_per_launch": useful_flops,
+                             "useful_tflops": useful_flops / (kern_ms / 1000.0) / 1e12,
+                             "alg_bytes_per_launch": alg_bytes, "achieved_hbm_gbs": achieved_hbm,
+                             "frac_hbm": achieved_hbm / hbm, "kernel_ms": kern_ms,
+                             "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst) and hbm_gbs" if peaks
+                                             else "fallback 1590 TFLOP/s and 6650 GB/s")},
                 "clocks": clk.summary()}
         if not args.no_cpu_baseline and world == 1:
             from polybin3d_b200 import synthetic as S

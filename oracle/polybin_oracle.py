@@ -321,9 +321,21 @@ class OracleBase:
         im = (rad * np.sin(2 * np.pi * u2)).reshape(tuple(self.gridsize))
         return re, im
 
-    def applyAinv_fourier(self, a):
+    def inverse_fiducial_draw(self):
+        """The shot-noise GRFs' spectrum P_A = 1/P_fid on the grid, as generate_data
+        interpolates it (zero outside the table), and 1/P_A extended by its end values
+        (0 at k = 0)  (pspec.py:504-508)."""
+        kP, PA = self.Pfid[0], 1.0 / self.Pfid[1]
+        draw = interp1d(kP, PA, bounds_error=False, fill_value=0.0)(self.modk_grid)
+        PA_grid = interp1d(kP, PA, bounds_error=False, fill_value=(PA[0], PA[-1]))(self.modk_grid)
+        inv = np.zeros_like(PA_grid)
+        nz = self.modk_grid != 0
+        inv[nz] = 1.0 / PA_grid[nz]
+        return draw, inv
+
+    def applyAinv_fourier(self, a, invP=None):
         """A^-1 a = a invP (/W^2)  (base.py:364-389), Fourier in and out."""
-        out = a * self.invPk0_grid
+        out = a * (self.invPk0_grid if invP is None else invP)
         if self.pixel_window != "none":
             out = self.div_fourier(self.div_fourier(out, self.pixel_window_grid), self.pixel_window_grid)
         return out
@@ -410,6 +422,23 @@ class OraclePSpec:
                     fish[row, lp * self.Nk:(lp + 1) * self.Nk] += scaling * b.cross_integrate(
                         Ainv, Q, self.k_bins, 2 * lp)
         return fish
+
+
+    def shot_contribution(self, noise_pair, mask_shot=None):
+        """compute_shot_contribution, global sightline (pspec.py:495-549): a = GRF of
+        P_A = 1/P_fid (pixel window included), S^-1 N A^-1 a with A^-1 = (1/P_A)/W^2 and N the
+        shot mask, then half the cross integral of S^-1 a with it."""
+        b = self.base
+        draw, invPA = b.inverse_fiducial_draw()
+        a = b.grf_from_noise(*noise_pair, Pk_grid=draw)                  # 511
+        if self.const_mask:                                              # 514-519
+            sna = self.mask_mean * b.applyAinv_fourier(a, invPA)
+        else:
+            sna = b.to_fourier(b.to_real(b.applyAinv_fourier(a, invPA)) * mask_shot)
+        shot = np.zeros(self.N_bins)
+        for li in range(self.Nl):                                        # 526-544
+            shot[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(a, sna, self.k_bins, 2 * li)
+        return shot * b.volume / b.gridsize.prod() ** 2
 
 
 # --------------------------------------------------------------------------------------
@@ -540,14 +569,92 @@ class OracleBSpec:
             x = x * self.invPk0 / self.cube_mask_mean ** (1.0 / 3.0)
         return x
 
-    def numerator(self, data, filtering="ideal", sym=None):
-        """_compute_bk_numerator without the linear term (bspec.py:895-983)."""
+    def numerator(self, data, filtering="ideal", sym=None, sims=None):
+        """_compute_bk_numerator (bspec.py:895-983); with `sims` (a list of bias-simulation
+        spectra from sim_spectrum / generated_sim) the linear term is included."""
         b = self.base
         sym = self.symmetry_factor() if sym is None else sym
         g = self.g_maps(self.weighted_data(data, filtering))
         flat = g.reshape(self.Nl * self.Nk_squeeze, -1)
         B3 = triplet_sum(flat, flat, flat, self.triplet_index(), b.nthreads)
+        if sims is not None:
+            B3 = B3 + self.linear_term(g, sims)
         return B3 * b.volume / b.gridsize.prod() / sym
+
+    def bshot_sum(self, A, B, C):
+        """assemble_bshot (utils.pyx:641-663): the triplet sums of all six orderings of the
+        map sets A, B, C over (b1, b2, (l, b3))."""
+        n = self.Nl * self.Nk_squeeze
+        f = [np.asarray(M).reshape(n, -1) for M in (A, B, C)]
+        idx = self.triplet_index()
+        out = np.zeros(len(idx))
+        for (i, j, k) in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+            out += triplet_sum(f[i], f[j], f[k], idx, self.base.nthreads)
+        return out
+
+    def shot_contribution(self, noise1, noise2, mask_shot, data=None, data2=None, sym=None, cubic_only=False):
+        """compute_shot_contribution, global sightline (bspec.py:695-861).  Two GRFs of
+        P_A = 1/P_fid with the pixel window; A^-1 = P_fid / W^2 (the base grid, 772); maps
+        A, B of S^-1 a1, S^-1 a2 (no window division), C of the shot-masked product
+        (A^-1 a1)(A^-1 a2), D, E of (A^-1 a_i) d2; cubic = bshot(A, B, C) V/(6 N^3 sym),
+        quadratic = (bshot(g, A, D) + bshot(g, B, E)) V/(4 N^3 sym); returns quadratic - 2 cubic."""
+        b = self.base
+        sym = self.symmetry_factor() if sym is None else sym
+        draw, _ = b.inverse_fiducial_draw()
+        a1 = b.grf_from_noise(*noise1, Pk_grid=draw)                     # 775-776
+        a2 = b.grf_from_noise(*noise2, Pk_grid=draw)
+        r1 = b.to_real(b.applyAinv_fourier(a1, b.Pk0_grid))              # 779-780
+        r2 = b.to_real(b.applyAinv_fourier(a2, b.Pk0_grid))
+        gA, gB = self.g_maps(a1), self.g_maps(a2)
+        gC = self.g_maps(b.to_fourier(r1 * r2 * mask_shot))             # 781
+        norm = b.volume / b.gridsize.prod() / sym
+        cubic = self.bshot_sum(gA, gB, gC) * norm / 6.0                  # 849-850
+        if cubic_only:
+            return cubic
+        g = self.g_maps(self.weighted_data(data, "Sinv"))               # 730-768
+        gD = self.g_maps(b.to_fourier(r1 * data2))                       # 783-784
+        gE = self.g_maps(b.to_fourier(r2 * data2))
+        quad = 0.5 * (self.bshot_sum(g, gA, gD) + self.bshot_sum(g, gB, gE)) * norm / 2.0   # 853-856
+        return quad - 2.0 * cubic
+
+    # bias simulations for the linear term (bspec.py:281-410)
+    def sim_spectrum(self, sim, input_type="real"):
+        """_process_sim before the g-maps (bspec.py:288-300): the Fourier map of one
+        simulation, divided by the pixel window when there is one (trivial S^-1)."""
+        b = self.base
+        if input_type == "real":
+            x = b.to_fourier(np.asarray(sim, dtype=np.float64))
+        else:
+            x = np.array(sim, dtype=np.complex128)
+        if b.pixel_window != "none":
+            x = x / b.pixel_window_grid
+        return x
+
+    def generated_sim(self, ii, Pk_grid=None):
+        """load_sim_data of generate_sims (bspec.py:377-392): the GRF of seed 1e5 + ii, times
+        the mask mean (constant mask) or through the mask in real space."""
+        b = self.base
+        re, im = b.reference_noise(int(1e5) + ii)
+        if self.const_mask:
+            return self.sim_spectrum(self.mask_mean * b.grf_from_noise(re, im, Pk_grid), "fourier")
+        s = b.to_real(b.grf_from_noise(re, im, Pk_grid, include_pixel_window=False)) * self.mask
+        if b.pixel_window != "none":
+            return self.sim_spectrum(b.to_fourier(s) * b.pixel_window_grid, "fourier")
+        return self.sim_spectrum(s, "real")
+
+    def linear_term(self, g, sims):
+        """B1 = -1/N_it sum_ii assemble_b1(g, g_ii) (bspec.py:963-978), where
+        assemble_b1 sums g[0,b1] s[0,b2] s[l/2,b3] + s[0,b1] g[0,b2] s[l/2,b3]
+        + s[0,b1] s[0,b2] g[l/2,b3] over voxels (utils.pyx:668-692)."""
+        n = self.Nl * self.Nk_squeeze
+        flat = g.reshape(n, -1)
+        idx = self.triplet_index()
+        out = np.zeros(len(idx))
+        for xs in sims:
+            s = self.g_maps(xs).reshape(n, -1)
+            out += (triplet_sum(flat, s, s, idx, self.base.nthreads) + triplet_sum(s, flat, s, idx, self.base.nthreads)
+                    + triplet_sum(s, s, flat, idx, self.base.nthreads))
+        return -out / len(sims)
 
     def fisher_ideal(self, discreteness_correction=True, sym=None):
         """compute_fisher_ideal (bspec.py:999-1083)."""

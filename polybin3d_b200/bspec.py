@@ -162,6 +162,7 @@ class BSpec:
         if not (isinstance(self.Pk_fid, str) and self.Pk_fid == 'default') and not self._unit_w:
             assert len(self.Pk_fid) == 2, "Pk should contain k and P_0(k) columns"
         self._plans = {}
+        self._set_idx = {}
         self._captured = None
         self._shell_modes = None
         self.map_grid = self._dealiased_grid() if dealias else tuple(int(n) for n in base.gridsize)
@@ -311,9 +312,10 @@ class BSpec:
             plan.contract(A, B, C, out, b.ws, method=nat.PB_TRIPLET_SIMT, scale=scale)
         return out
 
-    def _binned_maps(self, src, specs, w, dtype, coarse=True):
+    def _binned_maps(self, src, specs, w, dtype, coarse=True, out=None):
         """Real maps irfftn(Theta_b L_l1 L_l2 * w^wp * src) for specs [(b, l1, l2, scale)], batched.
-        coarse: synthesise them on the dealiased map grid (same 1/N^3 normalisation)."""
+        coarse: synthesise them on the dealiased map grid (same 1/N^3 normalisation).
+        out: optional contiguous (len(specs), *grid) tensor to write them into."""
         b = self.base
         ks = self.k_bins_squeeze
         cd = torch.complex128 if dtype == torch.float64 else torch.complex64
@@ -322,7 +324,8 @@ class BSpec:
         wp = 0 if w is None else 1
         maps = [(0, ks[bb], ks[bb + 1], l1, l2, sc / b.nreal, wp) for (bb, l1, l2, sc) in specs]
         if self.synthesis != 'cufft' and self._synth_ok.get(dims, True):
-            out = torch.empty((len(specs),) + tuple(dims), dtype=dtype, device=b.device)
+            if out is None:
+                out = torch.empty((len(specs),) + tuple(dims), dtype=dtype, device=b.device)
             try:
                 nat.shell_synth(b.grid, prec, src, out, maps, dims, b.ws, w=w, src_stride=b.nhalf)
                 b.n_FFTs_reverse += len(specs)
@@ -336,7 +339,7 @@ class BSpec:
         nat.spectral_filter(b.grid, prec, src, half, maps, w=w, src_stride=b.nhalf,
                             out_n=None if coarse is False or dims == tuple(int(n) for n in b.gridsize) else dims)
         b.n_FFTs_reverse += len(specs)
-        return b.fft_c2r(half)
+        return b.fft_c2r(half, out=out)
 
     # ------------------------------------------------------------------------------
     # symmetry factors (bspec.py:222-279)
@@ -396,10 +399,10 @@ class BSpec:
         ab = self.all_bins
         return np.stack([ab[:, 0], ab[:, 1], (ab[:, 3] // 2) * self.Nk_squeeze + ab[:, 2]], axis=1).astype(np.int32)
 
-    def _g_maps(self, xk, w, scale):
+    def _g_maps(self, xk, w, scale, out=None):
         """All Nl x Nk_squeeze bin-filtered maps g[l/2, b] of one weighted spectrum."""
         specs = [(bb, l, 0, scale) for l in range(0, self.lmax + 1, 2) for bb in range(self.Nk_squeeze)]
-        return self._binned_maps(xk, specs, w, xk.real.dtype)
+        return self._binned_maps(xk, specs, w, xk.real.dtype, out=out)
 
     def _compute_bk_numerator(self, data, include_linear_term=True, filtering='ideal', verb=False):
         assert filtering in ['ideal', 'Sinv'], "Unknown filtering option supplied!"
@@ -410,12 +413,14 @@ class BSpec:
             assert type(data[0, 0, 0]) in [np.float32, np.float64], "Data must be of type float32 or float64!"
         if not hasattr(self, 'sym_factor'):
             self._compute_symmetry_factor()
-        B3 = self._bk_cubic(data, filtering)
+        B3 = self._bk_cubic(data, filtering, linear=include_linear_term)
         norm = b.volume / float(b.gridsize.prod()) / self.sym_factor
         return B3.cpu().numpy() * norm
 
-    def _bk_cubic(self, data, filtering):
-        """Device FP64 cubic sums B3[i] (assemble_b3 of the g-maps)."""
+    def _bk_cubic(self, data, filtering, linear=False):
+        """Device FP64 sums B3[i] (assemble_b3 of the g-maps), plus the linear term
+        B1 = -1/N_it sum_ii assemble_b1(g, g_ii) of the bias simulations when `linear`
+        (bspec.py:958-978)."""
         b = self.base
         x = b.as_device(data)
         xk = b.to_fourier(x)
@@ -428,8 +433,99 @@ class BSpec:
             if b.pixel_window != 'none':
                 w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), rd)
             scale = 1.0
-        G = self._g_maps(xk, w, scale)
-        return self._contract('b3', G, G, G, self._triplet_index())
+        if not linear:
+            G = self._g_maps(xk, w, scale)
+            return self._contract('b3', G, G, G, self._triplet_index())
+        # data maps and one simulation's maps side by side: X = [g; g_ii]
+        n = self.Nl * self.Nk_squeeze
+        X = torch.empty((2 * n,) + tuple(self.map_grid), dtype=rd, device=b.device)
+        G, S = X[:n], X[n:]
+        self._g_maps(xk, w, scale, out=G)
+        out = self._contract('b3', G, G, G, self._triplet_index())
+        b1 = torch.zeros(self.N_bins, dtype=torch.float64, device=b.device)
+        for ii in range(self.N_it):
+            self._g_maps(self._sim_spectrum(ii, rd), None, 1.0, out=S)
+            b1 += self._set_sums('b1', X, n, ((0, 1, 1), (1, 0, 1), (1, 1, 0)))
+        return out - b1 / self.N_it
+
+    def _set_sums(self, key, X, n, terms):
+        """FP64 sum over `terms` (ta, tb, tc) of the triplet sums
+        sum_x X_ta[0,b1](x) X_tb[0,b2](x) X_tc[l,b3](x), where X holds map sets of n maps each
+        side by side (set t = X[t n:(t+1) n], maps ordered (l/2, b)).  Terms that share the
+        C set go through one contraction with A = B = X and C = that set (rows of X, staged
+        once); each pair is listed with its smaller map index first, since the products
+        commute, so the pair rows of different terms are shared, and triplets that coincide
+        (b1 = b2 in the two mixed orderings) are contracted once and gathered back."""
+        t = self._triplet_index().astype(np.int64)
+        i1, i2, i3 = t[:, 0], t[:, 1], t[:, 2]
+        nb = self.N_bins
+        by_c = {}
+        for (ta, tb, tc) in terms:
+            by_c.setdefault(tc, []).append((ta, tb))
+        total = None
+        for tc in sorted(by_c):
+            ab = tuple(by_c[tc])
+            ck = (key, tc, ab)
+            hit = self._set_idx.get(ck)
+            if hit is None:
+                rows = []
+                for (ta, tb) in ab:
+                    p, q = ta * n + i1, tb * n + i2
+                    rows.append(np.stack([np.minimum(p, q), np.maximum(p, q), i3], axis=1))
+                uniq, inv = np.unique(np.concatenate(rows), axis=0, return_inverse=True)
+                hit = (uniq.astype(np.int32), torch.as_tensor(inv.reshape(-1), device=self.base.device))
+                self._set_idx[ck] = hit
+            idx, inv = hit
+            out = self._contract(ck, X, X, X[tc * n:(tc + 1) * n], idx)[inv].view(len(ab), nb).sum(0)
+            total = out if total is None else total + out
+        return total
+
+    # ------------------------------------------------------------------------------
+    # bias simulations for the linear term (bspec.py:281-410)
+    # ------------------------------------------------------------------------------
+    def _sim_spectrum(self, ii, dtype):
+        """The Fourier map of bias simulation ii, pixel window divided out, as the map dtype."""
+        xs = self._sim_store[ii] if self.preload else self.load_sim_data(ii)
+        cd = torch.complex128 if dtype == torch.float64 else torch.complex64
+        return xs if xs.dtype == cd else xs.to(cd)
+
+    def _process_sim(self, sim, input_type='real'):
+        """_process_sim up to its g-maps (bspec.py:281-300): the Fourier map of one
+        simulation with the pixel window divided out (trivial S^-1), stored in the base
+        precision.  The g-maps are synthesised from it when the linear term is formed, so a
+        simulation holds one half spectrum of device memory instead of Nl x Nk maps."""
+        b = self.base
+        if input_type == 'real':
+            xk = b.to_fourier(b.as_device(sim))
+        else:
+            xk = torch.as_tensor(sim, device=b.device).to(b.complex_dtype).contiguous()
+        if b.pixel_window != 'none':
+            prec = nat.precision_of(xk.dtype)
+            rd = torch.float64 if prec == nat.PB_F64 else torch.float32
+            w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), rd)
+            out = torch.empty_like(xk)
+            nat.spectral_filter(b.grid, prec, xk, out, [(0, -1.0, np.inf, 0, 0, 1.0, 1)], w=w)
+            xk = out
+        return xk
+
+    def _generated_sim(self, ii, Pk_input):
+        """load_sim_data of generate_sims (bspec.py:377-392): the GRF of seed 1e5 + ii
+        (the reference's own noise draw), times the mask mean (constant mask) or through the
+        mask in real space, in FP64.  The pixel window that the reference multiplies in and
+        _process_sim divides out again is left out of both steps."""
+        b = self.base
+        re, im = b.reference_noise(int(1e5) + ii)
+        nre = torch.as_tensor(re, device=b.device)
+        nim = torch.as_tensor(im, device=b.device)
+        a = b.grf_from_noise(nre, nim, Pk_input if len(Pk_input) else None, include_pixel_window=False)
+        F64 = nat.PB_F64
+        if self.const_mask:
+            out = torch.empty_like(a)
+            nat.spectral_filter(b.grid, F64, a, out, [(0, -1.0, np.inf, 0, 0, float(self.mask_mean), 0)])
+            return out.to(b.complex_dtype)
+        s = b.to_real(a)
+        nat.elementwise(nat.PB_EW_MUL, s, self._mask_device(), out=s, y_period=b.nreal)
+        return b.to_fourier(s).to(b.complex_dtype)
 
     def _inv_window(self):
         W = self.base.pixel_window_grid
@@ -438,7 +534,7 @@ class BSpec:
 
     def Bk_numerator(self, data, include_linear_term=True, verb=False):
         """Numerator of the unwindowed estimator (bspec.py:429-439); the linear term needs
-        bias simulations, which this backend does not generate."""
+        bias simulations (generate_sims or load_sims)."""
         if not self.const_mask:
             assert data.shape == self.mask.shape, "Data must have same shape as the mask!"
         return self._compute_bk_numerator(data, include_linear_term=include_linear_term, filtering='Sinv', verb=verb)
@@ -450,10 +546,37 @@ class BSpec:
         return self._compute_bk_numerator(data, include_linear_term=False, filtering='ideal', verb=verb)
 
     def load_sims(self, load_sim, N_sims, verb=False, input_type='real', preload=True):
-        raise NotImplementedError("the linear term (bias simulations) is not implemented in backend='cuda'")
+        """Bias simulations for the linear term from a loader load_sim(ii), real- or
+        Fourier-space (bspec.py:324-352).  preload=True keeps each simulation's filtered
+        Fourier map on the device; preload=False calls the loader again every time."""
+        self.N_it = N_sims
+        print("Using %d Monte Carlo simulations" % self.N_it)
+        if preload:
+            self.preload = True
+            self._sim_store = []
+            for ii in range(self.N_it):
+                if verb: print("Loading bias simulation %d of %d" % (ii + 1, self.N_it))
+                self._sim_store.append(self._process_sim(load_sim(ii), input_type=input_type))
+        else:
+            self.preload = False
+            if verb: print("No preloading; simulations will be loaded and accessed at runtime.")
+            self.load_sim_data = lambda ii: self._process_sim(load_sim(ii), input_type=input_type)
 
     def generate_sims(self, N_sim, Pk_input=[], verb=False, preload=True):
-        raise NotImplementedError("the linear term (bias simulations) is not implemented in backend='cuda'")
+        """N_sim Gaussian bias simulations of the fiducial (or given) spectrum through the
+        mask, seeds 1e5 + ii (bspec.py:354-410)."""
+        self.N_it = N_sim
+        print("Using %d Monte Carlo simulations" % self.N_it)
+        if preload:
+            self.preload = True
+            self._sim_store = []
+            for ii in range(self.N_it):
+                if verb: print("Generating bias simulation %d of %d" % (ii + 1, self.N_it))
+                self._sim_store.append(self._generated_sim(ii, Pk_input))
+        else:
+            self.preload = False
+            if verb: print("No preloading; simulations will be loaded and accessed at runtime.")
+            self.load_sim_data = lambda ii: self._generated_sim(ii, Pk_input)
 
     # ------------------------------------------------------------------------------
     # ideal Fisher (bspec.py:999-1083)
@@ -736,7 +859,73 @@ class BSpec:
         return Bk_dict
 
     def compute_shot_contribution(self, seed, verb=False, data=None, data2=None, cubic_only=False):
-        raise NotImplementedError("shot-noise Monte Carlo is not implemented in backend='cuda'")
+        """Shot-noise contribution of one pair of GRFs of spectrum 1/P_fid, global sightline
+        (bspec.py:695-861): the cubic term from the maps of S^-1 a1, S^-1 a2 and the
+        shot-masked product (A^-1 a1)(A^-1 a2), and unless cubic_only the quadratic term from
+        the data's maps with those of (A^-1 a_i) d2.  Returns quadratic - 2 cubic."""
+        if not cubic_only:
+            assert data is not None, "Must supply data to compute the quadratic shot-noise contribution!"
+            if data2 is None:
+                print("## Caution: assuming uniform weights!")
+                data2 = data
+            if not self.const_mask:
+                assert data.shape == self.mask.shape, "Data must have same shape as the mask!"
+            for dd in (data, data2):
+                if not isinstance(dd, torch.Tensor):
+                    assert type(dd[0, 0, 0]) in [np.float32, np.float64], "Data must be of type float32 or float64!"
+        else:
+            print("## Caution: Dropping quadratic (~ P(k)/n) term!")
+        assert hasattr(self, 'mask_shot'), "Must supply triply-weighted mask to compute the shot-noise contribution!"
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        b = self.base
+        dev = b.device
+        rd = b.real_dtype
+        F64 = nat.PB_F64
+        PkA = [b.Pfid[0], 1. / b.Pfid[1]]
+        a = []
+        for off in (int(1e7), int(2e7)):
+            re, im = b.reference_noise(seed + off)
+            a.append(b.grf_from_noise(torch.as_tensor(re, device=dev), torch.as_tensor(im, device=dev), Pk_input=PkA))
+        # A^-1 a_i with the base fiducial spectrum in place of 1/P (bspec.py:772, 779-780)
+        r = [b.applyAinv(ai, invPk0_grid=b.Pk0_grid, input_type='fourier', output_type='real') for ai in a]
+        mshot = b.to_device_grid(('bk_mask_shot', id(self)), lambda: self.mask_shot, torch.float64)
+        n = self.Nl * self.Nk_squeeze
+        X = torch.empty((3 * n,) + tuple(self.map_grid), dtype=rd, device=dev)
+        cd = torch.complex128 if rd == torch.float64 else torch.complex64
+        sets = [X[i * n:(i + 1) * n] for i in range(3)]
+        perms = ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0))
+
+        def maps_of(spec, out, w=None):
+            self._g_maps(spec if spec.dtype == cd else spec.to(cd), w, 1.0, out=out)
+
+        def product_spectrum(x, y, z=None):
+            prod = nat.elementwise(nat.PB_EW_MUL, x, y)
+            if z is not None:
+                nat.elementwise(nat.PB_EW_MUL, prod, z, out=prod, y_period=b.nreal)
+            return b.to_fourier(prod)
+
+        maps_of(a[0], sets[0])
+        maps_of(a[1], sets[1])
+        maps_of(product_spectrum(r[0], r[1], mshot), sets[2])
+        norm = b.volume / float(b.gridsize.prod()) / self.sym_factor
+        cubic = self._set_sums('bshot', X, n, perms).cpu().numpy() * norm / 6.
+        if cubic_only:
+            return cubic
+        xk = b.to_fourier(b.as_device(data))
+        w = None
+        if b.pixel_window != 'none':
+            w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), xk.real.dtype)
+        d2 = b.as_device(data2, torch.float64)
+        # (g, a1-maps, D) in the three sets, then (a2-maps, g, E)
+        maps_of(xk, sets[1], w)
+        maps_of(product_spectrum(r[0], d2), sets[2])
+        quad = self._set_sums('bshot', X, n, perms)
+        maps_of(a[1], sets[0])
+        maps_of(product_spectrum(r[1], d2), sets[2])
+        quad = quad + self._set_sums('bshot', X, n, perms)
+        quad = 0.5 * quad.cpu().numpy() * norm / 2.
+        return quad - 2. * cubic
 
     def compute_covariance_contribution(self, seed, Pk_cov, verb=False, mask_shot_2pt=None):
         raise NotImplementedError("covariance Monte Carlo is not implemented in backend='cuda'")

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <set>
 #include <string>
 #include <vector>
 #include "pb_common.cuh"
@@ -23,10 +24,15 @@ int triplet_build_items(int n_a, int n_b, int n_c, const int32_t *idx, int n_tri
     if (!idx) return fail(PB_ERR_INVALID, "triplet index array is NULL");
     // a -> list of (b, c, t)
     std::map<int, std::vector<std::array<int, 3>>> by_a;
+    std::set<std::array<int, 3>> seen;
     for (int t = 0; t < n_trip; ++t) {
         int a = idx[3 * t], b = idx[3 * t + 1], c = idx[3 * t + 2];
         if (a < 0 || a >= n_a || b < 0 || b >= n_b || c < 0 || c >= n_c)
             return fail(PB_ERR_INVALID, "triplet index out of range at row " + std::to_string(t));
+        // each output is written by exactly one work item: a repeated triplet would leave
+        // one of its rows unwritten
+        if (!seen.insert({a, b, c}).second)
+            return fail(PB_ERR_INVALID, "duplicate triplet at row " + std::to_string(t));
         by_a[a].push_back({b, c, t});
     }
     for (auto &kv : by_a) {

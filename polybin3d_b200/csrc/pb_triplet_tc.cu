@@ -28,7 +28,6 @@
 
 namespace pb {
 
-constexpr int TC_THREADS = 512;
 constexpr int TC_KT = 64;                  // voxels per tile (4 MMA K steps of 16)
 constexpr int TC_NCHUNK = TC_KT / 8;       // 16-byte K chunks per tile
 constexpr int TC_STAGE_LD = TC_KT;         // fp32 staging row stride (elements; TMA box rows are dense)
@@ -40,7 +39,8 @@ constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 
 struct TcGeom {
     int n_rows;                 // staged map rows
-    int off_b, off_c;
+    int off_b, off_c;           // first staged row of the B and C map sets
+    int load_b, load_c;         // B / C rows staged from their own pointers (else they lie in A's rows)
     int n_pairs, n_c;
     int M;                      // MMA M: 64 or 128 (C-map rows, hi/lo interleaved)
     int a_lbo, a_bytes;         // C operand: K-chunk stride, bytes per buffer
@@ -185,9 +185,20 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 
 // Warp roles: warps 0..TC_PROD-1 produce operands (TC_EPI of them also fold the TMEM
 // accumulators), warp TC_PROD stages tiles (TMA, or cp.async), warp TC_PROD+1 issues MMAs.
-constexpr int TC_PROD = 14;        // producer warps
-constexpr int TC_UPT = 3;          // units per producer thread handled with hoisted loads
-constexpr int TC_EPI = 12;         // producer warps that also fold accumulators (3 per TMEM lane quarter)
+#ifndef TC_NPROD
+#define TC_NPROD 14
+#endif
+#ifndef TC_NUPT
+#define TC_NUPT 3
+#endif
+#ifndef TC_NEPI
+#define TC_NEPI 12
+#endif
+constexpr int TC_PROD = TC_NPROD;  // producer warps
+constexpr int TC_UPT = TC_NUPT;    // units per producer thread handled with hoisted loads
+constexpr int TC_EPI = TC_NEPI;    // producer warps that also fold accumulators (TC_EPI / 4 per TMEM lane quarter)
+constexpr int TC_THREADS = 32 * (TC_PROD + 2);
+static_assert(TC_EPI % 4 == 0 && TC_EPI <= TC_PROD, "fold warps: a multiple of 4, all producers");
 constexpr int TC_LOADW = TC_PROD;  // staging warp
 constexpr int TC_MMAW = TC_PROD + 1;
 
@@ -269,9 +280,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (lane == 0) {
                     mbar_expect_tx(&full[slot], (uint32_t)(geo.n_rows * TC_KT * 4));
                     tma_load_2d(dst, &map_a, (int)v0, 0, &full[slot]);
-                    if (geo.off_b > 0) tma_load_2d(dst + geo.off_b * TC_STAGE_LD, &map_b, (int)v0, 0, &full[slot]);
-                    if (geo.off_c >= geo.off_b + (geo.off_b > 0 ? n_b : n_a) && geo.off_c > 0)
-                        tma_load_2d(dst + geo.off_c * TC_STAGE_LD, &map_c, (int)v0, 0, &full[slot]);
+                    if (geo.load_b) tma_load_2d(dst + geo.off_b * TC_STAGE_LD, &map_b, (int)v0, 0, &full[slot]);
+                    if (geo.load_c) tma_load_2d(dst + geo.off_c * TC_STAGE_LD, &map_c, (int)v0, 0, &full[slot]);
                 }
             } else {
                 for (int e = lane; e < geo.n_rows * TC_KT; e += 32) {
@@ -279,7 +289,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const float *src;
                     int m;
                     if (r < n_a) { src = A; m = r; }
-                    else if (geo.off_b > 0 && r < geo.off_b + n_b) { src = B; m = r - geo.off_b; }
+                    else if (geo.load_b && r < geo.off_b + n_b) { src = B; m = r - geo.off_b; }
                     else { src = C; m = r - geo.off_c; }
                     int64_t x = v0 + v;
                     bool ok = x < n_vox;
@@ -534,11 +544,18 @@ __global__ void triplet_tc_finalize(const double *partials, int n_cta, int n_pai
     if (lane == 0) out[t] = s * scale;
 }
 
-static int tc_geometry(int n_rows, int off_b, int off_c, int n_pairs, int n_c, TcGeom *g) {
+struct TcRows {
+    int n_rows, off_b, off_c, load_b, load_c;
+};
+
+static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, TcGeom *g) {
     memset(g, 0, sizeof(*g));
+    const int n_rows = rw.n_rows;
     g->n_rows = n_rows;
-    g->off_b = off_b;
-    g->off_c = off_c;
+    g->off_b = rw.off_b;
+    g->off_c = rw.off_c;
+    g->load_b = rw.load_b;
+    g->load_c = rw.load_c;
     g->n_pairs = n_pairs;
     g->n_c = n_c;
     if (n_c > TC_MAX_NC) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 64 C maps");
@@ -613,22 +630,40 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
     PB_CUDA(cudaGetDevice(&dev));
     PB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
     if (major != 10) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction needs an sm_100 device");
-    int off_b = (B == A && n_b == n_a) ? 0 : n_a;
-    int after_b = off_b > 0 ? off_b + n_b : n_a;
-    int off_c;
-    if (C == A && n_c == n_a) off_c = 0;
-    else if (C == B && n_c == n_b) off_c = off_b;
-    else off_c = after_b;
-    int n_rows = (off_c == after_b) ? after_b + n_c : after_b;
+    // staged rows: A's maps, then B's and C's unless they are rows of A already (the same
+    // maps, or a contiguous run of them: B = A + k maps) or C is B
+    const size_t map_bytes = (size_t)n_vox * 4;
+    auto rows_of_a = [&](const void *P, int n_p, int *k) {
+        if ((const char *)P < (const char *)A) return false;
+        const size_t d = (size_t)((const char *)P - (const char *)A);
+        if (d % map_bytes) return false;
+        *k = (int)(d / map_bytes);
+        return *k + n_p <= n_a && d / map_bytes < (size_t)n_a;
+    };
+    TcRows rw{n_a, 0, 0, 0, 0};
+    if (!rows_of_a(B, n_b, &rw.off_b)) {
+        rw.off_b = rw.n_rows;
+        rw.load_b = 1;
+        rw.n_rows += n_b;
+    }
+    if (!rows_of_a(C, n_c, &rw.off_c)) {
+        if (rw.load_b && C == B && n_c <= n_b) {
+            rw.off_c = rw.off_b;
+        } else {
+            rw.off_c = rw.n_rows;
+            rw.load_c = 1;
+            rw.n_rows += n_c;
+        }
+    }
     // pairs go through in chunks small enough for shared memory and TMEM (the FP64
     // accumulators and the pair operands grow with the pair count)
     const int n_pairs = counts[1];
     TcGeom g;
     int chunk = std::min(n_pairs, 512);
-    int st = tc_geometry(n_rows, off_b, off_c, chunk, n_c, &g);
+    int st = tc_geometry(rw, chunk, n_c, &g);
     while (st == PB_ERR_UNSUPPORTED && chunk > 16 && n_c <= TC_MAX_NC) {
         chunk = (chunk + 1) / 2;
-        st = tc_geometry(n_rows, off_b, off_c, chunk, n_c, &g);
+        st = tc_geometry(rw, chunk, n_c, &g);
     }
     if (st) return st;
     int gx = tc_grid(n_vox);
@@ -666,7 +701,7 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
     for (int p_lo = 0; p_lo < n_pairs; p_lo += chunk) {
         const int pk = std::min(chunk, n_pairs - p_lo);
         TcGeom gk;
-        st = tc_geometry(n_rows, off_b, off_c, pk, n_c, &gk);
+        st = tc_geometry(rw, pk, n_c, &gk);
         if (st) return st;
         if (gk.smem_bytes > smem_max) {
             PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, gk.smem_bytes));

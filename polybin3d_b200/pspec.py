@@ -327,7 +327,44 @@ class PSpec:
         return Pk_dict
 
     def compute_shot_contribution(self, seed):
-        raise NotImplementedError("shot-noise Monte Carlo is not implemented in backend='cuda'")
+        """Shot-noise contribution of one GRF, global sightline (pspec.py:495-549): a is drawn
+        with spectrum P_A = 1/P_fid (pixel window included), A^-1 = (1/P_A) / W^2, and the
+        k-binned cross spectrum of S^-1 a with S^-1 N A^-1 a (N: mask_shot, or the mask mean
+        for a constant mask) is halved and normalised by V / N^6."""
+        if not self.const_mask:
+            assert hasattr(self, 'mask_shot'), "Must supply mask_shot to compute shot-noise contribution"
+        b = self.base
+        dev = b.device
+        F64 = nat.PB_F64
+        PkA = [b.Pfid[0], 1. / b.Pfid[1]]
+        if getattr(self, '_invPA', None) is None:
+            self._invPA = self._shot_inv_pa(PkA)
+        invPA = self._invPA
+        re, im = b.reference_noise(seed + int(1e7))
+        a = b.grf_from_noise(torch.as_tensor(re, device=dev), torch.as_tensor(im, device=dev), Pk_input=PkA)
+        sna = b.applyAinv(a, invPk0_grid=invPA, input_type='fourier',
+                          output_type='fourier' if self.const_mask else 'real')
+        scale = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
+        if self.const_mask:
+            scale *= self.mask_mean
+        else:
+            m = b.to_device_grid(('pk_mask_shot', id(self)), lambda: self.mask_shot, torch.float64)
+            nat.elementwise(nat.PB_EW_MUL, sna, m, out=sna, y_period=b.nreal)
+            sna = b.to_fourier(sna)
+        out = torch.empty(self.N_bins, dtype=torch.float64, device=dev)
+        nat.bin_reduce(b.grid, F64, nat.PB_RED_CROSS, a, sna, 1, self.k_bins, self._ells(self.Nl), scale, out, b.ws)
+        return out.cpu().numpy()
+
+    def _shot_inv_pa(self, PkA):
+        """1/P_A on the grid, P_A interpolated with its end values beyond the table, 0 at
+        k = 0 (pspec.py:505-508)."""
+        from scipy.interpolate import interp1d
+        b = self.base
+        PA = interp1d(PkA[0], PkA[1], bounds_error=False, fill_value=(PkA[1][0], PkA[1][-1]))(b.modk_grid)
+        inv = np.zeros_like(PA)
+        nz = b.modk_grid != 0
+        inv[nz] = 1. / PA[nz]
+        return inv
 
     def compute_covariance_contribution(self, seed, Pk_cov, verb=False):
         raise NotImplementedError("covariance Monte Carlo is not implemented in backend='cuda'")

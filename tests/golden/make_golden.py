@@ -232,6 +232,60 @@ def bk_fisher_nomask(pb):
     return dict(N=N, L=L, edges=edges, bk_lmax=2, pw="cic", bins=bs.all_bins, sym=bs.sym_factor, f3=f3)
 
 
+@case
+def bk_linear(pb):
+    """24^3, L=600, 4 bins, TSC: Bk_numerator with the linear term.
+    (a) lmax=2, shell-sector mask, generate_sims(3), lognormal data seed 13;
+    (b) lmax=0, constant mask 0.5, generate_sims(2) with a tabulated P(k), data seed 14;
+    (c) lmax=2, shell-sector mask, load_sims of two real-space GRFs (seeds 60, 61) times the mask."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="tsc", backend="mkl")
+    data = synthetic.lognormal(N, L, seed=13).astype(np.float64) * mask
+    bs = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask)
+    _quiet(bs.generate_sims, 3)
+    num_a = _quiet(bs.Bk_numerator, data)
+    out = dict(N=N, L=L, edges=edges, bins=bs.all_bins, sym=bs.sym_factor, num_a=num_a,
+               cub_a=_quiet(bs.Bk_numerator, data, include_linear_term=False))
+    kt = np.linspace(0.0, 1.0, 400)
+    pt = 2e3 * np.exp(-(kt / 0.2) ** 2) + 50.0
+    cmask = 0.5 * np.ones((N, N, N))
+    data_b = synthetic.lognormal(N, L, seed=14).astype(np.float64) * 0.5
+    bs2 = _quiet(pb.BSpec, base, edges, lmax=0, mask=cmask)
+    _quiet(bs2.generate_sims, 2, Pk_input=[kt, pt])
+    out.update(pk_k=kt, pk_p=pt, bins_b=bs2.all_bins, num_b=_quiet(bs2.Bk_numerator, data_b))
+    bs3 = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask)
+    _quiet(bs3.load_sims, lambda ii: synthetic.grf(N, L, seed=60 + ii) * mask, 2)
+    out.update(num_c=_quiet(bs3.Bk_numerator, data))
+    return out
+
+
+@case
+def shot(pb):
+    """24^3, L=600, 4 bins, TSC, tabulated positive fiducial P(k): shot-noise contributions.
+    PSpec lmax=2 with the shell-sector mask and mask_shot = 0.8 mask (seed 1), PSpec with
+    no mask (seed 2); BSpec lmax=2 with the mask and mask_shot = 0.6 mask (seed 1, data =
+    lognormal seed 16 times the mask, data2 = 0.7 data; and the cubic-only term)."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    kt = np.linspace(0.0, 1.0, 2000)
+    pt = 2e3 * np.exp(-(kt / 0.3) ** 2) + 100.0
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, Pk=[kt, pt], pixel_window="tsc", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=2, mask=mask, mask_shot=0.8 * mask)
+    ps2 = _quiet(pb.PSpec, base, edges, lmax=2)
+    data = synthetic.lognormal(N, L, seed=16).astype(np.float64) * mask
+    bs = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask, mask_shot=0.6 * mask)
+    b_full = _quiet(bs.compute_shot_contribution, 1, data=data, data2=0.7 * data)
+    b_cub = _quiet(bs.compute_shot_contribution, 1, cubic_only=True)
+    return dict(N=N, L=L, edges=edges, pk_k=kt, pk_p=pt, p_mask=_quiet(ps.compute_shot_contribution, 1),
+                p_nomask=_quiet(ps2.compute_shot_contribution, 2), bins=bs.all_bins, sym=bs.sym_factor,
+                b_full=b_full, b_cubic=b_cub)
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

@@ -119,6 +119,16 @@ def test_triplet_plan_rejects_out_of_range():
     assert st == -1 and b"out of range" in lib.pb_last_error()
 
 
+def test_triplet_plan_rejects_duplicates():
+    """A repeated (a, b, c) row would leave one output unwritten: refused."""
+    lib = nat.load()
+    idx = np.array([[0, 1, 2], [1, 1, 2], [0, 1, 2]], dtype=np.int32)
+    nb = ctypes.c_size_t()
+    counts = np.zeros(4, dtype=np.int32)
+    st = lib.pb_triplet_plan(4, 4, 4, nat.hptr(idx), 3, None, ctypes.byref(nb), nat.hptr(counts))
+    assert st == -1 and b"duplicate triplet at row 2" in lib.pb_last_error()
+
+
 def test_bilinear_plan_host_logic():
     """pb_bilinear_plan: i <= j canonical order, duplicates merged, empty outputs get a zero
     term, out-of-range indices refused (host only)."""

@@ -145,6 +145,57 @@ def test_bk_fisher_nomask_lmax2():
     assert rel(f, g["f3"]) < TOL
 
 
+def test_bk_linear_term():
+    """Bk_numerator with the linear term: generate_sims under a varying mask (a) and a
+    constant mask with a tabulated P(k) (b), load_sims of real-space maps (c).  The linear
+    term itself (numerator minus the cubic part) is checked on its own in (a): it is ~1e-5
+    of the numerator there."""
+    from scipy.interpolate import interp1d
+    g = gold("bk_linear")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc")
+    m = mask24(N, L)
+    d = synthetic.lognormal(N, L, seed=13).astype(np.float64) * m
+    bs = O.OracleBSpec(b, g["edges"], lmax=2, mask=m)
+    assert np.array_equal(bs.all_bins, g["bins"])
+    sym = g["sym"]
+    sims = [bs.generated_sim(i) for i in range(3)]
+    num = bs.numerator(d, "Sinv", sym=sym, sims=sims)
+    cub = bs.numerator(d, "Sinv", sym=sym)
+    assert rel(cub, g["cub_a"]) < TOL
+    assert rel(num, g["num_a"]) < TOL
+    assert rel(num - cub, g["num_a"] - g["cub_a"]) < 1e-8
+    # (b)
+    bs2 = O.OracleBSpec(b, g["edges"], lmax=0, mask=0.5 * np.ones((N, N, N)))
+    assert bs2.const_mask
+    pk = interp1d(g["pk_k"], g["pk_p"], bounds_error=False, fill_value=0.)(b.modk_grid)
+    d2 = synthetic.lognormal(N, L, seed=14).astype(np.float64) * 0.5
+    sims2 = [bs2.generated_sim(i, Pk_grid=pk) for i in range(2)]
+    assert rel(bs2.numerator(d2, "Sinv", sims=sims2), g["num_b"]) < TOL
+    # (c)
+    sims3 = [bs.sim_spectrum(synthetic.grf(N, L, seed=60 + i) * m) for i in range(2)]
+    assert rel(bs.numerator(d, "Sinv", sym=sym, sims=sims3), g["num_c"]) < TOL
+
+
+def test_shot_noise():
+    """compute_shot_contribution of PSpec (masked and unmasked) and BSpec (full and cubic
+    only), tabulated fiducial spectrum, TSC window."""
+    g = gold("shot")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, Pk=[g["pk_k"], g["pk_p"]], pixel_window="tsc")
+    m = mask24(N, L)
+    ps = O.OraclePSpec(b, g["edges"], lmax=2, mask=m)
+    assert rel(ps.shot_contribution(b.reference_noise(1 + 10 ** 7), mask_shot=0.8 * m), g["p_mask"]) < TOL
+    ps2 = O.OraclePSpec(b, g["edges"], lmax=2)
+    assert rel(ps2.shot_contribution(b.reference_noise(2 + 10 ** 7)), g["p_nomask"]) < TOL
+    bs = O.OracleBSpec(b, g["edges"], lmax=2, mask=m)
+    assert np.array_equal(bs.all_bins, g["bins"])
+    n1, n2 = b.reference_noise(1 + 10 ** 7), b.reference_noise(1 + 2 * 10 ** 7)
+    d = synthetic.lognormal(N, L, seed=16).astype(np.float64) * m
+    assert rel(bs.shot_contribution(n1, n2, 0.6 * m, cubic_only=True, sym=g["sym"]), g["b_cubic"]) < TOL
+    assert rel(bs.shot_contribution(n1, n2, 0.6 * m, data=d, data2=0.7 * d, sym=g["sym"]), g["b_full"]) < TOL
+
+
 def test_philox_known_answers():
     """Philox4x32-10 known-answer vectors of the Random123 distribution (kat_vectors)."""
     cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
