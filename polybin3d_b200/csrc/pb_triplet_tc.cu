@@ -32,6 +32,12 @@ constexpr int TC_KT = 64;                  // voxels per tile (4 MMA K steps of 
 constexpr int TC_NCHUNK = TC_KT / 8;       // 16-byte K chunks per tile
 constexpr int TC_STAGE_LD = TC_KT;         // fp32 staging row stride (elements; TMA box rows are dense)
 constexpr int TC_STAGES = 4;               // staging ring depth (tiles in flight per CTA)
+#ifndef TC_NBUF
+#define TC_NBUF 3
+#endif
+// operand buffers: producers run TC_NBUF - 1 tiles ahead of the MMAs, which hides the
+// commit -> mbarrier -> wake-up round trip of the tensor-core pipe behind operand building
+constexpr int TC_OPBUF = TC_NBUF;
 constexpr int TC_CHAIN = 16;               // tiles accumulated in TMEM between FP64 folds
 constexpr int TC_MAX_NT = 4;               // pair tiles (N <= 256 each)
 constexpr int TC_MAX_NC = 64;              // C maps (M = 2 * n_c <= 128)
@@ -220,12 +226,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     double *const acc = (double *)smem;
     unsigned char *const stage0 = smem + geo.acc_bytes;
     unsigned char *const abuf0 = stage0 + TC_STAGES * geo.stage_bytes;
-    unsigned char *const bbuf0 = abuf0 + 2 * geo.a_bytes;
-    int32_t *const spairs = (int32_t *)(bbuf0 + 2 * geo.b_bytes);
+    unsigned char *const bbuf0 = abuf0 + TC_OPBUF * geo.a_bytes;
+    int32_t *const spairs = (int32_t *)(bbuf0 + TC_OPBUF * geo.b_bytes);
     auto stage = [&](int k) { return (float *)(stage0 + k * geo.stage_bytes); };
 
     __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES];
-    __shared__ __align__(8) uint64_t opready[2], opfree[2], accfree[2];
+    __shared__ __align__(8) uint64_t opready[TC_OPBUF], opfree[TC_OPBUF], accfree[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
@@ -234,7 +240,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int64_t my_tiles = n_tiles > blockIdx.x ? (n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
     // operand buffers start at zero: padding rows stay zero for the whole kernel
-    for (int i = tid; i < (2 * geo.a_bytes + 2 * geo.b_bytes) / 16; i += TC_THREADS)
+    for (int i = tid; i < TC_OPBUF * (geo.a_bytes + geo.b_bytes) / 16; i += TC_THREADS)
         reinterpret_cast<uint4 *>(abuf0)[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < 2 * geo.n_pairs; i += TC_THREADS) spairs[i] = pairs[i];
     for (int i = tid; i < geo.n_pairs * n_c; i += TC_THREADS) acc[i] = 0.0;
@@ -243,11 +249,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             mbar_init(&full[k], use_tma ? 1 : 32);
             mbar_init(&empty[k], TC_PROD);
         }
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < TC_OPBUF; ++k) {
             mbar_init(&opready[k], TC_PROD);
             mbar_init(&opfree[k], 1);
-            mbar_init(&accfree[k], TC_EPI);
         }
+        for (int k = 0; k < 2; ++k) mbar_init(&accfree[k], TC_EPI);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -304,8 +310,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const uint64_t adesc0 = umma_desc(0, geo.a_lbo, 128);
             int chain = 0, chain_pos = 0;
             for (int64_t it = 0; it < my_tiles; ++it) {
-                const int buf = (int)(it & 1);
-                if (!mbar_wait_bounded(&opready[buf], (uint32_t)((it >> 1) & 1))) { atomicExch(&abort_flag, 1); break; }
+                const int buf = (int)(it % TC_OPBUF);
+                if (!mbar_wait_bounded(&opready[buf], (uint32_t)((it / TC_OPBUF) & 1))) {
+                    atomicExch(&abort_flag, 1);
+                    break;
+                }
                 if (chain_pos == 0 && chain >= geo.dsets) {
                     const int pc = chain - geo.dsets;
                     if (!mbar_wait_bounded(&accfree[pc % geo.dsets], (uint32_t)((pc / geo.dsets) & 1))) {
@@ -387,12 +396,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         int chain = 0, chain_pos = 0;
         for (int64_t it = 0; it < my_tiles; ++it) {
-            const int buf = (int)(it & 1);
+            const int buf = (int)(it % TC_OPBUF);
             const int slot = (int)(it % TC_STAGES);
             bool good = true;
             if (lane == 0) {
                 good = mbar_wait_bounded(&full[slot], (uint32_t)((it / TC_STAGES) & 1));
-                if (good && it >= 2) good = mbar_wait_bounded(&opfree[buf], (uint32_t)(((it - 2) >> 1) & 1));
+                if (good && it >= TC_OPBUF)
+                    good = mbar_wait_bounded(&opfree[buf], (uint32_t)(((it - TC_OPBUF) / TC_OPBUF) & 1));
             }
             good = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
             if (!good) { atomicExch(&abort_flag, 1); break; }
@@ -454,7 +464,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int dset = chain % geo.dsets;
                 if (warp < TC_EPI) {
                     good = true;
-                    if (lane == 0) good = mbar_wait_bounded(&opfree[buf], (uint32_t)((it >> 1) & 1));
+                    if (lane == 0) good = mbar_wait_bounded(&opfree[buf], (uint32_t)((it / TC_OPBUF) & 1));
                     good = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
                     if (!good) { atomicExch(&abort_flag, 1); break; }
                     tc_fence_after();
@@ -507,7 +517,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // ---------------- teardown ----------------
     if (warp == TC_MMAW && lane == 0 && last_issued >= 0) {
         // the MMAs of the last tile must drain before TMEM is freed (bounded)
-        mbar_wait_bounded(&opfree[last_issued & 1], (uint32_t)((last_issued >> 1) & 1));
+        mbar_wait_bounded(&opfree[last_issued % TC_OPBUF], (uint32_t)((last_issued / TC_OPBUF) & 1));
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     tc_fence_before();
@@ -586,7 +596,7 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, TcGeom *g) {
     g->stage_bytes = n_rows * TC_STAGE_LD * 4;
     g->table_bytes = (int)(2 * g->n_pairs * sizeof(int32_t));
     g->acc_bytes = (g->n_pairs * n_c * 8 + 127) / 128 * 128;
-    g->smem_bytes = g->acc_bytes + TC_STAGES * g->stage_bytes + 2 * g->a_bytes + 2 * g->b_bytes +
+    g->smem_bytes = g->acc_bytes + TC_STAGES * g->stage_bytes + TC_OPBUF * (g->a_bytes + g->b_bytes) +
                     (g->table_bytes + 15) / 16 * 16;
     if (g->smem_bytes > 225 * 1024)
         return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: tile too large for shared memory");
