@@ -189,24 +189,23 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Warp roles: warps 0..TC_PROD-1 produce operands (TC_EPI of them also fold the TMEM
-// accumulators), warp TC_PROD stages tiles (TMA, or cp.async), warp TC_PROD+1 issues MMAs.
+// Warp roles: warps 0..TC_PROD-1 produce operands, warp TC_PROD stages tiles (TMA, or
+// cp.async), warp TC_PROD+1 issues MMAs, warps TC_FOLD0.. fold the TMEM accumulators of each
+// finished chain into the FP64 sums while the producers go on with the next one.
 #ifndef TC_NPROD
 #define TC_NPROD 14
 #endif
 #ifndef TC_NUPT
 #define TC_NUPT 3
 #endif
-#ifndef TC_NEPI
-#define TC_NEPI 12
-#endif
 constexpr int TC_PROD = TC_NPROD;  // producer warps
 constexpr int TC_UPT = TC_NUPT;    // units per producer thread handled with hoisted loads
-constexpr int TC_EPI = TC_NEPI;    // producer warps that also fold accumulators (TC_EPI / 4 per TMEM lane quarter)
-constexpr int TC_THREADS = 32 * (TC_PROD + 2);
-static_assert(TC_EPI % 4 == 0 && TC_EPI <= TC_PROD, "fold warps: a multiple of 4, all producers");
+constexpr int TC_FOLDW = 4;        // fold warps, one per TMEM lane quarter
+constexpr int TC_THREADS = 32 * (TC_PROD + 2 + TC_FOLDW);
 constexpr int TC_LOADW = TC_PROD;  // staging warp
 constexpr int TC_MMAW = TC_PROD + 1;
+constexpr int TC_FOLD0 = TC_PROD + 2;
+static_assert(TC_FOLD0 % 4 == 0, "fold warp w reads TMEM lane quarter w % 4: they must start on a multiple of 4");
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
@@ -231,7 +230,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     auto stage = [&](int k) { return (float *)(stage0 + k * geo.stage_bytes); };
 
     __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES];
-    __shared__ __align__(8) uint64_t opready[TC_OPBUF], opfree[TC_OPBUF], accfree[2];
+    __shared__ __align__(8) uint64_t opready[TC_OPBUF], opfree[TC_OPBUF], accready[2], accfree[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
@@ -253,7 +252,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             mbar_init(&opready[k], TC_PROD);
             mbar_init(&opfree[k], 1);
         }
-        for (int k = 0; k < 2; ++k) mbar_init(&accfree[k], TC_EPI);
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&accready[k], 1);
+            mbar_init(&accfree[k], TC_FOLDW);
+        }
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -346,12 +348,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 umma_commit(&opfree[buf]);
                 last_issued = (int)it;
                 if (++chain_pos == TC_CHAIN || it + 1 == my_tiles) {
+                    umma_commit(&accready[dset]);  // the chain's sums are complete in TMEM
                     chain_pos = 0;
                     ++chain;
                 }
             }
         }
-    } else {
+    } else if (warp < TC_PROD) {
         // ---------------- producer warps ----------------
         // Units of 8 voxels; K chunk c holds tile voxels {4c..4c+3, 32+4c..32+4c+3} for both
         // operands (the sum over K is order-free), so the 8 lanes of one row read 128
@@ -394,7 +397,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             u_pair[k] = false;
             if (u_ok[k]) unit_info(u, u_ra[k], u_rb[k], u_dst[k], u_lo[k], u_pair[k]);
         }
-        int chain = 0, chain_pos = 0;
         for (int64_t it = 0; it < my_tiles; ++it) {
             const int buf = (int)(it % TC_OPBUF);
             const int slot = (int)(it % TC_STAGES);
@@ -458,60 +460,59 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 mbar_arrive(&empty[slot]);
                 mbar_arrive(&opready[buf]);
             }
-            if (++chain_pos == TC_CHAIN || it + 1 == my_tiles) {
-                // fold this chain: wait for its last MMAs, read TMEM, sum the hi and lo rows
-                // of each map (neighbouring lanes) and add into the FP64 sums
-                const int dset = chain % geo.dsets;
-                if (warp < TC_EPI) {
-                    good = true;
-                    if (lane == 0) good = mbar_wait_bounded(&opfree[buf], (uint32_t)((it / TC_OPBUF) & 1));
-                    good = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
-                    if (!good) { atomicExch(&abort_flag, 1); break; }
-                    tc_fence_after();
-                    const int q = warp & 3, h = warp >> 2;  // lane quarter, column share 0..2
-                    // D row held by this lane: M = 64 -> rows 16q..16q+15 in lanes 0..15
-                    const int m = geo.M == 64 ? (lane < 16 ? 16 * q + lane : -1) : 32 * q + lane;
-                    const int j = m >= 0 ? (m >> 1) : -1;
-                    // after the hi + lo shuffle both lanes of a map hold its sums: the hi lane
-                    // adds columns 0..3 of each group of 8, the lo lane columns 4..7
-                    const bool writer = m >= 0 && j < n_c;
-                    const int half = m & 1;
-                    const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(dset * geo.ntot);
-                    const int ngrp = geo.ntot / 8;
-                    for (int cc = h; cc < ngrp; cc += 2 * (TC_EPI / 4)) {
-                        // two column groups per TMEM wait
-                        const int cc2 = cc + TC_EPI / 4;
-                        float v[2][8];
-                        tmem_ld8_issue(tbase + cc * 8, v[0]);
-                        if (cc2 < ngrp) tmem_ld8_issue(tbase + cc2 * 8, v[1]);
-                        tmem_ld_wait();
+        }
+    }
+    if (warp >= TC_FOLD0) {
+        // ---------------- fold warps ----------------
+        // chain c lives in accumulator set c % dsets; its last MMAs commit accready
+        const int q = warp & 3;  // TMEM lane quarter
+        // D row held by this lane: M = 64 -> rows 16q..16q+15 in lanes 0..15
+        const int m = geo.M == 64 ? (lane < 16 ? 16 * q + lane : -1) : 32 * q + lane;
+        const int j = m >= 0 ? (m >> 1) : -1;
+        // after the hi + lo shuffle both lanes of a map hold its sums: the hi lane adds
+        // columns 0..3 of each group of 8, the lo lane columns 4..7
+        const bool writer = m >= 0 && j < n_c;
+        const int half = m & 1;
+        const int ngrp = geo.ntot / 8;
+        const int64_t n_chains = (my_tiles + TC_CHAIN - 1) / TC_CHAIN;
+        for (int64_t c = 0; c < n_chains; ++c) {
+            const int dset = (int)(c % geo.dsets);
+            bool good = true;
+            if (lane == 0) good = mbar_wait_bounded(&accready[dset], (uint32_t)((c / geo.dsets) & 1));
+            good = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
+            if (!good) { atomicExch(&abort_flag, 1); break; }
+            tc_fence_after();
+            const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(dset * geo.ntot);
+            for (int cc = 0; cc < ngrp; cc += 2) {
+                // two column groups per TMEM wait
+                const int cc2 = cc + 1;
+                float v[2][8];
+                tmem_ld8_issue(tbase + cc * 8, v[0]);
+                if (cc2 < ngrp) tmem_ld8_issue(tbase + cc2 * 8, v[1]);
+                tmem_ld_wait();
 #pragma unroll
-                        for (int g2 = 0; g2 < 2; ++g2) {
-                            const int c8 = g2 == 0 ? cc : cc2;
-                            if (c8 >= ngrp) break;
+                for (int g2 = 0; g2 < 2; ++g2) {
+                    const int c8 = cc + g2;
+                    if (c8 >= ngrp) break;
 #pragma unroll
-                            for (int k = 0; k < 8; ++k) v[g2][k] += __shfl_xor_sync(0xffffffffu, v[g2][k], 1);
-                            if (writer) {
-                                const int col0 = c8 * 8;
-                                int t = 0;
-                                while (t + 1 < geo.n_nt && col0 >= geo.nt_col[t + 1]) ++t;
-                                const int pend = (t + 1 < geo.n_nt) ? geo.nt_start[t + 1] : geo.n_pairs;
+                    for (int k = 0; k < 8; ++k) v[g2][k] += __shfl_xor_sync(0xffffffffu, v[g2][k], 1);
+                    if (writer) {
+                        const int col0 = c8 * 8;
+                        int t = 0;
+                        while (t + 1 < geo.n_nt && col0 >= geo.nt_col[t + 1]) ++t;
+                        const int pend = (t + 1 < geo.n_nt) ? geo.nt_start[t + 1] : geo.n_pairs;
 #pragma unroll
-                                for (int k = 0; k < 4; ++k) {
-                                    const float val = half ? v[g2][4 + k] : v[g2][k];
-                                    const int p = geo.nt_start[t] + (col0 + 4 * half + k - geo.nt_col[t]);
-                                    if (p < pend) acc[p * n_c + j] += (double)val;
-                                }
-                            }
+                        for (int k = 0; k < 4; ++k) {
+                            const float val = half ? v[g2][4 + k] : v[g2][k];
+                            const int p = geo.nt_start[t] + (col0 + 4 * half + k - geo.nt_col[t]);
+                            if (p < pend) acc[p * n_c + j] += (double)val;
                         }
                     }
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&accfree[dset]);
                 }
-                chain_pos = 0;
-                ++chain;
             }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&accfree[dset]);
         }
     }
     // ---------------- teardown ----------------
