@@ -61,7 +61,8 @@ struct TcGeom {
     int stage_bytes;
     int tmem_cols, dsets;
     int table_bytes;            // pair table staged in shared memory
-    int acc_bytes;              // FP64 accumulators [n_pairs][n_c]
+    int acc_ld;                 // row stride (doubles) of the FP64 accumulators [n_c][acc_ld], = 2 mod 16
+    int acc_bytes;
     int smem_bytes;
 };
 
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int i = tid; i < TC_OPBUF * (geo.a_bytes + geo.b_bytes) / 16; i += TC_THREADS)
         reinterpret_cast<uint4 *>(abuf0)[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < 2 * geo.n_pairs; i += TC_THREADS) spairs[i] = pairs[i];
-    for (int i = tid; i < geo.n_pairs * n_c; i += TC_THREADS) acc[i] = 0.0;
+    for (int i = tid; i < n_c * geo.acc_ld; i += TC_THREADS) acc[i] = 0.0;
     if (tid == 0) {
         for (int k = 0; k < TC_STAGES; ++k) {
             mbar_init(&full[k], use_tma ? 1 : 32);
@@ -469,8 +470,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // D row held by this lane: M = 64 -> rows 16q..16q+15 in lanes 0..15
         const int m = geo.M == 64 ? (lane < 16 ? 16 * q + lane : -1) : 32 * q + lane;
         const int j = m >= 0 ? (m >> 1) : -1;
-        // after the hi + lo shuffle both lanes of a map hold its sums: the hi lane adds
-        // columns 0..3 of each group of 8, the lo lane columns 4..7
+        // after the hi + lo shuffle both lanes of a map hold its sums: the hi lane adds the
+        // even columns of each group of 8, the lo lane the odd ones; with the accumulator row
+        // stride = 2 mod 16 the 16 lanes of one store hit 16 different bank pairs
         const bool writer = m >= 0 && j < n_c;
         const int half = m & 1;
         const int ngrp = geo.ntot / 8;
@@ -503,9 +505,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         const int pend = (t + 1 < geo.n_nt) ? geo.nt_start[t + 1] : geo.n_pairs;
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
-                            const float val = half ? v[g2][4 + k] : v[g2][k];
-                            const int p = geo.nt_start[t] + (col0 + 4 * half + k - geo.nt_col[t]);
-                            if (p < pend) acc[p * n_c + j] += (double)val;
+                            const float val = half ? v[g2][2 * k + 1] : v[g2][2 * k];
+                            const int p = geo.nt_start[t] + (col0 + 2 * k + half - geo.nt_col[t]);
+                            if (p < pend) acc[j * geo.acc_ld + p] += (double)val;
                         }
                     }
                 }
@@ -526,7 +528,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_fence_after();
     if (tid == 0 && abort_flag) atomicExch(err, PB_ERR_TIMEOUT);
     double *part = partials + (size_t)blockIdx.x * geo.n_pairs * n_c;
-    for (int i = tid; i < geo.n_pairs * n_c; i += TC_THREADS) part[i] = acc[i];
+    for (int i = tid; i < geo.n_pairs * n_c; i += TC_THREADS) {
+        const int p = i / n_c;
+        part[i] = acc[(i - p * n_c) * geo.acc_ld + p];
+    }
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(geo.tmem_cols));
 }
@@ -596,7 +601,8 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, TcGeom *g) {
     g->tmem_cols = cols;
     g->stage_bytes = n_rows * TC_STAGE_LD * 4;
     g->table_bytes = (int)(2 * g->n_pairs * sizeof(int32_t));
-    g->acc_bytes = (g->n_pairs * n_c * 8 + 127) / 128 * 128;
+    g->acc_ld = g->n_pairs + (2 - g->n_pairs % 16 + 16) % 16;
+    g->acc_bytes = (n_c * g->acc_ld * 8 + 127) / 128 * 128;
     g->smem_bytes = g->acc_bytes + TC_STAGES * g->stage_bytes + TC_OPBUF * (g->a_bytes + g->b_bytes) +
                     (g->table_bytes + 15) / 16 * 16;
     if (g->smem_bytes > 225 * 1024)
