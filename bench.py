@@ -35,7 +35,7 @@ METRIC = "Bk fields/s at 256^3 (16 bins, lmax=2, TSC, mixed precision)"
 WORKLOAD = "Bk_ideal 256^3 box 2000 Mpc/h, TSC, lmax=2, 16 linear bins 2pi/2000..0.2, 888 triangle bins"
 # DRAM bytes (read + write) of one contraction launch of this workload, from one ncu capture
 # (profiles/triplet_tc_bk256.md)
-TC_TRAFFIC_BYTES = 909_507_840
+TC_TRAFFIC_BYTES = 911_428_352
 
 
 FISHER = {

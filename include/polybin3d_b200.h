@@ -34,7 +34,7 @@ extern "C" {
 #define PB_API
 #endif
 
-#define PB_ABI_VERSION 1
+#define PB_ABI_VERSION 2
 
 #define PB_OK 0
 #define PB_ERR_INVALID (-1)     /* bad argument (shape, size, null pointer, range)      */
@@ -49,9 +49,13 @@ extern "C" {
 
 typedef struct pb_grid {
     int32_t n[3];      /* real-space grid; n[2] even                                        */
-    int32_t reserved;  /* 0                                                                 */
+    int32_t flags;     /* bit 0 (PB_GRID_LOS): los[] holds the line of sight of mu          */
     double kf[3];      /* fundamental frequencies 2 pi / L_i                                */
+    double los[3];     /* unit line-of-sight vector, read when flags & PB_GRID_LOS:         */
+                       /* mu = (k . los)/|k|, the local-sightline mu grid of                */
+                       /* PolyBin3D/base.py:111-116; otherwise mu = k_z/|k| (global)        */
 } pb_grid_t;
+#define PB_GRID_LOS 1
 
 /* Library identity and errors.  No reference counterpart (the reference raises Python
  * exceptions: e.g. PolyBin3D/base.py:54, pspec.py:591). */

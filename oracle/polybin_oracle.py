@@ -175,7 +175,8 @@ def pixel_window_1d(kind, x):
 class OracleBase:
     """Grids and FFTs of the reference base class, global sightline, real FFTs."""
 
-    def __init__(self, boxsize, gridsize, Pk=None, pixel_window="none", nthreads=None, kernels=None):
+    def __init__(self, boxsize, gridsize, Pk=None, pixel_window="none", nthreads=None, kernels=None,
+                 boxcenter=None, sightline="global"):
         """kernels: optionally the reference's compiled Cython module (oracle/_ref, built from
         utils.pyx); its IntegrationUtils / MapUtils then run fourier_filter, cross_integrate,
         integrate_row and prod_real_diff (same results, multithreaded): the CPU-baseline
@@ -184,6 +185,8 @@ class OracleBase:
         self.gridsize = np.asarray(gridsize, dtype=int)
         self.nthreads = nthreads or os.cpu_count()
         self.pixel_window = pixel_window
+        self.sightline = sightline
+        self.boxcenter = np.zeros(3) if boxcenter is None else np.asarray(boxcenter, dtype=np.float64)
         self.volume = self.boxsize.prod()
         self.kF = 2.0 * np.pi / self.boxsize                         # base.py:64
         self.kNy = self.gridsize * self.kF * 0.5                        # base.py:65
@@ -206,7 +209,11 @@ class OracleBase:
             self.pixel_window_grid = np.asarray(np.meshgrid(*w1d, indexing="ij")).prod(axis=0)
         self.muk_grid = np.zeros(self.modk_grid.shape)                  # base.py:115-116
         nz = self.modk_grid != 0
-        self.muk_grid[nz] = self.k_grids[2][nz] / self.modk_grid[nz]
+        if sightline == "global":                                       # base.py:111-114
+            sv = np.asarray([0.0, 0.0, 1.0])
+        else:
+            sv = self.boxcenter / np.sqrt(np.sum(self.boxcenter ** 2))
+        self.muk_grid[nz] = np.sum(sv[:, None] * np.asarray(self.k_grids)[:, nz], axis=0) / self.modk_grid[nz]
         self.Pk0_grid = interp1d(self.Pfid[0], self.Pfid[1], bounds_error=False,
                                  fill_value=0.0)(self.modk_grid)         # base.py:122
         self.invPk0_grid = np.zeros(self.modk_grid.shape)               # base.py:125-131
@@ -215,6 +222,10 @@ class OracleBase:
         self.Pk0_grid[~np.isfinite(self.Pk0_grid)] = 0.0
         self.invPk0_grid[self.modk_grid == 0] = 1.0
         self.Pk0_grid[self.modk_grid == 0] = 1.0
+        if sightline == "local":                                        # base.py:75-79
+            r_arrs = [np.fft.fftshift(np.arange(-self.gridsize[i] // 2, self.gridsize[i] // 2)) * self.boxsize[i]
+                      / self.gridsize[i] + self.boxcenter[i] for i in range(3)]
+            self.r_grids = np.meshgrid(*r_arrs, indexing="ij")
         self._iu = self._mu = None
         if kernels is not None:                                         # base.py:138-144
             self._iu = kernels.IntegrationUtils(self.modk_grid, True, self.nthreads, self.degeneracy_factor,
@@ -321,6 +332,16 @@ class OracleBase:
         im = (rad * np.sin(2 * np.pi * u2)).reshape(tuple(self.gridsize))
         return re, im
 
+    def apply_fourier_harmonics(self, a_real, l):
+        """sum_m Y_lm(k) rfftn(Y_lm(x) a(x)) (base.py:402-411) with the real harmonics of the
+        positions and of the wavevectors (utils.pyx:518-609), even l."""
+        yr = real_harmonics_fourier(self.r_grids, l)[l]
+        yk = real_harmonics_fourier(self.k_grids, l)[l]
+        out = np.zeros(self.modk_grid.shape, dtype=np.complex128)
+        for m in range(len(yr)):
+            out += self.to_fourier(a_real * yr[m]) * yk[m]
+        return out
+
     def inverse_fiducial_draw(self):
         """The shot-noise GRFs' spectrum P_A = 1/P_fid on the grid, as generate_data
         interpolates it (zero outside the table), and 1/P_A extended by its end values
@@ -374,7 +395,11 @@ class OraclePSpec:
             x = x * b.invPk0_grid / np.sqrt(self.sq_mask_mean)
         out = np.zeros(self.N_bins)
         for li in range(self.Nl):
-            out[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.integrate(x, self.k_bins, 2 * li)
+            if b.sightline == "global" or li == 0:
+                out[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.integrate(x, self.k_bins, 2 * li)
+            else:                                                        # pspec.py:672-680
+                lm = b.apply_fourier_harmonics(b.to_real(x), 2 * li)
+                out[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(x, lm, self.k_bins, 0)
         return out * b.volume / b.gridsize.prod() ** 2
 
     def fisher_ideal(self, discreteness_correction=True):
@@ -554,9 +579,14 @@ class OracleBSpec:
         b = self.base
         ks = self.k_bins_squeeze
         g = np.zeros((self.Nl, self.Nk_squeeze) + tuple(b.gridsize))
+        real = b.to_real(weighted_fourier) if (b.sightline == "local" and self.lmax > 0) else None
         for l in range(0, self.lmax + 1, 2):
+            if l > 0 and b.sightline == "local":                        # bspec.py:950-954
+                src, ll = b.apply_fourier_harmonics(real, l), 0
+            else:
+                src, ll = weighted_fourier, l
             for i in range(self.Nk_squeeze):
-                g[l // 2, i] = b.to_real(b.fourier_filter(weighted_fourier, l, ks[i], ks[i + 1]))
+                g[l // 2, i] = b.to_real(b.fourier_filter(src, ll, ks[i], ks[i + 1]))
         return g
 
     def weighted_data(self, data, filtering="ideal"):

@@ -27,8 +27,12 @@ _ERRORS = {-1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: MemoryError, 
            -6: TimeoutError}
 
 
+PB_GRID_LOS = 1
+
+
 class PBGrid(ctypes.Structure):
-    _fields_ = [("n", ctypes.c_int32 * 3), ("reserved", ctypes.c_int32), ("kf", ctypes.c_double * 3)]
+    _fields_ = [("n", ctypes.c_int32 * 3), ("flags", ctypes.c_int32), ("kf", ctypes.c_double * 3),
+                ("los", ctypes.c_double * 3)]
 
 
 _lib = None
@@ -82,7 +86,7 @@ def load(path=LIB_PATH):
             fn = getattr(lib, name)
             fn.argtypes = args
             fn.restype = res
-        if lib.pb_abi_version() != 1:
+        if lib.pb_abi_version() != 2:
             raise ImportError("polybin3d_b200: ABI version mismatch")
         _lib = lib
         return lib

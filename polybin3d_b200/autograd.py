@@ -54,6 +54,8 @@ class PkNumerator(torch.autograd.Function):
     @staticmethod
     def forward(ctx, d, ps):
         b = ps.base
+        if b.sightline == 'local' and ps.lmax > 0:
+            raise NotImplementedError("differentiable numerators are implemented for the global sightline")
         d = d.to(torch.float64).contiguous()
         ctx.ps = ps
         ctx.save_for_backward(d)
@@ -115,6 +117,8 @@ class BkNumerator(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, d, bs):
+        if bs.base.sightline == 'local' and bs.lmax > 0:
+            raise NotImplementedError("differentiable numerators are implemented for the global sightline")
         if not hasattr(bs, 'sym_factor'):
             bs._compute_symmetry_factor()
         ctx.in_dtype = d.dtype

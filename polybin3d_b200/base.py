@@ -70,7 +70,13 @@ class PolyBin3D:
             assert np.abs(self.boxcenter).sum() == 0., "Global sightlines should only be used for simulation data!"
         if self.sightline == 'local':
             assert np.abs(self.boxcenter).sum() != 0., "Local sightlines should only be used for lightcone data!"
-            raise NotImplementedError("backend='cuda' implements the global (z-axis) sightline only")
+        # line of sight of the mu grid: the z axis, or the direction of the box centre
+        # (base.py:111-114); the local-sightline multipoles also use the real harmonics of
+        # the voxel positions (harmonics.py)
+        if self.sightline == 'global':
+            self.sight_vector = np.asarray([0., 0., 1.])
+        else:
+            self.sight_vector = self.boxcenter / np.sqrt(np.sum(self.boxcenter ** 2))
 
         # derived parameters (base.py:63-74)
         self.volume = self.boxsize.prod()
@@ -101,11 +107,7 @@ class PolyBin3D:
         # device set-up
         nat.require_cuda()
         self.device = torch.device(device) if device is not None else torch.device('cuda', torch.cuda.current_device())
-        self.grid = nat.PBGrid()
-        for i in range(3):
-            self.grid.n[i] = int(self.gridsize[i])
-            self.grid.kf[i] = float(self.kF[i])
-        self.grid.reserved = 0
+        self.grid = self.grid_of(self.gridsize)
         self.nhalf_shape = (int(self.gridsize[0]), int(self.gridsize[1]), int(self.gridsize[2]) // 2 + 1)
         self.nreal = int(self.gridsize.prod())
         self.nhalf = int(np.prod(self.nhalf_shape))
@@ -149,9 +151,29 @@ class PolyBin3D:
             mk = self.modk_grid
             mu = np.zeros(mk.shape)
             nz = mk != 0
-            mu[nz] = self.k_grids[2][nz] / mk[nz]
+            mu[nz] = np.sum(self.sight_vector[:, None] * np.asarray(self.k_grids)[:, nz], axis=0) / mk[nz]
             return mu
         return self._lazy('muk', f)
+
+    @property
+    def r_grids(self):
+        """Voxel positions relative to the observer: fftshift order plus the box centre
+        (base.py:75-79); local sightline only."""
+        assert self.sightline == 'local', "r_grids are defined for the local sightline"
+
+        def f():
+            r_arrs = [np.fft.fftshift(np.arange(-self.gridsize[i] // 2, self.gridsize[i] // 2)) * self.boxsize[i]
+                      / self.gridsize[i] + self.boxcenter[i] for i in range(3)]
+            return np.meshgrid(*r_arrs, indexing='ij')
+        return self._lazy('rgrids', f)
+
+    @property
+    def harmonics(self):
+        """Device real-harmonic grids of this box (local-sightline multipoles)."""
+        if getattr(self, '_harm', None) is None:
+            from .harmonics import Harmonics
+            self._harm = Harmonics(self)
+        return self._harm
 
     def _pixel_window_1d(self, k):
         """Pixel window functions including first-order alias corrections (base.py:231-254)."""
@@ -256,7 +278,12 @@ class PolyBin3D:
         for i in range(3):
             g.n[i] = int(dims[i])
             g.kf[i] = float(self.kF[i])
-        g.reserved = 0
+        g.flags = 0
+        if self.sightline == 'local':
+            # mu = (k . n)/|k| with n the unit vector to the box centre (base.py:111-116)
+            g.flags = nat.PB_GRID_LOS
+            for i in range(3):
+                g.los[i] = float(self.sight_vector[i])
         return g
 
     def _plan(self, batch, precision, direction, dims=None):

@@ -13,34 +13,7 @@ from scipy.interpolate import interp1d
 
 from . import _native as nat
 from . import realisations
-
-
-def real_harmonics(k_grids, l):
-    """Real spherical harmonics of the unit vector for even l = 2, 4; the same functions and
-    normalisation as compute_real_harmonics (PolyBin3D/cython/utils.pyx:518-609), so that
-    sum_m Y_lm(k) Y_lm(k') = L_l(k.k')."""
-    kx, ky, kz = k_grids
-    norm = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
-    safe = np.where(norm == 0, 1.0, norm)
-    xh, yh, zh = [np.where(norm == 0, 0.0, c / safe) for c in (kx, ky, kz)]
-    if l == 2:
-        return [6.0 * xh * yh * np.sqrt(1.0 / 12.0),
-                3.0 * yh * zh * np.sqrt(1.0 / 3.0),
-                zh ** 2 - xh ** 2 / 2.0 - yh ** 2 / 2.0,
-                3.0 * xh * zh * np.sqrt(1.0 / 3.0),
-                (3 * xh ** 2 - 3 * yh ** 2) * np.sqrt(1.0 / 12.0)]
-    if l == 4:
-        x2, y2, z2 = xh * xh, yh * yh, zh * zh
-        return [(420.0 * x2 * xh * yh - 420.0 * xh * y2 * yh) * np.sqrt(1.0 / 20160.0),
-                (315.0 * x2 * yh * zh - 105.0 * y2 * yh * zh) * np.sqrt(1.0 / 2520.0),
-                (-15.0 * x2 * xh * yh - 15.0 * xh * y2 * yh + 90.0 * xh * yh * z2) * np.sqrt(1.0 / 180.0),
-                (-7.5 * x2 * yh * zh - 7.5 * y2 * yh * zh + 10.0 * yh * z2 * zh) * np.sqrt(1.0 / 10.0),
-                35.0 / 8.0 * z2 * z2 - 15.0 / 4.0 * z2 + 3.0 / 8.0,
-                (-7.5 * x2 * xh * zh - 7.5 * xh * y2 * zh + 10.0 * xh * z2 * zh) * np.sqrt(1.0 / 10.0),
-                (-7.5 * x2 * x2 + 45.0 * x2 * z2 + 7.5 * y2 * y2 - 45.0 * y2 * z2) * np.sqrt(1.0 / 180.0),
-                (105.0 * x2 * xh * zh - 315.0 * xh * y2 * zh) * np.sqrt(1.0 / 2520.0),
-                (105.0 * x2 * x2 - 630.0 * x2 * y2 + 105.0 * y2 * y2) * np.sqrt(1.0 / 20160.0)]
-    raise ValueError("l must be 2 or 4")
+from .harmonics import real_harmonics
 
 
 class BSpec:
@@ -259,13 +232,17 @@ class BSpec:
         return self.base.to_device_grid(('bk_invp', id(self)), lambda: self.invPk0, torch.float64)
 
     def _data_weight(self, dtype):
-        """invP / W on the half grid for the ideal numerator (None when identically 1)."""
+        """invP / W on the half grid for the ideal numerator (None when identically 1 on the
+        binned modes).  With unit weighting invP is 1 on every binned mode, so the global
+        sightline skips it; the local sightline's l > 0 maps mix all modes of the weighted
+        field (through the real-space harmonics), so there invP keeps its zero at k = 0."""
         b = self.base
-        if self._unit_w and b.pixel_window == 'none':
+        unit = self._unit_w and not (b.sightline == 'local' and self.lmax > 0)
+        if unit and b.pixel_window == 'none':
             return None
 
         def f():
-            w = np.ones(b.nhalf_shape) if self._unit_w else self.invPk0.copy()
+            w = np.ones(b.nhalf_shape) if unit else self.invPk0.copy()
             if b.pixel_window != 'none':
                 W = b.pixel_window_grid
                 nz = W != 0
@@ -322,7 +299,9 @@ class BSpec:
         prec = nat.precision_of(dtype)
         dims = self.map_grid if coarse else tuple(int(n) for n in b.gridsize)
         wp = 0 if w is None else 1
-        maps = [(0, ks[bb], ks[bb + 1], l1, l2, sc / b.nreal, wp) for (bb, l1, l2, sc) in specs]
+        # spec: (bin, l1, l2, scale[, source index]); the sources lie src_stride apart
+        maps = [(sp[4] if len(sp) > 4 else 0, ks[sp[0]], ks[sp[0] + 1], sp[1], sp[2], sp[3] / b.nreal, wp)
+                for sp in specs]
         if self.synthesis != 'cufft' and self._synth_ok.get(dims, True):
             if out is None:
                 out = torch.empty((len(specs),) + tuple(dims), dtype=dtype, device=b.device)
@@ -401,8 +380,24 @@ class BSpec:
 
     def _g_maps(self, xk, w, scale, out=None):
         """All Nl x Nk_squeeze bin-filtered maps g[l/2, b] of one weighted spectrum."""
+        if self.base.sightline == 'local' and self.lmax > 0:
+            return self._g_maps_local(xk, w, scale, out)
         specs = [(bb, l, 0, scale) for l in range(0, self.lmax + 1, 2) for bb in range(self.Nk_squeeze)]
         return self._binned_maps(xk, specs, w, xk.real.dtype, out=out)
+
+    def _g_maps_local(self, xk, w, scale, out=None):
+        """Local sightline (bspec.py:932-954): with D = scale w xk and d = irfftn(D), the
+        l = 0 maps filter D and the l > 0 maps filter sum_m Y_lm(k) FT[Y_lm(r) d(r)], all with
+        the plain bin filter, in one synthesis over the stacked sources."""
+        b = self.base
+        prec = nat.precision_of(xk.dtype)
+        D = torch.empty_like(xk)
+        nat.spectral_filter(b.grid, prec, xk.contiguous(), D,
+                            [(0, -1.0, np.inf, 0, 0, float(scale), 0 if w is None else 1)], w=w)
+        d = b.to_real(D)
+        srcs = torch.stack([D] + [b.harmonics.apply_fourier(d, l) for l in range(2, self.lmax + 1, 2)])
+        specs = [(bb, 0, 0, 1.0, l // 2) for l in range(0, self.lmax + 1, 2) for bb in range(self.Nk_squeeze)]
+        return self._binned_maps(srcs, specs, None, xk.real.dtype, out=out)
 
     def _compute_bk_numerator(self, data, include_linear_term=True, filtering='ideal', verb=False):
         assert filtering in ['ideal', 'Sinv'], "Unknown filtering option supplied!"
@@ -741,6 +736,9 @@ class BSpec:
 
     def _fisher_from_fields(self, a1, a2):
         b = self.base
+        if b.sightline == 'local' and self.lmax > 0:
+            raise NotImplementedError("backend='cuda' implements the Monte Carlo Fisher matrix for the global "
+                                      "sightline; with the local sightline supply fish= to Bk_unwindowed")
         ab = self.all_bins
         ks = self.k_bins_squeeze
         F64 = nat.PB_F64
@@ -863,6 +861,8 @@ class BSpec:
         (bspec.py:695-861): the cubic term from the maps of S^-1 a1, S^-1 a2 and the
         shot-masked product (A^-1 a1)(A^-1 a2), and unless cubic_only the quadratic term from
         the data's maps with those of (A^-1 a_i) d2.  Returns quadratic - 2 cubic."""
+        if self.base.sightline == 'local' and self.lmax > 0:
+            raise NotImplementedError("backend='cuda' implements shot noise for the global sightline")
         if not cubic_only:
             assert data is not None, "Must supply data to compute the quadratic shot-noise contribution!"
             if data2 is None:

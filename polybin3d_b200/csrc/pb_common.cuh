@@ -30,6 +30,8 @@ int num_sms();
 struct Grid {
     int n0, n1, n2, nh2;     // real dims and half-axis length n2/2+1
     double kf0, kf1, kf2;
+    int los;                 // 1: mu = (k . (l0, l1, l2)) / |k|, else kz / |k|
+    double l0, l1, l2;
     int64_t nhalf;           // n0*n1*nh2
     int64_t nreal;           // n0*n1*n2
 };
@@ -41,9 +43,17 @@ __device__ __forceinline__ int freq_index(int i, int n) { return i < (n >> 1) ? 
 
 struct Mode {
     double k;    // |k|
-    double mu;   // kz/|k| (0 at k=0)
+    double mu;   // (k . line of sight)/|k| (0 at k=0)
     double deg;  // 1 + (kz > 0)
 };
+
+// k . line of sight with the three products summed left to right without FMA, as numpy
+// sums them; kz itself for the global (z-axis) line of sight
+__device__ __forceinline__ double k_dot_los(int los, double l0, double l1, double l2, double kx, double ky,
+                                            double kz) {
+    if (!los) return kz;
+    return __dadd_rn(__dadd_rn(__dmul_rn(l0, kx), __dmul_rn(l1, ky)), __dmul_rn(l2, kz));
+}
 
 // |k| exactly as numpy: k_i = (double)idx*kF_i, sqrt((kx*kx + ky*ky) + kz*kz), no FMA.
 __device__ __forceinline__ Mode mode_of(const Grid &g, int64_t idx) {
@@ -57,7 +67,7 @@ __device__ __forceinline__ Mode mode_of(const Grid &g, int64_t idx) {
     double s = __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
     Mode m;
     m.k = __dsqrt_rn(s);
-    m.mu = (m.k != 0.0) ? __ddiv_rn(kz, m.k) : 0.0;
+    m.mu = (m.k != 0.0) ? __ddiv_rn(k_dot_los(g.los, g.l0, g.l1, g.l2, kx, ky, kz), m.k) : 0.0;
     m.deg = (l > 0) ? 2.0 : 1.0;
     return m;
 }

@@ -45,6 +45,12 @@ int make_grid(const pb_grid_t *g, Grid *out) {
     out->kf0 = g->kf[0];
     out->kf1 = g->kf[1];
     out->kf2 = g->kf[2];
+    out->los = (g->flags & PB_GRID_LOS) ? 1 : 0;
+    out->l0 = out->los ? g->los[0] : 0.0;
+    out->l1 = out->los ? g->los[1] : 0.0;
+    out->l2 = out->los ? g->los[2] : 1.0;
+    if (out->los && !(out->l0 * out->l0 + out->l1 * out->l1 + out->l2 * out->l2 > 0.0))
+        return fail(PB_ERR_INVALID, "line of sight must be a non-zero vector");
     out->nhalf = (int64_t)out->n0 * out->n1 * out->nh2;
     out->nreal = (int64_t)out->n0 * out->n1 * out->n2;
     return PB_OK;

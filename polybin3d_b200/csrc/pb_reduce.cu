@@ -100,6 +100,111 @@ __global__ void __launch_bounds__(RED_THREADS) binred_kernel(Grid g, const typen
     for (int i = threadIdx.x; i < ne * nk; i += blockDim.x) dst[i] = acc[i];
 }
 
+// Many rows over the same modes (the Fisher rows: CROSS of one spectrum with N_bins Q rows,
+// or ABS2 of a batch).  The mode geometry -- bin, degeneracy x Legendre weights, the shared
+// spectrum a -- is computed once per tile of modes into shared memory and then used by every
+// row of the group, instead of once per row: the FP64 |k|, mu, bin search and Legendre
+// polynomials no longer scale with the row count, and each row is one streaming read.
+constexpr int RR_TILE = 512;                 // modes per tile (2 per thread)
+constexpr int RR_PER = RR_TILE / RED_THREADS;
+constexpr int RR_ACC_DOUBLES = 6144;         // shared accumulators per block (48 KB)
+
+// accumulator doubles rounded up to an even count, so the double2 tile after them is aligned
+__host__ __device__ __forceinline__ size_t rr_acc_len(int rows, int ne, int nk) {
+    return ((size_t)rows * ne * nk + 1) & ~(size_t)1;
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(RED_THREADS) binred_rows_kernel(Grid g, const typename cplx<T>::type *a,
+                                                                 const typename cplx<T>::type *b,
+                                                                 int64_t row_stride, RedParams p, int n_rows,
+                                                                 int rows_per_group, double *partials) {
+    using C = typename cplx<T>::type;
+    extern __shared__ __align__(16) unsigned char rr_smem[];
+    const int nk = p.nk, ne = p.n_ell;
+    const int r0 = blockIdx.y * rows_per_group;
+    const int nr = min(rows_per_group, n_rows - r0);
+    double *acc = reinterpret_cast<double *>(rr_smem);          // [nr][ne][nk]
+    double *wt = acc + rr_acc_len(rows_per_group, ne, nk);       // [ne][RR_TILE]
+    double2 *as = reinterpret_cast<double2 *>(wt + (size_t)ne * RR_TILE);  // [RR_TILE] (CROSS)
+    int *bins = reinterpret_cast<int *>(as + RR_TILE);            // [RR_TILE]
+    __shared__ double edges[PB_RED_MAX_BINS + 1];
+    for (int i = threadIdx.x; i < nr * ne * nk; i += blockDim.x) acc[i] = 0.0;
+    for (int i = threadIdx.x; i <= nk; i += blockDim.x) edges[i] = p.edges[i];
+    const int64_t n_tiles = (g.nhalf + RR_TILE - 1) / RR_TILE;
+    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int64_t t0 = tile * RR_TILE;
+        __syncthreads();  // previous tile's readers are done (and the set-up above is visible)
+        for (int j = threadIdx.x; j < RR_TILE; j += blockDim.x) {
+            const int64_t idx = t0 + j;
+            int bin = -1;
+            if (idx < g.nhalf) {
+                const Mode md = mode_of(g, idx);
+                bin = find_bin(edges, nk, md.k);
+                if (bin >= 0) {
+#pragma unroll
+                    for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                        if (e < ne) wt[e * RR_TILE + j] = md.deg * legendre(p.la[e], md.mu) * legendre(p.lb[e], md.mu);
+                }
+                if (MODE == PB_RED_CROSS) {
+                    const C v = a[idx];
+                    as[j] = make_double2((double)v.x, (double)v.y);
+                }
+            }
+            bins[j] = bin;
+        }
+        __syncthreads();
+        // each thread: RR_PER consecutive modes of the tile for every row of the group
+        const int j0 = threadIdx.x * RR_PER;
+        for (int r = 0; r < nr; ++r) {
+            const int64_t rowoff = (int64_t)(r0 + r) * row_stride;
+            double *accr = acc + (size_t)r * ne * nk;
+            int cur = -1;
+            double run[PB_RED_MAX_ELLS];
+#pragma unroll
+            for (int e = 0; e < PB_RED_MAX_ELLS; ++e) run[e] = 0.0;
+#pragma unroll
+            for (int q = 0; q < RR_PER; ++q) {
+                const int j = j0 + q;
+                const int bin = bins[j];
+                if (bin != cur) {
+                    if (cur >= 0) {
+#pragma unroll
+                        for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                            if (e < ne) atomicAdd(&accr[e * nk + cur], run[e]);
+                    }
+#pragma unroll
+                    for (int e = 0; e < PB_RED_MAX_ELLS; ++e) run[e] = 0.0;
+                    cur = bin;
+                }
+                if (bin < 0) continue;
+                double f;
+                if (MODE == PB_RED_CROSS) {
+                    const C v = b[rowoff + t0 + j];
+                    const double2 u = as[j];
+                    f = u.x * (double)v.x + u.y * (double)v.y;
+                } else {
+                    const C v = a[rowoff + t0 + j];
+                    f = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+                }
+#pragma unroll
+                for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                    if (e < ne) run[e] += f * wt[e * RR_TILE + j];
+            }
+            if (cur >= 0) {
+#pragma unroll
+                for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                    if (e < ne) atomicAdd(&accr[e * nk + cur], run[e]);
+            }
+        }
+    }
+    __syncthreads();
+    for (int r = 0; r < nr; ++r) {
+        double *dst = partials + ((int64_t)(r0 + r) * gridDim.x + blockIdx.x) * (ne * nk);
+        for (int i = threadIdx.x; i < ne * nk; i += blockDim.x) dst[i] = acc[(size_t)r * ne * nk + i];
+    }
+}
+
 __global__ void binred_finalize(const double *partials, int n_blocks, int per_row, int n_rows, double scale,
                                 double *out, int accumulate) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -160,8 +265,39 @@ extern "C" int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const 
     if (!workspace || workspace_bytes < need)
         return fail(PB_ERR_WORKSPACE, "pb_bin_reduce: workspace too small (need " + std::to_string(need) + " bytes)");
     double *partials = (double *)workspace;
-    dim3 grid(nb, n_rows);
     cudaStream_t s = as_stream(stream);
+    if (mode != PB_RED_REAL2 && n_rows >= 4) {
+        // many rows: mode geometry once per tile for a group of rows (binred_rows_kernel)
+        const int per = nk * n_ell;
+        const int rpg = std::max(1, std::min(n_rows, RR_ACC_DOUBLES / per));
+        const size_t smem = rr_acc_len(rpg, n_ell, nk) * sizeof(double) + (size_t)n_ell * RR_TILE * sizeof(double) +
+                            (size_t)RR_TILE * (sizeof(double2) + sizeof(int));
+        dim3 rgrid(nb, (n_rows + rpg - 1) / rpg);
+#define PB_RR_LAUNCH(T, M)                                                                                   \
+    do {                                                                                                     \
+        PB_CUDA(cudaFuncSetAttribute(binred_rows_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)smem));                                                            \
+        binred_rows_kernel<T, M><<<rgrid, RED_THREADS, smem, s>>>(G, (const cplx<T>::type *)a,              \
+                                                                  (const cplx<T>::type *)b, row_stride, p,   \
+                                                                  n_rows, rpg, partials);                    \
+    } while (0)
+        if (precision == PB_F32) {
+            if (mode == PB_RED_ABS2) PB_RR_LAUNCH(float, PB_RED_ABS2);
+            else PB_RR_LAUNCH(float, PB_RED_CROSS);
+        } else if (precision == PB_F64) {
+            if (mode == PB_RED_ABS2) PB_RR_LAUNCH(double, PB_RED_ABS2);
+            else PB_RR_LAUNCH(double, PB_RED_CROSS);
+        } else {
+            return fail(PB_ERR_INVALID, "bad precision");
+        }
+#undef PB_RR_LAUNCH
+        PB_LAUNCH_CHECK("pb_bin_reduce(rows)");
+        const int total = per * n_rows;
+        binred_finalize<<<(total + 255) / 256, 256, 0, s>>>(partials, nb, per, n_rows, scale, out, accumulate);
+        PB_LAUNCH_CHECK("pb_bin_reduce(finalize)");
+        return PB_OK;
+    }
+    dim3 grid(nb, n_rows);
 #define PB_RED_LAUNCH(T, M)                                                                        \
     binred_kernel<T, M><<<grid, RED_THREADS, 0, s>>>(G, (const cplx<T>::type *)a, (const cplx<T>::type *)b, \
                                                       (const T *)a, row_stride, p, partials)

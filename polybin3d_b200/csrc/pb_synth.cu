@@ -50,6 +50,8 @@ struct SynthParams {
     int n0, n1, n2, nh2;        // source grid
     int m0, m1, m2;             // output grid
     double kf0, kf1, kf2;
+    int los;                    // line of sight of the Legendre weights (see Grid)
+    double l0, l1, l2;
     int64_t src_stride;
     FftAxis ax, ay, az;
     int c1;                     // S1 column chunks per plane (max over maps)
@@ -455,7 +457,8 @@ __global__ void __launch_bounds__(SY_THREADS) synth_x_kernel(SynthParams p, cons
                 const double kk = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(kxv, kxv), __dmul_rn(kyv, kyv)),
                                                        __dmul_rn(kzz, kzz)));
                 if (mp.lo <= kk && kk < mp.hi) {
-                    const double mu = kk != 0.0 ? __ddiv_rn(kzz, kk) : 0.0;
+                    const double mu =
+                        kk != 0.0 ? __ddiv_rn(k_dot_los(p.los, p.l0, p.l1, p.l2, kxv, kyv, kzz), kk) : 0.0;
                     const int si = kx < 0 ? kx + p.n0 : kx;
                     const int64_t sidx = ((int64_t)si * p.n1 + sj) * p.nh2 + kz;
                     double f = mp.scale * legendre(mp.l1, mu) * legendre(mp.l2, mu);
@@ -718,6 +721,10 @@ static int synth_layout(const pb_grid_t *g, const int32_t *out_n, int precision,
     p.kf0 = G.kf0;
     p.kf1 = G.kf1;
     p.kf2 = G.kf2;
+    p.los = G.los;
+    p.l0 = G.l0;
+    p.l1 = G.l1;
+    p.l2 = G.l2;
     p.src_stride = src_stride;
     for (int i = 0; i < 3; ++i)
         if (out_n[i] < 2 || (out_n[i] & 1)) return fail(PB_ERR_INVALID, "pb_shell_synth: output dims must be even");

@@ -137,8 +137,21 @@ class PSpec:
         Nl = self.Nl if filtering == 'Sinv' else self.Nl_even
         out = torch.empty(Nl * self.Nk, dtype=torch.float64, device=b.device)
         scale = 0.5 * s2 * b.volume / float(b.gridsize.prod()) ** 2
-        nat.bin_reduce(b.grid, nat.precision_of(xk.dtype), nat.PB_RED_ABS2, xk, None, 1, self.k_bins,
-                       self._ells(Nl), scale, out, b.ws)
+        prec = nat.precision_of(xk.dtype)
+        if b.sightline == 'global' or Nl == 1:
+            nat.bin_reduce(b.grid, prec, nat.PB_RED_ABS2, xk, None, 1, self.k_bins, self._ells(Nl), scale, out, b.ws)
+            return out.cpu().numpy()
+        # local sightline (pspec.py:643-680): the monopole as above; multipole l is the
+        # binned cross spectrum of x with sum_m Y_lm(k) FT[Y_lm(r) x(r)]
+        if self.odd_l:
+            raise NotImplementedError("backend='cuda' implements even multipoles for the local sightline")
+        Nk = self.Nk
+        nat.bin_reduce(b.grid, prec, nat.PB_RED_ABS2, xk, None, 1, self.k_bins, [(0, 0)], scale, out[:Nk], b.ws)
+        x_real = b.to_real(xk)
+        for li in range(1, Nl):
+            lm = b.harmonics.apply_fourier(x_real, 2 * li)
+            nat.bin_reduce(b.grid, prec, nat.PB_RED_CROSS, xk, lm, 1, self.k_bins, [(0, 0)], scale,
+                           out[li * Nk:(li + 1) * Nk], b.ws)
         return out.cpu().numpy()
 
     # ------------------------------------------------------------------------------
@@ -156,6 +169,9 @@ class PSpec:
     def _fisher_from_fields(self, a):
         """Fisher contributions of a batch of GRFs a (B, half) complex128 (pspec.py:264-456)."""
         b = self.base
+        if b.sightline == 'local' and self.lmax > 0:
+            raise NotImplementedError("backend='cuda' implements the Monte Carlo Fisher matrix for the global "
+                                      "sightline; with the local sightline supply fish= to Pk_unwindowed")
         B = a.shape[0]
         nh = b.nhalf
         grid = b.grid
@@ -334,6 +350,8 @@ class PSpec:
         if not self.const_mask:
             assert hasattr(self, 'mask_shot'), "Must supply mask_shot to compute shot-noise contribution"
         b = self.base
+        if b.sightline == 'local' and self.lmax > 0:
+            raise NotImplementedError("backend='cuda' implements shot noise for the global sightline")
         dev = b.device
         F64 = nat.PB_F64
         PkA = [b.Pfid[0], 1. / b.Pfid[1]]

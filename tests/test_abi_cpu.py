@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), n
     assert set(nat.SIGNATURES) >= set(names) - set(), set(names) - set(nat.SIGNATURES)
-    assert lib.pb_abi_version() == 1
+    assert lib.pb_abi_version() == 2
 
 
 def test_invalid_grid_rejected_without_device():
@@ -42,6 +42,20 @@ def test_invalid_grid_rejected_without_device():
     assert b"Last dimension of grid must be even" in lib.pb_last_error()
     with pytest.raises(ValueError, match="Last dimension"):
         nat.check(st)
+
+
+def test_zero_line_of_sight_rejected():
+    """A grid that asks for a line of sight (local sightline) must give a non-zero one."""
+    lib = nat.load()
+    g = nat.PBGrid()
+    g.n[0] = g.n[1] = g.n[2] = 8
+    for i in range(3):
+        g.kf[i] = 0.1
+    g.flags = nat.PB_GRID_LOS
+    h = ctypes.c_void_p()
+    ws = ctypes.c_size_t()
+    st = lib.pb_fft_plan_create(ctypes.byref(g), 1, 1, 0, ctypes.byref(h), ctypes.byref(ws))
+    assert st == -1 and b"line of sight must be a non-zero vector" in lib.pb_last_error()
 
 
 def test_bin_reduce_argument_checks():

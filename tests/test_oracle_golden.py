@@ -196,6 +196,33 @@ def test_shot_noise():
     assert rel(bs.shot_contribution(n1, n2, 0.6 * m, data=d, data2=0.7 * d, sym=g["sym"]), g["b_full"]) < TOL
 
 
+def test_local_line_of_sight():
+    """Pk and Bk with the local (Yamamoto) line of sight: multipoles of the numerators through
+    the real harmonics of positions and wavevectors; the ideal Fisher matrices are the
+    distant-observer ones with mu measured from the direction of the box centre."""
+    g = gold("local_los")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic", boxcenter=g["center"], sightline="local")
+    m = mask24(N, L)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * m
+    ps = O.OraclePSpec(b, g["edges"], lmax=4, mask=m)
+    assert rel(ps.numerator(d, "ideal"), g["pk_num_ideal"]) < TOL
+    assert rel(ps.numerator(d, "Sinv"), g["pk_num"]) < TOL
+    assert rel(ps.fisher_ideal(), g["pk_fish_ideal"]) < TOL
+    pk = ps.Pk_ideal(d)
+    for k in ("p0", "p2", "p4"):
+        assert rel(pk[k], g["Pk_" + k]) < TOL
+    bs = O.OracleBSpec(b, g["bedges"], lmax=2, mask=m)
+    assert np.array_equal(bs.all_bins, g["bk_bins"])
+    assert rel(bs.symmetry_factor(), g["bk_sym"]) < TOL
+    assert rel(bs.numerator(d, "ideal", sym=g["bk_sym"]), g["bk_num_ideal"]) < TOL
+    assert rel(bs.numerator(d, "Sinv", sym=g["bk_sym"]), g["bk_num"]) < TOL
+    assert rel(bs.fisher_ideal(sym=g["bk_sym"]), g["bk_fish_ideal"]) < TOL
+    bk = bs.Bk_ideal(d, sym=g["bk_sym"])
+    for k in ("b0", "b2"):
+        assert rel(bk[k], g["Bk_" + k]) < TOL
+
+
 def test_philox_known_answers():
     """Philox4x32-10 known-answer vectors of the Random123 distribution (kat_vectors)."""
     cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),

@@ -23,7 +23,7 @@ def _grid(n, L):
     for i in range(3):
         g.n[i] = n
         g.kf[i] = 2 * np.pi / L
-    g.reserved = 0
+    g.flags = 0
     return g
 
 
