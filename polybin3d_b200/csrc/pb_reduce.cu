@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(RED_THREADS) binred_kernel(Grid g, const typen
 constexpr int RR_TILE = 512;                 // modes per tile (2 per thread)
 constexpr int RR_PER = RR_TILE / RED_THREADS;
 constexpr int RR_ACC_DOUBLES = 6144;         // shared accumulators per block (48 KB)
+constexpr int RR_RB = 8;                     // rows loaded ahead per thread
 
 // accumulator doubles rounded up to an even count, so the double2 tile after them is aligned
 __host__ __device__ __forceinline__ size_t rr_acc_len(int rows, int ne, int nk) {
@@ -154,47 +155,59 @@ __global__ void __launch_bounds__(RED_THREADS) binred_rows_kernel(Grid g, const 
             bins[j] = bin;
         }
         __syncthreads();
-        // each thread: RR_PER consecutive modes of the tile for every row of the group
-        const int j0 = threadIdx.x * RR_PER;
-        for (int r = 0; r < nr; ++r) {
-            const int64_t rowoff = (int64_t)(r0 + r) * row_stride;
-            double *accr = acc + (size_t)r * ne * nk;
-            int cur = -1;
-            double run[PB_RED_MAX_ELLS];
+        // lane <-> consecutive mode (coalesced row reads).  Consecutive modes mostly share a
+        // bin, so a warp first sums each contiguous run of equal bins with a segmented
+        // shuffle reduction and only the run's first lane adds to shared memory: one atomic
+        // per run and Legendre order instead of one per mode on the same address.
+        const int lane = threadIdx.x & 31;
+        for (int pass = 0; pass < RR_PER; ++pass) {
+            const int j = pass * RED_THREADS + threadIdx.x;
+            const int bin = bins[j];
+            const bool head = lane == 0 || bins[j - 1] != bin;
+            const unsigned heads = __ballot_sync(0xffffffffu, head);
+            const int seg = __popc(heads & (0xffffffffu >> (31 - lane)));  // run index of this lane
+            unsigned same = 0;                                              // bit k: lane + 2^k in my run
 #pragma unroll
-            for (int e = 0; e < PB_RED_MAX_ELLS; ++e) run[e] = 0.0;
-#pragma unroll
-            for (int q = 0; q < RR_PER; ++q) {
-                const int j = j0 + q;
-                const int bin = bins[j];
-                if (bin != cur) {
-                    if (cur >= 0) {
-#pragma unroll
-                        for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
-                            if (e < ne) atomicAdd(&accr[e * nk + cur], run[e]);
-                    }
-#pragma unroll
-                    for (int e = 0; e < PB_RED_MAX_ELLS; ++e) run[e] = 0.0;
-                    cur = bin;
-                }
-                if (bin < 0) continue;
-                double f;
-                if (MODE == PB_RED_CROSS) {
-                    const C v = b[rowoff + t0 + j];
-                    const double2 u = as[j];
-                    f = u.x * (double)v.x + u.y * (double)v.y;
-                } else {
-                    const C v = a[rowoff + t0 + j];
-                    f = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
-                }
-#pragma unroll
-                for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
-                    if (e < ne) run[e] += f * wt[e * RR_TILE + j];
+            for (int k = 0; k < 5; ++k) {
+                const int o = 1 << k;
+                const int sg = __shfl_down_sync(0xffffffffu, seg, o);
+                if (lane + o < 32 && sg == seg) same |= 1u << k;
             }
-            if (cur >= 0) {
+            double2 u = make_double2(0.0, 0.0);
+            if (MODE == PB_RED_CROSS && bin >= 0) u = as[j];
+            double w[PB_RED_MAX_ELLS];
 #pragma unroll
-                for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
-                    if (e < ne) atomicAdd(&accr[e * nk + cur], run[e]);
+            for (int e = 0; e < PB_RED_MAX_ELLS; ++e) w[e] = (e < ne && bin >= 0) ? wt[e * RR_TILE + j] : 0.0;
+            // RR_RB rows' values are loaded before any of them is reduced, so each thread
+            // keeps RR_RB independent reads in flight
+            const C *src = (MODE == PB_RED_CROSS) ? b : a;
+            for (int rb = 0; rb < nr; rb += RR_RB) {
+                C vals[RR_RB];
+#pragma unroll
+                for (int q = 0; q < RR_RB; ++q) {
+                    vals[q].x = 0;
+                    vals[q].y = 0;
+                    if (bin >= 0 && rb + q < nr) vals[q] = src[(int64_t)(r0 + rb + q) * row_stride + t0 + j];
+                }
+#pragma unroll
+                for (int q = 0; q < RR_RB; ++q) {
+                    if (rb + q >= nr) break;
+                    double f;
+                    if (MODE == PB_RED_CROSS) f = u.x * (double)vals[q].x + u.y * (double)vals[q].y;
+                    else f = (double)vals[q].x * (double)vals[q].x + (double)vals[q].y * (double)vals[q].y;
+                    double *accr = acc + (size_t)(rb + q) * ne * nk;
+#pragma unroll
+                    for (int e = 0; e < PB_RED_MAX_ELLS; ++e) {
+                        if (e >= ne) break;
+                        double v = f * w[e];
+#pragma unroll
+                        for (int k = 0; k < 5; ++k) {
+                            const double up = __shfl_down_sync(0xffffffffu, v, 1 << k);
+                            if (same & (1u << k)) v += up;
+                        }
+                        if (head && bin >= 0) atomicAdd(&accr[e * nk + bin], v);
+                    }
+                }
             }
         }
     }
@@ -266,8 +279,8 @@ extern "C" int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const 
         return fail(PB_ERR_WORKSPACE, "pb_bin_reduce: workspace too small (need " + std::to_string(need) + " bytes)");
     double *partials = (double *)workspace;
     cudaStream_t s = as_stream(stream);
-    if (mode != PB_RED_REAL2 && n_rows >= 4) {
-        // many rows: mode geometry once per tile for a group of rows (binred_rows_kernel)
+    if (mode != PB_RED_REAL2) {
+        // spectra: mode geometry once per tile for a group of rows (binred_rows_kernel)
         const int per = nk * n_ell;
         const int rpg = std::max(1, std::min(n_rows, RR_ACC_DOUBLES / per));
         const size_t smem = rr_acc_len(rpg, n_ell, nk) * sizeof(double) + (size_t)n_ell * RR_TILE * sizeof(double) +
