@@ -435,6 +435,8 @@ class OraclePSpec:
             SinvP = b.to_fourier(self.mask * a_real)
         fish = np.zeros((self.N_bins, self.N_bins))
         scaling = 0.5 * b.volume / b.gridsize.prod() ** 2                # 390
+        if b.sightline == "local" and self.Nl > 1:
+            return self._fisher_local(Ainv, SinvP, scaling)
         for li in range(self.Nl):
             for ki in range(self.Nk):
                 kmap = b.fourier_filter(SinvP, 2 * li, self.k_bins[ki], self.k_bins[ki + 1])
@@ -448,6 +450,48 @@ class OraclePSpec:
                         Ainv, Q, self.k_bins, 2 * lp)
         return fish
 
+
+    def _fisher_local(self, Ainv, SinvP, scaling):
+        """_compute_fisher, local sightline, even l (pspec.py:334-352, 380-407, 440-486).
+        Monopole rows Q = (S^-1 P)^dag Theta_b SinvP; multipole rows
+        Q = 1/2 (S^-1 P)^dag Theta_b H_l[SinvP] + 1/2 (S^-1 P)^dag sum_m Y_lm(r) IFT[Theta_b Y_lm(k) SinvP]
+        with H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x]; the row against column block l is the
+        cross integral of Q with A^-1 a (l = 0) or with H_l[A^-1 a]."""
+        b = self.base
+
+        def dagger(x, real):                                             # 291-305
+            if self.const_mask:
+                return self.mask_mean * (b.to_fourier(x) if real else x)
+            return b.to_fourier(self.mask * (x if real else b.to_real(x)))
+
+        legA = {2 * li: b.apply_fourier_harmonics(b.to_real(Ainv), 2 * li) for li in range(1, self.Nl)}
+        SinvP_real = b.to_real(SinvP)
+        fish = np.zeros((self.N_bins, self.N_bins))
+
+        def add(row, Q):                                                 # 380-407
+            fish[row, :self.Nk] += scaling * b.cross_integrate(Ainv, Q, self.k_bins, 0)
+            for li in range(1, self.Nl):
+                fish[row, li * self.Nk:(li + 1) * self.Nk] += scaling * b.cross_integrate(legA[2 * li], Q,
+                                                                                          self.k_bins, 0)
+
+        for ki in range(self.Nk):                                        # 442-445
+            add(ki, dagger(b.fourier_filter(SinvP, 0, self.k_bins[ki], self.k_bins[ki + 1]), False))
+        for li in range(1, self.Nl):                                     # 456-486
+            l = 2 * li
+            leg = b.apply_fourier_harmonics(SinvP_real, l)
+            yr = real_harmonics_fourier(b.r_grids, l)[l]
+            yk = real_harmonics_fourier(b.k_grids, l)[l]
+            for ki in range(self.Nk):
+                Q = 0.5 * dagger(b.fourier_filter(leg, 0, self.k_bins[ki], self.k_bins[ki + 1]), False)
+                real_map = np.zeros(tuple(b.gridsize))
+                m = b.in_bin(self.k_bins[ki], self.k_bins[ki + 1])
+                for mi in range(len(yr)):
+                    km = np.zeros(b.modk_grid.shape, dtype=np.complex128)
+                    km[m] = SinvP[m] * yk[mi][m]
+                    real_map += b.to_real(km) * yr[mi]
+                Q = Q + 0.5 * dagger(real_map, True)
+                add(li * self.Nk + ki, Q)
+        return fish
 
     def shot_contribution(self, noise_pair, mask_shot=None):
         """compute_shot_contribution, global sightline (pspec.py:495-549): a = GRF of

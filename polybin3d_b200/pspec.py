@@ -169,9 +169,8 @@ class PSpec:
     def _fisher_from_fields(self, a):
         """Fisher contributions of a batch of GRFs a (B, half) complex128 (pspec.py:264-456)."""
         b = self.base
-        if b.sightline == 'local' and self.lmax > 0:
-            raise NotImplementedError("backend='cuda' implements the Monte Carlo Fisher matrix for the global "
-                                      "sightline; with the local sightline supply fish= to Pk_unwindowed")
+        if b.sightline == 'local' and self.lmax > 0 and self.odd_l:
+            raise NotImplementedError("backend='cuda' implements even multipoles for the local sightline")
         B = a.shape[0]
         nh = b.nhalf
         grid = b.grid
@@ -197,6 +196,11 @@ class PSpec:
             qscale = 1.0
         fish = torch.empty((B, self.N_bins, self.N_bins), dtype=torch.float64, device=b.device)
         scaling = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
+        if b.sightline == 'local' and self.Nl > 1:
+            for i in range(B):
+                S = SinvP[i] * self.mask_mean if self.const_mask else SinvP[i]
+                self._fisher_local(Ainv[i], S, scaling, fish[i])
+            return fish
         rows = [(li, ki) for li in range(self.Nl) for ki in range(self.Nk)]
         for i in range(B):
             Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
@@ -211,6 +215,70 @@ class PSpec:
                 b.n_FFTs_forward += self.N_bins
             nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, self.k_bins, self._ells(self.Nl),
                            scaling, fish[i], b.ws)
+        return fish
+
+    def _fisher_local(self, Ainv, S, scaling, fish):
+        """One realisation's Fisher rows for the local sightline, even l (pspec.py:334-352,
+        380-407, 440-486).  With H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x] and D = (S^-1 P)^dag:
+        monopole rows Q = D Theta_b S; multipole rows
+        Q = 1/2 D Theta_b H_l[S] + 1/2 D sum_m Y_lm(r) IFT[Theta_b Y_lm(k) S]; column block 0 is
+        the binned cross spectrum of Q with A^-1 a, block l the one with H_l[A^-1 a].  All
+        rows of a multipole go through each step as one batch."""
+        b = self.base
+        grid, F64, Nk = b.grid, nat.PB_F64, self.Nk
+        invN = 1.0 / b.nreal
+        harm = b.harmonics
+        Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+        m = None if self.const_mask else self._mask_device()
+        mm = float(self.mask_mean) if self.const_mask else 1.0
+
+        def dagger_rows(R, real=None):
+            """R <- D R for a block of rows whose Fourier part R (already scaled by 1/N^3 for
+            a varying mask, by the mask mean for a constant one) may come with a real-space
+            part `real` (unnormalised, added before the mask)."""
+            if self.const_mask:
+                if real is not None:
+                    R.add_(b.fft_r2c(real), alpha=mm)
+                    b.n_FFTs_forward += R.shape[0]
+                return R
+            rr = b.fft_c2r(R)
+            b.n_FFTs_reverse += R.shape[0]
+            if real is not None:
+                rr.add_(real)
+            nat.elementwise(nat.PB_EW_MUL, rr, m, out=rr, y_period=b.nreal)
+            b.n_FFTs_forward += R.shape[0]
+            return b.fft_r2c(rr, out=R)
+
+        qs = mm if self.const_mask else invN
+        bands = [(0, self.k_bins[ki], self.k_bins[ki + 1], 0, 0, qs, 0) for ki in range(Nk)]
+        nat.spectral_filter(grid, F64, S, Q[:Nk], bands)
+        dagger_rows(Q[:Nk])
+        S_real = b.to_real(S)
+        for li in range(1, self.Nl):
+            l = 2 * li
+            R = Q[li * Nk:(li + 1) * Nk]
+            nat.spectral_filter(grid, F64, harm.apply_fourier(S_real, l), R,
+                                [(0, lo, hi, 0, 0, 0.5 * sc, 0) for (_, lo, hi, _, _, sc, _) in bands])
+            yr = harm._grid('r', l, torch.float64)
+            yk = harm._grid('k', l, torch.float64)
+            real_map = torch.zeros((Nk,) + tuple(int(n) for n in b.gridsize), dtype=torch.float64, device=b.device)
+            T = torch.empty((Nk,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+            for mi in range(yr.shape[0]):
+                nat.spectral_filter(grid, F64, S, T, [(0, lo, hi, 0, 0, 0.5 * invN, 1) for (_, lo, hi, _, _, _, _) in bands],
+                                    w=yk[mi])
+                t = b.fft_c2r(T)
+                b.n_FFTs_reverse += Nk
+                real_map.addcmul_(t, yr[mi])
+            dagger_rows(R, real_map)
+        tmp = torch.empty((self.N_bins, Nk), dtype=torch.float64, device=b.device)
+        nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv, Q, self.N_bins, self.k_bins, [(0, 0)], scaling, tmp, b.ws)
+        fish[:, :Nk] = tmp
+        A_real = b.to_real(Ainv)
+        for li in range(1, self.Nl):
+            legA = harm.apply_fourier(A_real, 2 * li)
+            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, legA, Q, self.N_bins, self.k_bins, [(0, 0)], scaling, tmp,
+                           b.ws)
+            fish[:, li * Nk:(li + 1) * Nk] = tmp
         return fish
 
     def compute_fisher_contribution(self, seed, verb=False):

@@ -317,6 +317,25 @@ def local_los(pb):
     return out
 
 
+@case
+def local_fisher(pb):
+    """Local line of sight, Monte Carlo Pk Fisher contributions: 24^3, L=600, box centred at
+    (700, 400, 900) Mpc/h, TSC window, lmax=4, 4 bins; shell-sector mask (seed 0) and a
+    constant mask 0.7 (seed 1)."""
+    N, L = 24, 600.0
+    center = [700.0, 400.0, 900.0]
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=center, sightline="local", pixel_window="tsc",
+                  backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=4, mask=mask)
+    f0 = _quiet(ps.compute_fisher_contribution, 0)
+    ps2 = _quiet(pb.PSpec, base, edges, lmax=4, mask=0.7 * np.ones((N, N, N)))
+    f1 = _quiet(ps2.compute_fisher_contribution, 1)
+    return dict(N=N, L=L, center=np.asarray(center), edges=edges, f0=f0, f1=f1)
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

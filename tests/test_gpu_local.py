@@ -87,10 +87,26 @@ def test_bk_local(pb, g, precision, contraction, tol):
         assert rel(bk[k], g["Bk_" + k]) < (tol if precision == "fp64" else 1e-4), k
 
 
+def test_local_pk_fisher_contribution(pb):
+    """Monte Carlo Pk Fisher contributions with the local line of sight on the reference's
+    own noise (tests/golden/local_fisher.npz): varying and constant mask, lmax=4."""
+    gf = np.load(os.path.join(GOLD, "local_fisher.npz"))
+    N, L = int(gf["N"]), float(gf["L"])
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=list(gf["center"]), sightline="local",
+              pixel_window="tsc", backend="cuda")
+    ps = quiet(pb.PSpec, b, gf["edges"], lmax=4, mask=mask24(N, L))
+    assert rel(ps.compute_fisher_contribution(0), gf["f0"]) < 1e-8
+    ps2 = quiet(pb.PSpec, b, gf["edges"], lmax=4, mask=0.7 * np.ones((N, N, N)))
+    assert rel(ps2.compute_fisher_contribution(1), gf["f1"]) < 1e-8
+
+
 def test_local_unsupported_paths_raise(pb, g):
-    """The Monte Carlo Fisher and shot noise with a local sightline are not implemented here
-    and say so (no silent global-sightline answer)."""
+    """Shot noise and the Bk Monte Carlo Fisher with a local sightline are not implemented
+    here and say so (no silent global-sightline answer)."""
     b = make_base(pb, g)
     ps = quiet(pb.PSpec, b, g["edges"], lmax=2)
-    with pytest.raises(NotImplementedError, match="local sightline"):
-        ps.compute_fisher_contribution(0)
+    with pytest.raises(NotImplementedError, match="global sightline"):
+        ps.compute_shot_contribution(0)
+    bs = quiet(pb.BSpec, b, g["bedges"], lmax=2)
+    with pytest.raises(NotImplementedError, match="global"):
+        quiet(bs.compute_fisher_contribution, 0)

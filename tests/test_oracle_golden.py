@@ -223,6 +223,18 @@ def test_local_line_of_sight():
         assert rel(bk[k], g["Bk_" + k]) < TOL
 
 
+def test_local_fisher_contribution():
+    """Monte Carlo Pk Fisher contribution with the local line of sight (varying and constant
+    mask), on the reference's own noise."""
+    g = gold("local_fisher")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc", boxcenter=g["center"], sightline="local")
+    ps = O.OraclePSpec(b, g["edges"], lmax=4, mask=mask24(N, L))
+    assert rel(ps.fisher_contribution(b.reference_noise(0 + 10 ** 7)), g["f0"]) < TOL
+    ps2 = O.OraclePSpec(b, g["edges"], lmax=4, mask=0.7 * np.ones((N, N, N)))
+    assert rel(ps2.fisher_contribution(b.reference_noise(1 + 10 ** 7)), g["f1"]) < TOL
+
+
 def test_philox_known_answers():
     """Philox4x32-10 known-answer vectors of the Random123 distribution (kat_vectors)."""
     cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
