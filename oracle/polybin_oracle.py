@@ -332,6 +332,15 @@ class OracleBase:
         im = (rad * np.sin(2 * np.pi * u2)).reshape(tuple(self.gridsize))
         return re, im
 
+    def apply_real_harmonics(self, a_fourier, l):
+        """sum_m Y_lm(x) irfftn(Y_lm(k) a(k)) (base.py:391-400), even l."""
+        yr = real_harmonics_fourier(self.r_grids, l)[l]
+        yk = real_harmonics_fourier(self.k_grids, l)[l]
+        out = np.zeros(tuple(self.gridsize))
+        for m in range(len(yr)):
+            out += self.to_real(a_fourier * yk[m]) * yr[m]
+        return out
+
     def apply_fourier_harmonics(self, a_real, l):
         """sum_m Y_lm(k) rfftn(Y_lm(x) a(x)) (base.py:402-411) with the real harmonics of the
         positions and of the wavevectors (utils.pyx:518-609), even l."""
@@ -775,7 +784,9 @@ class OracleBSpec:
         return {"b%d" % l: out[l // 2 * self.N3:(l // 2 + 1) * self.N3] for l in range(0, self.lmax + 1, 2)}
 
     def fisher_contribution(self, noise1, noise2, sym=None, return_Q=False):
-        """_compute_fisher, global sightline, no covariance, trivial S^-1 (bspec.py:473-676)."""
+        """_compute_fisher, no covariance, trivial S^-1 (bspec.py:473-676); for the local
+        sightline the l > 0 maps come from the harmonic transform of each weighted map
+        (548-577) and the l leg of the A^-1 Q maps is applied in real space (621-631)."""
         b = self.base
         sym = self.symmetry_factor() if sym is None else sym
         ks = self.k_bins_squeeze
@@ -796,8 +807,16 @@ class OracleBSpec:
             g2 = np.asarray([b.to_real(b.fourier_filter(w2, 0, ks[i], ks[i + 1])) for i in range(nks)])
             return g1, g2
 
+        local = b.sightline == "local" and self.lmax > 0
+        legs = {}
+
         def gl_maps(w, B):
-            return [b.to_real(b.fourier_filter(w, l, ks[B], ks[B + 1])) for l in range(2, self.lmax + 1, 2)]
+            if not local:
+                return [b.to_real(b.fourier_filter(w, l, ks[B], ks[B + 1])) for l in range(2, self.lmax + 1, 2)]
+            key = id(w)
+            if key not in legs:
+                legs[key] = (w, [b.apply_fourier_harmonics(b.to_real(w), l) for l in range(2, self.lmax + 1, 2)])
+            return [b.to_real(b.fourier_filter(h, 0, ks[B], ks[B + 1])) for h in legs[key][1]]
 
         Nh = b.modk_grid.shape
         Q = np.zeros((self.N_bins,) + Nh, dtype=np.complex128)           # 643
@@ -817,7 +836,10 @@ class OracleBSpec:
                     ft.append(b.to_fourier(b.prod_real_diff(g1[A], gl1[l // 2 - 1], g2[A], gl2[l // 2 - 1])))
                 for ii in i1:                                            # leg b3, L_l on it
                     C, l = ab[ii, 2], ab[ii, 3]
-                    Q[ii] += b.fourier_filter(ft[0], l, ks[C], ks[C + 1])
+                    if local and l > 0:
+                        Q[ii] += b.to_fourier(b.apply_real_harmonics(b.fourier_filter(ft[0], 0, ks[C], ks[C + 1]), l))
+                    else:
+                        Q[ii] += b.fourier_filter(ft[0], l, ks[C], ks[C + 1])
                 for ii in i2:                                            # leg b1
                     C, l = ab[ii, 0], ab[ii, 3]
                     Q[ii] += b.fourier_filter(ft[l // 2], 0, ks[C], ks[C + 1])

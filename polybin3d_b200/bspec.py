@@ -385,7 +385,7 @@ class BSpec:
         specs = [(bb, l, 0, scale) for l in range(0, self.lmax + 1, 2) for bb in range(self.Nk_squeeze)]
         return self._binned_maps(xk, specs, w, xk.real.dtype, out=out)
 
-    def _g_maps_local(self, xk, w, scale, out=None):
+    def _g_maps_local(self, xk, w, scale, out=None, coarse=True):
         """Local sightline (bspec.py:932-954): with D = scale w xk and d = irfftn(D), the
         l = 0 maps filter D and the l > 0 maps filter sum_m Y_lm(k) FT[Y_lm(r) d(r)], all with
         the plain bin filter, in one synthesis over the stacked sources."""
@@ -397,7 +397,7 @@ class BSpec:
         d = b.to_real(D)
         srcs = torch.stack([D] + [b.harmonics.apply_fourier(d, l) for l in range(2, self.lmax + 1, 2)])
         specs = [(bb, 0, 0, 1.0, l // 2) for l in range(0, self.lmax + 1, 2) for bb in range(self.Nk_squeeze)]
-        return self._binned_maps(srcs, specs, None, xk.real.dtype, out=out)
+        return self._binned_maps(srcs, specs, None, xk.real.dtype, coarse=coarse, out=out)
 
     def _compute_bk_numerator(self, data, include_linear_term=True, filtering='ideal', verb=False):
         assert filtering in ['ideal', 'Sinv'], "Unknown filtering option supplied!"
@@ -720,6 +720,9 @@ class BSpec:
 
     def _all_g(self, w1, w2):
         nks = self.Nk_squeeze
+        if self.base.sightline == 'local' and self.lmax > 0:
+            # l > 0 maps from the harmonic transform of each weighted map (bspec.py:548-577)
+            return (self._g_maps_local(w1, None, 1.0, coarse=False), self._g_maps_local(w2, None, 1.0, coarse=False))
         specs = [(bb, l, 0, 1.0) for l in range(0, self.lmax + 1, 2) for bb in range(nks)]
         G1 = self._binned_maps(w1, specs, None, torch.float64, coarse=False)
         G2 = self._binned_maps(w2, specs, None, torch.float64, coarse=False)
@@ -736,9 +739,7 @@ class BSpec:
 
     def _fisher_from_fields(self, a1, a2):
         b = self.base
-        if b.sightline == 'local' and self.lmax > 0:
-            raise NotImplementedError("backend='cuda' implements the Monte Carlo Fisher matrix for the global "
-                                      "sightline; with the local sightline supply fish= to Bk_unwindowed")
+        local = b.sightline == 'local' and self.lmax > 0
         ab = self.all_bins
         ks = self.k_bins_squeeze
         F64 = nat.PB_F64
@@ -757,12 +758,36 @@ class BSpec:
         del G1, G2
         qs = self.mask_mean if self.const_mask else invN
         Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
-        leg1 = [(kpos[(r[0], r[1], 0)], ks[r[2]], ks[r[2] + 1], r[3], 0, qs, 0) for r in ab.tolist()]
+        # leg b3 carries L_l; with the local sightline that leg is applied in real space below
+        leg1 = [(kpos[(r[0], r[1], 0)], ks[r[2]], ks[r[2] + 1], 0 if local else r[3], 0,
+                 0.0 if (local and r[3] > 0) else qs, 0) for r in ab.tolist()]
         leg2 = [(kpos[(r[1], r[2], r[3])], ks[r[0]], ks[r[0] + 1], 0, 0, qs, 0) for r in ab.tolist()]
         leg3 = [(kpos[(r[0], r[2], r[3])], ks[r[1]], ks[r[1] + 1], 0, 0, qs, 0) for r in ab.tolist()]
         nat.spectral_filter(b.grid, F64, FT, Q, leg1, src_stride=nh)
         nat.spectral_filter(b.grid, F64, FT, Q, leg2, src_stride=nh, accumulate=True)
         nat.spectral_filter(b.grid, F64, FT, Q, leg3, src_stride=nh, accumulate=True)
+        if local:
+            # Q += FT[sum_m Y_lm(x) IFT(Y_lm(k) Theta_b3 FT_AB0)] for the rows of multipole l
+            # (bspec.py:621-631), batched over the rows
+            harm = b.harmonics
+            for l in range(2, self.lmax + 1, 2):
+                rows = [i for i, r in enumerate(ab.tolist()) if r[3] == l]
+                if not rows:
+                    continue
+                bands = [(kpos[(int(ab[i, 0]), int(ab[i, 1]), 0)], ks[ab[i, 2]], ks[ab[i, 2] + 1], 0, 0, invN, 1)
+                         for i in rows]
+                yr = harm._grid('r', l, torch.float64)
+                yk = harm._grid('k', l, torch.float64)
+                acc = torch.zeros((len(rows),) + tuple(int(n) for n in b.gridsize), dtype=torch.float64,
+                                  device=b.device)
+                T = torch.empty((len(rows),) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
+                for mi in range(yr.shape[0]):
+                    nat.spectral_filter(b.grid, F64, FT, T, bands, src_stride=nh, w=yk[mi])
+                    acc.addcmul_(b.fft_c2r(T), yr[mi])
+                    b.n_FFTs_reverse += len(rows)
+                b.n_FFTs_forward += len(rows)
+                idx = torch.as_tensor(rows, device=b.device)
+                Q[idx] = Q[idx] + b.fft_r2c(acc) * qs
         del FT
         Q = self._apply_filter_spectra(Q, True)
         # --- rows from Q[S^-1 P a] (compute_Q 'Sinv', bspec.py:528-597)

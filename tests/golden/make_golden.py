@@ -319,9 +319,9 @@ def local_los(pb):
 
 @case
 def local_fisher(pb):
-    """Local line of sight, Monte Carlo Pk Fisher contributions: 24^3, L=600, box centred at
-    (700, 400, 900) Mpc/h, TSC window, lmax=4, 4 bins; shell-sector mask (seed 0) and a
-    constant mask 0.7 (seed 1)."""
+    """Local line of sight, Monte Carlo Fisher contributions: 24^3, L=600, box centred at
+    (700, 400, 900) Mpc/h, TSC window, 4 bins; Pk lmax=4 and Bk lmax=2, each with the
+    shell-sector mask (seed 0) and a constant mask 0.7 (seed 1)."""
     N, L = 24, 600.0
     center = [700.0, 400.0, 900.0]
     kF = 2 * np.pi / L
@@ -333,7 +333,12 @@ def local_fisher(pb):
     f0 = _quiet(ps.compute_fisher_contribution, 0)
     ps2 = _quiet(pb.PSpec, base, edges, lmax=4, mask=0.7 * np.ones((N, N, N)))
     f1 = _quiet(ps2.compute_fisher_contribution, 1)
-    return dict(N=N, L=L, center=np.asarray(center), edges=edges, f0=f0, f1=f1)
+    bs = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask)
+    bf0 = _quiet(bs.compute_fisher_contribution, 0)
+    bs2 = _quiet(pb.BSpec, base, edges, lmax=2, mask=0.7 * np.ones((N, N, N)))
+    bf1 = _quiet(bs2.compute_fisher_contribution, 1)
+    return dict(N=N, L=L, center=np.asarray(center), edges=edges, f0=f0, f1=f1, bk_bins=bs.all_bins,
+                bk_sym=bs.sym_factor, bf0=bf0, bf1=bf1)
 
 
 def main(names=None):

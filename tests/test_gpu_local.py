@@ -100,13 +100,27 @@ def test_local_pk_fisher_contribution(pb):
     assert rel(ps2.compute_fisher_contribution(1), gf["f1"]) < 1e-8
 
 
+def test_local_bk_fisher_contribution(pb):
+    """Monte Carlo Bk Fisher contributions (lmax=2) with the local line of sight on the
+    reference's own noise pair: varying and constant mask."""
+    gf = np.load(os.path.join(GOLD, "local_fisher.npz"))
+    N, L = int(gf["N"]), float(gf["L"])
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=list(gf["center"]), sightline="local",
+              pixel_window="tsc", backend="cuda")
+    bs = quiet(pb.BSpec, b, gf["edges"], lmax=2, mask=mask24(N, L))
+    assert np.array_equal(bs.all_bins, gf["bk_bins"])
+    assert rel(quiet(bs.compute_fisher_contribution, 0), gf["bf0"]) < 1e-8
+    bs2 = quiet(pb.BSpec, b, gf["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)))
+    assert rel(quiet(bs2.compute_fisher_contribution, 1), gf["bf1"]) < 1e-8
+
+
 def test_local_unsupported_paths_raise(pb, g):
-    """Shot noise and the Bk Monte Carlo Fisher with a local sightline are not implemented
-    here and say so (no silent global-sightline answer)."""
+    """Shot noise with a local sightline is not implemented here and says so (no silent
+    global-sightline answer)."""
     b = make_base(pb, g)
     ps = quiet(pb.PSpec, b, g["edges"], lmax=2)
     with pytest.raises(NotImplementedError, match="global sightline"):
         ps.compute_shot_contribution(0)
-    bs = quiet(pb.BSpec, b, g["bedges"], lmax=2)
-    with pytest.raises(NotImplementedError, match="global"):
-        quiet(bs.compute_fisher_contribution, 0)
+    bs = quiet(pb.BSpec, b, g["bedges"], lmax=2, mask_shot=np.ones((int(g["N"]),) * 3))
+    with pytest.raises(NotImplementedError, match="global sightline"):
+        quiet(bs.compute_shot_contribution, 0, cubic_only=True)

@@ -224,8 +224,8 @@ def test_local_line_of_sight():
 
 
 def test_local_fisher_contribution():
-    """Monte Carlo Pk Fisher contribution with the local line of sight (varying and constant
-    mask), on the reference's own noise."""
+    """Monte Carlo Pk and Bk Fisher contributions with the local line of sight (varying and
+    constant mask), on the reference's own noise."""
     g = gold("local_fisher")
     N, L = int(g["N"]), float(g["L"])
     b = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc", boxcenter=g["center"], sightline="local")
@@ -233,6 +233,13 @@ def test_local_fisher_contribution():
     assert rel(ps.fisher_contribution(b.reference_noise(0 + 10 ** 7)), g["f0"]) < TOL
     ps2 = O.OraclePSpec(b, g["edges"], lmax=4, mask=0.7 * np.ones((N, N, N)))
     assert rel(ps2.fisher_contribution(b.reference_noise(1 + 10 ** 7)), g["f1"]) < TOL
+    bs = O.OracleBSpec(b, g["edges"], lmax=2, mask=mask24(N, L))
+    assert np.array_equal(bs.all_bins, g["bk_bins"])
+    f = bs.fisher_contribution(b.reference_noise(10 ** 7), b.reference_noise(2 * 10 ** 7), sym=g["bk_sym"])
+    assert rel(f, g["bf0"]) < TOL
+    bs2 = O.OracleBSpec(b, g["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)))
+    f = bs2.fisher_contribution(b.reference_noise(1 + 10 ** 7), b.reference_noise(1 + 2 * 10 ** 7), sym=g["bk_sym"])
+    assert rel(f, g["bf1"]) < TOL
 
 
 def test_philox_known_answers():
