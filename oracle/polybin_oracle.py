@@ -515,7 +515,11 @@ class OraclePSpec:
             sna = b.to_fourier(b.to_real(b.applyAinv_fourier(a, invPA)) * mask_shot)
         shot = np.zeros(self.N_bins)
         for li in range(self.Nl):                                        # 526-544
-            shot[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(a, sna, self.k_bins, 2 * li)
+            if b.sightline == "global" or li == 0:
+                shot[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(a, sna, self.k_bins, 2 * li)
+            else:                                                        # 535-544
+                lm = b.apply_fourier_harmonics(b.to_real(a), 2 * li)
+                shot[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(lm, sna, self.k_bins, 0)
         return shot * b.volume / b.gridsize.prod() ** 2
 
 

@@ -882,12 +882,10 @@ class BSpec:
         return Bk_dict
 
     def compute_shot_contribution(self, seed, verb=False, data=None, data2=None, cubic_only=False):
-        """Shot-noise contribution of one pair of GRFs of spectrum 1/P_fid, global sightline
-        (bspec.py:695-861): the cubic term from the maps of S^-1 a1, S^-1 a2 and the
+        """Shot-noise contribution of one pair of GRFs of spectrum 1/P_fid (bspec.py:695-861;
+        with the local sightline every map set's l > 0 maps come from the harmonic transform): the cubic term from the maps of S^-1 a1, S^-1 a2 and the
         shot-masked product (A^-1 a1)(A^-1 a2), and unless cubic_only the quadratic term from
         the data's maps with those of (A^-1 a_i) d2.  Returns quadratic - 2 cubic."""
-        if self.base.sightline == 'local' and self.lmax > 0:
-            raise NotImplementedError("backend='cuda' implements shot noise for the global sightline")
         if not cubic_only:
             assert data is not None, "Must supply data to compute the quadratic shot-noise contribution!"
             if data2 is None:

@@ -411,15 +411,15 @@ class PSpec:
         return Pk_dict
 
     def compute_shot_contribution(self, seed):
-        """Shot-noise contribution of one GRF, global sightline (pspec.py:495-549): a is drawn
+        """Shot-noise contribution of one GRF (pspec.py:495-549): a is drawn
         with spectrum P_A = 1/P_fid (pixel window included), A^-1 = (1/P_A) / W^2, and the
         k-binned cross spectrum of S^-1 a with S^-1 N A^-1 a (N: mask_shot, or the mask mean
         for a constant mask) is halved and normalised by V / N^6."""
         if not self.const_mask:
             assert hasattr(self, 'mask_shot'), "Must supply mask_shot to compute shot-noise contribution"
         b = self.base
-        if b.sightline == 'local' and self.lmax > 0:
-            raise NotImplementedError("backend='cuda' implements shot noise for the global sightline")
+        if b.sightline == 'local' and self.lmax > 0 and self.odd_l:
+            raise NotImplementedError("backend='cuda' implements even multipoles for the local sightline")
         dev = b.device
         F64 = nat.PB_F64
         PkA = [b.Pfid[0], 1. / b.Pfid[1]]
@@ -438,7 +438,18 @@ class PSpec:
             nat.elementwise(nat.PB_EW_MUL, sna, m, out=sna, y_period=b.nreal)
             sna = b.to_fourier(sna)
         out = torch.empty(self.N_bins, dtype=torch.float64, device=dev)
-        nat.bin_reduce(b.grid, F64, nat.PB_RED_CROSS, a, sna, 1, self.k_bins, self._ells(self.Nl), scale, out, b.ws)
+        if b.sightline == 'global' or self.Nl == 1:
+            nat.bin_reduce(b.grid, F64, nat.PB_RED_CROSS, a, sna, 1, self.k_bins, self._ells(self.Nl), scale, out,
+                           b.ws)
+            return out.cpu().numpy()
+        # local sightline (pspec.py:522-544): multipole l crosses sum_m Y_lm(k) FT[Y_lm(r) a(r)]
+        Nk = self.Nk
+        nat.bin_reduce(b.grid, F64, nat.PB_RED_CROSS, a, sna, 1, self.k_bins, [(0, 0)], scale, out[:Nk], b.ws)
+        a_real = b.to_real(a)
+        for li in range(1, self.Nl):
+            lm = b.harmonics.apply_fourier(a_real, 2 * li)
+            nat.bin_reduce(b.grid, F64, nat.PB_RED_CROSS, lm, sna, 1, self.k_bins, [(0, 0)], scale,
+                           out[li * Nk:(li + 1) * Nk], b.ws)
         return out.cpu().numpy()
 
     def _shot_inv_pa(self, PkA):

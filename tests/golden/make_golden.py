@@ -341,6 +341,29 @@ def local_fisher(pb):
                 bk_sym=bs.sym_factor, bf0=bf0, bf1=bf1)
 
 
+@case
+def local_shot(pb):
+    """Local line of sight, shot-noise contributions: 24^3, L=600, box centred at
+    (700, 400, 900) Mpc/h, TSC window, tabulated positive P(k), 4 bins; PSpec lmax=4 with the
+    shell-sector mask and mask_shot = 0.8 mask (seed 1); BSpec lmax=2 with mask_shot =
+    0.6 mask (seed 1, data = lognormal seed 16 times the mask, data2 = 0.7 data)."""
+    N, L = 24, 600.0
+    center = [700.0, 400.0, 900.0]
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    kt = np.linspace(0.0, 1.0, 2000)
+    pt = 2e3 * np.exp(-(kt / 0.3) ** 2) + 100.0
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, Pk=[kt, pt], boxcenter=center, sightline="local",
+                  pixel_window="tsc", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=4, mask=mask, mask_shot=0.8 * mask)
+    data = synthetic.lognormal(N, L, seed=16).astype(np.float64) * mask
+    bs = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask, mask_shot=0.6 * mask)
+    b_full = _quiet(bs.compute_shot_contribution, 1, data=data, data2=0.7 * data)
+    return dict(N=N, L=L, center=np.asarray(center), edges=edges, pk_k=kt, pk_p=pt,
+                p_mask=_quiet(ps.compute_shot_contribution, 1), bins=bs.all_bins, sym=bs.sym_factor, b_full=b_full)
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

@@ -114,13 +114,17 @@ def test_local_bk_fisher_contribution(pb):
     assert rel(quiet(bs2.compute_fisher_contribution, 1), gf["bf1"]) < 1e-8
 
 
-def test_local_unsupported_paths_raise(pb, g):
-    """Shot noise with a local sightline is not implemented here and says so (no silent
-    global-sightline answer)."""
-    b = make_base(pb, g)
-    ps = quiet(pb.PSpec, b, g["edges"], lmax=2)
-    with pytest.raises(NotImplementedError, match="global sightline"):
-        ps.compute_shot_contribution(0)
-    bs = quiet(pb.BSpec, b, g["bedges"], lmax=2, mask_shot=np.ones((int(g["N"]),) * 3))
-    with pytest.raises(NotImplementedError, match="global sightline"):
-        quiet(bs.compute_shot_contribution, 0, cubic_only=True)
+def test_local_shot_noise(pb):
+    """Shot-noise contributions with the local line of sight (PSpec lmax=4, BSpec lmax=2)
+    against the reference's own outputs (tests/golden/local_shot.npz)."""
+    gs = np.load(os.path.join(GOLD, "local_shot.npz"))
+    N, L = int(gs["N"]), float(gs["L"])
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, Pk=[gs["pk_k"], gs["pk_p"]], boxcenter=list(gs["center"]),
+              sightline="local", pixel_window="tsc", backend="cuda")
+    m = mask24(N, L)
+    ps = quiet(pb.PSpec, b, gs["edges"], lmax=4, mask=m, mask_shot=0.8 * m)
+    assert rel(ps.compute_shot_contribution(1), gs["p_mask"]) < 1e-10
+    bs = quiet(pb.BSpec, b, gs["edges"], lmax=2, mask=m, mask_shot=0.6 * m)
+    assert np.array_equal(bs.all_bins, gs["bins"])
+    d = synthetic.lognormal(N, L, seed=16).astype(np.float64) * m
+    assert rel(quiet(bs.compute_shot_contribution, 1, data=d, data2=0.7 * d), gs["b_full"]) < 1e-10

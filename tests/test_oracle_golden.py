@@ -242,6 +242,22 @@ def test_local_fisher_contribution():
     assert rel(f, g["bf1"]) < TOL
 
 
+def test_local_shot_noise():
+    """Shot-noise contributions with the local line of sight (PSpec lmax=4, BSpec lmax=2)."""
+    g = gold("local_shot")
+    N, L = int(g["N"]), float(g["L"])
+    b = O.OracleBase([L] * 3, [N] * 3, Pk=[g["pk_k"], g["pk_p"]], pixel_window="tsc", boxcenter=g["center"],
+                     sightline="local")
+    m = mask24(N, L)
+    ps = O.OraclePSpec(b, g["edges"], lmax=4, mask=m)
+    assert rel(ps.shot_contribution(b.reference_noise(1 + 10 ** 7), mask_shot=0.8 * m), g["p_mask"]) < TOL
+    bs = O.OracleBSpec(b, g["edges"], lmax=2, mask=m)
+    assert np.array_equal(bs.all_bins, g["bins"])
+    n1, n2 = b.reference_noise(1 + 10 ** 7), b.reference_noise(1 + 2 * 10 ** 7)
+    d = synthetic.lognormal(N, L, seed=16).astype(np.float64) * m
+    assert rel(bs.shot_contribution(n1, n2, 0.6 * m, data=d, data2=0.7 * d, sym=g["sym"]), g["b_full"]) < TOL
+
+
 def test_philox_known_answers():
     """Philox4x32-10 known-answer vectors of the Random123 distribution (kat_vectors)."""
     cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
