@@ -432,56 +432,137 @@ class OraclePSpec:
         return {"p%d" % (2 * li): out[li * self.Nk:(li + 1) * self.Nk] for li in range(self.Nl)}
 
     def fisher_contribution(self, noise_pair):
-        """_compute_fisher global, no covariance, no theory, trivial S^-1 (pspec.py:215-493)."""
+        """_compute_fisher, no covariance, no theory, trivial S^-1 (pspec.py:215-493)."""
+        return self._contribution(noise_pair)
+
+    def covariance_contribution(self, noise_pair, Pk_cov, mask_shot=None):
+        """compute_covariance_contribution (pspec.py:149-162): the Fisher rows with the
+        filter S^-1 P replaced by S^-1 [P xi P^dag + N] S^-dag, xi the correlation of the
+        spectrum Pk_cov = [k, P0(, P2(, P4))] and N the shot mask (the mask mean for a
+        constant mask)."""
+        assert len(np.asarray(Pk_cov).shape) == 2 and len(Pk_cov) in (2, 3, 4)
+        assert (len(Pk_cov) - 2) * 2 <= self.lmax
+        return self._contribution(noise_pair, xi=self.xi_grids(Pk_cov), mask_shot=mask_shot)
+
+    def theory_contribution(self, noise_pair, k_bins_theory, lmax_theory=None):
+        """compute_theory_contribution without wide-angle terms (pspec.py:164-196): the
+        Fisher contribution and the rectangular binning matrix whose column block l_t holds
+        the cross integrals of each Q-map with A^-1 a (global: weighted by L_l_t(mu); local:
+        with sum_m Y_lm(k) FT[Y_lm(r) A^-1 a]) in the theory k-bins."""
+        k_th = np.asarray(k_bins_theory, dtype=np.float64)
+        lt = self.lmax if lmax_theory is None else lmax_theory
+        return self._contribution(noise_pair, theory=(k_th, lt // 2 + 1))
+
+    def xi_grids(self, Pk_cov):
+        """Pk_grid of _compute_fisher (pspec.py:241-252): global, one grid
+        P0(k) + L2(mu) P2(k) + L4(mu) P4(k); local, one grid per multipole.  Linear
+        interpolation, zero outside the table."""
+        from scipy.special import legendre as sp_legendre
+        b = self.base
+        terms = [interp1d(Pk_cov[0], Pk_cov[i], bounds_error=False, fill_value=0.0)(b.modk_grid)
+                 for i in range(1, len(Pk_cov))]
+        if b.sightline == "global":
+            g = terms[0]
+            for i, t in enumerate(terms[1:]):
+                g = g + sp_legendre(2 * (i + 1))(b.muk_grid) * t
+            return {0: g}
+        return {2 * i: t for i, t in enumerate(terms)}
+
+    def apply_xi(self, X, x_real, xi, output):
+        """apply_xi (base.py:413-437): P0 X, plus for the local sightline and each l > 0
+        1/2 P_l sum_m Y_lm(k) FT[Y_lm(r) x] and 1/2 sum_m Y_lm(r) IFT[Y_lm(k) P_l X]."""
+        b = self.base
+        PF = X * xi[0]
+        if len(xi) == 1:
+            return PF if output == "fourier" else b.to_real(PF)
+        if x_real is None:
+            raise ValueError("local multipoles of the covariance spectrum need the real-space map")
+        PR = np.zeros(tuple(b.gridsize))
+        for l in sorted(xi)[1:]:
+            PF = PF + 0.5 * b.apply_fourier_harmonics(x_real, l) * xi[l]
+            PR = PR + 0.5 * b.apply_real_harmonics(X * xi[l], l)
+        return PF + b.to_fourier(PR) if output == "fourier" else b.to_real(PF) + PR
+
+    def cov_filter(self, x, real, xi, mask_shot):
+        """S^-1 [P xi P^dag + N] S^-dag x with the trivial S^-1 (pspec.py:277-290, 307-323);
+        x is a real map if `real`, else a half spectrum; the output is a half spectrum."""
+        b = self.base
+        if self.const_mask:
+            Sid = b.to_fourier(x) if real else x
+            return self.mask_mean ** 2 * self.apply_xi(Sid, None, xi, "fourier") + self.mask_mean * Sid
+        Sid = x if real else b.to_real(x)
+        Pd_real = self.mask * Sid
+        C = self.apply_xi(b.to_fourier(Pd_real), Pd_real, xi, "real")
+        return b.to_fourier(self.mask * C + mask_shot * Sid)
+
+    def _contribution(self, noise_pair, xi=None, mask_shot=None, theory=None):
+        """_compute_fisher, global and local (even l) sightlines (pspec.py:215-493)."""
         b = self.base
         a = b.grf_from_noise(*noise_pair)                                # pspec.py:266
         if not self.const_mask:
             a_real = b.to_real(a)                                        # 268
         Ainv = b.applyAinv_fourier(a)                                    # 328
-        if self.const_mask:                                              # 273-276
-            SinvP = self.mask_mean * a
-        else:
-            SinvP = b.to_fourier(self.mask * a_real)
-        fish = np.zeros((self.N_bins, self.N_bins))
-        scaling = 0.5 * b.volume / b.gridsize.prod() ** 2                # 390
-        if b.sightline == "local" and self.Nl > 1:
-            return self._fisher_local(Ainv, SinvP, scaling)
-        for li in range(self.Nl):
-            for ki in range(self.Nk):
-                kmap = b.fourier_filter(SinvP, 2 * li, self.k_bins[ki], self.k_bins[ki + 1])
-                if self.const_mask:                                      # 296-304
-                    Q = self.mask_mean * kmap
-                else:
-                    Q = b.to_fourier(self.mask * b.to_real(kmap))
-                row = li * self.Nk + ki
-                for lp in range(self.Nl):                                # 394-401
-                    fish[row, lp * self.Nk:(lp + 1) * self.Nk] += scaling * b.cross_integrate(
-                        Ainv, Q, self.k_bins, 2 * lp)
-        return fish
 
-
-    def _fisher_local(self, Ainv, SinvP, scaling):
-        """_compute_fisher, local sightline, even l (pspec.py:334-352, 380-407, 440-486).
-        Monopole rows Q = (S^-1 P)^dag Theta_b SinvP; multipole rows
-        Q = 1/2 (S^-1 P)^dag Theta_b H_l[SinvP] + 1/2 (S^-1 P)^dag sum_m Y_lm(r) IFT[Theta_b Y_lm(k) SinvP]
-        with H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x]; the row against column block l is the
-        cross integral of Q with A^-1 a (l = 0) or with H_l[A^-1 a]."""
-        b = self.base
-
-        def dagger(x, real):                                             # 291-305
+        def dagger(x, real):                                             # 291-323
+            if xi is not None:
+                return self.cov_filter(x, real, xi, mask_shot)
             if self.const_mask:
                 return self.mask_mean * (b.to_fourier(x) if real else x)
             return b.to_fourier(self.mask * (x if real else b.to_real(x)))
 
-        legA = {2 * li: b.apply_fourier_harmonics(b.to_real(Ainv), 2 * li) for li in range(1, self.Nl)}
-        SinvP_real = b.to_real(SinvP)
+        if xi is not None:                                               # 270-290, 330-332
+            SinvP = dagger(a, False) if self.const_mask else dagger(a_real, True)
+        elif self.const_mask:                                            # 273-276
+            SinvP = self.mask_mean * a
+        else:
+            SinvP = b.to_fourier(self.mask * a_real)
         fish = np.zeros((self.N_bins, self.N_bins))
+        bm = None if theory is None else np.zeros((self.N_bins, theory[1] * (len(theory[0]) - 1)))
+        scaling = 0.5 * b.volume / b.gridsize.prod() ** 2                # 390
+        if b.sightline == "local":
+            self._fisher_local(Ainv, SinvP, scaling, dagger, fish, theory, bm)
+            return fish if theory is None else (fish, bm)
+        for li in range(self.Nl):
+            for ki in range(self.Nk):
+                Q = dagger(b.fourier_filter(SinvP, 2 * li, self.k_bins[ki], self.k_bins[ki + 1]), False)
+                row = li * self.Nk + ki
+                for lp in range(self.Nl):                                # 394-401
+                    fish[row, lp * self.Nk:(lp + 1) * self.Nk] += scaling * b.cross_integrate(
+                        Ainv, Q, self.k_bins, 2 * lp)
+                if theory is not None:                                   # 395-402
+                    kt, nlt = theory
+                    nkt = len(kt) - 1
+                    for lt in range(nlt):
+                        bm[row, lt * nkt:(lt + 1) * nkt] += scaling * b.cross_integrate(Ainv, Q, kt, 2 * lt)
+        return fish if theory is None else (fish, bm)
 
-        def add(row, Q):                                                 # 380-407
+    def _fisher_local(self, Ainv, SinvP, scaling, dagger, fish, theory=None, bm=None):
+        """_compute_fisher, local sightline, even l (pspec.py:334-352, 380-407, 440-486).
+        Monopole rows Q = D Theta_b SinvP; multipole rows
+        Q = 1/2 D Theta_b H_l[SinvP] + 1/2 D sum_m Y_lm(r) IFT[Theta_b Y_lm(k) SinvP]
+        with D = (S^-1 P)^dag (or its covariance form) and H_l[x] = sum_m Y_lm(k) FT[Y_lm(r)
+        IFT x]; the row against column block l is the cross integral of Q with A^-1 a
+        (l = 0) or with H_l[A^-1 a], in the data bins and, for the theory matrix, the theory
+        bins."""
+        b = self.base
+        nl_leg = self.Nl if theory is None else theory[1]
+        if theory is not None:
+            assert theory[1] >= self.Nl, "Can't use larger lmax for data than for theory!"
+        A_real = b.to_real(Ainv)
+        legA = {2 * li: b.apply_fourier_harmonics(A_real, 2 * li) for li in range(1, nl_leg)}
+        SinvP_real = b.to_real(SinvP)
+
+        def add(row, Q):                                                 # 380-430
             fish[row, :self.Nk] += scaling * b.cross_integrate(Ainv, Q, self.k_bins, 0)
             for li in range(1, self.Nl):
                 fish[row, li * self.Nk:(li + 1) * self.Nk] += scaling * b.cross_integrate(legA[2 * li], Q,
                                                                                           self.k_bins, 0)
+            if theory is not None:
+                kt, nlt = theory
+                nkt = len(kt) - 1
+                bm[row, :nkt] += scaling * b.cross_integrate(Ainv, Q, kt, 0)
+                for li in range(1, nlt):
+                    bm[row, li * nkt:(li + 1) * nkt] += scaling * b.cross_integrate(legA[2 * li], Q, kt, 0)
 
         for ki in range(self.Nk):                                        # 442-445
             add(ki, dagger(b.fourier_filter(SinvP, 0, self.k_bins[ki], self.k_bins[ki + 1]), False))

@@ -166,8 +166,11 @@ class PSpec:
     def _mask_device(self):
         return self.base.to_device_grid(('pk_mask', id(self)), lambda: self.mask, torch.float64)
 
-    def _fisher_from_fields(self, a):
-        """Fisher contributions of a batch of GRFs a (B, half) complex128 (pspec.py:264-456)."""
+    def _fisher_from_fields(self, a, xi=None, theory=None):
+        """Fisher contributions of a batch of GRFs a (B, half) complex128 (pspec.py:215-493).
+        xi: device grids of the covariance spectrum (covariance contributions: every S^-1 P
+        becomes S^-1 [P xi P^dag + N] S^-dag); theory: (k_bins_theory, Nl_theory), which adds
+        the binning matrix of each realisation, (B, N_bins, Nl_theory * Nk_theory)."""
         b = self.base
         if b.sightline == 'local' and self.lmax > 0 and self.odd_l:
             raise NotImplementedError("backend='cuda' implements even multipoles for the local sightline")
@@ -180,7 +183,19 @@ class PSpec:
         Ainv = torch.empty_like(a)
         nat.spectral_filter(grid, F64, a, Ainv, [(i, -1.0, np.inf, 0, 0, 1.0, 1) for i in range(B)], w=ainv_w,
                             src_stride=nh)
-        if self.const_mask:
+        bm = None
+        if theory is not None:
+            k_th, nl_th = theory
+            bm = torch.empty((B, self.N_bins, nl_th * (len(k_th) - 1)), dtype=torch.float64, device=b.device)
+        if xi is not None:
+            # S^-1 P a -> S^-1 [P xi P^dag + N] S^-dag a (pspec.py:270-290, 330-332)
+            SinvP = a.clone()
+            if not self.const_mask:
+                nat.spectral_filter(grid, F64, SinvP, SinvP, [(i, -1.0, np.inf, 0, 0, invN, 0) for i in range(B)],
+                                    src_stride=nh)
+            SinvP = self._cov_rows(SinvP, xi)
+            qscale = 1.0
+        elif self.const_mask:
             SinvP = a
             qscale = self.mask_mean * self.mask_mean
         else:
@@ -196,18 +211,21 @@ class PSpec:
             qscale = 1.0
         fish = torch.empty((B, self.N_bins, self.N_bins), dtype=torch.float64, device=b.device)
         scaling = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
-        if b.sightline == 'local' and self.Nl > 1:
+        if b.sightline == 'local' and (self.Nl > 1 or theory is not None):
             for i in range(B):
-                S = SinvP[i] * self.mask_mean if self.const_mask else SinvP[i]
-                self._fisher_local(Ainv[i], S, scaling, fish[i])
-            return fish
+                S = SinvP[i] * self.mask_mean if (self.const_mask and xi is None) else SinvP[i]
+                self._fisher_local(Ainv[i], S, scaling, fish[i], xi=xi, theory=theory,
+                                   bm=None if bm is None else bm[i])
+            return fish if theory is None else (fish, bm)
         rows = [(li, ki) for li in range(self.Nl) for ki in range(self.Nk)]
         for i in range(B):
             Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
             maps = [(i, self.k_bins[ki], self.k_bins[ki + 1], 2 * li, 0, qscale if self.const_mask else invN, 0)
                     for (li, ki) in rows]
             nat.spectral_filter(grid, F64, SinvP, Q, maps, src_stride=nh)
-            if not self.const_mask:
+            if xi is not None:
+                Q = self._cov_rows(Q, xi)
+            elif not self.const_mask:
                 qr = b.fft_c2r(Q)
                 b.n_FFTs_reverse += self.N_bins
                 nat.elementwise(nat.PB_EW_MUL, qr, m, out=qr, y_period=b.nreal)
@@ -215,15 +233,105 @@ class PSpec:
                 b.n_FFTs_forward += self.N_bins
             nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, self.k_bins, self._ells(self.Nl),
                            scaling, fish[i], b.ws)
-        return fish
+            if theory is not None:                                       # pspec.py:395-402
+                nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, theory[0],
+                               self._ells(theory[1]), scaling, bm[i], b.ws)
+        return fish if theory is None else (fish, bm)
 
-    def _fisher_local(self, Ainv, S, scaling, fish):
+    def _xi_grids(self, Pk_cov):
+        """Device grids of the covariance spectrum Pk_cov = [k, P0(, P2(, P4))] keyed by
+        multipole (pspec.py:241-252): global, one grid P0 + L2(mu) P2 + L4(mu) P4; local, one
+        grid per multipole.  Linear interpolation, zero outside the table."""
+        from scipy.interpolate import interp1d
+        from scipy.special import legendre
+        b = self.base
+        terms = [interp1d(Pk_cov[0], Pk_cov[i], bounds_error=False, fill_value=0.)(b.modk_grid)
+                 for i in range(1, len(Pk_cov))]
+        if b.sightline == 'global':
+            g = terms[0]
+            for i, t in enumerate(terms[1:]):
+                g = g + legendre(2 * (i + 1))(b.muk_grid) * t
+            grids = {0: g}
+        else:
+            grids = {2 * i: t for i, t in enumerate(terms)}
+        return {l: torch.as_tensor(np.ascontiguousarray(v, dtype=np.float64), device=b.device)
+                for l, v in grids.items()}
+
+    def _xi_real(self, X, x_real, xi):
+        """apply_xi with real output (base.py:413-437) for a block of maps: X (R, half) half
+        spectra, x_real (R, n0, n1, n2) the same maps in real space.  P0 X, plus for each
+        local multipole l > 0 one half of P_l sum_m Y_lm(k) FT[Y_lm(r) x] and one half of
+        sum_m Y_lm(r) IFT[Y_lm(k) P_l X]."""
+        b = self.base
+        grid, F64, nh = b.grid, nat.PB_F64, b.nhalf
+        invN = 1.0 / b.nreal
+        nrow = X.shape[0]
+        P = torch.empty_like(X)
+        nat.spectral_filter(grid, F64, X, P, [(i, -1.0, np.inf, 0, 0, invN, 1) for i in range(nrow)], w=xi[0],
+                            src_stride=nh)
+        ells = sorted(xi)[1:]
+        harm = b.harmonics if ells else None
+        for l in ells:
+            for i in range(nrow):
+                H = harm.apply_fourier(x_real[i], l)
+                nat.spectral_filter(grid, F64, H[None], P, [(0, -1.0, np.inf, 0, 0, 0.5 * invN, 1)], w=xi[l],
+                                    accumulate=True, dst=[i])
+        b.n_FFTs_reverse += nrow
+        out = b.fft_c2r(P)
+        for l in ells:
+            yr = harm._grid('r', l, torch.float64)
+            yk = harm._grid('k', l, torch.float64)
+            for mi in range(yr.shape[0]):
+                nat.spectral_filter(grid, F64, X, P, [(i, -1.0, np.inf, 0, 0, 0.5 * invN, 1) for i in range(nrow)],
+                                    w=(yk[mi] * xi[l]).contiguous(), src_stride=nh)
+                b.n_FFTs_reverse += nrow
+                out.addcmul_(b.fft_c2r(P), yr[mi])
+        return out
+
+    def _cov_rows(self, R, xi, real=None):
+        """R <- S^-1 [P xi P^dag + N] S^-dag of a block of maps, trivial S^-1 (pspec.py:277-290,
+        307-323).  R (R, half) holds the half spectra, multiplied by 1/N^3 beforehand for a
+        varying mask; `real` optional real-space maps added to them.  Constant mask: the
+        diagonal weight m^2 xi + m; varying mask: N is mask_shot, and
+        mask x IFT[xi FT[mask x]] + mask_shot x."""
+        b = self.base
+        nrow = R.shape[0]
+        if self.const_mask:
+            if len(xi) > 1:
+                raise ValueError("local multipoles of Pk_cov need a varying mask (the reference applies xi "
+                                 "without a real-space map for a constant mask)")
+            if real is not None:
+                b.n_FFTs_forward += nrow
+                R.add_(b.fft_r2c(real))
+            mm = float(self.mask_mean)
+            w = (xi[0] * (mm * mm) + mm).contiguous()
+            nat.spectral_filter(b.grid, nat.PB_F64, R, R, [(i, -1.0, np.inf, 0, 0, 1.0, 1) for i in range(nrow)],
+                                w=w, src_stride=b.nhalf)
+            return R
+        m = self._mask_device()
+        ms = b.to_device_grid(('pk_mask_shot', id(self)), lambda: self.mask_shot, torch.float64)
+        b.n_FFTs_reverse += nrow
+        sid = b.fft_c2r(R)
+        if real is not None:
+            sid.add_(real)
+        t = nat.elementwise(nat.PB_EW_MUL, sid, m, y_period=b.nreal)
+        b.n_FFTs_forward += nrow
+        u = self._xi_real(b.fft_r2c(t, out=R), t, xi)
+        nat.elementwise(nat.PB_EW_MUL, u, m, out=u, y_period=b.nreal)
+        u.add_(nat.elementwise(nat.PB_EW_MUL, sid, ms, out=t, y_period=b.nreal))
+        b.n_FFTs_forward += nrow
+        return b.fft_r2c(u, out=R)
+
+    def _fisher_local(self, Ainv, S, scaling, fish, xi=None, theory=None, bm=None):
         """One realisation's Fisher rows for the local sightline, even l (pspec.py:334-352,
         380-407, 440-486).  With H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x] and D = (S^-1 P)^dag:
         monopole rows Q = D Theta_b S; multipole rows
         Q = 1/2 D Theta_b H_l[S] + 1/2 D sum_m Y_lm(r) IFT[Theta_b Y_lm(k) S]; column block 0 is
         the binned cross spectrum of Q with A^-1 a, block l the one with H_l[A^-1 a].  All
-        rows of a multipole go through each step as one batch."""
+        rows of a multipole go through each step as one batch.  With xi, D is the covariance
+        form S^-1 [P xi P^dag + N] S^-dag; with theory = (k_bins_theory, Nl_theory) the
+        binning matrix bm gets the same cross spectra in the theory bins for multipoles
+        0..2(Nl_theory - 1) (pspec.py:395-423)."""
         b = self.base
         grid, F64, Nk = b.grid, nat.PB_F64, self.Nk
         invN = 1.0 / b.nreal
@@ -236,6 +344,8 @@ class PSpec:
             """R <- D R for a block of rows whose Fourier part R (already scaled by 1/N^3 for
             a varying mask, by the mask mean for a constant one) may come with a real-space
             part `real` (unnormalised, added before the mask)."""
+            if xi is not None:
+                return self._cov_rows(R, xi, real)
             if self.const_mask:
                 if real is not None:
                     R.add_(b.fft_r2c(real), alpha=mm)
@@ -249,7 +359,7 @@ class PSpec:
             b.n_FFTs_forward += R.shape[0]
             return b.fft_r2c(rr, out=R)
 
-        qs = mm if self.const_mask else invN
+        qs = invN if not self.const_mask else (1.0 if xi is not None else mm)
         bands = [(0, self.k_bins[ki], self.k_bins[ki + 1], 0, 0, qs, 0) for ki in range(Nk)]
         nat.spectral_filter(grid, F64, S, Q[:Nk], bands)
         dagger_rows(Q[:Nk])
@@ -273,12 +383,24 @@ class PSpec:
         tmp = torch.empty((self.N_bins, Nk), dtype=torch.float64, device=b.device)
         nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv, Q, self.N_bins, self.k_bins, [(0, 0)], scaling, tmp, b.ws)
         fish[:, :Nk] = tmp
-        A_real = b.to_real(Ainv)
-        for li in range(1, self.Nl):
+        nl_th = 0 if theory is None else theory[1]
+        if theory is not None:
+            k_th = theory[0]
+            nkt = len(k_th) - 1
+            tth = torch.empty((self.N_bins, nkt), dtype=torch.float64, device=b.device)
+            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv, Q, self.N_bins, k_th, [(0, 0)], scaling, tth, b.ws)
+            bm[:, :nkt] = tth
+        A_real = b.to_real(Ainv) if max(self.Nl, nl_th) > 1 else None
+        for li in range(1, max(self.Nl, nl_th)):
             legA = harm.apply_fourier(A_real, 2 * li)
-            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, legA, Q, self.N_bins, self.k_bins, [(0, 0)], scaling, tmp,
-                           b.ws)
-            fish[:, li * Nk:(li + 1) * Nk] = tmp
+            if li < self.Nl:
+                nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, legA, Q, self.N_bins, self.k_bins, [(0, 0)], scaling,
+                               tmp, b.ws)
+                fish[:, li * Nk:(li + 1) * Nk] = tmp
+            if li < nl_th:
+                nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, legA, Q, self.N_bins, k_th, [(0, 0)], scaling, tth,
+                               b.ws)
+                bm[:, li * nkt:(li + 1) * nkt] = tth
         return fish
 
     def compute_fisher_contribution(self, seed, verb=False):
@@ -463,9 +585,51 @@ class PSpec:
         inv[nz] = 1. / PA[nz]
         return inv
 
+    def _reference_field(self, seed):
+        b = self.base
+        re, im = b.reference_noise(seed + int(1e7))
+        return b.grf_from_noise(torch.as_tensor(re, device=b.device)[None], torch.as_tensor(im, device=b.device)[None])
+
     def compute_covariance_contribution(self, seed, Pk_cov, verb=False):
-        raise NotImplementedError("covariance Monte Carlo is not implemented in backend='cuda'")
+        """Contribution of one GRF to the Gaussian covariance of the unwindowed estimator
+        (pspec.py:149-162): the Fisher rows with S^-1 P replaced by S^-1 [P xi P^dag + N] S^-dag,
+        xi the correlation of Pk_cov = [k, P0(, P2(, P4))] (no shot noise) and N the shot
+        mask (the mask mean for a constant mask).  Same noise as compute_fisher_contribution."""
+        if not self.const_mask:
+            assert hasattr(self, 'mask_shot'), "Must supply mask_shot to compute shot-noise contribution"
+        assert len(Pk_cov) != 0, "Must provide fiducial power spectrum if computing covariance!"
+        assert len(np.asarray(Pk_cov).shape) == 2, "Pk should contain k and P_0, (and optionally P_2, P_4) columns"
+        assert len(Pk_cov) in [2, 3, 4], "Pk should contain k and P_0, (and optionally P_2, P_4) columns"
+        assert (len(Pk_cov) - 2) * 2 <= self.lmax, "Can't use higher multipoles than lmax"
+        xi = self._xi_grids(np.asarray(Pk_cov, dtype=np.float64))
+        return self._fisher_from_fields(self._reference_field(seed), xi=xi)[0].cpu().numpy()
 
     def compute_theory_contribution(self, seed, k_bins_theory, lmax_theory=None, include_wideangle=False,
                                     verb=False):
-        raise NotImplementedError("theory matrices are not implemented in backend='cuda'")
+        """Fisher contribution and rectangular binning matrix of one GRF (pspec.py:164-196):
+        row b of the binning matrix holds the cross spectra of the Fisher Q-map of bin b with
+        A^-1 a in the theory k-bins, weighted by L_l(mu) (global) or with the harmonic
+        transform sum_m Y_lm(k) FT[Y_lm(r) A^-1 a] (local), for l = 0, 2, .. lmax_theory.
+        Returns (fisher, binning_matrix)."""
+        b = self.base
+        k_bins_theory = np.asarray(k_bins_theory)
+        assert np.max(k_bins_theory) < np.min(b.kNy), "k_max must be less than k_Nyquist!"
+        assert np.min(k_bins_theory) >= np.max(b.kF), "k_min must be at least the k_fundamental!"
+        assert np.max(k_bins_theory) <= b.Pfid[0][-1], "Fiducial power spectrum should extend up to k_max!"
+        assert np.min(k_bins_theory) >= b.Pfid[0][0], "Fiducial power spectrum should extend down to k_min!"
+        if lmax_theory is None:
+            lmax_theory = self.lmax
+        if include_wideangle:
+            assert not b.sightline == 'global', "Wide-angle effects require local lines-of-sight!"
+            raise NotImplementedError("backend='cuda' does not implement the odd-l wide-angle theory terms")
+        if not self.odd_l:
+            assert lmax_theory % 2 == 0, "Must use even lmax if not including wide-angle effects!"
+        if lmax_theory > 4:
+            raise NotImplementedError("backend='cuda' implements theory multipoles up to l = 4")
+        if b.sightline == 'local':
+            assert lmax_theory >= self.lmax, "Can't use larger lmax for data than for theory!"
+        if not np.all(np.diff(k_bins_theory) > 0):
+            raise ValueError("k_bins_theory must be strictly increasing")
+        fish, bm = self._fisher_from_fields(self._reference_field(seed),
+                                            theory=(k_bins_theory.astype(np.float64), lmax_theory // 2 + 1))
+        return fish[0].cpu().numpy(), bm[0].cpu().numpy()

@@ -364,6 +364,41 @@ def local_shot(pb):
                 p_mask=_quiet(ps.compute_shot_contribution, 1), bins=bs.all_bins, sym=bs.sym_factor, b_full=b_full)
 
 
+@case
+def pk_cov_theory(pb):
+    """PSpec (global sightline) covariance and theory-matrix contributions: 24^3, L=600, CIC
+    window, lmax=4, 4 bins.  Covariance with Pk_cov = [k, P0, P2] (shell-sector mask,
+    mask_shot = 0.5 mask, seed 2; constant mask 0.7, seed 3); theory matrix with 6 theory
+    bins to 0.12 and lmax_theory = 4 (mask, seed 4).  Local sightline (box centred at
+    (700, 400, 900) Mpc/h, TSC window, lmax=2): covariance with [k, P0, P2] (mask, mask_shot =
+    0.5 mask, seed 5), theory matrix with lmax_theory = 4 (seed 6), covariance with [k, P0]
+    and the constant mask 0.7 (seed 7)."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    kt = np.linspace(0.0, 1.0, 2000)
+    p0 = 3e3 * np.exp(-(kt / 0.25) ** 2) + 200.0
+    p2 = 800.0 * np.exp(-(kt / 0.2) ** 2)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=4, mask=mask, mask_shot=0.5 * mask)
+    c2 = _quiet(ps.compute_covariance_contribution, 2, [kt, p0, p2])
+    ps2 = _quiet(pb.PSpec, base, edges, lmax=4, mask=0.7 * np.ones((N, N, N)))
+    c3 = _quiet(ps2.compute_covariance_contribution, 3, [kt, p0, p2])
+    kth = np.linspace(kF, 0.12, 7)
+    f4, t4 = _quiet(ps.compute_theory_contribution, 4, kth, lmax_theory=4)
+    center = [700.0, 400.0, 900.0]
+    lbase = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=center, sightline="local", pixel_window="tsc",
+                   backend="mkl")
+    lps = _quiet(pb.PSpec, lbase, edges, lmax=2, mask=mask, mask_shot=0.5 * mask)
+    lc5 = _quiet(lps.compute_covariance_contribution, 5, [kt, p0, p2])
+    lf6, lt6 = _quiet(lps.compute_theory_contribution, 6, kth, lmax_theory=4)
+    lps2 = _quiet(pb.PSpec, lbase, edges, lmax=2, mask=0.7 * np.ones((N, N, N)))
+    lc7 = _quiet(lps2.compute_covariance_contribution, 7, [kt, p0])
+    return dict(N=N, L=L, edges=edges, pk_k=kt, p0=p0, p2=p2, c2=c2, c3=c3, kth=kth, f4=f4, t4=t4,
+                center=np.asarray(center), lc5=lc5, lf6=lf6, lt6=lt6, lc7=lc7)
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

@@ -276,3 +276,28 @@ def test_philox_noise_is_gaussian():
     assert abs(x.mean()) < 5e-3 and abs(x.std() - 1) < 5e-3
     re2, _ = b.philox_noise(12346)
     assert abs(np.corrcoef(re.ravel(), re2.ravel())[0, 1]) < 5e-3
+
+
+def test_pk_covariance_and_theory():
+    """Covariance (Pk_cov with P0, P2; varying mask with mask_shot, constant mask) and theory
+    matrix contributions (lmax_theory = 4), global and local sightlines, on the reference's
+    own noise."""
+    g = gold("pk_cov_theory")
+    N, L = int(g["N"]), float(g["L"])
+    m = mask24(N, L)
+    pk_cov = [g["pk_k"], g["p0"], g["p2"]]
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic")
+    ps = O.OraclePSpec(b, g["edges"], lmax=4, mask=m)
+    assert rel(ps.covariance_contribution(b.reference_noise(2 + 10 ** 7), pk_cov, mask_shot=0.5 * m), g["c2"]) < TOL
+    ps2 = O.OraclePSpec(b, g["edges"], lmax=4, mask=0.7 * np.ones((N, N, N)))
+    assert rel(ps2.covariance_contribution(b.reference_noise(3 + 10 ** 7), pk_cov), g["c3"]) < TOL
+    f, t = ps.theory_contribution(b.reference_noise(4 + 10 ** 7), g["kth"], lmax_theory=4)
+    assert rel(f, g["f4"]) < TOL and rel(t, g["t4"]) < TOL
+    lb = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc", boxcenter=g["center"], sightline="local")
+    lps = O.OraclePSpec(lb, g["edges"], lmax=2, mask=m)
+    assert rel(lps.covariance_contribution(lb.reference_noise(5 + 10 ** 7), pk_cov, mask_shot=0.5 * m),
+               g["lc5"]) < TOL
+    f, t = lps.theory_contribution(lb.reference_noise(6 + 10 ** 7), g["kth"], lmax_theory=4)
+    assert rel(f, g["lf6"]) < TOL and rel(t, g["lt6"]) < TOL
+    lps2 = O.OraclePSpec(lb, g["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)))
+    assert rel(lps2.covariance_contribution(lb.reference_noise(7 + 10 ** 7), pk_cov[:2]), g["lc7"]) < TOL
