@@ -372,6 +372,52 @@ class OracleBase:
 
 
 # --------------------------------------------------------------------------------------
+# covariance filter (pspec.py:241-323, bspec.py:481-519, base.py:413-437)
+# --------------------------------------------------------------------------------------
+def xi_grids(b, Pk_cov):
+    """Pk_grid of _compute_fisher (pspec.py:241-252, bspec.py:481-496): global, one grid
+    P0(k) + L2(mu) P2(k) + L4(mu) P4(k); local, one grid per multipole.  Linear
+    interpolation, zero outside the table."""
+    from scipy.special import legendre as sp_legendre
+    terms = [interp1d(Pk_cov[0], Pk_cov[i], bounds_error=False, fill_value=0.0)(b.modk_grid)
+             for i in range(1, len(Pk_cov))]
+    if b.sightline == "global":
+        g = terms[0]
+        for i, t in enumerate(terms[1:]):
+            g = g + sp_legendre(2 * (i + 1))(b.muk_grid) * t
+        return {0: g}
+    return {2 * i: t for i, t in enumerate(terms)}
+
+
+def apply_xi(b, X, x_real, xi, output):
+    """apply_xi (base.py:413-437): P0 X, plus for the local sightline and each l > 0
+    1/2 P_l sum_m Y_lm(k) FT[Y_lm(r) x] and 1/2 sum_m Y_lm(r) IFT[Y_lm(k) P_l X]."""
+    PF = X * xi[0]
+    if len(xi) == 1:
+        return PF if output == "fourier" else b.to_real(PF)
+    if x_real is None:
+        raise ValueError("local multipoles of the covariance spectrum need the real-space map")
+    PR = np.zeros(tuple(b.gridsize))
+    for l in sorted(xi)[1:]:
+        PF = PF + 0.5 * b.apply_fourier_harmonics(x_real, l) * xi[l]
+        PR = PR + 0.5 * b.apply_real_harmonics(X * xi[l], l)
+    return PF + b.to_fourier(PR) if output == "fourier" else b.to_real(PF) + PR
+
+
+def cov_filter(b, x, real, xi, const_mask, mask_mean, mask, mask_shot):
+    """S^-1 [P xi P^dag + N] S^-dag x with the trivial S^-1 (pspec.py:277-290, 307-323;
+    bspec.py:499-519); x is a real map if `real`, else a half spectrum; the output is a
+    half spectrum."""
+    if const_mask:
+        Sid = b.to_fourier(x) if real else x
+        return mask_mean ** 2 * apply_xi(b, Sid, None, xi, "fourier") + mask_mean * Sid
+    Sid = x if real else b.to_real(x)
+    Pd_real = mask * Sid
+    C = apply_xi(b, b.to_fourier(Pd_real), Pd_real, xi, "real")
+    return b.to_fourier(mask * C + mask_shot * Sid)
+
+
+# --------------------------------------------------------------------------------------
 # power spectrum (pspec.py)
 # --------------------------------------------------------------------------------------
 class OraclePSpec:
@@ -454,46 +500,11 @@ class OraclePSpec:
         return self._contribution(noise_pair, theory=(k_th, lt // 2 + 1))
 
     def xi_grids(self, Pk_cov):
-        """Pk_grid of _compute_fisher (pspec.py:241-252): global, one grid
-        P0(k) + L2(mu) P2(k) + L4(mu) P4(k); local, one grid per multipole.  Linear
-        interpolation, zero outside the table."""
-        from scipy.special import legendre as sp_legendre
-        b = self.base
-        terms = [interp1d(Pk_cov[0], Pk_cov[i], bounds_error=False, fill_value=0.0)(b.modk_grid)
-                 for i in range(1, len(Pk_cov))]
-        if b.sightline == "global":
-            g = terms[0]
-            for i, t in enumerate(terms[1:]):
-                g = g + sp_legendre(2 * (i + 1))(b.muk_grid) * t
-            return {0: g}
-        return {2 * i: t for i, t in enumerate(terms)}
-
-    def apply_xi(self, X, x_real, xi, output):
-        """apply_xi (base.py:413-437): P0 X, plus for the local sightline and each l > 0
-        1/2 P_l sum_m Y_lm(k) FT[Y_lm(r) x] and 1/2 sum_m Y_lm(r) IFT[Y_lm(k) P_l X]."""
-        b = self.base
-        PF = X * xi[0]
-        if len(xi) == 1:
-            return PF if output == "fourier" else b.to_real(PF)
-        if x_real is None:
-            raise ValueError("local multipoles of the covariance spectrum need the real-space map")
-        PR = np.zeros(tuple(b.gridsize))
-        for l in sorted(xi)[1:]:
-            PF = PF + 0.5 * b.apply_fourier_harmonics(x_real, l) * xi[l]
-            PR = PR + 0.5 * b.apply_real_harmonics(X * xi[l], l)
-        return PF + b.to_fourier(PR) if output == "fourier" else b.to_real(PF) + PR
+        return xi_grids(self.base, Pk_cov)
 
     def cov_filter(self, x, real, xi, mask_shot):
-        """S^-1 [P xi P^dag + N] S^-dag x with the trivial S^-1 (pspec.py:277-290, 307-323);
-        x is a real map if `real`, else a half spectrum; the output is a half spectrum."""
-        b = self.base
-        if self.const_mask:
-            Sid = b.to_fourier(x) if real else x
-            return self.mask_mean ** 2 * self.apply_xi(Sid, None, xi, "fourier") + self.mask_mean * Sid
-        Sid = x if real else b.to_real(x)
-        Pd_real = self.mask * Sid
-        C = self.apply_xi(b.to_fourier(Pd_real), Pd_real, xi, "real")
-        return b.to_fourier(self.mask * C + mask_shot * Sid)
+        return cov_filter(self.base, x, real, xi, self.const_mask, getattr(self, "mask_mean", None),
+                          None if self.const_mask else self.mask, mask_shot)
 
     def _contribution(self, noise_pair, xi=None, mask_shot=None, theory=None):
         """_compute_fisher, global and local (even l) sightlines (pspec.py:215-493)."""
@@ -868,10 +879,18 @@ class OracleBSpec:
         out = np.linalg.inv(fish) @ self.numerator(data, "ideal", sym=sym)   # bspec.py:1110
         return {"b%d" % l: out[l // 2 * self.N3:(l // 2 + 1) * self.N3] for l in range(0, self.lmax + 1, 2)}
 
-    def fisher_contribution(self, noise1, noise2, sym=None, return_Q=False):
-        """_compute_fisher, no covariance, trivial S^-1 (bspec.py:473-676); for the local
-        sightline the l > 0 maps come from the harmonic transform of each weighted map
-        (548-577) and the l leg of the A^-1 Q maps is applied in real space (621-631)."""
+    def covariance_contribution(self, noise1, noise2, Pk_cov, mask_shot_2pt=None, sym=None):
+        """compute_covariance_contribution (bspec.py:447-471): the Fisher contribution with
+        S^-1 P replaced by S^-1 [P xi P^dag + N] S^-dag, N the two-point shot mask."""
+        assert len(np.asarray(Pk_cov).shape) == 2 and len(Pk_cov) in (2, 3, 4)
+        return self.fisher_contribution(noise1, noise2, sym=sym, xi=xi_grids(self.base, Pk_cov),
+                                        mask_shot=mask_shot_2pt)
+
+    def fisher_contribution(self, noise1, noise2, sym=None, return_Q=False, xi=None, mask_shot=None):
+        """_compute_fisher, trivial S^-1 (bspec.py:473-676); for the local sightline the
+        l > 0 maps come from the harmonic transform of each weighted map (548-577) and the
+        l leg of the A^-1 Q maps is applied in real space (621-631).  With xi, the
+        covariance form of the filter (499-519)."""
         b = self.base
         sym = self.symmetry_factor() if sym is None else sym
         ks = self.k_bins_squeeze
@@ -882,7 +901,11 @@ class OracleBSpec:
         if not self.const_mask:
             ar1, ar2 = b.to_real(a1), b.to_real(a2)                      # 651-653
 
-        def apply_filter(x_fourier=None, x_real=None):                   # 499-505
+        def apply_filter(x_fourier=None, x_real=None):                   # 499-519
+            if xi is not None:
+                return cov_filter(b, x_fourier if self.const_mask else x_real, not self.const_mask, xi,
+                                  self.const_mask, getattr(self, "mask_mean", None),
+                                  None if self.const_mask else self.mask, mask_shot)
             if self.const_mask:
                 return self.mask_mean * x_fourier
             return b.to_fourier(self.mask * x_real)

@@ -12,6 +12,7 @@ import torch
 from scipy.interpolate import interp1d
 
 from . import _native as nat
+from . import covariance
 from . import realisations
 from .harmonics import real_harmonics
 
@@ -737,7 +738,22 @@ class BSpec:
         b.n_FFTs_forward += len(keys)
         return b.fft_r2c(prods)
 
-    def _fisher_from_fields(self, a1, a2):
+    def _filter_rows(self, R, xi, mask_shot):
+        """S^-1 P (xi None) or its covariance form S^-1 [P xi P^dag + N] S^-dag on a block of
+        half spectra prescaled as `_apply_filter_spectra` takes them (1 instead of the mask
+        mean for the covariance form), 64 maps at a time; in place."""
+        if xi is None:
+            return self._apply_filter_spectra(R, True)
+        m = None if self.const_mask else self._mask_device()
+        for c0 in range(0, R.shape[0], 64):
+            covariance.cov_rows(self.base, R[c0:c0 + 64], xi, self.const_mask, getattr(self, "mask_mean", None), m,
+                                mask_shot)
+        return R
+
+    def _fisher_from_fields(self, a1, a2, xi=None, mask_shot=None):
+        """Fisher contribution of one GRF pair (bspec.py:473-676); with xi (device grids of
+        a covariance spectrum) and mask_shot (device two-point shot mask, varying masks) the
+        covariance contribution (bspec.py:447-471)."""
         b = self.base
         local = b.sightline == 'local' and self.lmax > 0
         ab = self.all_bins
@@ -756,7 +772,7 @@ class BSpec:
         kpos = {k: i for i, k in enumerate(keys)}
         FT = self._key_fts(G1, G2, keys)
         del G1, G2
-        qs = self.mask_mean if self.const_mask else invN
+        qs = invN if not self.const_mask else (1.0 if xi is not None else self.mask_mean)
         Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
         # leg b3 carries L_l; with the local sightline that leg is applied in real space below
         leg1 = [(kpos[(r[0], r[1], 0)], ks[r[2]], ks[r[2] + 1], 0 if local else r[3], 0,
@@ -789,18 +805,20 @@ class BSpec:
                 idx = torch.as_tensor(rows, device=b.device)
                 Q[idx] = Q[idx] + b.fft_r2c(acc) * qs
         del FT
-        Q = self._apply_filter_spectra(Q, True)
+        Q = self._filter_rows(Q, xi, mask_shot)
         # --- rows from Q[S^-1 P a] (compute_Q 'Sinv', bspec.py:528-597)
         if self.const_mask:
             ws = torch.empty((2,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
-            nat.spectral_filter(b.grid, F64, a1, ws[0:1], [(0, -1.0, np.inf, 0, 0, self.mask_mean, 0)])
-            nat.spectral_filter(b.grid, F64, a2, ws[1:2], [(0, -1.0, np.inf, 0, 0, self.mask_mean, 0)])
+            nat.spectral_filter(b.grid, F64, a1, ws[0:1], [(0, -1.0, np.inf, 0, 0, qs, 0)])
+            nat.spectral_filter(b.grid, F64, a2, ws[1:2], [(0, -1.0, np.inf, 0, 0, qs, 0)])
+            if xi is not None:
+                ws = self._filter_rows(ws, xi, mask_shot)
         else:
             ws = torch.empty((2,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
             nat.spectral_filter(b.grid, F64, a1, ws[0:1], [(0, -1.0, np.inf, 0, 0, invN, 0)])
             nat.spectral_filter(b.grid, F64, a2, ws[1:2], [(0, -1.0, np.inf, 0, 0, invN, 0)])
             b.n_FFTs_reverse += 2
-            ws = self._apply_filter_spectra(ws, True)
+            ws = self._filter_rows(ws, xi, mask_shot)
         G1, G2 = self._all_g(ws[0], ws[1])
         skeys = sorted({(int(r[0]), int(r[2]), int(r[3])) for r in ab})
         spos = {k: i for i, k in enumerate(skeys)}
@@ -951,7 +969,36 @@ class BSpec:
         return quad - 2. * cubic
 
     def compute_covariance_contribution(self, seed, Pk_cov, verb=False, mask_shot_2pt=None):
-        raise NotImplementedError("covariance Monte Carlo is not implemented in backend='cuda'")
+        """Contribution of one GRF pair to the Gaussian covariance of the unwindowed
+        bispectrum (bspec.py:447-471): the Fisher computation with S^-1 P replaced by
+        S^-1 [P xi P^dag + N] S^-dag, xi the correlation of Pk_cov = [k, P0(, P2(, P4))]
+        (no shot noise) and N the two-point shot mask (mask_shot_2pt, else the bispectrum's
+        mask_shot; the mask mean for a constant mask).  Same noise as
+        compute_fisher_contribution."""
+        if (not self.const_mask) and (mask_shot_2pt is None):
+            assert getattr(self, 'mask_shot', None) is not None, \
+                "Must supply a shot-noise mask to compute the shot-noise contribution!"
+            print("## Caution: assuming the same shot-noise mask for the power spectrum and bispectrum!")
+            self.mask_shot_2pt = self.mask_shot
+        elif mask_shot_2pt is not None:
+            self.mask_shot_2pt = np.asarray(mask_shot_2pt).astype(np.float64)
+        else:
+            self.mask_shot_2pt = None
+        assert len(Pk_cov) != 0, "Must provide fiducial power spectrum if computing covariance!"
+        assert len(np.asarray(Pk_cov).shape) == 2, "Pk should contain k and P_0 (and optionally P_2, P_4) columns"
+        assert len(Pk_cov) in [2, 3, 4], "Pk should contain k and P_0 (and optionally P_2, P_4) columns"
+        if not hasattr(self, 'sym_factor'):
+            self._compute_symmetry_factor()
+        b = self.base
+        ms = None
+        if not self.const_mask:
+            ms = torch.as_tensor(np.ascontiguousarray(self.mask_shot_2pt), dtype=torch.float64, device=b.device)
+        xi = covariance.xi_grids(b, Pk_cov)
+        r1 = b.reference_noise(seed + int(1e7))
+        r2 = b.reference_noise(seed + int(2e7))
+        a1 = b.grf_from_noise(torch.as_tensor(r1[0], device=b.device), torch.as_tensor(r1[1], device=b.device))
+        a2 = b.grf_from_noise(torch.as_tensor(r2[0], device=b.device), torch.as_tensor(r2[1], device=b.device))
+        return self._fisher_from_fields(a1, a2, xi=xi, mask_shot=ms).cpu().numpy()
 
 
 _TC_OK = None

@@ -9,6 +9,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
+from . import covariance
 from . import realisations
 
 
@@ -239,88 +240,13 @@ class PSpec:
         return fish if theory is None else (fish, bm)
 
     def _xi_grids(self, Pk_cov):
-        """Device grids of the covariance spectrum Pk_cov = [k, P0(, P2(, P4))] keyed by
-        multipole (pspec.py:241-252): global, one grid P0 + L2(mu) P2 + L4(mu) P4; local, one
-        grid per multipole.  Linear interpolation, zero outside the table."""
-        from scipy.interpolate import interp1d
-        from scipy.special import legendre
-        b = self.base
-        terms = [interp1d(Pk_cov[0], Pk_cov[i], bounds_error=False, fill_value=0.)(b.modk_grid)
-                 for i in range(1, len(Pk_cov))]
-        if b.sightline == 'global':
-            g = terms[0]
-            for i, t in enumerate(terms[1:]):
-                g = g + legendre(2 * (i + 1))(b.muk_grid) * t
-            grids = {0: g}
-        else:
-            grids = {2 * i: t for i, t in enumerate(terms)}
-        return {l: torch.as_tensor(np.ascontiguousarray(v, dtype=np.float64), device=b.device)
-                for l, v in grids.items()}
-
-    def _xi_real(self, X, x_real, xi):
-        """apply_xi with real output (base.py:413-437) for a block of maps: X (R, half) half
-        spectra, x_real (R, n0, n1, n2) the same maps in real space.  P0 X, plus for each
-        local multipole l > 0 one half of P_l sum_m Y_lm(k) FT[Y_lm(r) x] and one half of
-        sum_m Y_lm(r) IFT[Y_lm(k) P_l X]."""
-        b = self.base
-        grid, F64, nh = b.grid, nat.PB_F64, b.nhalf
-        invN = 1.0 / b.nreal
-        nrow = X.shape[0]
-        P = torch.empty_like(X)
-        nat.spectral_filter(grid, F64, X, P, [(i, -1.0, np.inf, 0, 0, invN, 1) for i in range(nrow)], w=xi[0],
-                            src_stride=nh)
-        ells = sorted(xi)[1:]
-        harm = b.harmonics if ells else None
-        for l in ells:
-            for i in range(nrow):
-                H = harm.apply_fourier(x_real[i], l)
-                nat.spectral_filter(grid, F64, H[None], P, [(0, -1.0, np.inf, 0, 0, 0.5 * invN, 1)], w=xi[l],
-                                    accumulate=True, dst=[i])
-        b.n_FFTs_reverse += nrow
-        out = b.fft_c2r(P)
-        for l in ells:
-            yr = harm._grid('r', l, torch.float64)
-            yk = harm._grid('k', l, torch.float64)
-            for mi in range(yr.shape[0]):
-                nat.spectral_filter(grid, F64, X, P, [(i, -1.0, np.inf, 0, 0, 0.5 * invN, 1) for i in range(nrow)],
-                                    w=(yk[mi] * xi[l]).contiguous(), src_stride=nh)
-                b.n_FFTs_reverse += nrow
-                out.addcmul_(b.fft_c2r(P), yr[mi])
-        return out
+        return covariance.xi_grids(self.base, Pk_cov)
 
     def _cov_rows(self, R, xi, real=None):
-        """R <- S^-1 [P xi P^dag + N] S^-dag of a block of maps, trivial S^-1 (pspec.py:277-290,
-        307-323).  R (R, half) holds the half spectra, multiplied by 1/N^3 beforehand for a
-        varying mask; `real` optional real-space maps added to them.  Constant mask: the
-        diagonal weight m^2 xi + m; varying mask: N is mask_shot, and
-        mask x IFT[xi FT[mask x]] + mask_shot x."""
-        b = self.base
-        nrow = R.shape[0]
-        if self.const_mask:
-            if len(xi) > 1:
-                raise ValueError("local multipoles of Pk_cov need a varying mask (the reference applies xi "
-                                 "without a real-space map for a constant mask)")
-            if real is not None:
-                b.n_FFTs_forward += nrow
-                R.add_(b.fft_r2c(real))
-            mm = float(self.mask_mean)
-            w = (xi[0] * (mm * mm) + mm).contiguous()
-            nat.spectral_filter(b.grid, nat.PB_F64, R, R, [(i, -1.0, np.inf, 0, 0, 1.0, 1) for i in range(nrow)],
-                                w=w, src_stride=b.nhalf)
-            return R
-        m = self._mask_device()
-        ms = b.to_device_grid(('pk_mask_shot', id(self)), lambda: self.mask_shot, torch.float64)
-        b.n_FFTs_reverse += nrow
-        sid = b.fft_c2r(R)
-        if real is not None:
-            sid.add_(real)
-        t = nat.elementwise(nat.PB_EW_MUL, sid, m, y_period=b.nreal)
-        b.n_FFTs_forward += nrow
-        u = self._xi_real(b.fft_r2c(t, out=R), t, xi)
-        nat.elementwise(nat.PB_EW_MUL, u, m, out=u, y_period=b.nreal)
-        u.add_(nat.elementwise(nat.PB_EW_MUL, sid, ms, out=t, y_period=b.nreal))
-        b.n_FFTs_forward += nrow
-        return b.fft_r2c(u, out=R)
+        ms = None if self.const_mask else self.base.to_device_grid(('pk_mask_shot', id(self)),
+                                                                   lambda: self.mask_shot, torch.float64)
+        return covariance.cov_rows(self.base, R, xi, self.const_mask, getattr(self, 'mask_mean', None),
+                                   None if self.const_mask else self._mask_device(), ms, real)
 
     def _fisher_local(self, Ainv, S, scaling, fish, xi=None, theory=None, bm=None):
         """One realisation's Fisher rows for the local sightline, even l (pspec.py:334-352,

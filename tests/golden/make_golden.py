@@ -399,6 +399,36 @@ def pk_cov_theory(pb):
                 center=np.asarray(center), lc5=lc5, lf6=lf6, lt6=lt6, lc7=lc7)
 
 
+@case
+def bk_cov(pb):
+    """BSpec covariance contributions: 24^3, L=600, 4 bins, lmax=2, Pk_cov = [k, P0, P2].
+    Global sightline, CIC window: shell-sector mask with mask_shot = 0.5 mask (seed 2; the
+    caution printed for the shared shot mask), the same mask with mask_shot_2pt = 0.8 mask
+    (seed 3), constant mask 0.7 with [k, P0] (seed 4; mask_shot_2pt given, as the
+    reference needs one there).  Local sightline (box centred at (700, 400, 900) Mpc/h,
+    TSC window): shell-sector mask, mask_shot = 0.5 mask (seed 5)."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    kt = np.linspace(0.0, 1.0, 2000)
+    p0 = 3e3 * np.exp(-(kt / 0.25) ** 2) + 200.0
+    p2 = 800.0 * np.exp(-(kt / 0.2) ** 2)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="mkl")
+    bs = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask, mask_shot=0.5 * mask)
+    c2 = _quiet(bs.compute_covariance_contribution, 2, [kt, p0, p2])
+    c3 = _quiet(bs.compute_covariance_contribution, 3, [kt, p0, p2], mask_shot_2pt=0.8 * mask)
+    bs2 = _quiet(pb.BSpec, base, edges, lmax=2, mask=0.7 * np.ones((N, N, N)))
+    c4 = _quiet(bs2.compute_covariance_contribution, 4, [kt, p0], mask_shot_2pt=np.ones((N, N, N)))
+    center = [700.0, 400.0, 900.0]
+    lbase = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=center, sightline="local", pixel_window="tsc",
+                   backend="mkl")
+    lbs = _quiet(pb.BSpec, lbase, edges, lmax=2, mask=mask, mask_shot=0.5 * mask)
+    lc5 = _quiet(lbs.compute_covariance_contribution, 5, [kt, p0, p2])
+    return dict(N=N, L=L, edges=edges, pk_k=kt, p0=p0, p2=p2, bins=bs.all_bins, sym=bs.sym_factor, c2=c2, c3=c3,
+                c4=c4, center=np.asarray(center), lsym=lbs.sym_factor, lc5=lc5)
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

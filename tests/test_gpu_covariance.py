@@ -83,3 +83,25 @@ def test_covariance_theory_local(g):
     assert rel(ps2.compute_covariance_contribution(7, pk_cov[:2]), g["lc7"]) < TOL
     with pytest.raises(ValueError):
         ps2.compute_covariance_contribution(7, pk_cov)
+
+
+def test_bk_covariance():
+    """BSpec covariance contributions (lmax=2, tests/golden/bk_cov.npz): global sightline
+    with the bispectrum's shot mask and with a separate two-point one, constant mask, and
+    the local sightline."""
+    import polybin3d_b200 as pb
+    gb = np.load(os.path.join(GOLD, "bk_cov.npz"))
+    N, L = int(gb["N"]), float(gb["L"])
+    m = mask24(N, L)
+    pk_cov = [gb["pk_k"], gb["p0"], gb["p2"]]
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="cuda")
+    bs = quiet(pb.BSpec, b, gb["edges"], lmax=2, mask=m, mask_shot=0.5 * m)
+    assert np.array_equal(bs.all_bins, gb["bins"])
+    assert rel(quiet(bs.compute_covariance_contribution, 2, pk_cov), gb["c2"]) < TOL
+    assert rel(quiet(bs.compute_covariance_contribution, 3, pk_cov, mask_shot_2pt=0.8 * m), gb["c3"]) < TOL
+    bs2 = quiet(pb.BSpec, b, gb["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)))
+    assert rel(quiet(bs2.compute_covariance_contribution, 4, pk_cov[:2]), gb["c4"]) < TOL
+    lb = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="tsc", backend="cuda", boxcenter=list(gb["center"]),
+               sightline="local")
+    lbs = quiet(pb.BSpec, lb, gb["edges"], lmax=2, mask=m, mask_shot=0.5 * m)
+    assert rel(quiet(lbs.compute_covariance_contribution, 5, pk_cov), gb["lc5"]) < TOL

@@ -301,3 +301,25 @@ def test_pk_covariance_and_theory():
     assert rel(f, g["lf6"]) < TOL and rel(t, g["lt6"]) < TOL
     lps2 = O.OraclePSpec(lb, g["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)))
     assert rel(lps2.covariance_contribution(lb.reference_noise(7 + 10 ** 7), pk_cov[:2]), g["lc7"]) < TOL
+
+
+def test_bk_covariance():
+    """BSpec covariance contributions (lmax=2, Pk_cov with P0, P2): global sightline with the
+    shared and a separate two-point shot mask, constant mask, local sightline."""
+    g = gold("bk_cov")
+    N, L = int(g["N"]), float(g["L"])
+    m = mask24(N, L)
+    pk_cov = [g["pk_k"], g["p0"], g["p2"]]
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic")
+    bs = O.OracleBSpec(b, g["edges"], lmax=2, mask=m)
+    assert np.array_equal(bs.all_bins, g["bins"])
+    sym = g["sym"]
+    n = lambda s: (b.reference_noise(s + 10 ** 7), b.reference_noise(s + 2 * 10 ** 7))
+    assert rel(bs.covariance_contribution(*n(2), pk_cov, mask_shot_2pt=0.5 * m, sym=sym), g["c2"]) < TOL
+    assert rel(bs.covariance_contribution(*n(3), pk_cov, mask_shot_2pt=0.8 * m, sym=sym), g["c3"]) < TOL
+    bs2 = O.OracleBSpec(b, g["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)))
+    assert rel(bs2.covariance_contribution(*n(4), pk_cov[:2], sym=sym), g["c4"]) < TOL
+    lb = O.OracleBase([L] * 3, [N] * 3, pixel_window="tsc", boxcenter=g["center"], sightline="local")
+    lbs = O.OracleBSpec(lb, g["edges"], lmax=2, mask=m)
+    ln = (lb.reference_noise(5 + 10 ** 7), lb.reference_noise(5 + 2 * 10 ** 7))
+    assert rel(lbs.covariance_contribution(*ln, pk_cov, mask_shot_2pt=0.5 * m, sym=g["lsym"]), g["lc5"]) < TOL
