@@ -404,24 +404,68 @@ def apply_xi(b, X, x_real, xi, output):
     return PF + b.to_fourier(PR) if output == "fourier" else b.to_real(PF) + PR
 
 
-def cov_filter(b, x, real, xi, const_mask, mask_mean, mask, mask_shot):
+def cov_filter(b, x, real, xi, const_mask, mask_mean, point, mask_shot):
     """S^-1 [P xi P^dag + N] S^-dag x with the trivial S^-1 (pspec.py:277-290, 307-323;
     bspec.py:499-519); x is a real map if `real`, else a half spectrum; the output is a
-    half spectrum."""
+    half spectrum.  point(x, transpose): the pointing matrix P or P^dag."""
     if const_mask:
         Sid = b.to_fourier(x) if real else x
         return mask_mean ** 2 * apply_xi(b, Sid, None, xi, "fourier") + mask_mean * Sid
     Sid = x if real else b.to_real(x)
-    Pd_real = mask * Sid
+    Pd_real = point(Sid, True)
     C = apply_xi(b, b.to_fourier(Pd_real), Pd_real, xi, "real")
-    return b.to_fourier(mask * C + mask_shot * Sid)
+    return b.to_fourier(point(C, False) + mask_shot * Sid)
+
+
+class Pointing:
+    """The pointing matrix P of a varying mask (pspec.py:199-213, bspec.py:412-427): the mask,
+    or with an integral constraint the mask times the map less its mean over mask_IC,
+    globally (pointing_GIC, utils.pyx:405-424) or in radial shells of |r| (pointing_RIC,
+    utils.pyx:448-481; voxels outside every shell give 0).  The transpose subtracts
+    mask_IC times the mean of mask x map (utils.pyx:426-446, 483-516)."""
+
+    def __init__(self, mask, mask_IC=None, kind="mask", radial_edges=None, modr=None):
+        self.mask, self.mask_IC, self.kind = mask, mask_IC, kind
+        if kind == "RIC":
+            edges = np.asarray(radial_edges, dtype=np.float64)
+            self.zidx = np.full(modr.shape, -1, dtype=np.int64)
+            for iz in range(len(edges) - 1):
+                self.zidx[(modr >= edges[iz]) & (modr < edges[iz + 1])] = iz
+            self.nz = len(edges) - 1
+
+    def __call__(self, x, transpose=False):
+        if self.kind == "mask":
+            return self.mask * x
+        w = self.mask if transpose else self.mask_IC
+        if self.kind == "GIC":
+            av = np.sum(x * w) / np.sum(self.mask_IC)
+            return self.mask * x - self.mask_IC * av if transpose else self.mask * (x - av)
+        inz = self.zidx >= 0
+        num = np.bincount(self.zidx[inz], weights=(x * w)[inz], minlength=self.nz)
+        den = np.bincount(self.zidx[inz], weights=self.mask_IC[inz], minlength=self.nz)
+        av = np.zeros(x.shape)
+        av[inz] = (num / den)[self.zidx[inz]]
+        out = self.mask * x - self.mask_IC * av if transpose else self.mask * (x - av)
+        return np.where(inz, out, 0.0)
 
 
 # --------------------------------------------------------------------------------------
 # power spectrum (pspec.py)
 # --------------------------------------------------------------------------------------
+def _pointing_of(base, mask, mask_IC, add_GIC, add_RIC, radial_bins_RIC):
+    """pspec.py:101-111, bspec.py:126-136: the RIC shells use |r| of the voxel positions."""
+    if add_RIC:
+        assert not add_GIC, "Radial integral constraint imposes global integral constraint automatically!"
+        modr = np.sqrt(base.r_grids[0] ** 2 + base.r_grids[1] ** 2 + base.r_grids[2] ** 2)
+        return Pointing(mask, np.asarray(mask_IC, dtype=np.float64), "RIC", radial_bins_RIC, modr)
+    if add_GIC:
+        return Pointing(mask, np.asarray(mask_IC, dtype=np.float64), "GIC")
+    return Pointing(mask)
+
+
 class OraclePSpec:
-    def __init__(self, base, k_bins, lmax=2, mask=None):
+    def __init__(self, base, k_bins, lmax=2, mask=None, mask_IC=None, add_GIC=False, add_RIC=False,
+                 radial_bins_RIC=None):
         self.base = base
         self.k_bins = np.asarray(k_bins, dtype=np.float64)
         self.lmax = lmax
@@ -438,6 +482,7 @@ class OraclePSpec:
             else:
                 self.const_mask = False
             self.sq_mask_mean = np.mean(self.mask ** 2)
+            self.point = _pointing_of(base, self.mask, mask_IC, add_GIC, add_RIC, radial_bins_RIC)
 
     def numerator(self, data, filtering="ideal"):
         """_compute_pk_numerator, global sightline (pspec.py:613-686); trivial S^-1."""
@@ -504,7 +549,7 @@ class OraclePSpec:
 
     def cov_filter(self, x, real, xi, mask_shot):
         return cov_filter(self.base, x, real, xi, self.const_mask, getattr(self, "mask_mean", None),
-                          None if self.const_mask else self.mask, mask_shot)
+                          None if self.const_mask else self.point, mask_shot)
 
     def _contribution(self, noise_pair, xi=None, mask_shot=None, theory=None):
         """_compute_fisher, global and local (even l) sightlines (pspec.py:215-493)."""
@@ -519,14 +564,14 @@ class OraclePSpec:
                 return self.cov_filter(x, real, xi, mask_shot)
             if self.const_mask:
                 return self.mask_mean * (b.to_fourier(x) if real else x)
-            return b.to_fourier(self.mask * (x if real else b.to_real(x)))
+            return b.to_fourier(self.point(x if real else b.to_real(x), True))
 
         if xi is not None:                                               # 270-290, 330-332
             SinvP = dagger(a, False) if self.const_mask else dagger(a_real, True)
         elif self.const_mask:                                            # 273-276
             SinvP = self.mask_mean * a
         else:
-            SinvP = b.to_fourier(self.mask * a_real)
+            SinvP = b.to_fourier(self.point(a_real, False))
         fish = np.zeros((self.N_bins, self.N_bins))
         bm = None if theory is None else np.zeros((self.N_bins, theory[1] * (len(theory[0]) - 1)))
         scaling = 0.5 * b.volume / b.gridsize.prod() ** 2                # 390
@@ -653,7 +698,8 @@ def all_bins_list(k_bins, lmax, k_bins_squeeze=None, include_partial_triangles=F
 
 class OracleBSpec:
     def __init__(self, base, k_bins, lmax=0, mask=None, k_bins_squeeze=None,
-                 include_partial_triangles=False):
+                 include_partial_triangles=False, mask_IC=None, add_GIC=False, add_RIC=False,
+                 radial_bins_RIC=None):
         self.base = base
         self.k_bins = np.asarray(k_bins, dtype=np.float64)
         self.k_bins_squeeze = self.k_bins.copy() if k_bins_squeeze is None else np.asarray(k_bins_squeeze, dtype=np.float64)
@@ -674,6 +720,7 @@ class OracleBSpec:
             else:
                 self.const_mask = False
             self.cube_mask_mean = np.mean(self.mask ** 3)
+            self.point = _pointing_of(base, self.mask, mask_IC, add_GIC, add_RIC, radial_bins_RIC)
         # Pk_fid=None: unit weighting on k >= kF/10 grid (bspec.py:139-153)
         b = base
         k_tmp = np.arange(np.min(b.kF) / 10.0, np.max(b.kNy) * 2, np.min(b.kF) / 10.0)
@@ -816,7 +863,7 @@ class OracleBSpec:
         re, im = b.reference_noise(int(1e5) + ii)
         if self.const_mask:
             return self.sim_spectrum(self.mask_mean * b.grf_from_noise(re, im, Pk_grid), "fourier")
-        s = b.to_real(b.grf_from_noise(re, im, Pk_grid, include_pixel_window=False)) * self.mask
+        s = self.point(b.to_real(b.grf_from_noise(re, im, Pk_grid, include_pixel_window=False)))
         if b.pixel_window != "none":
             return self.sim_spectrum(b.to_fourier(s) * b.pixel_window_grid, "fourier")
         return self.sim_spectrum(s, "real")
@@ -905,10 +952,10 @@ class OracleBSpec:
             if xi is not None:
                 return cov_filter(b, x_fourier if self.const_mask else x_real, not self.const_mask, xi,
                                   self.const_mask, getattr(self, "mask_mean", None),
-                                  None if self.const_mask else self.mask, mask_shot)
+                                  None if self.const_mask else self.point, mask_shot)
             if self.const_mask:
                 return self.mask_mean * x_fourier
-            return b.to_fourier(self.mask * x_real)
+            return b.to_fourier(self.point(x_real))
 
         def g_sets(w1, w2):
             g1 = np.asarray([b.to_real(b.fourier_filter(w1, 0, ks[i], ks[i + 1])) for i in range(nks)])

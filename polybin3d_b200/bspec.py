@@ -13,6 +13,7 @@ from scipy.interpolate import interp1d
 
 from . import _native as nat
 from . import covariance
+from . import pointing
 from . import realisations
 from .harmonics import real_harmonics
 
@@ -125,8 +126,19 @@ class BSpec:
 
         if self.applySinv is not None:
             raise NotImplementedError("backend='cuda' implements the trivial S^-1 weighting (applySinv=None)")
-        if self.add_GIC or self.add_RIC:
-            raise NotImplementedError("backend='cuda' does not implement integral constraints")
+        # integral constraints (bspec.py:126-136)
+        if self.add_GIC:
+            if verb:
+                print("Accounting for global integral constraint")
+            assert hasattr(self, 'mask_IC'), "Need to supply mask_IC!"
+        if self.add_RIC:
+            assert not self.add_GIC, "Radial integral constraint imposes global integral constraint automatically!"
+            assert hasattr(self, 'mask_IC'), "Need to supply mask_IC!"
+            assert len(radial_bins_RIC) > 0, "Radial bins need to be supplied for radial integral constraint!"
+            if verb:
+                print("Accounting for radial integral constraint across %d bins" % (len(radial_bins_RIC) - 1))
+            self.radial_bins_RIC = np.asarray(radial_bins_RIC, dtype=np.float64)
+        self._pt = None
         self.applySinv = self.base.applySinv_trivial
         self.applySinv_transpose = self.base.applySinv_trivial
 
@@ -520,7 +532,7 @@ class BSpec:
             nat.spectral_filter(b.grid, F64, a, out, [(0, -1.0, np.inf, 0, 0, float(self.mask_mean), 0)])
             return out.to(b.complex_dtype)
         s = b.to_real(a)
-        nat.elementwise(nat.PB_EW_MUL, s, self._mask_device(), out=s, y_period=b.nreal)
+        self._pointing()(s, False, out=s)
         return b.to_fourier(s).to(b.complex_dtype)
 
     def _inv_window(self):
@@ -697,6 +709,14 @@ class BSpec:
     def _mask_device(self):
         return self.base.to_device_grid(('bk_mask', id(self)), lambda: self.mask, torch.float64)
 
+    def _pointing(self):
+        """The pointing matrix of the varying mask, with the integral constraint asked for."""
+        if self._pt is None:
+            kind = 'RIC' if self.add_RIC else ('GIC' if self.add_GIC else 'mask')
+            self._pt = pointing.Pointing(self.base, self._mask_device(), getattr(self, 'mask_IC', None), kind,
+                                         getattr(self, 'radial_bins_RIC', None))
+        return self._pt
+
     def _modes_of_shell(self, s):
         if self._shell_modes is None:
             b = self.base
@@ -707,14 +727,14 @@ class BSpec:
         return self._shell_modes[s]
 
     def _apply_filter_spectra(self, Q, prescaled):
-        """S^-1 P on a batch of half spectra: mask_mean * Q, or rfftn(mask * irfftn(Q)); in place.
+        """S^-1 P on a batch of half spectra: mask_mean * Q, or rfftn(P irfftn(Q)) with P the
+        mask's pointing matrix (bspec.py:499-505); in place.
         `prescaled`: Q already carries mask_mean (constant mask) or 1/N^3 (varying mask)."""
         b = self.base
         if self.const_mask:
             return Q
-        m = self._mask_device()
         qr = b.fft_c2r(Q)
-        nat.elementwise(nat.PB_EW_MUL, qr, m, out=qr, y_period=b.nreal)
+        self._pointing()(qr, False, out=qr)
         b.n_FFTs_reverse += Q.shape[0]
         b.n_FFTs_forward += Q.shape[0]
         return b.fft_r2c(qr, out=Q)
@@ -744,7 +764,7 @@ class BSpec:
         mean for the covariance form), 64 maps at a time; in place."""
         if xi is None:
             return self._apply_filter_spectra(R, True)
-        m = None if self.const_mask else self._mask_device()
+        m = None if self.const_mask else self._pointing()
         for c0 in range(0, R.shape[0], 64):
             covariance.cov_rows(self.base, R[c0:c0 + 64], xi, self.const_mask, getattr(self, "mask_mean", None), m,
                                 mask_shot)

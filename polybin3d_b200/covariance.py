@@ -8,7 +8,8 @@ harmonic transforms of its l > 0 multipoles; base.py:413-437), P the mask and N 
 mask.  With the trivial S^-1 this is, on a block of maps held as half spectra:
 
 * constant mask m: the diagonal weight m^2 xi(k) + m;
-* varying mask: mask x IFT[xi FT[mask x]] + mask_shot x, x the real-space map.
+* varying mask: P IFT[xi FT[P^dag x]] + mask_shot x, x the real-space map and P the mask
+  (with an integral constraint, its pointing matrix).
 
 Every step is a batched spectral filter, cuFFT transform or elementwise product on the
 device; the maps of a block go through each step together.
@@ -70,11 +71,12 @@ def xi_real(base, X, x_real, xi):
     return out
 
 
-def cov_rows(base, R, xi, const_mask, mask_mean, mask, mask_shot, real=None):
+def cov_rows(base, R, xi, const_mask, mask_mean, point, mask_shot, real=None):
     """R <- S^-1 [P xi P^dag + N] S^-dag of a block of maps, trivial S^-1 (pspec.py:277-290,
     307-323; bspec.py:499-519).  R (R, half) holds the half spectra, multiplied by 1/N^3
-    beforehand for a varying mask; `real` optional real-space maps added to them.  mask,
-    mask_shot: device grids (varying mask only).  Returns R."""
+    beforehand for a varying mask; `real` optional real-space maps added to them.  point:
+    the pointing matrix (`pointing.Pointing`: P, and P^dag with transpose=True), mask_shot
+    the device shot mask (varying mask only).  Returns R."""
     nrow = R.shape[0]
     if const_mask:
         if len(xi) > 1:
@@ -92,10 +94,10 @@ def cov_rows(base, R, xi, const_mask, mask_mean, mask, mask_shot, real=None):
     sid = base.fft_c2r(R)
     if real is not None:
         sid.add_(real)
-    t = nat.elementwise(nat.PB_EW_MUL, sid, mask, y_period=base.nreal)
+    t = point(sid, True)
     base.n_FFTs_forward += nrow
     u = xi_real(base, base.fft_r2c(t, out=R), t, xi)
-    nat.elementwise(nat.PB_EW_MUL, u, mask, out=u, y_period=base.nreal)
+    point(u, False, out=u)
     u.add_(nat.elementwise(nat.PB_EW_MUL, sid, mask_shot, out=t, y_period=base.nreal))
     base.n_FFTs_forward += nrow
     return base.fft_r2c(u, out=R)

@@ -10,6 +10,7 @@ import torch
 
 from . import _native as nat
 from . import covariance
+from . import pointing
 from . import realisations
 
 
@@ -75,8 +76,19 @@ class PSpec:
 
         if self.applySinv is not None:
             raise NotImplementedError("backend='cuda' implements the trivial S^-1 weighting (applySinv=None)")
-        if self.add_GIC or self.add_RIC:
-            raise NotImplementedError("backend='cuda' does not implement integral constraints")
+        # integral constraints (pspec.py:101-111)
+        if self.add_GIC:
+            if verb:
+                print("Accounting for global integral constraint")
+            assert hasattr(self, 'mask_IC'), "Need to supply mask_IC!"
+        if self.add_RIC:
+            assert not self.add_GIC, "Radial integral constraint imposes global integral constraint automatically!"
+            assert hasattr(self, 'mask_IC'), "Need to supply mask_IC!"
+            assert len(radial_bins_RIC) > 0, "Radial bins need to be supplied for radial integral constraint!"
+            if verb:
+                print("Accounting for radial integral constraint across %d bins" % (len(radial_bins_RIC) - 1))
+            self.radial_bins_RIC = np.asarray(radial_bins_RIC, dtype=np.float64)
+        self._pt = None
         self.applySinv = self.base.applySinv_trivial
         self.applySinv_transpose = self.base.applySinv_trivial
         self.Ylm_real = None
@@ -167,6 +179,14 @@ class PSpec:
     def _mask_device(self):
         return self.base.to_device_grid(('pk_mask', id(self)), lambda: self.mask, torch.float64)
 
+    def _pointing(self):
+        """The pointing matrix of the varying mask, with the integral constraint asked for."""
+        if self._pt is None:
+            kind = 'RIC' if self.add_RIC else ('GIC' if self.add_GIC else 'mask')
+            self._pt = pointing.Pointing(self.base, self._mask_device(), getattr(self, 'mask_IC', None), kind,
+                                         getattr(self, 'radial_bins_RIC', None))
+        return self._pt
+
     def _fisher_from_fields(self, a, xi=None, theory=None):
         """Fisher contributions of a batch of GRFs a (B, half) complex128 (pspec.py:215-493).
         xi: device grids of the covariance spectrum (covariance contributions: every S^-1 P
@@ -200,13 +220,12 @@ class PSpec:
             SinvP = a
             qscale = self.mask_mean * self.mask_mean
         else:
-            m = self._mask_device()
             ar = a.clone()
             nat.spectral_filter(grid, F64, ar, ar, [(i, -1.0, np.inf, 0, 0, invN, 0) for i in range(B)],
                                 src_stride=nh)
             ar = b.fft_c2r(ar)
             b.n_FFTs_reverse += B
-            nat.elementwise(nat.PB_EW_MUL, ar, m, out=ar, y_period=b.nreal)
+            self._pointing()(ar, False, out=ar)
             SinvP = b.fft_r2c(ar)
             b.n_FFTs_forward += B
             qscale = 1.0
@@ -229,7 +248,7 @@ class PSpec:
             elif not self.const_mask:
                 qr = b.fft_c2r(Q)
                 b.n_FFTs_reverse += self.N_bins
-                nat.elementwise(nat.PB_EW_MUL, qr, m, out=qr, y_period=b.nreal)
+                self._pointing()(qr, True, out=qr)
                 Q = b.fft_r2c(qr, out=Q)
                 b.n_FFTs_forward += self.N_bins
             nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, self.k_bins, self._ells(self.Nl),
@@ -246,7 +265,7 @@ class PSpec:
         ms = None if self.const_mask else self.base.to_device_grid(('pk_mask_shot', id(self)),
                                                                    lambda: self.mask_shot, torch.float64)
         return covariance.cov_rows(self.base, R, xi, self.const_mask, getattr(self, 'mask_mean', None),
-                                   None if self.const_mask else self._mask_device(), ms, real)
+                                   None if self.const_mask else self._pointing(), ms, real)
 
     def _fisher_local(self, Ainv, S, scaling, fish, xi=None, theory=None, bm=None):
         """One realisation's Fisher rows for the local sightline, even l (pspec.py:334-352,
@@ -263,7 +282,6 @@ class PSpec:
         invN = 1.0 / b.nreal
         harm = b.harmonics
         Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
-        m = None if self.const_mask else self._mask_device()
         mm = float(self.mask_mean) if self.const_mask else 1.0
 
         def dagger_rows(R, real=None):
@@ -281,7 +299,7 @@ class PSpec:
             b.n_FFTs_reverse += R.shape[0]
             if real is not None:
                 rr.add_(real)
-            nat.elementwise(nat.PB_EW_MUL, rr, m, out=rr, y_period=b.nreal)
+            self._pointing()(rr, True, out=rr)
             b.n_FFTs_forward += R.shape[0]
             return b.fft_r2c(rr, out=R)
 

@@ -429,6 +429,51 @@ def bk_cov(pb):
                 c4=c4, center=np.asarray(center), lsym=lbs.sym_factor, lc5=lc5)
 
 
+@case
+def integral_constraints(pb):
+    """Integral constraints in the Monte Carlo matrices: 24^3, L=600, 4 bins, CIC window,
+    shell-sector mask, mask_IC = (mask > 0).  Global sightline with the global constraint:
+    PSpec lmax=2 Fisher (seed 0), covariance with [k, P0, P2] and mask_shot = 0.5 mask
+    (seed 1), theory matrix lmax_theory = 4 (seed 2); BSpec lmax=2 Fisher (seed 0),
+    covariance (seed 1), Bk_numerator with the linear term from generate_sims(2) (lognormal
+    data seed 13).  Local sightline (box centred at (700, 400, 900) Mpc/h) with the radial
+    constraint in |r| shells [1300, 1360, 1410, 1450, 1700) Mpc/h (mask voxels below 1300
+    give 0): PSpec lmax=2 Fisher (seed 3), BSpec lmax=2 Fisher (seed 2)."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    mask_ic = (mask > 0).astype(np.float64)
+    kt = np.linspace(0.0, 1.0, 2000)
+    p0 = 3e3 * np.exp(-(kt / 0.25) ** 2) + 200.0
+    p2 = 800.0 * np.exp(-(kt / 0.2) ** 2)
+    kth = np.linspace(kF, 0.12, 7)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=2, mask=mask, mask_shot=0.5 * mask, add_GIC=True, mask_IC=mask_ic)
+    out = dict(N=N, L=L, edges=edges, pk_k=kt, p0=p0, p2=p2, kth=kth)
+    out["pf0"] = _quiet(ps.compute_fisher_contribution, 0)
+    out["pc1"] = _quiet(ps.compute_covariance_contribution, 1, [kt, p0, p2])
+    out["pf2"], out["pt2"] = _quiet(ps.compute_theory_contribution, 2, kth, lmax_theory=4)
+    bs = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask, mask_shot=0.5 * mask, add_GIC=True, mask_IC=mask_ic)
+    out["bf0"] = _quiet(bs.compute_fisher_contribution, 0)
+    out["bc1"] = _quiet(bs.compute_covariance_contribution, 1, [kt, p0, p2])
+    out["bins"], out["sym"] = bs.all_bins, bs.sym_factor
+    data = synthetic.lognormal(N, L, seed=13).astype(np.float64) * mask
+    _quiet(bs.generate_sims, 2)
+    out["bnum"] = _quiet(bs.Bk_numerator, data)
+    out["bcub"] = _quiet(bs.Bk_numerator, data, include_linear_term=False)
+    center = [700.0, 400.0, 900.0]
+    redges = np.array([1300.0, 1360.0, 1410.0, 1450.0, 1700.0])
+    lbase = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=center, sightline="local", pixel_window="cic",
+                   backend="mkl")
+    lps = _quiet(pb.PSpec, lbase, edges, lmax=2, mask=mask, add_RIC=True, mask_IC=mask_ic, radial_bins_RIC=redges)
+    out["lpf3"] = _quiet(lps.compute_fisher_contribution, 3)
+    lbs = _quiet(pb.BSpec, lbase, edges, lmax=2, mask=mask, add_RIC=True, mask_IC=mask_ic, radial_bins_RIC=redges)
+    out["lbf2"] = _quiet(lbs.compute_fisher_contribution, 2)
+    out.update(center=np.asarray(center), redges=redges, lsym=lbs.sym_factor)
+    return out
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

@@ -323,3 +323,36 @@ def test_bk_covariance():
     lbs = O.OracleBSpec(lb, g["edges"], lmax=2, mask=m)
     ln = (lb.reference_noise(5 + 10 ** 7), lb.reference_noise(5 + 2 * 10 ** 7))
     assert rel(lbs.covariance_contribution(*ln, pk_cov, mask_shot_2pt=0.5 * m, sym=g["lsym"]), g["lc5"]) < TOL
+
+
+def test_integral_constraints():
+    """Global (GIC) and radial (RIC) integral constraints in the pointing matrix of the Monte
+    Carlo Fisher, covariance and theory matrices and of the linear term's simulations."""
+    g = gold("integral_constraints")
+    N, L = int(g["N"]), float(g["L"])
+    m = mask24(N, L)
+    mic = (m > 0).astype(np.float64)
+    pk_cov = [g["pk_k"], g["p0"], g["p2"]]
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic")
+    ps = O.OraclePSpec(b, g["edges"], lmax=2, mask=m, mask_IC=mic, add_GIC=True)
+    assert rel(ps.fisher_contribution(b.reference_noise(10 ** 7)), g["pf0"]) < TOL
+    assert rel(ps.covariance_contribution(b.reference_noise(1 + 10 ** 7), pk_cov, mask_shot=0.5 * m), g["pc1"]) < TOL
+    f, t = ps.theory_contribution(b.reference_noise(2 + 10 ** 7), g["kth"], lmax_theory=4)
+    assert rel(f, g["pf2"]) < TOL and rel(t, g["pt2"]) < TOL
+    bs = O.OracleBSpec(b, g["edges"], lmax=2, mask=m, mask_IC=mic, add_GIC=True)
+    assert np.array_equal(bs.all_bins, g["bins"])
+    sym = g["sym"]
+    n = lambda s, bb: (bb.reference_noise(s + 10 ** 7), bb.reference_noise(s + 2 * 10 ** 7))
+    assert rel(bs.fisher_contribution(*n(0, b), sym=sym), g["bf0"]) < TOL
+    assert rel(bs.covariance_contribution(*n(1, b), pk_cov, mask_shot_2pt=0.5 * m, sym=sym), g["bc1"]) < TOL
+    d = synthetic.lognormal(N, L, seed=13).astype(np.float64) * m
+    sims = [bs.generated_sim(i) for i in range(2)]
+    num = bs.numerator(d, "Sinv", sym=sym, sims=sims)
+    cub = bs.numerator(d, "Sinv", sym=sym)
+    assert rel(num, g["bnum"]) < TOL and rel(cub, g["bcub"]) < TOL
+    assert rel(num - cub, g["bnum"] - g["bcub"]) < 1e-8
+    lb = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic", boxcenter=g["center"], sightline="local")
+    lps = O.OraclePSpec(lb, g["edges"], lmax=2, mask=m, mask_IC=mic, add_RIC=True, radial_bins_RIC=g["redges"])
+    assert rel(lps.fisher_contribution(lb.reference_noise(3 + 10 ** 7)), g["lpf3"]) < TOL
+    lbs = O.OracleBSpec(lb, g["edges"], lmax=2, mask=m, mask_IC=mic, add_RIC=True, radial_bins_RIC=g["redges"])
+    assert rel(lbs.fisher_contribution(*n(2, lb), sym=g["lsym"]), g["lbf2"]) < TOL
