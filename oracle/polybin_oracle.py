@@ -117,7 +117,8 @@ def legendre(l, mu):
 
 
 def real_harmonics_fourier(k_grids, lmax):
-    """Real spherical harmonics of the unit k-vector, l = 2, 4 (utils.pyx:518-609, even l)."""
+    """Real spherical harmonics of the unit vector, l = 1..4 (utils.pyx:518-609); the odd l
+    are the reference's odd_l set."""
     kx, ky, kz = k_grids
     norm = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
     safe = np.where(norm == 0, 1.0, norm)
@@ -125,6 +126,17 @@ def real_harmonics_fourier(k_grids, lmax):
     yh = np.where(norm == 0, 0.0, ky / safe)
     zh = np.where(norm == 0, 0.0, kz / safe)
     out = {}
+    if lmax >= 1:
+        out[1] = np.asarray([yh, zh, xh])
+    if lmax >= 3:
+        out[3] = np.asarray([
+            (45.0 * xh ** 2 * yh - 15.0 * yh ** 3) * np.sqrt(1.0 / 360.0),
+            (30.0 * xh * yh * zh) * np.sqrt(1.0 / 60.0),
+            (-1.5 * xh ** 2 * yh - 1.5 * yh ** 3 + 6.0 * yh * zh ** 2) * np.sqrt(1.0 / 6.0),
+            (-1.5 * xh ** 2 * zh - 1.5 * yh ** 2 * zh + zh ** 3),
+            (-1.5 * xh ** 3 - 1.5 * xh * yh ** 2 + 6.0 * xh * zh ** 2) * np.sqrt(1.0 / 6.0),
+            (15.0 * xh ** 2 * zh - 15.0 * yh ** 2 * zh) * np.sqrt(1.0 / 60.0),
+            (15.0 * xh ** 3 - 45.0 * xh * yh ** 2) * np.sqrt(1.0 / 360.0)])
     if lmax >= 2:
         out[2] = np.asarray([
             6.0 * xh * yh * np.sqrt(1.0 / 12.0),
@@ -465,12 +477,14 @@ def _pointing_of(base, mask, mask_IC, add_GIC, add_RIC, radial_bins_RIC):
 
 class OraclePSpec:
     def __init__(self, base, k_bins, lmax=2, mask=None, mask_IC=None, add_GIC=False, add_RIC=False,
-                 radial_bins_RIC=None):
+                 radial_bins_RIC=None, odd_l=False):
         self.base = base
         self.k_bins = np.asarray(k_bins, dtype=np.float64)
         self.lmax = lmax
+        self.odd_l = odd_l
         self.Nk = len(k_bins) - 1
-        self.Nl = lmax // 2 + 1                                      # pspec.py:38 (odd_l=False)
+        self.Nl = lmax + 1 if odd_l else lmax // 2 + 1               # pspec.py:37-39
+        self.Nl_even = lmax // 2 + 1
         self.N_bins = self.Nk * self.Nl
         if mask is None:                                             # pspec.py:62-81
             self.const_mask, self.mask_mean, self.sq_mask_mean = True, 1.0, 1.0
@@ -484,8 +498,14 @@ class OraclePSpec:
             self.sq_mask_mean = np.mean(self.mask ** 2)
             self.point = _pointing_of(base, self.mask, mask_IC, add_GIC, add_RIC, radial_bins_RIC)
 
+    def ell(self, li):
+        """Multipole of block li: 2 li, or li with odd_l (pspec.py:667)."""
+        return li * (2 - self.odd_l)
+
     def numerator(self, data, filtering="ideal"):
-        """_compute_pk_numerator, global sightline (pspec.py:613-686); trivial S^-1."""
+        """_compute_pk_numerator (pspec.py:613-686); trivial S^-1.  The ideal numerator has
+        the even multipoles only; with odd_l the S^-1 one has l = 0..lmax, the odd blocks
+        crossed with -i H_l[x] so that they are real (pspec.py:674-676)."""
         b = self.base
         data = np.asarray(data, dtype=np.float64)
         x = b.to_fourier(data)
@@ -493,34 +513,40 @@ class OraclePSpec:
             x = b.div_fourier(x, b.pixel_window_grid)
         if filtering == "ideal":
             x = x * b.invPk0_grid / np.sqrt(self.sq_mask_mean)
-        out = np.zeros(self.N_bins)
-        for li in range(self.Nl):
+        Nl = self.Nl if filtering != "ideal" else self.Nl_even
+        odd = self.odd_l and filtering != "ideal"
+        out = np.zeros(Nl * self.Nk)
+        for li in range(Nl):
+            l = li * (2 - odd)
             if b.sightline == "global" or li == 0:
-                out[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.integrate(x, self.k_bins, 2 * li)
+                out[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.integrate(x, self.k_bins, l)
             else:                                                        # pspec.py:672-680
-                lm = b.apply_fourier_harmonics(b.to_real(x), 2 * li)
+                lm = b.apply_fourier_harmonics(b.to_real(x), l)
+                if l % 2 == 1:
+                    lm = -1.0j * lm
                 out[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(x, lm, self.k_bins, 0)
         return out * b.volume / b.gridsize.prod() ** 2
 
     def fisher_ideal(self, discreteness_correction=True):
         """compute_fisher_ideal with the base fiducial spectrum (pspec.py:702-752)."""
         b = self.base
-        fish = np.zeros((self.N_bins, self.N_bins))
+        nb = self.Nl_even * self.Nk
+        fish = np.zeros((nb, nb))
         if discreteness_correction:
-            for la in range(self.Nl):
-                for lb in range(self.Nl):
+            for la in range(self.Nl_even):
+                for lb in range(self.Nl_even):
                     fish[la * self.Nk:(la + 1) * self.Nk, lb * self.Nk:(lb + 1) * self.Nk] = np.diag(
                         0.5 * b.real_integrate_double(b.invPk0_grid, 2 * la, 2 * lb, self.k_bins))
         else:
             d = 0.5 * b.real_integrate_double(b.invPk0_grid, 0, 0, self.k_bins)
-            for la in range(self.Nl):
+            for la in range(self.Nl_even):
                 fish[la * self.Nk:(la + 1) * self.Nk, la * self.Nk:(la + 1) * self.Nk] = np.diag(d) / (4.0 * la + 1.0)
         return fish
 
     def Pk_ideal(self, data, fish=None):
         fish = self.fisher_ideal() if fish is None else fish
         out = np.linalg.inv(fish) @ self.numerator(data, "ideal")      # pspec.py:775
-        return {"p%d" % (2 * li): out[li * self.Nk:(li + 1) * self.Nk] for li in range(self.Nl)}
+        return {"p%d" % (2 * li): out[li * self.Nk:(li + 1) * self.Nk] for li in range(self.Nl_even)}
 
     def fisher_contribution(self, noise_pair):
         """_compute_fisher, no covariance, no theory, trivial S^-1 (pspec.py:215-493)."""
@@ -535,14 +561,17 @@ class OraclePSpec:
         assert (len(Pk_cov) - 2) * 2 <= self.lmax
         return self._contribution(noise_pair, xi=self.xi_grids(Pk_cov), mask_shot=mask_shot)
 
-    def theory_contribution(self, noise_pair, k_bins_theory, lmax_theory=None):
-        """compute_theory_contribution without wide-angle terms (pspec.py:164-196): the
-        Fisher contribution and the rectangular binning matrix whose column block l_t holds
-        the cross integrals of each Q-map with A^-1 a (global: weighted by L_l_t(mu); local:
-        with sum_m Y_lm(k) FT[Y_lm(r) A^-1 a]) in the theory k-bins."""
+    def theory_contribution(self, noise_pair, k_bins_theory, lmax_theory=None, include_wideangle=False):
+        """compute_theory_contribution (pspec.py:164-196): the Fisher contribution and the
+        rectangular binning matrix whose column block l_t holds the cross integrals of each
+        Q-map with A^-1 a (global: weighted by L_l_t(mu); local: with
+        sum_m Y_lm(k) FT[Y_lm(r) A^-1 a]) in the theory k-bins; with include_wideangle the
+        odd-l terms of A^-1 a / |r| add to the l = 2, 4 blocks (pspec.py:424-438)."""
         k_th = np.asarray(k_bins_theory, dtype=np.float64)
         lt = self.lmax if lmax_theory is None else lmax_theory
-        return self._contribution(noise_pair, theory=(k_th, lt // 2 + 1))
+        odd_t = True if include_wideangle else self.odd_l
+        nlt = lt + 1 if (odd_t and not include_wideangle) else lt // 2 + 1     # pspec.py:222-228
+        return self._contribution(noise_pair, theory=(k_th, nlt, lt, include_wideangle, odd_t))
 
     def xi_grids(self, Pk_cov):
         return xi_grids(self.base, Pk_cov)
@@ -586,58 +615,113 @@ class OraclePSpec:
                     fish[row, lp * self.Nk:(lp + 1) * self.Nk] += scaling * b.cross_integrate(
                         Ainv, Q, self.k_bins, 2 * lp)
                 if theory is not None:                                   # 395-402
-                    kt, nlt = theory
+                    kt, nlt = theory[:2]
                     nkt = len(kt) - 1
                     for lt in range(nlt):
                         bm[row, lt * nkt:(lt + 1) * nkt] += scaling * b.cross_integrate(Ainv, Q, kt, 2 * lt)
         return fish if theory is None else (fish, bm)
 
+    @staticmethod
+    def derivative_coefficient(k):
+        """Coefficients of the numerical k dP/dk in the theory bins (pspec.py:368-378)."""
+        nk = len(k) - 1
+        kfac = np.zeros(nk)
+        for ki in range(nk):
+            if 0 < ki - 1 < nk - 1:
+                kfac[ki] += k[ki - 1] / (k[ki] - k[ki - 2])
+            if 0 < ki + 1 < nk - 1:
+                kfac[ki] -= k[ki + 1] / (k[ki + 2] - k[ki])
+            kfac[ki] += k[0] / (k[1] - k[0]) * ((ki == 1) - (ki == 0))
+            kfac[ki] -= k[-1] / (k[-1] - k[-2]) * ((ki == nk - 1) - (ki == nk - 2))
+        return kfac
+
     def _fisher_local(self, Ainv, SinvP, scaling, dagger, fish, theory=None, bm=None):
-        """_compute_fisher, local sightline, even l (pspec.py:334-352, 380-407, 440-486).
+        """_compute_fisher, local sightline (pspec.py:334-366, 380-438, 456-486).
         Monopole rows Q = D Theta_b SinvP; multipole rows
         Q = 1/2 D Theta_b H_l[SinvP] + 1/2 D sum_m Y_lm(r) IFT[Theta_b Y_lm(k) SinvP]
-        with D = (S^-1 P)^dag (or its covariance form) and H_l[x] = sum_m Y_lm(k) FT[Y_lm(r)
-        IFT x]; the row against column block l is the cross integral of Q with A^-1 a
-        (l = 0) or with H_l[A^-1 a], in the data bins and, for the theory matrix, the theory
-        bins."""
+        (odd l: both parts times -i) with D = (S^-1 P)^dag (or its covariance form) and
+        H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x]; the row against column block l is the
+        cross integral of Q (odd l: i Q) with A^-1 a (l = 0) or with H_l[A^-1 a], in the data
+        bins and, for the theory matrix, the theory bins.  Wide-angle theory terms: the odd
+        l maps H_l[A^-1 a / |r|] enter the l = 2, 4 blocks with the complex per-bin
+        coefficients of pspec.py:424-438."""
         b = self.base
-        nl_leg = self.Nl if theory is None else theory[1]
-        if theory is not None:
-            assert theory[1] >= self.Nl, "Can't use larger lmax for data than for theory!"
         A_real = b.to_real(Ainv)
-        legA = {2 * li: b.apply_fourier_harmonics(A_real, 2 * li) for li in range(1, nl_leg)}
+        legA = {}
+
+        def leg(l, src="A"):
+            key = (l, src)
+            if key not in legA:
+                if src == "A":
+                    x = A_real
+                else:                                                    # div_real, utils.pyx:265-278
+                    r = np.sqrt(b.r_grids[0] ** 2 + b.r_grids[1] ** 2 + b.r_grids[2] ** 2)
+                    x = np.where(r != 0, A_real / np.where(r != 0, r, 1.0), 0.0)
+                legA[key] = b.apply_fourier_harmonics(x, l)
+            return legA[key]
+
         SinvP_real = b.to_real(SinvP)
 
-        def add(row, Q):                                                 # 380-430
+        def add(row, Q):                                                 # 380-438
             fish[row, :self.Nk] += scaling * b.cross_integrate(Ainv, Q, self.k_bins, 0)
             for li in range(1, self.Nl):
-                fish[row, li * self.Nk:(li + 1) * self.Nk] += scaling * b.cross_integrate(legA[2 * li], Q,
-                                                                                          self.k_bins, 0)
-            if theory is not None:
-                kt, nlt = theory
-                nkt = len(kt) - 1
-                bm[row, :nkt] += scaling * b.cross_integrate(Ainv, Q, kt, 0)
+                l = self.ell(li)
+                fish[row, li * self.Nk:(li + 1) * self.Nk] += scaling * b.cross_integrate(
+                    leg(l), 1.0j * Q if l % 2 else Q, self.k_bins, 0)
+            if theory is None:
+                return
+            kt, nlt, lt, wide, odd_t = theory
+            nkt = len(kt) - 1
+            bm[row, :nkt] += scaling * b.cross_integrate(Ainv, Q, kt, 0)
+            if not wide:
                 for li in range(1, nlt):
-                    bm[row, li * nkt:(li + 1) * nkt] += scaling * b.cross_integrate(legA[2 * li], Q, kt, 0)
+                    l = li * (2 - odd_t)
+                    bm[row, li * nkt:(li + 1) * nkt] += scaling * b.cross_integrate(
+                        leg(l), 1.0j * Q if l % 2 else Q, kt, 0)
+                return
+            kfac = self.derivative_coefficient(kt)
+            for l in range(1, lt + 1):
+                if l % 2 == 0:
+                    bm[row, l // 2 * nkt:(l // 2 + 1) * nkt] += scaling * b.cross_integrate(leg(l), Q, kt, 0)
+                    continue
+                terms = []
+                if l == 1 and lt >= 2:
+                    terms.append((1, 3.0j / 5.0 * (3 + kfac)))
+                if l == 3 and lt >= 2:
+                    terms.append((1, 3.0j / 5.0 * (2 - kfac)))
+                if l == 3 and lt >= 4:
+                    terms.append((2, 10.0j / 9.0 * (5 + kfac)))
+                for blk, coeff in terms:                                 # utils.pyx:139-157
+                    bm[row, blk * nkt:(blk + 1) * nkt] += scaling * self.cross_wcoeff(coeff, leg(l, "A/r"), Q, kt)
 
         for ki in range(self.Nk):                                        # 442-445
             add(ki, dagger(b.fourier_filter(SinvP, 0, self.k_bins[ki], self.k_bins[ki + 1]), False))
         for li in range(1, self.Nl):                                     # 456-486
-            l = 2 * li
-            leg = b.apply_fourier_harmonics(SinvP_real, l)
+            l = self.ell(li)
+            ph = -1.0j if l % 2 else 1.0
+            lg = b.apply_fourier_harmonics(SinvP_real, l)
             yr = real_harmonics_fourier(b.r_grids, l)[l]
             yk = real_harmonics_fourier(b.k_grids, l)[l]
             for ki in range(self.Nk):
-                Q = 0.5 * dagger(b.fourier_filter(leg, 0, self.k_bins[ki], self.k_bins[ki + 1]), False)
+                Q = 0.5 * dagger(ph * b.fourier_filter(lg, 0, self.k_bins[ki], self.k_bins[ki + 1]), False)
                 real_map = np.zeros(tuple(b.gridsize))
                 m = b.in_bin(self.k_bins[ki], self.k_bins[ki + 1])
                 for mi in range(len(yr)):
                     km = np.zeros(b.modk_grid.shape, dtype=np.complex128)
                     km[m] = SinvP[m] * yk[mi][m]
-                    real_map += b.to_real(km) * yr[mi]
+                    real_map += b.to_real(ph * km) * yr[mi]
                 Q = Q + 0.5 * dagger(real_map, True)
                 add(li * self.Nk + ki, Q)
         return fish
+
+    def cross_wcoeff(self, coeff, s1, s2, k_edges):
+        """cross_integrate_wcoeff (utils.pyx:139-157): sum deg Re(c_b s1 conj(s2)) per bin."""
+        b = self.base
+        out = np.zeros(len(k_edges) - 1)
+        for i in range(len(out)):
+            m = b.in_bin(k_edges[i], k_edges[i + 1])
+            out[i] = np.sum(b.degeneracy_factor[m] * (coeff[i] * s1[m] * np.conj(s2[m])).real)
+        return out
 
     def shot_contribution(self, noise_pair, mask_shot=None):
         """compute_shot_contribution, global sightline (pspec.py:495-549): a = GRF of
@@ -655,7 +739,10 @@ class OraclePSpec:
             if b.sightline == "global" or li == 0:
                 shot[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(a, sna, self.k_bins, 2 * li)
             else:                                                        # 535-544
-                lm = b.apply_fourier_harmonics(b.to_real(a), 2 * li)
+                l = self.ell(li)
+                lm = b.apply_fourier_harmonics(b.to_real(a), l)
+                if l % 2:
+                    lm = -1.0j * lm
                 shot[li * self.Nk:(li + 1) * self.Nk] = 0.5 * b.cross_integrate(lm, sna, self.k_bins, 0)
         return shot * b.volume / b.gridsize.prod() ** 2
 

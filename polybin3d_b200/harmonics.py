@@ -14,13 +14,23 @@ from . import _native as nat
 
 
 def real_harmonics(k_grids, l):
-    """Real spherical harmonics of the unit vector for even l = 2, 4; the same functions and
-    normalisation as compute_real_harmonics (PolyBin3D/cython/utils.pyx:518-609), so that
-    sum_m Y_lm(k) Y_lm(k') = L_l(k.k')."""
+    """Real spherical harmonics of the unit vector for l = 1..4 (odd l: the odd_l set); the
+    same functions and normalisation as compute_real_harmonics
+    (PolyBin3D/cython/utils.pyx:518-609), so that sum_m Y_lm(k) Y_lm(k') = L_l(k.k')."""
     kx, ky, kz = k_grids
     norm = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
     safe = np.where(norm == 0, 1.0, norm)
     xh, yh, zh = [np.where(norm == 0, 0.0, c / safe) for c in (kx, ky, kz)]
+    if l == 1:
+        return [yh, zh, xh]
+    if l == 3:
+        return [(45. * xh ** 2 * yh - 15. * yh ** 3) * np.sqrt(1. / 360.),
+                (30. * xh * yh * zh) * np.sqrt(1. / 60.),
+                (-1.5 * xh ** 2 * yh - 1.5 * yh ** 3 + 6. * yh * zh ** 2) * np.sqrt(1. / 6.),
+                (-1.5 * xh ** 2 * zh - 1.5 * yh ** 2 * zh + zh ** 3),
+                (-1.5 * xh ** 3 - 1.5 * xh * yh ** 2 + 6. * xh * zh ** 2) * np.sqrt(1. / 6.),
+                (15. * xh ** 2 * zh - 15. * yh ** 2 * zh) * np.sqrt(1. / 60.),
+                (15. * xh ** 3 - 45. * xh * yh ** 2) * np.sqrt(1. / 360.)]
     if l == 2:
         return [6.0 * xh * yh * np.sqrt(1.0 / 12.0),
                 3.0 * yh * zh * np.sqrt(1.0 / 3.0),
@@ -38,11 +48,11 @@ def real_harmonics(k_grids, l):
                 (-7.5 * x2 * x2 + 45.0 * x2 * z2 + 7.5 * y2 * y2 - 45.0 * y2 * z2) * np.sqrt(1.0 / 180.0),
                 (105.0 * x2 * xh * zh - 315.0 * xh * y2 * zh) * np.sqrt(1.0 / 2520.0),
                 (105.0 * x2 * x2 - 630.0 * x2 * y2 + 105.0 * y2 * y2) * np.sqrt(1.0 / 20160.0)]
-    raise ValueError("l must be 2 or 4")
+    raise ValueError("l must be 1, 2, 3 or 4")
 
 
 class Harmonics:
-    """Device harmonic grids of one box for the even multipoles 2..lmax, and their use."""
+    """Device harmonic grids of one box for the multipoles 1..4, and their use."""
 
     def __init__(self, base):
         self.base = base

@@ -143,7 +143,7 @@ class PSpec:
         return w
 
     def _compute_pk_numerator(self, data, filtering='ideal'):
-        """Numerator, global sightline (pspec.py:613-686)."""
+        """Numerator (pspec.py:613-686): the ideal one has the even multipoles only."""
         assert filtering in ['ideal', 'Sinv'], "Unknown filtering option supplied!"
         b = self.base
         xk, s2 = self._weighted_spectrum(data, filtering)
@@ -155,14 +155,17 @@ class PSpec:
             nat.bin_reduce(b.grid, prec, nat.PB_RED_ABS2, xk, None, 1, self.k_bins, self._ells(Nl), scale, out, b.ws)
             return out.cpu().numpy()
         # local sightline (pspec.py:643-680): the monopole as above; multipole l is the
-        # binned cross spectrum of x with sum_m Y_lm(k) FT[Y_lm(r) x(r)]
-        if self.odd_l:
-            raise NotImplementedError("backend='cuda' implements even multipoles for the local sightline")
+        # binned cross spectrum of x with sum_m Y_lm(k) FT[Y_lm(r) x(r)], times -i for odd l
+        # (odd_l, S^-1 numerator only) so that it is real
+        odd = self.odd_l and filtering == 'Sinv'
         Nk = self.Nk
         nat.bin_reduce(b.grid, prec, nat.PB_RED_ABS2, xk, None, 1, self.k_bins, [(0, 0)], scale, out[:Nk], b.ws)
         x_real = b.to_real(xk)
         for li in range(1, Nl):
-            lm = b.harmonics.apply_fourier(x_real, 2 * li)
+            l = li * (2 - odd)
+            lm = b.harmonics.apply_fourier(x_real, l)
+            if l % 2:
+                lm = lm * (-1j)
             nat.bin_reduce(b.grid, prec, nat.PB_RED_CROSS, xk, lm, 1, self.k_bins, [(0, 0)], scale,
                            out[li * Nk:(li + 1) * Nk], b.ws)
         return out.cpu().numpy()
@@ -193,8 +196,6 @@ class PSpec:
         becomes S^-1 [P xi P^dag + N] S^-dag); theory: (k_bins_theory, Nl_theory), which adds
         the binning matrix of each realisation, (B, N_bins, Nl_theory * Nk_theory)."""
         b = self.base
-        if b.sightline == 'local' and self.lmax > 0 and self.odd_l:
-            raise NotImplementedError("backend='cuda' implements even multipoles for the local sightline")
         B = a.shape[0]
         nh = b.nhalf
         grid = b.grid
@@ -206,8 +207,8 @@ class PSpec:
                             src_stride=nh)
         bm = None
         if theory is not None:
-            k_th, nl_th = theory
-            bm = torch.empty((B, self.N_bins, nl_th * (len(k_th) - 1)), dtype=torch.float64, device=b.device)
+            k_th, nl_th = theory[:2]
+            bm = torch.zeros((B, self.N_bins, nl_th * (len(k_th) - 1)), dtype=torch.float64, device=b.device)
         if xi is not None:
             # S^-1 P a -> S^-1 [P xi P^dag + N] S^-dag a (pspec.py:270-290, 330-332)
             SinvP = a.clone()
@@ -268,15 +269,17 @@ class PSpec:
                                    None if self.const_mask else self._pointing(), ms, real)
 
     def _fisher_local(self, Ainv, S, scaling, fish, xi=None, theory=None, bm=None):
-        """One realisation's Fisher rows for the local sightline, even l (pspec.py:334-352,
-        380-407, 440-486).  With H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x] and D = (S^-1 P)^dag:
+        """One realisation's Fisher rows for the local sightline (pspec.py:334-366, 380-438,
+        440-486).  With H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x] and D = (S^-1 P)^dag:
         monopole rows Q = D Theta_b S; multipole rows
-        Q = 1/2 D Theta_b H_l[S] + 1/2 D sum_m Y_lm(r) IFT[Theta_b Y_lm(k) S]; column block 0 is
-        the binned cross spectrum of Q with A^-1 a, block l the one with H_l[A^-1 a].  All
-        rows of a multipole go through each step as one batch.  With xi, D is the covariance
-        form S^-1 [P xi P^dag + N] S^-dag; with theory = (k_bins_theory, Nl_theory) the
-        binning matrix bm gets the same cross spectra in the theory bins for multipoles
-        0..2(Nl_theory - 1) (pspec.py:395-423)."""
+        Q = 1/2 D Theta_b H_l[S] + 1/2 D sum_m Y_lm(r) IFT[Theta_b Y_lm(k) S], both parts
+        times -i for odd l (odd_l); column block 0 is the binned cross spectrum of Q with
+        A^-1 a, block l the one of i Q (odd l) or Q with H_l[A^-1 a].  All rows of a
+        multipole go through each step as one batch.  With xi, D is the covariance form
+        S^-1 [P xi P^dag + N] S^-dag.  theory = (k_bins_theory, Nl_theory, lmax_theory,
+        wide-angle, odd multipoles): the binning matrix bm gets the same cross spectra in the
+        theory bins; with the wide-angle terms the odd-l maps H_l[A^-1 a / |r|] add to the
+        l = 2, 4 blocks with the per-bin coefficients of pspec.py:424-438."""
         b = self.base
         grid, F64, Nk = b.grid, nat.PB_F64, self.Nk
         invN = 1.0 / b.nreal
@@ -309,10 +312,12 @@ class PSpec:
         dagger_rows(Q[:Nk])
         S_real = b.to_real(S)
         for li in range(1, self.Nl):
-            l = 2 * li
+            l = li * (2 - self.odd_l)
             R = Q[li * Nk:(li + 1) * Nk]
             nat.spectral_filter(grid, F64, harm.apply_fourier(S_real, l), R,
                                 [(0, lo, hi, 0, 0, 0.5 * sc, 0) for (_, lo, hi, _, _, sc, _) in bands])
+            if l % 2:
+                R.mul_(-1j)
             yr = harm._grid('r', l, torch.float64)
             yk = harm._grid('k', l, torch.float64)
             real_map = torch.zeros((Nk,) + tuple(int(n) for n in b.gridsize), dtype=torch.float64, device=b.device)
@@ -320,32 +325,81 @@ class PSpec:
             for mi in range(yr.shape[0]):
                 nat.spectral_filter(grid, F64, S, T, [(0, lo, hi, 0, 0, 0.5 * invN, 1) for (_, lo, hi, _, _, _, _) in bands],
                                     w=yk[mi])
+                if l % 2:
+                    T.mul_(-1j)
                 t = b.fft_c2r(T)
                 b.n_FFTs_reverse += Nk
                 real_map.addcmul_(t, yr[mi])
             dagger_rows(R, real_map)
-        tmp = torch.empty((self.N_bins, Nk), dtype=torch.float64, device=b.device)
-        nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv, Q, self.N_bins, self.k_bins, [(0, 0)], scaling, tmp, b.ws)
-        fish[:, :Nk] = tmp
-        nl_th = 0 if theory is None else theory[1]
-        if theory is not None:
-            k_th = theory[0]
-            nkt = len(k_th) - 1
-            tth = torch.empty((self.N_bins, nkt), dtype=torch.float64, device=b.device)
-            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv, Q, self.N_bins, k_th, [(0, 0)], scaling, tth, b.ws)
-            bm[:, :nkt] = tth
-        A_real = b.to_real(Ainv) if max(self.Nl, nl_th) > 1 else None
-        for li in range(1, max(self.Nl, nl_th)):
-            legA = harm.apply_fourier(A_real, 2 * li)
-            if li < self.Nl:
-                nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, legA, Q, self.N_bins, self.k_bins, [(0, 0)], scaling,
-                               tmp, b.ws)
-                fish[:, li * Nk:(li + 1) * Nk] = tmp
-            if li < nl_th:
-                nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, legA, Q, self.N_bins, k_th, [(0, 0)], scaling, tth,
-                               b.ws)
-                bm[:, li * nkt:(li + 1) * nkt] = tth
+        leg_cache = {}
+        A_real = b.to_real(Ainv) if (self.Nl > 1 or theory is not None) else None
+
+        def leg(l, over_r=False):
+            """H_l[A^-1 a] (or of A^-1 a / |r|), times -i for odd l: its cross spectrum with Q
+            is the one of H_l with i Q (pspec.py:409-413, 418-421)."""
+            key = (l, over_r)
+            if key not in leg_cache:
+                x = A_real
+                if over_r:                                               # div_real (utils.pyx:265-278)
+                    r = b.to_device_grid('modr', lambda: np.sqrt(b.r_grids[0] ** 2. + b.r_grids[1] ** 2.
+                                                                 + b.r_grids[2] ** 2.), torch.float64)
+                    x = torch.where(r != 0, A_real / torch.where(r != 0, r, torch.ones_like(r)),
+                                    torch.zeros_like(r))
+                h = harm.apply_fourier(x, l)
+                leg_cache[key] = h * (-1j) if l % 2 else h
+            return leg_cache[key]
+
+        def cross(a, edges):
+            out = torch.empty((self.N_bins, len(edges) - 1), dtype=torch.float64, device=b.device)
+            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, a, Q, self.N_bins, edges, [(0, 0)], scaling, out, b.ws)
+            return out
+
+        fish[:, :Nk] = cross(Ainv, self.k_bins)
+        for li in range(1, self.Nl):
+            fish[:, li * Nk:(li + 1) * Nk] = cross(leg(li * (2 - self.odd_l)), self.k_bins)
+        if theory is None:
+            return fish
+        k_th, nl_th, lmax_th, wide, odd_t = theory
+        nkt = len(k_th) - 1
+        bm.zero_()
+        bm[:, :nkt] = cross(Ainv, k_th)
+        if not wide:
+            for li in range(1, nl_th):
+                bm[:, li * nkt:(li + 1) * nkt] = cross(leg(li * (2 - odd_t)), k_th)
+            return fish
+        # wide-angle terms (pspec.py:424-438): even l as usual; odd l from A^-1 a / |r| with
+        # coefficient i alpha_b per theory bin, Re(i alpha s1 s2*) = alpha Re((i s1) s2*)
+        kfac = torch.as_tensor(self.derivative_coefficient(k_th), device=b.device)
+        for l in range(1, lmax_th + 1):
+            if l % 2 == 0:
+                bm[:, l // 2 * nkt:(l // 2 + 1) * nkt] += cross(leg(l), k_th)
+                continue
+            terms = []
+            if l == 1 and lmax_th >= 2:
+                terms.append((1, 3.0 / 5.0 * (3 + kfac)))
+            if l == 3 and lmax_th >= 2:
+                terms.append((1, 3.0 / 5.0 * (2 - kfac)))
+            if l == 3 and lmax_th >= 4:
+                terms.append((2, 10.0 / 9.0 * (5 + kfac)))
+            if terms:
+                c = cross(leg(l, over_r=True) * (-1.0), k_th)    # leg carries -i: (-1)(-i) = i
+                for blk, alpha in terms:
+                    bm[:, blk * nkt:(blk + 1) * nkt] += c * alpha[None, :]
         return fish
+
+    @staticmethod
+    def derivative_coefficient(k):
+        """Coefficients of the numerical k dP/dk over the theory bins (pspec.py:368-378)."""
+        nk = len(k) - 1
+        kfac = np.zeros(nk)
+        for ki in range(nk):
+            if 0 < ki - 1 < nk - 1:
+                kfac[ki] += k[ki - 1] / (k[ki] - k[ki - 2])
+            if 0 < ki + 1 < nk - 1:
+                kfac[ki] -= k[ki + 1] / (k[ki + 2] - k[ki])
+            kfac[ki] += k[0] / (k[1] - k[0]) * ((ki == 1) - (ki == 0))
+            kfac[ki] -= k[-1] / (k[-1] - k[-2]) * ((ki == nk - 1) - (ki == nk - 2))
+        return kfac
 
     def compute_fisher_contribution(self, seed, verb=False):
         """Fisher contribution of one GRF with the reference's noise for this seed (pspec.py:141-147)."""
@@ -484,8 +538,6 @@ class PSpec:
         if not self.const_mask:
             assert hasattr(self, 'mask_shot'), "Must supply mask_shot to compute shot-noise contribution"
         b = self.base
-        if b.sightline == 'local' and self.lmax > 0 and self.odd_l:
-            raise NotImplementedError("backend='cuda' implements even multipoles for the local sightline")
         dev = b.device
         F64 = nat.PB_F64
         PkA = [b.Pfid[0], 1. / b.Pfid[1]]
@@ -509,11 +561,15 @@ class PSpec:
                            b.ws)
             return out.cpu().numpy()
         # local sightline (pspec.py:522-544): multipole l crosses sum_m Y_lm(k) FT[Y_lm(r) a(r)]
+        # (times -i for odd l)
         Nk = self.Nk
         nat.bin_reduce(b.grid, F64, nat.PB_RED_CROSS, a, sna, 1, self.k_bins, [(0, 0)], scale, out[:Nk], b.ws)
         a_real = b.to_real(a)
         for li in range(1, self.Nl):
-            lm = b.harmonics.apply_fourier(a_real, 2 * li)
+            l = li * (2 - self.odd_l)
+            lm = b.harmonics.apply_fourier(a_real, l)
+            if l % 2:
+                lm = lm * (-1j)
             nat.bin_reduce(b.grid, F64, nat.PB_RED_CROSS, lm, sna, 1, self.k_bins, [(0, 0)], scale,
                            out[li * Nk:(li + 1) * Nk], b.ws)
         return out.cpu().numpy()
@@ -553,7 +609,9 @@ class PSpec:
         """Fisher contribution and rectangular binning matrix of one GRF (pspec.py:164-196):
         row b of the binning matrix holds the cross spectra of the Fisher Q-map of bin b with
         A^-1 a in the theory k-bins, weighted by L_l(mu) (global) or with the harmonic
-        transform sum_m Y_lm(k) FT[Y_lm(r) A^-1 a] (local), for l = 0, 2, .. lmax_theory.
+        transform sum_m Y_lm(k) FT[Y_lm(r) A^-1 a] (local), for l = 0, 2, .. lmax_theory (every
+        l with odd_l).  include_wideangle (local, even l): the odd-l transforms of
+        A^-1 a / |r| add the wide-angle terms to the l = 2, 4 blocks.
         Returns (fisher, binning_matrix)."""
         b = self.base
         k_bins_theory = np.asarray(k_bins_theory)
@@ -565,8 +623,10 @@ class PSpec:
             lmax_theory = self.lmax
         if include_wideangle:
             assert not b.sightline == 'global', "Wide-angle effects require local lines-of-sight!"
-            raise NotImplementedError("backend='cuda' does not implement the odd-l wide-angle theory terms")
-        if not self.odd_l:
+            assert not self.odd_l, "Cannot include wide-angle effects for odd l!"
+            assert lmax_theory > 1, "There are no wide-angle effects for the monopole!"
+            assert lmax_theory <= 4, "Higher-order effects not yet implemented!"
+        elif not self.odd_l:
             assert lmax_theory % 2 == 0, "Must use even lmax if not including wide-angle effects!"
         if lmax_theory > 4:
             raise NotImplementedError("backend='cuda' implements theory multipoles up to l = 4")
@@ -574,6 +634,9 @@ class PSpec:
             assert lmax_theory >= self.lmax, "Can't use larger lmax for data than for theory!"
         if not np.all(np.diff(k_bins_theory) > 0):
             raise ValueError("k_bins_theory must be strictly increasing")
+        odd_t = True if include_wideangle else bool(self.odd_l)
+        nl_th = lmax_theory + 1 if (odd_t and not include_wideangle) else lmax_theory // 2 + 1   # pspec.py:218-228
         fish, bm = self._fisher_from_fields(self._reference_field(seed),
-                                            theory=(k_bins_theory.astype(np.float64), lmax_theory // 2 + 1))
+                                            theory=(k_bins_theory.astype(np.float64), nl_th, lmax_theory,
+                                                    bool(include_wideangle), odd_t))
         return fish[0].cpu().numpy(), bm[0].cpu().numpy()

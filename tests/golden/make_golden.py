@@ -474,6 +474,37 @@ def integral_constraints(pb):
     return out
 
 
+@case
+def local_odd(pb):
+    """Local line of sight with odd multipoles (odd_l=True, lmax=3): 24^3, L=600, box centred
+    at (700, 400, 900) Mpc/h, TSC window, tabulated positive P(k), 4 bins, shell-sector mask
+    with mask_shot = 0.8 mask.  Pk_numerator and Pk_numerator_ideal of lognormal data
+    (seed 21) times the mask, the Fisher contribution (seed 0), the shot-noise contribution
+    (seed 1), the theory matrix with odd_l (lmax_theory = 4, seed 2); and with lmax=2 (even)
+    the theory matrix with the wide-angle terms (lmax_theory = 4, seed 3)."""
+    N, L = 24, 600.0
+    center = [700.0, 400.0, 900.0]
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    kth = np.linspace(kF, 0.12, 7)
+    mask = _mask24(N, L)
+    kt = np.linspace(0.0, 1.0, 2000)
+    pt = 3e3 * np.exp(-(kt / 0.25) ** 2) + 200.0
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, Pk=[kt, pt], boxcenter=center, sightline="local",
+                  pixel_window="tsc", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=3, mask=mask, mask_shot=0.8 * mask, odd_l=True)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * mask
+    out = dict(N=N, L=L, center=np.asarray(center), edges=edges, kth=kth, pk_k=kt, pk_p=pt)
+    out["num"] = _quiet(ps.Pk_numerator, d)
+    out["num_ideal"] = _quiet(ps.Pk_numerator_ideal, d)
+    out["f0"] = _quiet(ps.compute_fisher_contribution, 0)
+    out["shot1"] = _quiet(ps.compute_shot_contribution, 1)
+    out["tf2"], out["tt2"] = _quiet(ps.compute_theory_contribution, 2, kth, lmax_theory=4)
+    ps2 = _quiet(pb.PSpec, base, edges, lmax=2, mask=mask)
+    out["wf3"], out["wt3"] = _quiet(ps2.compute_theory_contribution, 3, kth, lmax_theory=4, include_wideangle=True)
+    return out
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

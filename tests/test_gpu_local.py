@@ -128,3 +128,29 @@ def test_local_shot_noise(pb):
     assert np.array_equal(bs.all_bins, gs["bins"])
     d = synthetic.lognormal(N, L, seed=16).astype(np.float64) * m
     assert rel(quiet(bs.compute_shot_contribution, 1, data=d, data2=0.7 * d), gs["b_full"]) < 1e-10
+
+
+def test_local_odd_multipoles(pb):
+    """Odd multipoles of the local sightline (odd_l=True, lmax=3) and the wide-angle theory
+    terms against the reference's outputs (tests/golden/local_odd.npz): S^-1 and ideal
+    numerators (1e-10), Fisher, shot-noise and theory contributions (1e-8)."""
+    go = np.load(os.path.join(GOLD, "local_odd.npz"))
+    N, L = int(go["N"]), float(go["L"])
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, Pk=[go["pk_k"], go["pk_p"]], boxcenter=list(go["center"]),
+              sightline="local", pixel_window="tsc", backend="cuda")
+    m = mask24(N, L)
+    ps = quiet(pb.PSpec, b, go["edges"], lmax=3, mask=m, mask_shot=0.8 * m, odd_l=True)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * m
+    assert blocks(ps.Pk_numerator(d), go["num"], 4) < 1e-10
+    assert blocks(ps.Pk_numerator_ideal(d), go["num_ideal"], 2) < 1e-10
+    assert rel(ps.compute_fisher_contribution(0), go["f0"]) < 1e-8
+    assert rel(ps.compute_shot_contribution(1), go["shot1"]) < 1e-8
+    f, t = ps.compute_theory_contribution(2, go["kth"], lmax_theory=4)
+    assert rel(f, go["tf2"]) < 1e-8 and rel(t, go["tt2"]) < 1e-8
+    pk = ps.Pk_unwindowed(d, fish=go["f0"])
+    assert sorted(pk) == ["p0", "p1", "p2", "p3"]
+    ps2 = quiet(pb.PSpec, b, go["edges"], lmax=2, mask=m)
+    f, t = ps2.compute_theory_contribution(3, go["kth"], lmax_theory=4, include_wideangle=True)
+    assert rel(f, go["wf3"]) < 1e-8 and rel(t, go["wt3"]) < 1e-8
+    with pytest.raises(AssertionError):
+        ps.compute_theory_contribution(2, go["kth"], lmax_theory=4, include_wideangle=True)

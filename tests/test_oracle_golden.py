@@ -356,3 +356,24 @@ def test_integral_constraints():
     assert rel(lps.fisher_contribution(lb.reference_noise(3 + 10 ** 7)), g["lpf3"]) < TOL
     lbs = O.OracleBSpec(lb, g["edges"], lmax=2, mask=m, mask_IC=mic, add_RIC=True, radial_bins_RIC=g["redges"])
     assert rel(lbs.fisher_contribution(*n(2, lb), sym=g["lsym"]), g["lbf2"]) < TOL
+
+
+def test_local_odd_multipoles():
+    """Odd multipoles of the local sightline (odd_l, lmax=3): numerators, Fisher, shot noise
+    and theory matrix; and the wide-angle theory terms (lmax=2, lmax_theory=4)."""
+    g = gold("local_odd")
+    N, L = int(g["N"]), float(g["L"])
+    m = mask24(N, L)
+    b = O.OracleBase([L] * 3, [N] * 3, Pk=[g["pk_k"], g["pk_p"]], pixel_window="tsc", boxcenter=g["center"],
+                     sightline="local")
+    ps = O.OraclePSpec(b, g["edges"], lmax=3, mask=m, odd_l=True)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * m
+    assert rel(ps.numerator(d, "Sinv"), g["num"]) < TOL
+    assert rel(ps.numerator(d, "ideal"), g["num_ideal"]) < TOL
+    assert rel(ps.fisher_contribution(b.reference_noise(10 ** 7)), g["f0"]) < TOL
+    assert rel(ps.shot_contribution(b.reference_noise(1 + 10 ** 7), mask_shot=0.8 * m), g["shot1"]) < TOL
+    f, t = ps.theory_contribution(b.reference_noise(2 + 10 ** 7), g["kth"], lmax_theory=4)
+    assert rel(f, g["tf2"]) < TOL and rel(t, g["tt2"]) < TOL
+    ps2 = O.OraclePSpec(b, g["edges"], lmax=2, mask=m)
+    f, t = ps2.theory_contribution(b.reference_noise(3 + 10 ** 7), g["kth"], lmax_theory=4, include_wideangle=True)
+    assert rel(f, g["wf3"]) < TOL and rel(t, g["wt3"]) < TOL
