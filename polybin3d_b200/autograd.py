@@ -9,7 +9,9 @@ For the power spectrum (PolyBin3D/pspec.py:613-686, trivial S^-1, data = m * d)
 so the reference's Q_{l b} = rfftn(m irfftn(Theta_b L_{2l} rfftn(m a)))  (pspec.py:443-456)
 is (N^3/V) rfftn(d num_{l b}/d d) at d = a.  The backward is one pass of the binned-weight
 filter kernel (pb_binned_filter) with the cotangent as per-bin weights, one c2r and one mask
-product.
+product.  For the local sightline multipole l is the cross spectrum of x = rfftn(m d)/W with
+H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x]; its gradient adds the adjoint transform, the same
+two parts as the reference's local Q-maps (pspec.py:456-486).
 
 For the bispectrum (PolyBin3D/bspec.py:895-983, no linear term) the numerator is
 V/(N^3 sym_i) sum_x g_b1 g_b2 g_{l,b3} with g_{l,b} = irfftn(Theta_b L_l rfftn(m d) / W);
@@ -49,29 +51,93 @@ KEY_CHUNK_BYTES = 16 << 30
 
 class PkNumerator(torch.autograd.Function):
     """num = PkNumerator.apply(d, pspec): the unwindowed numerator of data m*d as a
-    differentiable FP64 device tensor (N_bins,)."""
+    differentiable FP64 device tensor (N_bins,); global and local sightlines (odd l too)."""
 
     @staticmethod
-    def forward(ctx, d, ps):
+    def _spectrum(ps, d):
+        """x = rfftn(m d) / W."""
         b = ps.base
-        if b.sightline == 'local' and ps.lmax > 0:
-            raise NotImplementedError("differentiable numerators are implemented for the global sightline")
-        d = d.to(torch.float64).contiguous()
-        ctx.ps = ps
-        ctx.save_for_backward(d)
-        y = d
         m = _mask_of(ps)
-        if m is not None:
-            y = nat.elementwise(nat.PB_EW_MUL, d, m)
+        y = d if m is None else nat.elementwise(nat.PB_EW_MUL, d, m)
         xk = b.fft_r2c(y)
         b.n_FFTs_forward += 1
         if b.pixel_window != 'none':
             w = b.to_device_grid('window', lambda: b.pixel_window_grid, torch.float64)
             nat.spectral_filter(b.grid, nat.PB_F64, xk, xk, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
+        return xk
+
+    @staticmethod
+    def forward(ctx, d, ps):
+        b = ps.base
+        d = d.to(torch.float64).contiguous()
+        ctx.ps = ps
+        ctx.save_for_backward(d)
+        xk = PkNumerator._spectrum(ps, d)
         out = torch.empty(ps.N_bins, dtype=torch.float64, device=b.device)
-        nat.bin_reduce(b.grid, nat.PB_F64, nat.PB_RED_ABS2, xk, None, 1, ps.k_bins, ps._ells(ps.Nl),
-                       0.5 * b.volume / float(b.gridsize.prod()) ** 2, out, b.ws)
+        scale = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
+        if b.sightline == 'global' or ps.Nl == 1:
+            nat.bin_reduce(b.grid, nat.PB_F64, nat.PB_RED_ABS2, xk, None, 1, ps.k_bins, ps._ells(ps.Nl), scale, out,
+                           b.ws)
+            return out
+        # local sightline (pspec.py:643-680): multipole l crosses x with p_l H_l[x],
+        # H_l[x] = sum_m Y_lm(k) FT[Y_lm(r) IFT x], p_l = -i for odd l, 1 for even l
+        Nk = ps.Nk
+        nat.bin_reduce(b.grid, nat.PB_F64, nat.PB_RED_ABS2, xk, None, 1, ps.k_bins, [(0, 0)], scale, out[:Nk], b.ws)
+        x_real = b.to_real(xk)
+        for li in range(1, ps.Nl):
+            l = li * (2 - ps.odd_l)
+            lm = b.harmonics.apply_fourier(x_real, l)
+            if l % 2:
+                lm = lm * (-1j)
+            nat.bin_reduce(b.grid, nat.PB_F64, nat.PB_RED_CROSS, xk, lm, 1, ps.k_bins, [(0, 0)], scale,
+                           out[li * Nk:(li + 1) * Nk], b.ws)
         return out
+
+    @staticmethod
+    def _local_backward(ps, d, coef):
+        """Gradient of sum_{l b} g_{l b} num_{l b} for the local sightline.  With
+        num_{l b} = 1/2 V/N^6 sum_k Theta_b Re(x conj(p_l H_l x)) and x = F(m d)/W, the
+        gradient of Re<x, Theta p H x> in x is Theta p H x + conj(p) H^dag Theta x, where
+        H^dag v = FT[sum_m Y_lm(r) IFT(Y_lm(k) v)] (the second part of the reference's local
+        Q-maps, pspec.py:466-483), and d/dd = m F^dag W^-1: grad = V/N^6 m c2r(S / W),
+        S = Theta_g0 x + sum_l 1/2 (p Theta_gl H_l x + conj(p) H_l^dag Theta_gl x),
+        Theta_g the bin filter weighted by the cotangent."""
+        b = ps.base
+        harm = b.harmonics
+        xk = PkNumerator._spectrum(ps, d)
+        S = torch.empty_like(xk)
+        nat.binned_filter(b.grid, xk, S, ps.k_bins, [0], coef[0:1])
+        x_real = b.to_real(xk)
+        R = torch.zeros_like(d)
+        t = torch.empty_like(xk)
+        u = torch.empty_like(xk)
+        for li in range(1, ps.Nl):
+            l = li * (2 - ps.odd_l)
+            nat.binned_filter(b.grid, harm.apply_fourier(x_real, l), t, ps.k_bins, [0], coef[li:li + 1], scale=0.5)
+            S.add_(t * (-1j) if l % 2 else t)
+            # H^dag Theta_g x; conj(p) = i goes in before the inverse transform, where it makes
+            # the odd-l spectrum Hermitian again
+            nat.binned_filter(b.grid, xk, u, ps.k_bins, [0], coef[li:li + 1], scale=0.5 / b.nreal)
+            if l % 2:
+                u.mul_(1j)
+            yr = harm._grid('r', l, torch.float64)
+            yk = harm._grid('k', l, torch.float64)
+            for mi in range(yr.shape[0]):
+                v = u * yk[mi]
+                b.n_FFTs_reverse += 1
+                R.addcmul_(b.fft_c2r(v), yr[mi])
+        b.n_FFTs_forward += 1
+        S.add_(b.fft_r2c(R))
+        if b.pixel_window != 'none':
+            w = b.to_device_grid('window', lambda: b.pixel_window_grid, torch.float64)
+            nat.spectral_filter(b.grid, nat.PB_F64, S, S, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
+        S.mul_(b.volume / float(b.gridsize.prod()) ** 2)
+        b.n_FFTs_reverse += 1
+        grad = b.fft_c2r(S)
+        m = _mask_of(ps)
+        if m is not None:
+            grad = nat.elementwise(nat.PB_EW_MUL, grad, m, out=grad)
+        return grad
 
     @staticmethod
     def backward(ctx, g):
@@ -79,11 +145,13 @@ class PkNumerator(torch.autograd.Function):
         ps = ctx.ps
         b = ps.base
         (d,) = ctx.saved_tensors
+        coef = g.to(torch.float64).reshape(ps.Nl, ps.Nk).contiguous()
+        if b.sightline == 'local' and ps.Nl > 1:
+            return PkNumerator._local_backward(ps, d, coef), None
         m = _mask_of(ps)
         y = d if m is None else nat.elementwise(nat.PB_EW_MUL, d, m)
         xk = b.fft_r2c(y)
         b.n_FFTs_forward += 1
-        coef = g.to(torch.float64).reshape(ps.Nl, ps.Nk).contiguous()
         w = None
         if b.pixel_window != 'none':
             w = b.to_device_grid('window', lambda: b.pixel_window_grid, torch.float64)
@@ -118,7 +186,7 @@ class BkNumerator(torch.autograd.Function):
     @staticmethod
     def forward(ctx, d, bs):
         if bs.base.sightline == 'local' and bs.lmax > 0:
-            raise NotImplementedError("differentiable numerators are implemented for the global sightline")
+            raise NotImplementedError("the differentiable bispectrum numerator is implemented for the global sightline")
         if not hasattr(bs, 'sym_factor'):
             bs._compute_symmetry_factor()
         ctx.in_dtype = d.dtype
