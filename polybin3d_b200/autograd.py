@@ -21,7 +21,9 @@ The backward recomputes the bin-filtered maps (nothing is stored by the forward)
 real space, the products of the other two maps of every leg that ends on the same (bin,
 multipole) with pb_bilinear_maps (one map per leg instead of one per pair of maps),
 transforms those, and gathers them into one spectrum with the accumulating spectral filter.  Maps, products and their transforms live
-on the dealiased map grid, which is exact for every frequency inside the bins.
+on the dealiased map grid, which is exact for every frequency inside the bins.  With the
+local sightline the l > 0 maps are IFT(Theta_b H_l x): their legs are gathered through the bin
+filter alone, one spectrum per l, and the adjoint H_l^dag applied once per l.
 """
 import numpy as np
 import torch
@@ -167,7 +169,7 @@ class PkNumerator(torch.autograd.Function):
 
 class BkNumerator(torch.autograd.Function):
     """num = BkNumerator.apply(d, bspec): the unwindowed numerator (no linear term) of data
-    m*d as a differentiable FP64 device tensor (N_bins,).  Maps, transforms and the gradient
+    m*d as a differentiable FP64 device tensor (N_bins,); global and local sightlines.  Maps, transforms and the gradient
     run in the base's precision (FP64, or FP32 with precision='mixed'); the cubic sums are
     FP64 either way."""
 
@@ -185,8 +187,6 @@ class BkNumerator(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, d, bs):
-        if bs.base.sightline == 'local' and bs.lmax > 0:
-            raise NotImplementedError("the differentiable bispectrum numerator is implemented for the global sightline")
         if not hasattr(bs, 'sym_factor'):
             bs._compute_symmetry_factor()
         ctx.in_dtype = d.dtype
@@ -229,7 +229,12 @@ class BkNumerator(torch.autograd.Function):
             c3 = (l // 2) * nks + b3
             for (kk, C, lc) in ((key_of(b2, c3), b1, 0), (key_of(b1, c3), b2, 0), (key_of(b1, b2), b3, l)):
                 legs[(kk, C, lc)] = legs.get((kk, C, lc), 0.0) + coef[t]
-        grad_spec = torch.zeros((1,) + b.nhalf_shape, dtype=cd, device=b.device)
+        # local sightline: the l > 0 maps are IFT(Theta_b H_l x), so a leg ending on (C, l > 0)
+        # goes through the bin filter alone into an accumulator per l, and H_l^dag is applied
+        # once per l below (H_l^dag v = FT[sum_m Y_lm(r) IFT(Y_lm(k) v)])
+        local = b.sightline == 'local' and bs.lmax > 0
+        n_acc = 1 + (bs.lmax // 2 if local else 0)
+        grad_spec = torch.zeros((n_acc,) + b.nhalf_shape, dtype=cd, device=b.device)
         if keys:
             # one real-space map per leg (bin C, multipole lc): the coefficient-weighted sum of
             # the products of the other two maps of every triplet ending on it (pb_bilinear_maps);
@@ -248,11 +253,23 @@ class BkNumerator(torch.autograd.Function):
                 o1 = min(len(outs), o0 + chunk)
                 FT = b.fft_r2c(R[o0:o1])
                 b.n_FFTs_forward += o1 - o0
-                entries = [(n - o0, ks[C], ks[C + 1], lc, 0, 1.0, 0) for n, (C, lc) in enumerate(outs[o0:o1], o0)]
+                entries = [(n - o0, ks[C], ks[C + 1], 0 if local else lc, 0, 1.0, 0)
+                           for n, (C, lc) in enumerate(outs[o0:o1], o0)]
+                dst = [lc // 2 if local else 0 for (C, lc) in outs[o0:o1]]
                 nat.spectral_filter(b.grid_of(Mdims), prec, FT, grad_spec, entries, accumulate=True,
-                                    src_stride=FT[0].numel(), out_n=[int(n) for n in b.gridsize],
-                                    dst=[0] * len(entries))
+                                    src_stride=FT[0].numel(), out_n=[int(n) for n in b.gridsize], dst=dst)
                 del FT
+        if n_acc > 1:
+            harm = b.harmonics
+            R = torch.zeros((1,) + tuple(int(n) for n in b.gridsize), dtype=rd, device=b.device)
+            for li in range(1, n_acc):
+                yr = harm._grid('r', 2 * li, rd)
+                yk = harm._grid('k', 2 * li, rd)
+                for mi in range(yr.shape[0]):
+                    b.n_FFTs_reverse += 1
+                    R[0].addcmul_(b.fft_c2r((grad_spec[li] * yk[mi]).contiguous()), yr[mi])
+            b.n_FFTs_forward += 1
+            grad_spec = grad_spec[0:1] + b.fft_r2c(R) * (1.0 / N3)
         if b.pixel_window != 'none':
             w = b.to_device_grid('window', lambda: b.pixel_window_grid, rd)
             nat.spectral_filter(b.grid, prec, grad_spec, grad_spec, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)

@@ -224,3 +224,20 @@ def test_pk_local_sightline(pb, case):
     # the mask covers a few per cent of the voxels: spread the direction over enough of them
     # that it reaches inside the mask
     check_fd(lambda x: pk_numerator(ps, x), d, ps.N_bins, cubic=False, seed=5, n_vox=4096)
+
+
+def test_bk_local_sightline(pb):
+    """Local sightline, lmax=2: the forward equals the reference's numerator without the linear
+    term (tests/golden/local_los.npz) and the gradient, whose l = 2 legs go through the
+    adjoint harmonic transform, matches finite differences."""
+    from polybin3d_b200.autograd import bk_numerator
+    g = gold("local_los")
+    N, L = int(g["N"]), float(g["L"])
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=list(g["center"]), sightline="local",
+              pixel_window="cic", backend="cuda")
+    bs = quiet(pb.BSpec, b, g["bedges"], lmax=2, mask=mask24(N, L))
+    d = torch.as_tensor(synthetic.lognormal(N, L, seed=21).astype(np.float64), device=b.device)
+    num = quiet(bk_numerator, bs, d).cpu().numpy()
+    nb = len(num) // 2
+    assert rel(num[:nb], g["bk_num"][:nb]) < 1e-10 and rel(num[nb:], g["bk_num"][nb:]) < 1e-10
+    check_fd(lambda x: bk_numerator(bs, x), d, bs.N_bins, cubic=True, seed=6, n_vox=4096)
