@@ -419,6 +419,51 @@ class PolyBin3D:
             return self.to_real(input_data)
         return self.to_fourier(input_data)
 
+    # ------------------------------------------------------------------------------
+    # harmonic transforms and the covariance kernel (base.py:391-437)
+    # ------------------------------------------------------------------------------
+    def _spectrum_in(self, k):
+        if isinstance(k, torch.Tensor):
+            return k.to(self.device)
+        return torch.as_tensor(np.ascontiguousarray(k), device=self.device)
+
+    def apply_real_harmonics(self, a_map_fourier, Ylm_real, Ylm_fourier):
+        """sum_m Y_lm(r) IFT[Y_lm(k) a(k)] (base.py:391-400) as a device real map; Ylm_real
+        (n_m, n0, n1, n2) and Ylm_fourier (n_m, half grid) as PSpec.Ylm_real[l] and
+        PSpec.Ylm_fourier[l] hold them (numpy or device)."""
+        a = self._spectrum_in(a_map_fourier)
+        rd = a.real.dtype
+        out = torch.zeros(tuple(int(n) for n in self.gridsize), dtype=rd, device=self.device)
+        for m in range(len(Ylm_real)):
+            out.addcmul_(self.to_real(a * self.as_device(Ylm_fourier[m], rd)), self.as_device(Ylm_real[m], rd))
+        return out
+
+    def apply_fourier_harmonics(self, a_map_real, Ylm_real, Ylm_fourier):
+        """sum_m Y_lm(k) FT[Y_lm(r) a(r)] (base.py:402-411) as a device half spectrum."""
+        x = self.as_device(a_map_real, a_map_real.dtype if isinstance(a_map_real, torch.Tensor) else torch.float64)
+        cd = torch.complex128 if x.dtype == torch.float64 else torch.complex64
+        out = torch.zeros(self.nhalf_shape, dtype=cd, device=self.device)
+        for m in range(len(Ylm_real)):
+            out.add_(self.to_fourier(x * self.as_device(Ylm_real[m], x.dtype)) * self.as_device(Ylm_fourier[m], x.dtype))
+        return out
+
+    def apply_xi(self, input_map_fourier, input_map_real=None, Ylm_real=None, Ylm_fourier=None, Pk_grid=[],
+                 output_type='real'):
+        """Apply xi(x, y), the correlation of the gridded spectrum Pk_grid = {l: P_l(k)}, to a
+        map (base.py:413-437): P_0 X, plus for the local sightline and each further l one half
+        of P_l sum_m Y_lm(k) FT[Y_lm(r) x] and one half of sum_m Y_lm(r) IFT[Y_lm(k) P_l X]."""
+        X = self._spectrum_in(input_map_fourier)
+        rd = X.real.dtype
+        PF = X * self.as_device(Pk_grid[0], rd)
+        if self.sightline == 'global' or len(Pk_grid.keys()) == 1:
+            return PF if output_type == 'fourier' else self.to_real(PF)
+        PR = torch.zeros(tuple(int(n) for n in self.gridsize), dtype=rd, device=self.device)
+        for ell in list(Pk_grid.keys())[1:]:
+            Pl = self.as_device(Pk_grid[ell], rd)
+            PF = PF + 0.5 * self.apply_fourier_harmonics(input_map_real, Ylm_real[ell], Ylm_fourier[ell]) * Pl
+            PR = PR + 0.5 * self.apply_real_harmonics(X * Pl, Ylm_real[ell], Ylm_fourier[ell])
+        return PF + self.to_fourier(PR) if output_type == 'fourier' else self.to_real(PF) + PR
+
     def _ainv_weight(self):
         """invP / W^2 (0 where W = 0) on the half grid, FP64 host array."""
         w = self.invPk0_grid.copy()

@@ -152,8 +152,13 @@ class BSpec:
         self._captured = None
         self._shell_modes = None
         self.map_grid = self._dealiased_grid() if dealias else tuple(int(n) for n in base.gridsize)
+        # real harmonics of positions and wavevectors (bspec.py:158-169): device grids, shared
+        # with the ones the local-sightline maps use
         self.Ylm_real = None
         self.Ylm_fourier = None
+        if base.sightline == 'local' and self.lmax > 0:
+            self.Ylm_real = {l: base.harmonics._grid('r', l, torch.float64) for l in range(2, self.lmax + 1, 2)}
+            self.Ylm_fourier = {l: base.harmonics._grid('k', l, torch.float64) for l in range(2, self.lmax + 1, 2)}
 
     # ------------------------------------------------------------------------------
     # binning helpers (bspec.py:171-220)

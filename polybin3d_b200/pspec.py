@@ -91,8 +91,14 @@ class PSpec:
         self._pt = None
         self.applySinv = self.base.applySinv_trivial
         self.applySinv_transpose = self.base.applySinv_trivial
+        # real harmonics of positions and wavevectors (pspec.py:86-91): device grids, shared
+        # with the ones the local-sightline multipoles use
         self.Ylm_real = None
         self.Ylm_fourier = None
+        if self.base.sightline == 'local' and self.lmax > 0:
+            ls = range(1, self.lmax + 1) if self.odd_l else range(2, self.lmax + 1, 2)
+            self.Ylm_real = {l: self.base.harmonics._grid('r', l, torch.float64) for l in ls}
+            self.Ylm_fourier = {l: self.base.harmonics._grid('k', l, torch.float64) for l in ls}
         self._captured = {}
 
     def get_ks(self):

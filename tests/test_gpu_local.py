@@ -154,3 +154,29 @@ def test_local_odd_multipoles(pb):
     assert rel(f, go["wf3"]) < 1e-8 and rel(t, go["wt3"]) < 1e-8
     with pytest.raises(AssertionError):
         ps.compute_theory_contribution(2, go["kth"], lmax_theory=4, include_wideangle=True)
+
+
+def test_base_harmonic_transforms(pb):
+    """PolyBin3D.apply_fourier_harmonics / apply_real_harmonics / apply_xi with the harmonic
+    grids PSpec keeps in Ylm_real / Ylm_fourier, against the oracle's restatement of
+    base.py:391-437 (local sightline, l = 2 and 4, Pk_grid with three multipoles)."""
+    from oracle import polybin_oracle as O
+    N, L = 24, 600.0
+    center = [700.0, 400.0, 900.0]
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=center, sightline="local", backend="cuda")
+    ps = quiet(pb.PSpec, b, np.linspace(2 * np.pi / L, 0.11, 5), lmax=4)
+    assert sorted(ps.Ylm_real) == [2, 4] and sorted(ps.Ylm_fourier) == [2, 4]
+    ob = O.OracleBase([L] * 3, [N] * 3, boxcenter=np.asarray(center), sightline="local")
+    x = synthetic.lognormal(N, L, seed=5).astype(np.float64)
+    X = ob.to_fourier(x)
+    for l in (2, 4):
+        got = b.apply_fourier_harmonics(x, ps.Ylm_real[l], ps.Ylm_fourier[l]).cpu().numpy()
+        assert rel(got, ob.apply_fourier_harmonics(x, l)) < 1e-12
+        got = b.apply_real_harmonics(X, ps.Ylm_real[l], ps.Ylm_fourier[l]).cpu().numpy()
+        assert rel(got, ob.apply_real_harmonics(X, l)) < 1e-12
+    kt = np.linspace(0.0, 1.0, 500)
+    pk_cov = [kt, 3e3 * np.exp(-(kt / 0.25) ** 2), 800.0 * np.exp(-(kt / 0.2) ** 2), 100.0 * np.exp(-kt / 0.2)]
+    xi = O.xi_grids(ob, pk_cov)
+    for out in ("real", "fourier"):
+        got = b.apply_xi(X, x, ps.Ylm_real, ps.Ylm_fourier, xi, output_type=out).cpu().numpy()
+        assert rel(got, O.apply_xi(ob, X, x, xi, out)) < 1e-12
