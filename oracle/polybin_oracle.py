@@ -416,17 +416,31 @@ def apply_xi(b, X, x_real, xi, output):
     return PF + b.to_fourier(PR) if output == "fourier" else b.to_real(PF) + PR
 
 
-def cov_filter(b, x, real, xi, const_mask, mask_mean, point, mask_shot):
-    """S^-1 [P xi P^dag + N] S^-dag x with the trivial S^-1 (pspec.py:277-290, 307-323;
-    bspec.py:499-519); x is a real map if `real`, else a half spectrum; the output is a
-    half spectrum.  point(x, transpose): the pointing matrix P or P^dag."""
+def trivial_sinv(b):
+    """applySinv_trivial (base.py:355-362): the identity with real / Fourier conversion."""
+    def f(x, input_type="real", output_type="real"):
+        if input_type == output_type:
+            return x
+        return b.to_real(x) if input_type == "fourier" else b.to_fourier(x)
+    return f
+
+
+def cov_filter(b, x, real, xi, const_mask, mask_mean, point, mask_shot, sinv=None, sinv_t=None):
+    """S^-1 [P xi P^dag + N] S^-dag x (pspec.py:277-290, 307-323; bspec.py:499-519); x is a
+    real map if `real`, else a half spectrum; the output is a half spectrum.  point(x,
+    transpose): the pointing matrix P or P^dag; sinv, sinv_t: S^-1 and S^-dag (default the
+    trivial one)."""
+    sinv = sinv or trivial_sinv(b)
+    sinv_t = sinv_t or trivial_sinv(b)
+    it = "real" if real else "fourier"
     if const_mask:
-        Sid = b.to_fourier(x) if real else x
-        return mask_mean ** 2 * apply_xi(b, Sid, None, xi, "fourier") + mask_mean * Sid
-    Sid = x if real else b.to_real(x)
+        Sid = sinv_t(x, it, "fourier")
+        C = mask_mean ** 2 * apply_xi(b, Sid, None, xi, "fourier") + mask_mean * Sid
+        return sinv(C, "fourier", "fourier")
+    Sid = sinv_t(x, it, "real")
     Pd_real = point(Sid, True)
     C = apply_xi(b, b.to_fourier(Pd_real), Pd_real, xi, "real")
-    return b.to_fourier(point(C, False) + mask_shot * Sid)
+    return sinv(point(C, False) + mask_shot * Sid, "real", "fourier")
 
 
 class Pointing:
@@ -477,8 +491,12 @@ def _pointing_of(base, mask, mask_IC, add_GIC, add_RIC, radial_bins_RIC):
 
 class OraclePSpec:
     def __init__(self, base, k_bins, lmax=2, mask=None, mask_IC=None, add_GIC=False, add_RIC=False,
-                 radial_bins_RIC=None, odd_l=False):
+                 radial_bins_RIC=None, odd_l=False, applySinv=None, applySinv_transpose=None):
         self.base = base
+        # S^-1 and S^-dag (pspec.py:92-99): the trivial filter, or the caller's, whose
+        # transpose defaults to itself
+        self.sinv = applySinv or trivial_sinv(base)
+        self.sinv_t = applySinv_transpose or (applySinv if applySinv is not None else trivial_sinv(base))
         self.k_bins = np.asarray(k_bins, dtype=np.float64)
         self.lmax = lmax
         self.odd_l = odd_l
@@ -513,6 +531,10 @@ class OraclePSpec:
             x = b.div_fourier(x, b.pixel_window_grid)
         if filtering == "ideal":
             x = x * b.invPk0_grid / np.sqrt(self.sq_mask_mean)
+        elif b.pixel_window != "none":                                   # pspec.py:629-640
+            x = self.sinv(x, "fourier", "fourier")
+        else:
+            x = self.sinv(data, "real", "fourier")
         Nl = self.Nl if filtering != "ideal" else self.Nl_even
         odd = self.odd_l and filtering != "ideal"
         out = np.zeros(Nl * self.Nk)
@@ -578,7 +600,7 @@ class OraclePSpec:
 
     def cov_filter(self, x, real, xi, mask_shot):
         return cov_filter(self.base, x, real, xi, self.const_mask, getattr(self, "mask_mean", None),
-                          None if self.const_mask else self.point, mask_shot)
+                          None if self.const_mask else self.point, mask_shot, self.sinv, self.sinv_t)
 
     def _contribution(self, noise_pair, xi=None, mask_shot=None, theory=None):
         """_compute_fisher, global and local (even l) sightlines (pspec.py:215-493)."""
@@ -591,16 +613,17 @@ class OraclePSpec:
         def dagger(x, real):                                             # 291-323
             if xi is not None:
                 return self.cov_filter(x, real, xi, mask_shot)
+            it = "real" if real else "fourier"
             if self.const_mask:
-                return self.mask_mean * (b.to_fourier(x) if real else x)
-            return b.to_fourier(self.point(x if real else b.to_real(x), True))
+                return self.mask_mean * self.sinv_t(x, it, "fourier")
+            return b.to_fourier(self.point(self.sinv_t(x, it, "real"), True))
 
         if xi is not None:                                               # 270-290, 330-332
             SinvP = dagger(a, False) if self.const_mask else dagger(a_real, True)
         elif self.const_mask:                                            # 273-276
-            SinvP = self.mask_mean * a
+            SinvP = self.mask_mean * self.sinv(a, "fourier", "fourier")
         else:
-            SinvP = b.to_fourier(self.point(a_real, False))
+            SinvP = self.sinv(self.point(a_real, False), "real", "fourier")
         fish = np.zeros((self.N_bins, self.N_bins))
         bm = None if theory is None else np.zeros((self.N_bins, theory[1] * (len(theory[0]) - 1)))
         scaling = 0.5 * b.volume / b.gridsize.prod() ** 2                # 390
@@ -731,9 +754,10 @@ class OraclePSpec:
         draw, invPA = b.inverse_fiducial_draw()
         a = b.grf_from_noise(*noise_pair, Pk_grid=draw)                  # 511
         if self.const_mask:                                              # 514-519
-            sna = self.mask_mean * b.applyAinv_fourier(a, invPA)
+            sna = self.mask_mean * self.sinv(b.applyAinv_fourier(a, invPA), "fourier", "fourier")
         else:
-            sna = b.to_fourier(b.to_real(b.applyAinv_fourier(a, invPA)) * mask_shot)
+            sna = self.sinv(b.to_real(b.applyAinv_fourier(a, invPA)) * mask_shot, "real", "fourier")
+        a = self.sinv(a, "fourier", "fourier")                           # 522
         shot = np.zeros(self.N_bins)
         for li in range(self.Nl):                                        # 526-544
             if b.sightline == "global" or li == 0:

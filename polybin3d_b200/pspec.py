@@ -74,8 +74,13 @@ class PSpec:
         if type(mask_shot) != type(None):
             self.mask_shot = mask_shot.astype(np.float64)
 
-        if self.applySinv is not None:
-            raise NotImplementedError("backend='cuda' implements the trivial S^-1 weighting (applySinv=None)")
+        # S^-1 (pspec.py:92-99): the trivial filter, or the caller's, applied to device maps
+        # (a real map or a half spectrum in, either out); its transpose defaults to itself
+        self._custom_sinv = self.applySinv is not None
+        if self._custom_sinv and type(self.applySinv_transpose) != type(lambda x: x):
+            self.applySinv_transpose = self.applySinv
+            if verb:
+                print("## Caution: assuming S^-1 is Hermitian!")
         # integral constraints (pspec.py:101-111)
         if self.add_GIC:
             if verb:
@@ -89,8 +94,9 @@ class PSpec:
                 print("Accounting for radial integral constraint across %d bins" % (len(radial_bins_RIC) - 1))
             self.radial_bins_RIC = np.asarray(radial_bins_RIC, dtype=np.float64)
         self._pt = None
-        self.applySinv = self.base.applySinv_trivial
-        self.applySinv_transpose = self.base.applySinv_trivial
+        if not self._custom_sinv:
+            self.applySinv = self.base.applySinv_trivial
+            self.applySinv_transpose = self.base.applySinv_trivial
         # real harmonics of positions and wavevectors (pspec.py:86-91): device grids, shared
         # with the ones the local-sightline multipoles use
         self.Ylm_real = None
@@ -135,8 +141,49 @@ class PSpec:
             if b.pixel_window != 'none':
                 w = b.to_device_grid('window', lambda: b.pixel_window_grid, rd)
                 nat.spectral_filter(b.grid, prec, xk, xk, [(0, -1.0, np.inf, 0, 0, 1.0, -1)], w=w)
+            if self._custom_sinv:                                        # pspec.py:629-640
+                y = self._sinv(xk, 'fourier', 'fourier') if b.pixel_window != 'none' else \
+                    self._sinv(x, 'real', 'fourier')
+                xk = y.to(xk.dtype)
             scale = 1.0
         return xk, scale
+
+    def _sinv(self, x, input_type, output_type, transpose=False):
+        """The caller's S^-1 (or S^-dag) on one device map (pspec.py:92-99); the result as
+        a contiguous FP64 device tensor (half spectrum or real map)."""
+        f = self.applySinv_transpose if transpose else self.applySinv
+        y = f(x, input_type=input_type, output_type=output_type)
+        if not isinstance(y, torch.Tensor):
+            y = torch.as_tensor(np.ascontiguousarray(y))
+        dt = torch.complex128 if output_type == 'fourier' else torch.float64
+        return y.to(device=self.base.device, dtype=dt).contiguous()
+
+    def _dagger_custom(self, x, real, xi=None):
+        """(S^-1 P)^dag x with the caller's S^-dag (pspec.py:291-305), or its covariance form
+        S^-1 [P xi P^dag + N] S^-dag (307-323), for one map: x a real map if `real`, else a
+        half spectrum; returns a half spectrum."""
+        b = self.base
+        it = 'real' if real else 'fourier'
+        if xi is None:
+            if self.const_mask:
+                return self._sinv(x, it, 'fourier', transpose=True) * float(self.mask_mean)
+            r = self._sinv(x, it, 'real', transpose=True)
+            b.n_FFTs_forward += 1
+            return b.fft_r2c(self._pointing()(r, True))
+        if self.const_mask:
+            sid = self._sinv(x, it, 'fourier', transpose=True)
+            if len(xi) > 1:
+                raise ValueError("local multipoles of Pk_cov need a varying mask (the reference applies xi "
+                                 "without a real-space map for a constant mask)")
+            mm = float(self.mask_mean)
+            return self._sinv(sid * (xi[0] * (mm * mm) + mm), 'fourier', 'fourier')
+        sid = self._sinv(x, it, 'real', transpose=True)
+        t = self._pointing()(sid, True)
+        b.n_FFTs_forward += 1
+        u = covariance.xi_real(b, b.fft_r2c(t)[None], t[None], xi)[0]
+        ms = b.to_device_grid(('pk_mask_shot', id(self)), lambda: self.mask_shot, torch.float64)
+        u = self._pointing()(u, False) + sid * ms
+        return self._sinv(u, 'real', 'fourier')
 
     def _ideal_weight(self):
         b = self.base
@@ -215,7 +262,19 @@ class PSpec:
         if theory is not None:
             k_th, nl_th = theory[:2]
             bm = torch.zeros((B, self.N_bins, nl_th * (len(k_th) - 1)), dtype=torch.float64, device=b.device)
-        if xi is not None:
+        if self._custom_sinv:
+            # the caller's S^-1, one map at a time as the reference applies it (pspec.py:270-290)
+            SinvP = torch.empty_like(a)
+            for i in range(B):
+                if xi is not None:
+                    SinvP[i] = self._dagger_custom(a[i] if self.const_mask else b.to_real(a[i]), not self.const_mask,
+                                                   xi)
+                elif self.const_mask:
+                    SinvP[i] = self._sinv(a[i], 'fourier', 'fourier') * float(self.mask_mean)
+                else:
+                    SinvP[i] = self._sinv(self._pointing()(b.to_real(a[i]), False), 'real', 'fourier')
+            qscale = 1.0
+        elif xi is not None:
             # S^-1 P a -> S^-1 [P xi P^dag + N] S^-dag a (pspec.py:270-290, 330-332)
             SinvP = a.clone()
             if not self.const_mask:
@@ -240,17 +299,21 @@ class PSpec:
         scaling = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
         if b.sightline == 'local' and (self.Nl > 1 or theory is not None):
             for i in range(B):
-                S = SinvP[i] * self.mask_mean if (self.const_mask and xi is None) else SinvP[i]
+                S = SinvP[i] * self.mask_mean if (self.const_mask and xi is None and not self._custom_sinv) \
+                    else SinvP[i]
                 self._fisher_local(Ainv[i], S, scaling, fish[i], xi=xi, theory=theory,
                                    bm=None if bm is None else bm[i])
             return fish if theory is None else (fish, bm)
         rows = [(li, ki) for li in range(self.Nl) for ki in range(self.Nk)]
         for i in range(B):
             Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
-            maps = [(i, self.k_bins[ki], self.k_bins[ki + 1], 2 * li, 0, qscale if self.const_mask else invN, 0)
-                    for (li, ki) in rows]
+            qs = 1.0 if self._custom_sinv else (qscale if self.const_mask else invN)
+            maps = [(i, self.k_bins[ki], self.k_bins[ki + 1], 2 * li, 0, qs, 0) for (li, ki) in rows]
             nat.spectral_filter(grid, F64, SinvP, Q, maps, src_stride=nh)
-            if xi is not None:
+            if self._custom_sinv:
+                for r in range(self.N_bins):
+                    Q[r] = self._dagger_custom(Q[r], False, xi)
+            elif xi is not None:
                 Q = self._cov_rows(Q, xi)
             elif not self.const_mask:
                 qr = b.fft_c2r(Q)
@@ -297,6 +360,14 @@ class PSpec:
             """R <- D R for a block of rows whose Fourier part R (already scaled by 1/N^3 for
             a varying mask, by the mask mean for a constant one) may come with a real-space
             part `real` (unnormalised, added before the mask)."""
+            if self._custom_sinv:
+                # the caller's S^-dag: each part of each row on its own (pspec.py:466-483)
+                for r in range(R.shape[0]):
+                    q = self._dagger_custom(R[r], False, xi)
+                    if real is not None:
+                        q = q + self._dagger_custom(real[r], True, xi)
+                    R[r] = q
+                return R
             if xi is not None:
                 return self._cov_rows(R, xi, real)
             if self.const_mask:
@@ -312,7 +383,7 @@ class PSpec:
             b.n_FFTs_forward += R.shape[0]
             return b.fft_r2c(rr, out=R)
 
-        qs = invN if not self.const_mask else (1.0 if xi is not None else mm)
+        qs = 1.0 if self._custom_sinv else (invN if not self.const_mask else (1.0 if xi is not None else mm))
         bands = [(0, self.k_bins[ki], self.k_bins[ki + 1], 0, 0, qs, 0) for ki in range(Nk)]
         nat.spectral_filter(grid, F64, S, Q[:Nk], bands)
         dagger_rows(Q[:Nk])
@@ -426,6 +497,9 @@ class PSpec:
         b = self.base
 
         def contrib(seeds):
+            if noise == 'philox' and self._custom_sinv:
+                # a caller's S^-1 may synchronise or allocate on the host: no graph capture
+                return self._fisher_from_fields(b.grf_philox(np.asarray(seeds, dtype=np.int64) + int(1e7)))
             if noise == 'philox':
                 cap = self._captured.get(batch)
                 if cap is None:
@@ -555,7 +629,14 @@ class PSpec:
         sna = b.applyAinv(a, invPk0_grid=invPA, input_type='fourier',
                           output_type='fourier' if self.const_mask else 'real')
         scale = 0.5 * b.volume / float(b.gridsize.prod()) ** 2
-        if self.const_mask:
+        if self._custom_sinv:                                            # pspec.py:514-522
+            if self.const_mask:
+                sna = self._sinv(sna, 'fourier', 'fourier') * float(self.mask_mean)
+            else:
+                m = b.to_device_grid(('pk_mask_shot', id(self)), lambda: self.mask_shot, torch.float64)
+                sna = self._sinv(sna * m, 'real', 'fourier')
+            a = self._sinv(a, 'fourier', 'fourier')
+        elif self.const_mask:
             scale *= self.mask_mean
         else:
             m = b.to_device_grid(('pk_mask_shot', id(self)), lambda: self.mask_shot, torch.float64)

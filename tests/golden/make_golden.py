@@ -505,6 +505,72 @@ def local_odd(pb):
     return out
 
 
+def sinv_pair(base, N):
+    """A non-trivial, non-symmetric S^-1 for the custom-weighting fixture: S^-1 x =
+    IFT[w(k) FT[u x]] with w(k) = 1/(1 + (|k|/0.05)^2) and u = 1 + 0.5 sin(2 pi i0/N) along
+    the first grid axis; its transpose is u IFT[w(k) FT[x]].  Both take and return real maps
+    or half spectra as the reference's applySinv does."""
+    w = 1.0 / (1.0 + (np.asarray(base.modk_grid) / 0.05) ** 2)
+    u = (1.0 + 0.5 * np.sin(2 * np.pi * np.arange(N) / N))[:, None, None] * np.ones((N, N, N))
+
+    def sinv(x, input_type="real", output_type="real"):
+        xr = base.to_real(x) if input_type == "fourier" else x
+        y = base.to_fourier(u * xr) * w
+        return y if output_type == "fourier" else base.to_real(y)
+
+    def sinv_t(x, input_type="real", output_type="real"):
+        X = x if input_type == "fourier" else base.to_fourier(x)
+        yr = u * base.to_real(X * w)
+        return base.to_fourier(yr) if output_type == "fourier" else yr
+    return sinv, sinv_t
+
+
+@case
+def custom_sinv(pb):
+    """PSpec with a user S^-1 (sinv_pair): 24^3, L=600, 4 bins, shell-sector mask with
+    mask_shot = 0.5 mask, lognormal data (seed 21) times the mask.  (a) global, CIC window,
+    lmax=2: numerator, Fisher (seed 0), shot noise (seed 1), covariance with [k, P0, P2]
+    (seed 2), theory matrix lmax_theory = 4 (seed 3); (b) constant mask 0.7: numerator,
+    Fisher (seed 4), covariance with [k, P0] (seed 5); (c) local sightline (box centred at
+    (700, 400, 900) Mpc/h), no window, lmax=2: numerator, Fisher (seed 6), shot noise (seed
+    7); (d) applySinv alone (taken as its own transpose), global, Fisher (seed 8)."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    kth = np.linspace(kF, 0.12, 7)
+    mask = _mask24(N, L)
+    kt = np.linspace(0.0, 1.0, 2000)
+    p0 = 3e3 * np.exp(-(kt / 0.25) ** 2) + 200.0
+    p2 = 800.0 * np.exp(-(kt / 0.2) ** 2)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * mask
+    out = dict(N=N, L=L, edges=edges, kth=kth, pk_k=kt, p0=p0, p2=p2)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="mkl")
+    si, st = sinv_pair(base, N)
+    ps = _quiet(pb.PSpec, base, edges, lmax=2, mask=mask, mask_shot=0.5 * mask, applySinv=si, applySinv_transpose=st)
+    out["a_num"] = _quiet(ps.Pk_numerator, d)
+    out["a_f0"] = _quiet(ps.compute_fisher_contribution, 0)
+    out["a_s1"] = _quiet(ps.compute_shot_contribution, 1)
+    out["a_c2"] = _quiet(ps.compute_covariance_contribution, 2, [kt, p0, p2])
+    out["a_f3"], out["a_t3"] = _quiet(ps.compute_theory_contribution, 3, kth, lmax_theory=4)
+    cm = 0.7 * np.ones((N, N, N))
+    ps2 = _quiet(pb.PSpec, base, edges, lmax=2, mask=cm, applySinv=si, applySinv_transpose=st)
+    out["b_num"] = _quiet(ps2.Pk_numerator, synthetic.lognormal(N, L, seed=21).astype(np.float64) * 0.7)
+    out["b_f4"] = _quiet(ps2.compute_fisher_contribution, 4)
+    out["b_c5"] = _quiet(ps2.compute_covariance_contribution, 5, [kt, p0])
+    center = [700.0, 400.0, 900.0]
+    lbase = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, boxcenter=center, sightline="local", backend="mkl")
+    lsi, lst = sinv_pair(lbase, N)
+    lps = _quiet(pb.PSpec, lbase, edges, lmax=2, mask=mask, mask_shot=0.5 * mask, applySinv=lsi,
+                 applySinv_transpose=lst)
+    out["c_num"] = _quiet(lps.Pk_numerator, d)
+    out["c_f6"] = _quiet(lps.compute_fisher_contribution, 6)
+    out["c_s7"] = _quiet(lps.compute_shot_contribution, 7)
+    ps4 = _quiet(pb.PSpec, base, edges, lmax=2, mask=mask, applySinv=si)
+    out["d_f8"] = _quiet(ps4.compute_fisher_contribution, 8)
+    out["center"] = np.asarray(center)
+    return out
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

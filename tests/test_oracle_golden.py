@@ -377,3 +377,52 @@ def test_local_odd_multipoles():
     ps2 = O.OraclePSpec(b, g["edges"], lmax=2, mask=m)
     f, t = ps2.theory_contribution(b.reference_noise(3 + 10 ** 7), g["kth"], lmax_theory=4, include_wideangle=True)
     assert rel(f, g["wf3"]) < TOL and rel(t, g["wt3"]) < TOL
+
+
+def sinv_pair(base, N):
+    """The fixture's S^-1 = IFT w(k) FT u and its transpose u IFT w(k) FT (make_golden.sinv_pair)."""
+    w = 1.0 / (1.0 + (np.asarray(base.modk_grid) / 0.05) ** 2)
+    u = (1.0 + 0.5 * np.sin(2 * np.pi * np.arange(N) / N))[:, None, None] * np.ones((N, N, N))
+
+    def sinv(x, input_type="real", output_type="real"):
+        xr = base.to_real(x) if input_type == "fourier" else x
+        y = base.to_fourier(u * xr) * w
+        return y if output_type == "fourier" else base.to_real(y)
+
+    def sinv_t(x, input_type="real", output_type="real"):
+        X = x if input_type == "fourier" else base.to_fourier(x)
+        yr = u * base.to_real(X * w)
+        return base.to_fourier(yr) if output_type == "fourier" else yr
+    return sinv, sinv_t
+
+
+def test_custom_sinv():
+    """A caller's S^-1 (and S^-dag) in the numerator, Fisher, shot-noise, covariance and
+    theory contributions; global and local sightlines, varying and constant masks."""
+    g = gold("custom_sinv")
+    N, L = int(g["N"]), float(g["L"])
+    m = mask24(N, L)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * m
+    pk_cov = [g["pk_k"], g["p0"], g["p2"]]
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic")
+    si, st = sinv_pair(b, N)
+    ps = O.OraclePSpec(b, g["edges"], lmax=2, mask=m, applySinv=si, applySinv_transpose=st)
+    n = lambda s, bb: bb.reference_noise(s + 10 ** 7)
+    assert rel(ps.numerator(d, "Sinv"), g["a_num"]) < TOL
+    assert rel(ps.fisher_contribution(n(0, b)), g["a_f0"]) < TOL
+    assert rel(ps.shot_contribution(n(1, b), mask_shot=0.5 * m), g["a_s1"]) < TOL
+    assert rel(ps.covariance_contribution(n(2, b), pk_cov, mask_shot=0.5 * m), g["a_c2"]) < TOL
+    f, t = ps.theory_contribution(n(3, b), g["kth"], lmax_theory=4)
+    assert rel(f, g["a_f3"]) < TOL and rel(t, g["a_t3"]) < TOL
+    ps2 = O.OraclePSpec(b, g["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)), applySinv=si, applySinv_transpose=st)
+    assert rel(ps2.numerator(synthetic.lognormal(N, L, seed=21).astype(np.float64) * 0.7, "Sinv"), g["b_num"]) < TOL
+    assert rel(ps2.fisher_contribution(n(4, b)), g["b_f4"]) < TOL
+    assert rel(ps2.covariance_contribution(n(5, b), pk_cov[:2]), g["b_c5"]) < TOL
+    lb = O.OracleBase([L] * 3, [N] * 3, boxcenter=g["center"], sightline="local")
+    lsi, lst = sinv_pair(lb, N)
+    lps = O.OraclePSpec(lb, g["edges"], lmax=2, mask=m, applySinv=lsi, applySinv_transpose=lst)
+    assert rel(lps.numerator(d, "Sinv"), g["c_num"]) < TOL
+    assert rel(lps.fisher_contribution(n(6, lb)), g["c_f6"]) < TOL
+    assert rel(lps.shot_contribution(n(7, lb), mask_shot=0.5 * m), g["c_s7"]) < TOL
+    ps4 = O.OraclePSpec(b, g["edges"], lmax=2, mask=m, applySinv=si)
+    assert rel(ps4.fisher_contribution(n(8, b)), g["d_f8"]) < TOL
