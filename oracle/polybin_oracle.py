@@ -810,8 +810,11 @@ def all_bins_list(k_bins, lmax, k_bins_squeeze=None, include_partial_triangles=F
 class OracleBSpec:
     def __init__(self, base, k_bins, lmax=0, mask=None, k_bins_squeeze=None,
                  include_partial_triangles=False, mask_IC=None, add_GIC=False, add_RIC=False,
-                 radial_bins_RIC=None):
+                 radial_bins_RIC=None, applySinv=None, applySinv_transpose=None):
         self.base = base
+        # S^-1 and S^-dag (bspec.py:117-124)
+        self.sinv = applySinv or trivial_sinv(base)
+        self.sinv_t = applySinv_transpose or (applySinv if applySinv is not None else trivial_sinv(base))
         self.k_bins = np.asarray(k_bins, dtype=np.float64)
         self.k_bins_squeeze = self.k_bins.copy() if k_bins_squeeze is None else np.asarray(k_bins_squeeze, dtype=np.float64)
         self.lmax = lmax
@@ -897,14 +900,17 @@ class OracleBSpec:
         return g
 
     def weighted_data(self, data, filtering="ideal"):
-        """S^-1 d in Fourier space (bspec.py:912-929); trivial S^-1 for 'Sinv'."""
+        """S^-1 d in Fourier space (bspec.py:912-929)."""
         b = self.base
-        x = b.to_fourier(np.asarray(data, dtype=np.float64))
+        data = np.asarray(data, dtype=np.float64)
+        x = b.to_fourier(data)
         if b.pixel_window != "none":
             x = b.div_fourier(x, b.pixel_window_grid)
         if filtering == "ideal":
-            x = x * self.invPk0 / self.cube_mask_mean ** (1.0 / 3.0)
-        return x
+            return x * self.invPk0 / self.cube_mask_mean ** (1.0 / 3.0)
+        if b.pixel_window != "none":
+            return self.sinv(x, "fourier", "fourier")
+        return self.sinv(data, "real", "fourier")
 
     def numerator(self, data, filtering="ideal", sym=None, sims=None):
         """_compute_bk_numerator (bspec.py:895-983); with `sims` (a list of bias-simulation
@@ -942,30 +948,31 @@ class OracleBSpec:
         a2 = b.grf_from_noise(*noise2, Pk_grid=draw)
         r1 = b.to_real(b.applyAinv_fourier(a1, b.Pk0_grid))              # 779-780
         r2 = b.to_real(b.applyAinv_fourier(a2, b.Pk0_grid))
-        gA, gB = self.g_maps(a1), self.g_maps(a2)
-        gC = self.g_maps(b.to_fourier(r1 * r2 * mask_shot))             # 781
+        gA = self.g_maps(self.sinv(a1, "fourier", "fourier"))          # 788-790
+        gB = self.g_maps(self.sinv(a2, "fourier", "fourier"))
+        gC = self.g_maps(self.sinv(r1 * r2 * mask_shot, "real", "fourier"))   # 781
         norm = b.volume / b.gridsize.prod() / sym
         cubic = self.bshot_sum(gA, gB, gC) * norm / 6.0                  # 849-850
         if cubic_only:
             return cubic
         g = self.g_maps(self.weighted_data(data, "Sinv"))               # 730-768
-        gD = self.g_maps(b.to_fourier(r1 * data2))                       # 783-784
-        gE = self.g_maps(b.to_fourier(r2 * data2))
+        gD = self.g_maps(self.sinv(r1 * data2, "real", "fourier"))      # 783-784
+        gE = self.g_maps(self.sinv(r2 * data2, "real", "fourier"))
         quad = 0.5 * (self.bshot_sum(g, gA, gD) + self.bshot_sum(g, gB, gE)) * norm / 2.0   # 853-856
         return quad - 2.0 * cubic
 
     # bias simulations for the linear term (bspec.py:281-410)
     def sim_spectrum(self, sim, input_type="real"):
-        """_process_sim before the g-maps (bspec.py:288-300): the Fourier map of one
-        simulation, divided by the pixel window when there is one (trivial S^-1)."""
+        """_process_sim before the g-maps (bspec.py:288-300): S^-1 of one simulation in
+        Fourier space, the pixel window divided out first when there is one."""
         b = self.base
+        if b.pixel_window == "none":
+            return self.sinv(sim, input_type, "fourier")
         if input_type == "real":
             x = b.to_fourier(np.asarray(sim, dtype=np.float64))
         else:
             x = np.array(sim, dtype=np.complex128)
-        if b.pixel_window != "none":
-            x = x / b.pixel_window_grid
-        return x
+        return self.sinv(x / b.pixel_window_grid, "fourier", "fourier")
 
     def generated_sim(self, ii, Pk_grid=None):
         """load_sim_data of generate_sims (bspec.py:377-392): the GRF of seed 1e5 + ii, times
@@ -1063,10 +1070,10 @@ class OracleBSpec:
             if xi is not None:
                 return cov_filter(b, x_fourier if self.const_mask else x_real, not self.const_mask, xi,
                                   self.const_mask, getattr(self, "mask_mean", None),
-                                  None if self.const_mask else self.point, mask_shot)
+                                  None if self.const_mask else self.point, mask_shot, self.sinv, self.sinv_t)
             if self.const_mask:
-                return self.mask_mean * x_fourier
-            return b.to_fourier(self.point(x_real))
+                return self.mask_mean * self.sinv(x_fourier, "fourier", "fourier")
+            return self.sinv(self.point(x_real), "real", "fourier")
 
         def g_sets(w1, w2):
             g1 = np.asarray([b.to_real(b.fourier_filter(w1, 0, ks[i], ks[i + 1])) for i in range(nks)])

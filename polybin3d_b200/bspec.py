@@ -124,8 +124,13 @@ class BSpec:
         if type(mask_shot) != type(None):
             self.mask_shot = mask_shot.astype(np.float64)
 
-        if self.applySinv is not None:
-            raise NotImplementedError("backend='cuda' implements the trivial S^-1 weighting (applySinv=None)")
+        # S^-1 (bspec.py:117-124): the trivial filter, or the caller's, applied to device maps;
+        # its transpose (used by the covariance) defaults to itself
+        self._custom_sinv = self.applySinv is not None
+        if self._custom_sinv and type(self.applySinv_transpose) != type(lambda x: x):
+            self.applySinv_transpose = self.applySinv
+            if verb:
+                print("## Caution: assuming S^-1 is Hermitian!")
         # integral constraints (bspec.py:126-136)
         if self.add_GIC:
             if verb:
@@ -139,8 +144,9 @@ class BSpec:
                 print("Accounting for radial integral constraint across %d bins" % (len(radial_bins_RIC) - 1))
             self.radial_bins_RIC = np.asarray(radial_bins_RIC, dtype=np.float64)
         self._pt = None
-        self.applySinv = self.base.applySinv_trivial
-        self.applySinv_transpose = self.base.applySinv_trivial
+        if not self._custom_sinv:
+            self.applySinv = self.base.applySinv_trivial
+            self.applySinv_transpose = self.base.applySinv_trivial
 
         # fiducial weighting 1/P_fid (bspec.py:138-156); None -> unit weight on every binned mode
         self._unit_w = (type(self.Pk_fid) != str and (np.asarray(self.Pk_fid) == None).all()) or \
@@ -441,6 +447,11 @@ class BSpec:
         if filtering == 'ideal':
             w = self._data_weight(rd)
             scale = 1.0 / self.cube_mask_mean ** (1. / 3.)
+        elif self._custom_sinv:                                          # bspec.py:912-929
+            cd = torch.complex128 if rd == torch.float64 else torch.complex64
+            xk = self._sinv_data(data).to(cd)
+            w = None
+            scale = 1.0
         else:
             w = None
             if b.pixel_window != 'none':
@@ -508,6 +519,8 @@ class BSpec:
         precision.  The g-maps are synthesised from it when the linear term is formed, so a
         simulation holds one half spectrum of device memory instead of Nl x Nk maps."""
         b = self.base
+        if self._custom_sinv:
+            return self._sinv_data(sim, input_type).to(b.complex_dtype)
         if input_type == 'real':
             xk = b.to_fourier(b.as_device(sim))
         else:
@@ -535,15 +548,46 @@ class BSpec:
         if self.const_mask:
             out = torch.empty_like(a)
             nat.spectral_filter(b.grid, F64, a, out, [(0, -1.0, np.inf, 0, 0, float(self.mask_mean), 0)])
+            if self._custom_sinv:
+                out = self._sinv(out, 'fourier', 'fourier')
             return out.to(b.complex_dtype)
         s = b.to_real(a)
         self._pointing()(s, False, out=s)
+        if self._custom_sinv:
+            y = self._sinv(b.to_fourier(s), 'fourier', 'fourier') if b.pixel_window != 'none' else \
+                self._sinv(s, 'real', 'fourier')
+            return y.to(b.complex_dtype)
         return b.to_fourier(s).to(b.complex_dtype)
 
     def _inv_window(self):
         W = self.base.pixel_window_grid
         nz = W != 0
         return np.where(nz, 1. / np.where(nz, W, 1.), 0.)
+
+    def _sinv(self, x, input_type, output_type, transpose=False):
+        """The caller's S^-1 (or S^-dag) on one device map; the result as a contiguous FP64
+        device tensor (half spectrum or real map)."""
+        f = self.applySinv_transpose if transpose else self.applySinv
+        y = f(x, input_type=input_type, output_type=output_type)
+        if not isinstance(y, torch.Tensor):
+            y = torch.as_tensor(np.ascontiguousarray(y))
+        dt = torch.complex128 if output_type == 'fourier' else torch.float64
+        return y.to(device=self.base.device, dtype=dt).contiguous()
+
+    def _sinv_data(self, data, input_type='real'):
+        """S^-1 of data or of a simulation in Fourier space with the caller's S^-1, the pixel
+        window divided out first when there is one (bspec.py:287-300, 733-742, 912-929)."""
+        b = self.base
+        if b.pixel_window == 'none':
+            x = b.as_device(data, torch.float64) if input_type == 'real' else data
+            return self._sinv(x, input_type, 'fourier')
+        if input_type == 'real':
+            xk = b.to_fourier(b.as_device(data, torch.float64))
+        else:
+            xk = torch.as_tensor(data, device=b.device).to(torch.complex128).contiguous().clone()
+        w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), torch.float64)
+        nat.spectral_filter(b.grid, nat.PB_F64, xk, xk, [(0, -1.0, np.inf, 0, 0, 1.0, 1)], w=w)
+        return self._sinv(xk, 'fourier', 'fourier')
 
     def Bk_numerator(self, data, include_linear_term=True, verb=False):
         """Numerator of the unwindowed estimator (bspec.py:429-439); the linear term needs
@@ -767,6 +811,23 @@ class BSpec:
         """S^-1 P (xi None) or its covariance form S^-1 [P xi P^dag + N] S^-dag on a block of
         half spectra prescaled as `_apply_filter_spectra` takes them (1 instead of the mask
         mean for the covariance form), 64 maps at a time; in place."""
+        if self._custom_sinv:
+            # the caller's S^-1, one map at a time as the reference applies it (bspec.py:499-519);
+            # R holds unscaled spectra here
+            b = self.base
+            for r in range(R.shape[0]):
+                if xi is not None:
+                    x = R[r] if self.const_mask else b.to_real(R[r])
+                    R[r] = covariance.cov_custom(b, x, not self.const_mask, xi, self.const_mask,
+                                                 getattr(self, "mask_mean", None),
+                                                 None if self.const_mask else self._pointing(), mask_shot,
+                                                 lambda y, i, o: self._sinv(y, i, o),
+                                                 lambda y, i, o: self._sinv(y, i, o, transpose=True))
+                elif self.const_mask:
+                    R[r] = self._sinv(R[r], 'fourier', 'fourier') * float(self.mask_mean)
+                else:
+                    R[r] = self._sinv(self._pointing()(b.to_real(R[r]), False), 'real', 'fourier')
+            return R
         if xi is None:
             return self._apply_filter_spectra(R, True)
         m = None if self.const_mask else self._pointing()
@@ -797,7 +858,7 @@ class BSpec:
         kpos = {k: i for i, k in enumerate(keys)}
         FT = self._key_fts(G1, G2, keys)
         del G1, G2
-        qs = invN if not self.const_mask else (1.0 if xi is not None else self.mask_mean)
+        qs = 1.0 if self._custom_sinv else (invN if not self.const_mask else (1.0 if xi is not None else self.mask_mean))
         Q = torch.empty((self.N_bins,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
         # leg b3 carries L_l; with the local sightline that leg is applied in real space below
         leg1 = [(kpos[(r[0], r[1], 0)], ks[r[2]], ks[r[2] + 1], 0 if local else r[3], 0,
@@ -832,7 +893,10 @@ class BSpec:
         del FT
         Q = self._filter_rows(Q, xi, mask_shot)
         # --- rows from Q[S^-1 P a] (compute_Q 'Sinv', bspec.py:528-597)
-        if self.const_mask:
+        if self._custom_sinv:
+            ws = torch.stack([a1.reshape(b.nhalf_shape), a2.reshape(b.nhalf_shape)]).to(torch.complex128)
+            ws = self._filter_rows(ws, xi, mask_shot)
+        elif self.const_mask:
             ws = torch.empty((2,) + b.nhalf_shape, dtype=torch.complex128, device=b.device)
             nat.spectral_filter(b.grid, F64, a1, ws[0:1], [(0, -1.0, np.inf, 0, 0, qs, 0)])
             nat.spectral_filter(b.grid, F64, a2, ws[1:2], [(0, -1.0, np.inf, 0, 0, qs, 0)])
@@ -889,6 +953,11 @@ class BSpec:
         b = self.base
 
         def contrib(seeds):
+            if noise == 'philox' and self._custom_sinv:
+                # a caller's S^-1 may synchronise or allocate on the host: no graph capture
+                return torch.cat([self._fisher_from_fields(b.grf_philox(np.asarray([s], dtype=np.int64) + int(1e7)),
+                                                           b.grf_philox(np.asarray([s], dtype=np.int64) + int(2e7)))[None]
+                                  for s in seeds])
             if noise == 'philox':
                 if self._captured is None:
                     self._captured = realisations.CapturedBatch(
@@ -969,8 +1038,12 @@ class BSpec:
             prod = nat.elementwise(nat.PB_EW_MUL, x, y)
             if z is not None:
                 nat.elementwise(nat.PB_EW_MUL, prod, z, out=prod, y_period=b.nreal)
+            if self._custom_sinv:                                        # bspec.py:781-785
+                return self._sinv(prod, 'real', 'fourier')
             return b.to_fourier(prod)
 
+        if self._custom_sinv:                                            # bspec.py:788-790
+            a = [self._sinv(ai, 'fourier', 'fourier') for ai in a]
         maps_of(a[0], sets[0])
         maps_of(a[1], sets[1])
         maps_of(product_spectrum(r[0], r[1], mshot), sets[2])
@@ -978,10 +1051,13 @@ class BSpec:
         cubic = self._set_sums('bshot', X, n, perms).cpu().numpy() * norm / 6.
         if cubic_only:
             return cubic
-        xk = b.to_fourier(b.as_device(data))
         w = None
-        if b.pixel_window != 'none':
-            w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), xk.real.dtype)
+        if self._custom_sinv:                                            # bspec.py:733-742
+            xk = self._sinv_data(data)
+        else:
+            xk = b.to_fourier(b.as_device(data))
+            if b.pixel_window != 'none':
+                w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), xk.real.dtype)
         d2 = b.as_device(data2, torch.float64)
         # (g, a1-maps, D) in the three sets, then (a2-maps, g, E)
         maps_of(xk, sets[1], w)

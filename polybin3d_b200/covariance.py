@@ -101,3 +101,22 @@ def cov_rows(base, R, xi, const_mask, mask_mean, point, mask_shot, real=None):
     u.add_(nat.elementwise(nat.PB_EW_MUL, sid, mask_shot, out=t, y_period=base.nreal))
     base.n_FFTs_forward += nrow
     return base.fft_r2c(u, out=R)
+
+
+def cov_custom(base, x, real, xi, const_mask, mask_mean, point, mask_shot, sinv, sinv_t):
+    """S^-1 [P xi P^dag + N] S^-dag of one map with a caller's S^-1 (pspec.py:277-290,
+    307-323; bspec.py:507-518): sinv / sinv_t(x, input_type, output_type) apply S^-1 and
+    S^-dag; x a real map if `real`, else a half spectrum; returns a half spectrum."""
+    it = 'real' if real else 'fourier'
+    if const_mask:
+        if len(xi) > 1:
+            raise ValueError("local multipoles of Pk_cov need a varying mask (the reference applies xi "
+                             "without a real-space map for a constant mask)")
+        sid = sinv_t(x, it, 'fourier')
+        mm = float(mask_mean)
+        return sinv(sid * (xi[0] * (mm * mm) + mm), 'fourier', 'fourier')
+    sid = sinv_t(x, it, 'real')
+    t = point(sid, True)
+    base.n_FFTs_forward += 1
+    u = xi_real(base, base.fft_r2c(t)[None], t[None], xi)[0]
+    return sinv(point(u, False) + sid * mask_shot, 'real', 'fourier')

@@ -571,6 +571,39 @@ def custom_sinv(pb):
     return out
 
 
+@case
+def bk_custom_sinv(pb):
+    """BSpec with a user S^-1 (sinv_pair): 24^3, L=600, 4 bins, lmax=2, CIC window,
+    shell-sector mask with mask_shot = 0.5 mask, lognormal data (seed 21) times the mask:
+    numerator without and with the linear term (generate_sims(2)), Fisher (seed 0),
+    shot noise with data2 = 0.7 data (seed 1), covariance with [k, P0, P2] (seed 2); and the
+    constant mask 0.7: numerator, Fisher (seed 3)."""
+    N, L = 24, 600.0
+    kF = 2 * np.pi / L
+    edges = np.linspace(kF, 0.11, 5)
+    mask = _mask24(N, L)
+    kt = np.linspace(0.0, 1.0, 2000)
+    p0 = 3e3 * np.exp(-(kt / 0.25) ** 2) + 200.0
+    p2 = 800.0 * np.exp(-(kt / 0.2) ** 2)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * mask
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="mkl")
+    si, st = sinv_pair(base, N)
+    bs = _quiet(pb.BSpec, base, edges, lmax=2, mask=mask, mask_shot=0.5 * mask, applySinv=si, applySinv_transpose=st)
+    out = dict(N=N, L=L, edges=edges, pk_k=kt, p0=p0, p2=p2, bins=bs.all_bins)
+    out["cub"] = _quiet(bs.Bk_numerator, d, include_linear_term=False)
+    out["sym"] = bs.sym_factor
+    _quiet(bs.generate_sims, 2)
+    out["num"] = _quiet(bs.Bk_numerator, d)
+    out["f0"] = _quiet(bs.compute_fisher_contribution, 0)
+    out["s1"] = _quiet(bs.compute_shot_contribution, 1, data=d, data2=0.7 * d)
+    out["c2"] = _quiet(bs.compute_covariance_contribution, 2, [kt, p0, p2])
+    bs2 = _quiet(pb.BSpec, base, edges, lmax=2, mask=0.7 * np.ones((N, N, N)), applySinv=si, applySinv_transpose=st)
+    out["b_cub"] = _quiet(bs2.Bk_numerator, synthetic.lognormal(N, L, seed=21).astype(np.float64) * 0.7,
+                          include_linear_term=False)
+    out["b_f3"] = _quiet(bs2.compute_fisher_contribution, 3)
+    return out
+
+
 def main(names=None):
     pb = load_reference()
     for name, fn in CASES.items():

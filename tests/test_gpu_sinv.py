@@ -92,3 +92,31 @@ def test_custom_sinv_local(g):
     assert rel(ps.Pk_numerator(d), g["c_num"]) < 1e-10
     assert rel(ps.compute_fisher_contribution(6), g["c_f6"]) < 1e-8
     assert rel(ps.compute_shot_contribution(7), g["c_s7"]) < 1e-8
+
+
+def test_custom_sinv_bispectrum():
+    """BSpec with the caller's S^-1 (tests/golden/bk_custom_sinv.npz, lmax=2, CIC window):
+    numerator without and with the linear term of generate_sims(2), Fisher, shot noise,
+    covariance; and a constant mask."""
+    import polybin3d_b200 as pb
+    g = np.load(os.path.join(GOLD, "bk_custom_sinv.npz"))
+    N, L = int(g["N"]), float(g["L"])
+    m = mask24(N, L)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * m
+    b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="cic", backend="cuda")
+    si, st = sinv_pair(b, N)
+    bs = quiet(pb.BSpec, b, g["edges"], lmax=2, mask=m, mask_shot=0.5 * m, applySinv=si, applySinv_transpose=st)
+    assert np.array_equal(bs.all_bins, g["bins"])
+    cub = quiet(bs.Bk_numerator, d, include_linear_term=False)
+    assert rel(bs.sym_factor, g["sym"]) < 1e-12
+    assert rel(cub, g["cub"]) < 1e-10
+    quiet(bs.generate_sims, 2)
+    num = quiet(bs.Bk_numerator, d)
+    assert rel(num, g["num"]) < 1e-10 and rel(num - cub, g["num"] - g["cub"]) < 1e-8
+    assert rel(quiet(bs.compute_fisher_contribution, 0), g["f0"]) < 1e-8
+    assert rel(quiet(bs.compute_shot_contribution, 1, data=d, data2=0.7 * d), g["s1"]) < 1e-8
+    assert rel(quiet(bs.compute_covariance_contribution, 2, [g["pk_k"], g["p0"], g["p2"]]), g["c2"]) < 1e-8
+    bs2 = quiet(pb.BSpec, b, g["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)), applySinv=si, applySinv_transpose=st)
+    d2 = synthetic.lognormal(N, L, seed=21).astype(np.float64) * 0.7
+    assert rel(quiet(bs2.Bk_numerator, d2, include_linear_term=False), g["b_cub"]) < 1e-10
+    assert rel(quiet(bs2.compute_fisher_contribution, 3), g["b_f3"]) < 1e-8

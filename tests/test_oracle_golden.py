@@ -426,3 +426,31 @@ def test_custom_sinv():
     assert rel(lps.shot_contribution(n(7, lb), mask_shot=0.5 * m), g["c_s7"]) < TOL
     ps4 = O.OraclePSpec(b, g["edges"], lmax=2, mask=m, applySinv=si)
     assert rel(ps4.fisher_contribution(n(8, b)), g["d_f8"]) < TOL
+
+
+def test_bk_custom_sinv():
+    """BSpec with a caller's S^-1: numerator with and without the linear term, Fisher, shot
+    noise, covariance; and a constant mask."""
+    g = gold("bk_custom_sinv")
+    N, L = int(g["N"]), float(g["L"])
+    m = mask24(N, L)
+    d = synthetic.lognormal(N, L, seed=21).astype(np.float64) * m
+    b = O.OracleBase([L] * 3, [N] * 3, pixel_window="cic")
+    si, st = sinv_pair(b, N)
+    bs = O.OracleBSpec(b, g["edges"], lmax=2, mask=m, applySinv=si, applySinv_transpose=st)
+    assert np.array_equal(bs.all_bins, g["bins"])
+    sym = g["sym"]
+    cub = bs.numerator(d, "Sinv", sym=sym)
+    assert rel(cub, g["cub"]) < TOL
+    sims = [bs.generated_sim(i) for i in range(2)]
+    num = bs.numerator(d, "Sinv", sym=sym, sims=sims)
+    assert rel(num, g["num"]) < TOL and rel(num - cub, g["num"] - g["cub"]) < 1e-8
+    n = lambda s: (b.reference_noise(s + 10 ** 7), b.reference_noise(s + 2 * 10 ** 7))
+    assert rel(bs.fisher_contribution(*n(0), sym=sym), g["f0"]) < TOL
+    assert rel(bs.shot_contribution(*n(1), 0.5 * m, data=d, data2=0.7 * d, sym=sym), g["s1"]) < TOL
+    pk_cov = [g["pk_k"], g["p0"], g["p2"]]
+    assert rel(bs.covariance_contribution(*n(2), pk_cov, mask_shot_2pt=0.5 * m, sym=sym), g["c2"]) < TOL
+    bs2 = O.OracleBSpec(b, g["edges"], lmax=2, mask=0.7 * np.ones((N, N, N)), applySinv=si, applySinv_transpose=st)
+    d2 = synthetic.lognormal(N, L, seed=21).astype(np.float64) * 0.7
+    assert rel(bs2.numerator(d2, "Sinv", sym=sym), g["b_cub"]) < TOL
+    assert rel(bs2.fisher_contribution(*n(3), sym=sym), g["b_f3"]) < TOL
