@@ -7,7 +7,6 @@ import io
 
 import numpy as np
 import pytest
-import torch
 
 from polybin3d_b200 import synthetic
 

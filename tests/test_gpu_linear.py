@@ -13,7 +13,6 @@ import os
 
 import numpy as np
 import pytest
-import torch
 
 from polybin3d_b200 import synthetic
 
