@@ -158,13 +158,22 @@ class BSpec:
         self._captured = None
         self._shell_modes = None
         self.map_grid = self._dealiased_grid() if dealias else tuple(int(n) for n in base.gridsize)
-        # real harmonics of positions and wavevectors (bspec.py:158-169): device grids, shared
-        # with the ones the local-sightline maps use
-        self.Ylm_real = None
-        self.Ylm_fourier = None
-        if base.sightline == 'local' and self.lmax > 0:
-            self.Ylm_real = {l: base.harmonics._grid('r', l, torch.float64) for l in range(2, self.lmax + 1, 2)}
-            self.Ylm_fourier = {l: base.harmonics._grid('k', l, torch.float64) for l in range(2, self.lmax + 1, 2)}
+
+    def _ylm(self, kind):
+        """Real harmonics of positions ('r') or wavevectors ('k') by even l, as the
+        reference's Ylm_real / Ylm_fourier (bspec.py:158-169): FP64 device grids, made on
+        first use; None unless the sightline is local and lmax > 0."""
+        if self.base.sightline != 'local' or self.lmax == 0:
+            return None
+        return {l: self.base.harmonics._grid(kind, l, torch.float64) for l in range(2, self.lmax + 1, 2)}
+
+    @property
+    def Ylm_real(self):
+        return self._ylm('r')
+
+    @property
+    def Ylm_fourier(self):
+        return self._ylm('k')
 
     # ------------------------------------------------------------------------------
     # binning helpers (bspec.py:171-220)

@@ -97,15 +97,25 @@ class PSpec:
         if not self._custom_sinv:
             self.applySinv = self.base.applySinv_trivial
             self.applySinv_transpose = self.base.applySinv_trivial
-        # real harmonics of positions and wavevectors (pspec.py:86-91): device grids, shared
-        # with the ones the local-sightline multipoles use
-        self.Ylm_real = None
-        self.Ylm_fourier = None
-        if self.base.sightline == 'local' and self.lmax > 0:
-            ls = range(1, self.lmax + 1) if self.odd_l else range(2, self.lmax + 1, 2)
-            self.Ylm_real = {l: self.base.harmonics._grid('r', l, torch.float64) for l in ls}
-            self.Ylm_fourier = {l: self.base.harmonics._grid('k', l, torch.float64) for l in ls}
         self._captured = {}
+
+    def _ylm(self, kind):
+        """Real harmonics of positions ('r') or wavevectors ('k') by l, as the reference's
+        Ylm_real / Ylm_fourier (pspec.py:86-91): FP64 device grids, made on first use and
+        shared with the ones the local-sightline multipoles use; None unless the sightline
+        is local and lmax > 0."""
+        if self.base.sightline != 'local' or self.lmax == 0:
+            return None
+        ls = range(1, self.lmax + 1) if self.odd_l else range(2, self.lmax + 1, 2)
+        return {l: self.base.harmonics._grid(kind, l, torch.float64) for l in ls}
+
+    @property
+    def Ylm_real(self):
+        return self._ylm('r')
+
+    @property
+    def Ylm_fourier(self):
+        return self._ylm('k')
 
     def get_ks(self):
         """Central k of each bin (pspec.py:122-128)."""
