@@ -8,7 +8,12 @@
 # -march=broadwell pin so the object runs on any x86-64 host; libmvec/libm as there.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-SRC="${PB_REFERENCE_ROOT:-/root/reference}/PolyBin3D/cython/utils.pyx"
+# PB_REFERENCE_ROOT: the reference tree's root (the directory holding PolyBin3D/); required
+if [ -z "${PB_REFERENCE_ROOT:-}" ]; then
+    echo "build_ref: PB_REFERENCE_ROOT not set; keeping prebuilt $HERE/_ref" >&2
+    exit 0
+fi
+SRC="$PB_REFERENCE_ROOT/PolyBin3D/cython/utils.pyx"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC" ]; then
     echo "build_ref: reference source not present; keeping prebuilt $OUT" >&2

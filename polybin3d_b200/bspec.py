@@ -960,6 +960,12 @@ class BSpec:
         if not hasattr(self, 'sym_factor'):
             self._compute_symmetry_factor()
         b = self.base
+        feed = None
+        if noise == 'reference' and realisations.prefetch_pays(2 * N_it, b.gridsize):
+            # the reference's two draws per seed for this rank's seeds, made ahead on host workers
+            rank, size = realisations.world(group)
+            feed = realisations.noise_pool(b.gridsize).stream(
+                [s + off for s in realisations.seeds_of_rank(N_it, rank, size) for off in (int(1e7), int(2e7))])
 
         def contrib(seeds):
             if noise == 'philox' and self._custom_sinv:
@@ -973,6 +979,13 @@ class BSpec:
                         lambda sd: self._fisher_from_fields(b.grf_philox(sd + int(1e7)),
                                                             b.grf_philox(sd + int(2e7)))[None], 1, b)
                 return torch.cat([self._captured.run([s]) for s in seeds])
+            if feed is not None:
+                out = []
+                for _ in seeds:
+                    nre, nim = feed.take(2, b.device)
+                    out.append(self._fisher_from_fields(b.grf_from_noise(nre[0], nim[0]),
+                                                        b.grf_from_noise(nre[1], nim[1]))[None])
+                return torch.cat(out)
             return np.stack([self.compute_fisher_contribution(s, verb=verb) for s in seeds])
 
         def progress(seeds):

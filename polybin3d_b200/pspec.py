@@ -18,7 +18,7 @@ class PSpec:
     """Power spectrum estimators (pspec.py:10-26 for the inputs)."""
 
     def __init__(self, base, k_bins, lmax=2, mask=None, applySinv=None, odd_l=False, add_GIC=False, mask_IC=None,
-                 add_RIC=False, radial_bins_RIC=[], mask_shot=None, applySinv_transpose=None, verb=True):
+                 add_RIC=False, radial_bins_RIC=[], mask_shot=None, applySinv_transpose=None, *, verb=True):
         self.base = base
         self.applySinv = applySinv
         self.k_bins = np.asarray(k_bins)
@@ -505,6 +505,12 @@ class PSpec:
         each batch of realisations replayed from one captured CUDA graph."""
         assert noise in ('reference', 'philox'), "noise must be 'reference' or 'philox'"
         b = self.base
+        feed = None
+        if noise == 'reference' and realisations.prefetch_pays(N_it, b.gridsize):
+            # the reference's draws for this rank's seeds, made ahead on host workers
+            rank, size = realisations.world(group)
+            feed = realisations.noise_pool(b.gridsize).stream(
+                [s + int(1e7) for s in realisations.seeds_of_rank(N_it, rank, size)])
 
         def contrib(seeds):
             if noise == 'philox' and self._custom_sinv:
@@ -517,9 +523,12 @@ class PSpec:
                         lambda sd: self._fisher_from_fields(b.grf_philox(sd + int(1e7))), batch, b)
                     self._captured[batch] = cap
                 return cap.run(seeds)
-            noise_ = [b.reference_noise(s + int(1e7)) for s in seeds]
-            nre = torch.as_tensor(np.stack([n[0] for n in noise_]), device=b.device)
-            nim = torch.as_tensor(np.stack([n[1] for n in noise_]), device=b.device)
+            if feed is not None:
+                nre, nim = feed.take(len(seeds), b.device)
+            else:
+                noise_ = [b.reference_noise(s + int(1e7)) for s in seeds]
+                nre = torch.as_tensor(np.stack([n[0] for n in noise_]), device=b.device)
+                nim = torch.as_tensor(np.stack([n[1] for n in noise_]), device=b.device)
             return self._fisher_from_fields(b.grf_from_noise(nre, nim))
 
         def progress(seeds):

@@ -9,6 +9,14 @@ it is bit-identical (the exchange is N_it x N_bins^2 FP64 values: 10.5 MB for 32
 realisations of 203 bins).
 Without an initialised process group (or with one rank) nothing is exchanged.
 """
+import atexit
+import multiprocessing
+import os
+from collections import deque
+from concurrent.futures import ProcessPoolExecutor
+from multiprocessing import shared_memory
+
+import numpy as np
 import torch
 
 from . import _native as nat
@@ -17,6 +25,112 @@ try:
     import torch.distributed as dist
 except ImportError:  # pragma: no cover
     dist = None
+
+
+# --------------------------------------------------------------------------------------
+# the reference's white noise, drawn ahead on host worker processes
+# --------------------------------------------------------------------------------------
+def _draw_reference_noise(shm_name, seed, shape):
+    """Worker: np.random.seed(seed); randn(*shape) twice (PolyBin3D/base.py:315-316, 332),
+    written into the shared-memory slot `shm_name` as [re, im]."""
+    shm = shared_memory.SharedMemory(name=shm_name)
+    try:
+        out = np.ndarray((2,) + tuple(shape), dtype=np.float64, buffer=shm.buf)
+        rs = np.random.RandomState(seed)  # the legacy global generator re-seeded with `seed`
+        out[0] = rs.randn(*shape)
+        out[1] = rs.randn(*shape)
+        del out
+    finally:
+        shm.close()
+    return seed
+
+
+class NoisePool:
+    """Spawned worker processes drawing the reference's MT19937 white noise into
+    shared-memory slots.  The draw (two legacy Gaussian arrays per realisation) is
+    single-threaded numpy in the reference and bounds a Monte Carlo loop fed with
+    reference-identical noise; here W processes draw the realisations ahead of the one the
+    device is working on.  Workers run numpy only (no CUDA), started with `spawn`."""
+
+    def __init__(self, shape, workers=None):
+        self.shape = tuple(int(n) for n in shape)
+        self.workers = workers or max(1, min(16, (os.cpu_count() or 2) - 1))
+        self.exe = ProcessPoolExecutor(max_workers=self.workers, mp_context=multiprocessing.get_context("spawn"))
+        nbytes = 2 * int(np.prod(self.shape)) * 8
+        self.slots = [shared_memory.SharedMemory(create=True, size=nbytes) for _ in range(2 * self.workers)]
+        self.free = list(range(len(self.slots)))
+        atexit.register(self.close)
+
+    def close(self):
+        if self.exe is not None:
+            self.exe.shutdown(wait=True, cancel_futures=True)
+            self.exe = None
+        for s in self.slots:
+            try:
+                s.close()
+                s.unlink()
+            except FileNotFoundError:
+                pass
+        self.slots = []
+
+    def stream(self, seeds):
+        return NoiseFeed(self, seeds)
+
+
+class NoiseFeed:
+    """Noise for `seeds` in order: take(n, device) returns the next n draws as device FP64
+    tensors (re, im) of shape (n, *grid); the freed slots go to the draws further ahead."""
+
+    def __init__(self, pool, seeds):
+        self.pool, self.todo, self.inflight = pool, deque(int(s) for s in seeds), deque()
+        self._fill()
+
+    def _fill(self):
+        p = self.pool
+        while self.todo and p.free:
+            slot = p.free.pop()
+            seed = self.todo.popleft()
+            fut = p.exe.submit(_draw_reference_noise, p.slots[slot].name, seed, p.shape)
+            self.inflight.append((seed, slot, fut))
+
+    def take(self, n, device):
+        p = self.pool
+        re = torch.empty((n,) + p.shape, dtype=torch.float64, device=device)
+        im = torch.empty_like(re)
+        for i in range(n):
+            if not self.inflight:
+                raise RuntimeError("NoiseFeed: no draws left")
+            seed, slot, fut = self.inflight.popleft()
+            fut.result()
+            view = np.ndarray((2,) + p.shape, dtype=np.float64, buffer=p.slots[slot].buf)
+            re[i].copy_(torch.from_numpy(view[0]))  # pageable source: the copy is staged before returning
+            im[i].copy_(torch.from_numpy(view[1]))
+            del view
+            p.free.append(slot)
+            self._fill()
+        return re, im
+
+    def seeds_ahead(self):
+        return [s for s, _, _ in self.inflight] + list(self.todo)
+
+
+_POOLS = {}
+
+
+def prefetch_pays(n_draws, shape):
+    """Worker processes pay off once the draws add up to about a second of host time (their
+    start-up costs a few seconds once per process)."""
+    return n_draws >= 4 and n_draws * int(np.prod([int(n) for n in shape])) >= 8 * 128 ** 3
+
+
+def noise_pool(shape):
+    """The process-wide NoisePool for a grid shape (created on first use)."""
+    key = tuple(int(n) for n in shape)
+    pool = _POOLS.get(key)
+    if pool is None:
+        pool = NoisePool(key)
+        _POOLS[key] = pool
+    return pool
 
 
 def world(group=None):

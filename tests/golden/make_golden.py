@@ -3,7 +3,7 @@
 Run in a container that holds the reference tree (its Python read in place, its Cython
 kernels compiled into oracle/_ref/ by oracle/build_ref.sh):
 
-    python tests/golden/make_golden.py
+    PB_REFERENCE_ROOT=<directory holding PolyBin3D/> python tests/golden/make_golden.py [case ...]
 
 Every input is regenerated from a seed by polybin3d_b200.synthetic (numpy), so the
 fixtures hold only the case parameters and the reference's outputs.  The Monte Carlo
@@ -602,6 +602,79 @@ def bk_custom_sinv(pb):
                           include_linear_term=False)
     out["b_f3"] = _quiet(bs2.compute_fisher_contribution, 3)
     return out
+
+
+def _sparse(m):
+    """Nonzero entries of a matrix as (rows, cols, values) (the ideal Fisher matrices couple
+    only the multipoles of one triangle bin, so they are block-sparse)."""
+    r, c = np.nonzero(m)
+    return r.astype(np.int32), c.astype(np.int32), m[r, c]
+
+
+def _survey_mask(N, L):
+    """The shell-sector mask of the 128^3 Monte Carlo Fisher workloads: 250 < r < 700 Mpc/h,
+    octant x,y,z > 0, 200 holes of radius 5-20 Mpc/h (seed 0)."""
+    return synthetic.shell_mask(N, L, r_in=250.0, r_out=700.0, n_holes=200, hole_r=(5.0, 20.0), hole_box=700.0,
+                                seed=0)
+
+
+@case
+def cfg2_bk256(pb):
+    """The headline: Bk_ideal at 256^3, L=2000, TSC, lmax=2, 16 linear bins 2pi/2000..0.2,
+    float32 lognormal seed 0.  Numerator, symmetry factors, ideal Fisher (sparse) and b0/b2."""
+    N, L = 256, 2000.0
+    edges = np.linspace(2 * np.pi / L, 0.2, 17)
+    data = synthetic.lognormal(N, L, seed=0)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="tsc", backend="mkl")
+    bs = _quiet(pb.BSpec, base, edges, lmax=2)
+    t = time.time()
+    num = _quiet(bs.Bk_numerator_ideal, data)
+    t_num = time.time() - t
+    t = time.time()
+    bk = _quiet(bs.Bk_ideal, data)
+    fr, fc, fv = _sparse(bs.fish_ideal)
+    out = dict(N=N, L=L, edges=edges, data_seed=0, data_kind="lognormal", pw="tsc", bk_lmax=2,
+               bk_bins=bs.all_bins, bk_sym=bs.sym_factor, bk_num=num, fish_rows=fr, fish_cols=fc, fish_vals=fv,
+               fish_n=bs.fish_ideal.shape[0], t_num=t_num, t_fisher=time.time() - t)
+    for k, v in bk.items():
+        out["Bk_" + k] = v
+    return out
+
+
+@case
+def cfg3_pk128(pb):
+    """Monte Carlo Pk Fisher at 128^3, L=1500, lmax=4, 20 linear bins 2pi/1500..0.25, the
+    survey mask: compute_fisher_contribution(0) (60 x 60) and the numerator of the masked
+    lognormal field (seed 31)."""
+    N, L = 128, 1500.0
+    edges = np.linspace(2 * np.pi / L, 0.25, 21)
+    mask = _survey_mask(N, L)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="none", backend="mkl")
+    ps = _quiet(pb.PSpec, base, edges, lmax=4, mask=mask)
+    t = time.time()
+    f0 = _quiet(ps.compute_fisher_contribution, 0)
+    t_f = time.time() - t
+    data = synthetic.lognormal(N, L, seed=31).astype(np.float64) * mask
+    return dict(N=N, L=L, edges=edges, pk_lmax=4, f0=f0, t_fisher=t_f, data_seed=31,
+                num=_quiet(ps.Pk_numerator, data))
+
+
+@case
+def cfg4_bk128(pb):
+    """Monte Carlo Bk Fisher at 128^3, L=1500, lmax=0, 12 linear bins 2pi/1500..0.2, the
+    survey mask: compute_fisher_contribution(0) (203 x 203), the symmetry factors and the
+    cubic numerator of the masked lognormal field (seed 41)."""
+    N, L = 128, 1500.0
+    edges = np.linspace(2 * np.pi / L, 0.2, 13)
+    mask = _survey_mask(N, L)
+    base = _quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="none", backend="mkl")
+    bs = _quiet(pb.BSpec, base, edges, lmax=0, mask=mask)
+    t = time.time()
+    f0 = _quiet(bs.compute_fisher_contribution, 0)
+    t_f = time.time() - t
+    data = synthetic.lognormal(N, L, seed=41).astype(np.float64) * mask
+    return dict(N=N, L=L, edges=edges, bk_lmax=0, bins=bs.all_bins, sym=bs.sym_factor, f0=f0, t_fisher=t_f,
+                data_seed=41, num=_quiet(bs.Bk_numerator, data, include_linear_term=False))
 
 
 def main(names=None):

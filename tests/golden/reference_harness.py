@@ -15,12 +15,13 @@ import types
 import numpy as np
 import scipy.fft
 
-REF_ROOT = os.environ.get("PB_REFERENCE_ROOT", "/root/reference")
+# the reference tree's root (the directory holding PolyBin3D/): required, no default
+REF_ROOT = os.environ.get("PB_REFERENCE_ROOT", "")
 _REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 
 def available():
-    return os.path.isfile(os.path.join(REF_ROOT, "PolyBin3D", "base.py"))
+    return bool(REF_ROOT) and os.path.isfile(os.path.join(REF_ROOT, "PolyBin3D", "base.py"))
 
 
 def _mkl_shim(workers):
@@ -37,7 +38,7 @@ def load_reference(workers=None):
     if "PolyBin3D" in sys.modules and hasattr(sys.modules["PolyBin3D"], "BSpec"):
         return sys.modules["PolyBin3D"]
     if not available():
-        raise RuntimeError("reference tree not present")
+        raise RuntimeError("reference tree not found: set PB_REFERENCE_ROOT to the directory holding PolyBin3D/")
     sys.dont_write_bytecode = True
     workers = workers or os.cpu_count()
     sys.modules["mkl_fft"] = _mkl_shim(workers)

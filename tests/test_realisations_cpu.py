@@ -90,3 +90,26 @@ def test_two_ranks_gloo_bit_identical(tmp_path, n_it, batch):
     for r in range(2):
         assert np.array_equal(fish[r], ref)
         assert list(seeds[r]) == realisations.seeds_of_rank(n_it, r, 2)
+
+
+def test_noise_pool_matches_the_reference_draw():
+    """The spawned workers' draws equal np.random.seed(s); randn; randn (the reference's
+    generate_data noise, base.py:315-332) for every seed, in order, through slot reuse."""
+    import numpy as np
+    import torch
+    from polybin3d_b200 import realisations
+    shape = (8, 8, 6)
+    seeds = [3, 10000003, 7, 5, 20000001]
+    pool = realisations.NoisePool(shape, workers=2)
+    try:
+        feed = pool.stream(seeds)
+        re1, im1 = feed.take(2, torch.device("cpu"))
+        re2, im2 = feed.take(3, torch.device("cpu"))
+        re, im = torch.cat([re1, re2]), torch.cat([im1, im2])
+        for i, s in enumerate(seeds):
+            np.random.seed(s)
+            r = np.random.randn(*shape)
+            m = np.random.randn(*shape)
+            assert np.array_equal(re[i].numpy(), r) and np.array_equal(im[i].numpy(), m), s
+    finally:
+        pool.close()
