@@ -11,6 +11,13 @@ public call Bk_ideal(field) on pinned host fields, H2D copy and result readback 
 Under torchrun every rank runs independent fields (replicas: a 256^3 field does not
 shard), timing is the max over ranks and `value` counts all ranks' fields.
 
+The same line carries the metric's second half under "fisher": Monte Carlo Fisher
+realisations/s at 128^3 for PSpec (lmax=4, 60 bins) and BSpec (lmax=0, 203 bins) on the
+200-hole shell-sector mask -- device noise in captured graphs as `value`, the
+reference-identical MT19937 noise (drawn by host worker processes) as `e2e` -- each with
+its HBM fraction and CPU baseline.  --workload bk256 runs the Bk line alone,
+fisher_pk128 | fisher_bk128 one Fisher workload, bk512grad the 512^3 forward + gradient.
+
 --impl reference times the reference's own CPU implementation of the same step on the
 host cores: its compiled Cython assemble_b3 (oracle/_ref, built from the reference's
 utils.pyx) with FP64 scipy FFTs and the filter loop of bspec.py:912-956, on a bounded
@@ -33,8 +40,8 @@ N, L, LMAX, NK = 256, 2000.0, 2, 16
 EDGES = np.linspace(2 * np.pi / L, 0.2, NK + 1)
 METRIC = "Bk fields/s at 256^3 (16 bins, lmax=2, TSC, mixed precision)"
 WORKLOAD = "Bk_ideal 256^3 box 2000 Mpc/h, TSC, lmax=2, 16 linear bins 2pi/2000..0.2, 888 triangle bins"
-# DRAM bytes (read + write) of one contraction launch of this workload, from one ncu capture
-# (profiles/triplet_tc_bk256.md)
+# DRAM bytes (read + write) of one tensor-core contraction launch of this workload (32 maps on
+# the 192^3 grid), dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture
 TC_TRAFFIC_BYTES = 911_428_352
 
 
@@ -52,6 +59,8 @@ FISHER = {
 }
 
 
+FISHER_STEPS = 4  # batches per Monte Carlo Fisher record of the default run
+
 # Bk_ideal + its gradient at 512^3: 24 bins to 0.35, lmax=2, TSC, mixed precision, streamed fields
 BK512 = dict(N=512, L=4000.0, lmax=2, edges=np.linspace(2 * np.pi / 4000.0, 0.35, 25),
              metric="Bk_ideal + dBk/ddelta fields/s at 512^3 (24 bins, lmax=2, TSC, mixed precision)",
@@ -65,12 +74,14 @@ def parse():
     p.add_argument("--steps", type=int, default=None)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="bk256", choices=["bk256", "bk512grad"] + sorted(FISHER))
+    # headline (default): the 256^3 Bk line with the Monte Carlo Fisher records inside it;
+    # bk256: the Bk line alone; fisher_*: one Fisher workload alone; bk512grad: 512^3 forward + gradient
+    p.add_argument("--workload", default="headline", choices=["headline", "bk256", "bk512grad"] + sorted(FISHER))
     p.add_argument("--contraction", default="auto", choices=["auto", "tc", "simt"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     a = p.parse_args()
     if a.steps is None:
-        a.steps = {"bk256": 50, "bk512grad": 16}.get(a.workload, 6)
+        a.steps = {"headline": 50, "bk256": 50, "bk512grad": 16}.get(a.workload, 6)
     return a
 
 
@@ -221,6 +232,9 @@ def run_reference(args, rank, world):
             "config": {"workload": WORKLOAD}, "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "fields/s", "cores": cores, "kind": kind, "sample": note},
             "e2e": {"value": v, "unit": "fields/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "headline":
+        # the metric's second half on the host: one Monte Carlo Fisher realisation per workload
+        line["fisher"] = {name: fisher_reference_line(name) for name in ("fisher_pk128", "fisher_bk128")}
     print(json.dumps(line))
 
 
@@ -231,15 +245,10 @@ def run_ours(args, rank, world, local):
     import torch
     import polybin3d_b200 as pb
     from polybin3d_b200 import _native as nat
+    from polybin3d_b200 import autotune
     from polybin3d_b200 import synthetic
 
-    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-
     with contextlib.redirect_stdout(io.StringIO()):
         base = pb.PolyBin3D([L] * 3, [N] * 3, pixel_window="tsc", backend="cuda", precision="mixed")
         bs = pb.BSpec(base, EDGES, lmax=LMAX, contraction=args.contraction)
@@ -268,7 +277,7 @@ def run_ours(args, rank, world, local):
         if record:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-        plan.contract(G, G, G, out, base.ws, method=method)
+        autotune.contract(plan, G, G, G, out, base.ws, method, 1.0)
         if record:
             e1.record()
             cev.append((e0, e1))
@@ -345,23 +354,35 @@ def run_ours(args, rank, world, local):
                 "e2e": {"value": e2e, "unit": "fields/s", "h2d_bytes_per_step": N ** 3 * 4,
                         "d2h_bytes_per_step": bs.N_bins * 8},
                 "gpu_launches": launches,
-                "roofline": {"bound": "tensor", "kernel": "triplet contraction (tcgen05)", "achieved": achieved,
-                             "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
-                             "traffic": TC_TRAFFIC_BYTES, "gemm_flops_per_launch": gemm_flops,
+                # the contraction reads every map once and does 68 GEMM flops per byte, below
+                # the ridge of the measured peaks (~250 flop/B): HBM is its binding roofline;
+                # the tensor-core (GEMM-form) figures are kept beside it
+                "roofline": {"bound": "hbm", "kernel": "triplet contraction (tcgen05)", "achieved": achieved_hbm,
+                             "peak": hbm, "unit": "GB/s", "frac": achieved_hbm / hbm,
+                             "traffic": TC_TRAFFIC_BYTES if method == nat.PB_TRIPLET_TC else None,
+                             "alg_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms,
+                             "gemm_flops_per_launch": gemm_flops, "gemm_tflops": achieved,
+                             "gemm_peak_tflops": bf16, "frac_tensor": achieved / bf16,
                              "useful_flops_per_launch": useful_flops,
                              "useful_tflops": useful_flops / (kern_ms / 1000.0) / 1e12,
-                             "alg_bytes_per_launch": alg_bytes, "achieved_hbm_gbs": achieved_hbm,
-                             "frac_hbm": achieved_hbm / hbm, "kernel_ms": kern_ms,
-                             "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst) and hbm_gbs" if peaks
-                                             else "fallback 1590 TFLOP/s and 6650 GB/s")},
+                             "peak_source": ("of measured: MEASURED_PEAKS.json hbm_gbs and bf16_tflops (burst)"
+                                             if peaks else "of fallback: 6650 GB/s and 1590 TFLOP/s")},
                 "clocks": clk.summary()}
         if not args.no_cpu_baseline and world == 1:
-            from polybin3d_b200 import synthetic as S
             v, kind, cores, note = cpu_baseline([host[0].numpy(), host[1].numpy()])
             line["cpu_baseline"] = {"value": v, "unit": "fields/s", "cores": cores, "kind": kind, "sample": note}
+    # the metric's second half: Monte Carlo Fisher realisations/s at 128^3 (Pk and Bk), every
+    # rank taking part (the seeds are shared over the ranks)
+    del bs, base, resident
+    torch.cuda.empty_cache()
+    if args.workload == "headline":
+        fisher = {}
+        for name in ("fisher_pk128", "fisher_bk128"):
+            fisher[name] = fisher_measure(name, FISHER_STEPS, 3, rank, world, local, not args.no_cpu_baseline)
+        if rank == 0:
+            line["fisher"] = fisher
+    if rank == 0:
         print(json.dumps(line))
-    if world > 1:
-        torch.distributed.destroy_process_group()
 
 
 def fisher_alg_bytes(kind, N, n_bins):
@@ -411,7 +432,24 @@ def fisher_cpu_baseline(cfg, kind):
     return 1.0 / dt, "reference" if ref_utils is not None else "port", nthreads, note
 
 
-def run_fisher(args, rank, world, local):
+def fisher_reference_line(name):
+    """The reference arm of one Monte Carlo Fisher workload (rank 0; host cores only)."""
+    cfg = FISHER[name]
+    kind = "pk" if name.startswith("fisher_pk") else "bk"
+    v, k, cores, note = fisher_cpu_baseline(cfg, kind)
+    return {"metric": cfg["metric"], "value": v, "unit": "sims/s", "ms_per_step": 1000.0 / v,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic (Gaussian random fields, shell-sector mask)",
+            "config": {"workload": cfg["workload"]}, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "sims/s", "cores": cores, "kind": k, "sample": note},
+            "e2e": {"value": v, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def fisher_measure(name, steps, warmup, rank, world, local, with_cpu):
+    """Monte Carlo Fisher throughput of one workload: `value` = realisations/s with the
+    white noise drawn on the device (one captured CUDA graph per batch), `e2e` = the
+    reference-identical path (the reference's MT19937 noise drawn by host workers, copied
+    in, the Fisher matrix read back).  Timed with CUDA events on the current stream, max
+    over ranks; seeds are shared round-robin over the ranks."""
     import contextlib
     import io
 
@@ -419,28 +457,9 @@ def run_fisher(args, rank, world, local):
     import polybin3d_b200 as pb
     from polybin3d_b200 import _native as nat
 
-    cfg = FISHER[args.workload]
-    kind = "pk" if args.workload.startswith("fisher_pk") else "bk"
-    if args.impl == "reference":
-        if rank == 0:
-            v, k, cores, note = fisher_cpu_baseline(cfg, kind)
-            print(json.dumps({"metric": cfg["metric"], "value": v, "unit": "sims/s", "n_gpus": args.gpus,
-                              "steps": 1, "warmup": 0, "ms_per_step": 1000.0 / v, "higher_is_better": True,
-                              "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                              "data": "synthetic (Gaussian random fields, shell-sector mask)",
-                              "config": {"workload": cfg["workload"]}, "impl": "reference",
-                              "cpu_baseline": {"value": v, "unit": "sims/s", "cores": cores, "kind": k,
-                                               "sample": note},
-                              "e2e": {"value": v, "unit": "sims/s", "h2d_bytes_per_step": 0,
-                                      "d2h_bytes_per_step": 0}}))
-        return
-    torch.cuda.set_device(local)
+    cfg = FISHER[name]
+    kind = "pk" if name.startswith("fisher_pk") else "bk"
     dev = torch.device("cuda", local)
-    group = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     N, L, B = cfg["N"], cfg["L"], cfg["batch"]
     with contextlib.redirect_stdout(io.StringIO()):
         base = pb.PolyBin3D([L] * 3, [N] * 3, backend="cuda")
@@ -456,8 +475,15 @@ def run_fisher(args, rank, world, local):
                 return est.compute_fisher(n_it, batch=B, noise=noise)
             return est.compute_fisher(n_it, noise=noise)
 
+    def max_over_ranks(x):
+        if world > 1:
+            tt = torch.tensor([x], device=dev)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            return float(tt.item())
+        return x
+
     per_step = B * world  # realisations per step over all ranks
-    fisher(args.warmup * per_step, "philox")  # capture + warm-up replays
+    fisher(max(3, warmup) * per_step, "philox")  # capture + warm-up replays
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -466,32 +492,27 @@ def run_fisher(args, rank, world, local):
     with Clocks(local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        fisher(args.steps * per_step, "philox")
+        fisher(steps * per_step, "philox")
         e1.record()
         torch.cuda.synchronize()
     launches = nat.LAUNCHES[0] - l0
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = args.steps * per_step / (ms / 1000.0)
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = steps * per_step / (ms / 1000.0)
 
-    # end to end: the reference-identical path (MT19937 noise drawn on the host, copied in)
-    n_e2e = max(1, min(args.steps, 2)) * per_step
-    fisher(per_step, "reference")
+    # end to end: the reference-identical path (the reference's MT19937 draws made on host
+    # worker processes, copied in; the Fisher matrix read back)
+    n_e2e = max(2, steps) * per_step
+    fisher(per_step * 4, "reference")  # worker start-up and warm-up
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    t0 = time.perf_counter()
+    e0.record()
     fisher(n_e2e, "reference")
+    e1.record()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
     e2e = n_e2e / e2e_s
+    rec = None
     if rank == 0:
         peaks = {}
         try:
@@ -500,32 +521,44 @@ def run_fisher(args, rank, world, local):
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         alg = fisher_alg_bytes(kind, N, est.N_bins)
-        achieved = alg / (ms / 1000.0 / (args.steps * B)) / 1e9
+        achieved = alg / (ms / 1000.0 / (steps * B)) / 1e9
         fields = 1 if kind == "pk" else 2
-        line = {"metric": cfg["metric"], "value": value, "unit": "sims/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (Gaussian random fields drawn on the device, shell-sector mask)",
-                "config": {"workload": cfg["workload"], "n_bins": est.N_bins, "realisations_per_step": per_step,
-                           "graph": "one captured CUDA graph per batch of %d" % B,
-                           "l2": "per-realisation working set > 3 GB >> 126 MB L2",
-                           "parallelism": "seeds round-robin over ranks" if world > 1 else "single GPU"},
-                "e2e": {"value": e2e, "unit": "sims/s",
-                        "h2d_bytes_per_step": per_step * fields * 2 * N ** 3 * 8,
-                        "d2h_bytes_per_step": est.N_bins ** 2 * 8,
-                        "path": "compute_fisher(noise='reference'): the reference's MT19937 draw on the host"},
-                "gpu_launches": launches,
-                "roofline": {"bound": "hbm", "kernel": "whole realisation (FFTs, filters, reductions)",
-                             "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                             "traffic": None, "alg_bytes_per_realisation": alg,
-                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
-                "clocks": clk.summary()}
-        if not args.no_cpu_baseline and world == 1:
+        rec = {"metric": cfg["metric"], "value": value, "unit": "sims/s", "n_gpus": world, "steps": steps,
+               "warmup": warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (Gaussian random fields drawn on the device, shell-sector mask)",
+               "config": {"workload": cfg["workload"], "n_bins": est.N_bins, "realisations_per_step": per_step,
+                          "graph": "one captured CUDA graph per batch of %d" % B,
+                          "l2": "per-realisation working set > 3 GB >> 126 MB L2",
+                          "parallelism": "seeds round-robin over ranks" if world > 1 else "single GPU"},
+               "e2e": {"value": e2e, "unit": "sims/s",
+                       "h2d_bytes_per_step": per_step * fields * 2 * N ** 3 * 8,
+                       "d2h_bytes_per_step": est.N_bins ** 2 * 8,
+                       "path": "compute_fisher(noise='reference'): the reference's MT19937 draws on host workers"},
+               "gpu_launches": launches,
+               "roofline": {"bound": "hbm", "kernel": "whole realisation (FFTs, filters, reductions)",
+                            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                            "traffic": None, "alg_bytes_per_realisation": alg,
+                            "peak_source": "of measured: MEASURED_PEAKS.json hbm_gbs" if peaks else "of fallback: 6650"},
+               "clocks": clk.summary()}
+        if with_cpu and world == 1:
             v, k, cores, note = fisher_cpu_baseline(cfg, kind)
-            line["cpu_baseline"] = {"value": v, "unit": "sims/s", "cores": cores, "kind": k, "sample": note}
-        print(json.dumps(line))
-    if world > 1:
-        torch.distributed.destroy_process_group()
+            rec["cpu_baseline"] = {"value": v, "unit": "sims/s", "cores": cores, "kind": k, "sample": note}
+    del est, base
+    torch.cuda.empty_cache()
+    return rec
+
+
+def run_fisher(args, rank, world, local):
+    if args.impl == "reference":
+        if rank == 0:
+            line = fisher_reference_line(args.workload)
+            line.update({"n_gpus": args.gpus, "steps": 1, "warmup": 0, "scaling": "weak", "vs_baseline": None})
+            print(json.dumps(line))
+        return
+    rec = fisher_measure(args.workload, args.steps, args.warmup, rank, world, local, not args.no_cpu_baseline)
+    if rank == 0:
+        print(json.dumps(rec))
 
 
 def run_bk512(args, rank, world, local):
@@ -546,12 +579,7 @@ def run_bk512(args, rank, world, local):
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient path; its 512^3 "
                               "numerator needs 48 FP64 maps (48 GB of host memory) per field"}))
         return
-    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
     N, L = cfg["N"], cfg["L"]
     with contextlib.redirect_stdout(io.StringIO()):
         base = pb.PolyBin3D([L] * 3, [N] * 3, pixel_window="tsc", backend="cuda", precision="mixed")
@@ -621,21 +649,38 @@ def run_bk512(args, rank, world, local):
                           "e2e": {"value": world * args.steps / (e2e_ms / 1000.0), "unit": "fields/s",
                                   "h2d_bytes_per_step": N ** 3 * 4, "d2h_bytes_per_step": N ** 3 * 4 + bs.N_bins * 8},
                           "gpu_launches": launches, "clocks": clk.summary()}))
-    if world > 1:
-        torch.distributed.destroy_process_group()
 
 
 def main():
     args = parse()
     rank, world, local = dist_setup(args)
-    if args.workload == "bk512grad":
-        run_bk512(args, rank, world, local)
-    elif args.workload != "bk256":
-        run_fisher(args, rank, world, local)
-    elif args.impl == "reference":
-        run_reference(args, rank, world)
-    else:
-        run_ours(args, rank, world, local)
+    if args.impl == "reference":
+        # host cores only: rank 0 runs the reference's CPU path, the other ranks exit
+        if args.workload == "bk512grad":
+            run_bk512(args, rank, world, local)
+        elif args.workload not in ("headline", "bk256"):
+            run_fisher(args, rank, world, local)
+        else:
+            run_reference(args, rank, world)
+        return
+    import datetime
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    try:
+        if args.workload == "bk512grad":
+            run_bk512(args, rank, world, local)
+        elif args.workload not in ("headline", "bk256"):
+            run_fisher(args, rank, world, local)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
 
 
 if __name__ == "__main__":

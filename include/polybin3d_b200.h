@@ -63,6 +63,24 @@ PB_API int pb_abi_version(void);
 PB_API const char *pb_last_error(void);
 
 /* ---------------------------------------------------------------------------------- */
+/* Launch shapes of the kernels that have more than one good shape, chosen per host      */
+/* thread (the autotuner of polybin3d_b200/autotune.py times the candidates on first use  */
+/* and sets the winner before each call).  Zero in a field means the built-in default.   */
+/* Results do not depend on these settings beyond FP summation order.  No reference      */
+/* counterpart (the reference has no launch configuration).                              */
+/* ---------------------------------------------------------------------------------- */
+typedef struct pb_tuning {
+    int32_t tc_tile;     /* tensor-core contraction: voxels per tile, 32 or 64 (0: 64)         */
+    int32_t tc_stages;   /* its staging ring depth in tiles, 2..6 (0: what ~64 KB holds)     */
+    int32_t tc_chain;    /* voxels summed in TMEM between FP64 folds: 512, 1024, 2048 (0: 1024) */
+    int32_t red_method;  /* k-bin reduction of many rows: 1 lane per row, 2 mode tiles (0: auto) */
+    int32_t red_warps;   /* lane-per-row reduction: warps per block, 1..8 (0: as 48 KB fit)   */
+    int32_t red_waves;   /* lane-per-row reduction: blocks per SM per 32-row group, 1..32 (0: 8) */
+} pb_tuning_t;
+PB_API int pb_set_tuning(const pb_tuning_t *t); /* NULL restores the defaults               */
+PB_API int pb_get_tuning(pb_tuning_t *t);
+
+/* ---------------------------------------------------------------------------------- */
 /* 3-D real FFTs.  Replace PolyBin3D/base.py:176-229 (`to_fourier`, `to_real`) and the   */
 /* plan set-up of base.py:256-302 (`_fft_setup`).  Forward r2c is unnormalised; the c2r  */
 /* is unnormalised too (the 1/N^3 of numpy's irfftn is folded into the kernels that      */
@@ -272,8 +290,9 @@ PB_API int pb_shell_rows(const pb_grid_t *g, int precision, const void *F, int n
 /* to a fixed 2 MiB device array inside the library (PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES   */
 /* doubles, held on every GPU that loads the library until exit).  Fails with           */
 /* PB_ERR_INVALID when n_rows * nk * n_ell exceeds it.  The first call on a device looks */
-/* up the array's device address and should come before any stream capture.  All calls  */
-/* share the array: calls that overlap on the GPU race and must be serialised.           */
+/* up the array's device address and should come before any stream capture; the address */
+/* is kept for the process's life (no calls after a cudaDeviceReset).  All calls share   */
+/* the array: calls that overlap on the GPU race and must be serialised.                 */
 /* ---------------------------------------------------------------------------------- */
 #define PB_BIN_REDUCE_NOALLOC_MAX_DOUBLES 262144
 PB_API int pb_bin_reduce_noalloc(const pb_grid_t *g, int precision, int mode, const void *a,

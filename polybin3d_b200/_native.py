@@ -35,6 +35,13 @@ class PBGrid(ctypes.Structure):
                 ("los", ctypes.c_double * 3)]
 
 
+class PBTuning(ctypes.Structure):
+    _fields_ = [("tc_tile", ctypes.c_int32), ("tc_stages", ctypes.c_int32), ("tc_chain", ctypes.c_int32),
+                ("red_method", ctypes.c_int32), ("red_warps", ctypes.c_int32), ("red_waves", ctypes.c_int32)]
+
+
+TUNING_FIELDS = [f for f, _ in PBTuning._fields_]
+
 _lib = None
 _lib_lock = threading.Lock()
 
@@ -60,6 +67,8 @@ SIGNATURES = {
     "pb_bin_reduce_workspace_size": ([_GP, _I, _I, _I, ctypes.POINTER(_SZ)], _I),
     "pb_bin_reduce": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P, _SZ, _P], _I),
     "pb_bin_reduce_noalloc": ([_GP, _I, _I, _P, _P, _I, _I64, _P, _I, _P, _I, _D, _P, _I, _P], _I),
+    "pb_set_tuning": ([ctypes.POINTER(PBTuning)], _I),
+    "pb_get_tuning": ([ctypes.POINTER(PBTuning)], _I),
     "pb_triplet_plan": ([_I, _I, _I, _P, _I, _P, ctypes.POINTER(_SZ), _P], _I),
     "pb_triplet_workspace_size": ([_I, _I, _I64, _P, _I, ctypes.POINTER(_SZ)], _I),
     "pb_triplet_contract": ([_I, _I, _P, _I, _P, _I, _P, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
@@ -109,6 +118,22 @@ def require_cuda():
     if not torch.cuda.is_available():
         raise RuntimeError("polybin3d_b200 backend='cuda' needs a CUDA device; there is no CPU fallback")
     load()
+
+
+def set_tuning(cfg=None):
+    """Launch shapes for this host thread (pb_set_tuning): a dict of PBTuning fields, missing
+    or zero fields meaning the built-in default; None restores every default."""
+    if cfg is None:
+        check(load().pb_set_tuning(None), "pb_set_tuning")
+        return
+    t = PBTuning(*[int(cfg.get(f, 0)) for f in TUNING_FIELDS])
+    check(load().pb_set_tuning(ctypes.byref(t)), "pb_set_tuning")
+
+
+def get_tuning():
+    t = PBTuning()
+    check(load().pb_get_tuning(ctypes.byref(t)), "pb_get_tuning")
+    return {f: int(getattr(t, f)) for f in TUNING_FIELDS}
 
 
 def stream_ptr():

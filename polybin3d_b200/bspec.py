@@ -14,6 +14,7 @@ from scipy.interpolate import interp1d
 from . import _native as nat
 from . import covariance
 from . import pointing
+from . import autotune
 from . import realisations
 from .harmonics import real_harmonics
 
@@ -312,7 +313,7 @@ class BSpec:
         if method == nat.PB_TRIPLET_TC and getattr(plan, "tc_unsupported", False):
             method = nat.PB_TRIPLET_SIMT
         try:
-            plan.contract(A, B, C, out, b.ws, method=method, scale=scale)
+            autotune.contract(plan, A, B, C, out, b.ws, method, scale)
         except NotImplementedError:
             # the tensor-core tiling does not fit this shape (too many pair rows or maps
             # for shared memory / TMEM): the CUDA-core kernel takes it

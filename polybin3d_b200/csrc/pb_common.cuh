@@ -26,6 +26,9 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 
 int num_sms();
 
+// launch shapes set through pb_set_tuning (this host thread's settings; zero = default)
+const pb_tuning_t &tuning();
+
 // ---- grid geometry ----------------------------------------------------------------
 struct Grid {
     int n0, n1, n2, nh2;     // real dims and half-axis length n2/2+1

@@ -23,6 +23,10 @@ int cuda_check(cudaError_t e, const char *where) {
     return fail(PB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
+static thread_local pb_tuning_t g_tuning = {0, 0, 0, 0, 0, 0};
+
+const pb_tuning_t &tuning() { return g_tuning; }
+
 int num_sms() {
     int dev = 0, n = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 148;
@@ -200,6 +204,30 @@ using namespace pb;
 extern "C" int pb_abi_version(void) { return PB_ABI_VERSION; }
 
 extern "C" const char *pb_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int pb_set_tuning(const pb_tuning_t *t) {
+    if (!t) {
+        g_tuning = pb_tuning_t{0, 0, 0, 0, 0, 0};
+        return PB_OK;
+    }
+    if (t->tc_tile != 0 && t->tc_tile != 32 && t->tc_tile != 64)
+        return fail(PB_ERR_INVALID, "pb_set_tuning: tc_tile must be 0, 32 or 64");
+    if (t->tc_stages != 0 && (t->tc_stages < 2 || t->tc_stages > 6))
+        return fail(PB_ERR_INVALID, "pb_set_tuning: tc_stages must be 0 or in [2, 6]");
+    if (t->tc_chain != 0 && t->tc_chain != 512 && t->tc_chain != 1024 && t->tc_chain != 2048)
+        return fail(PB_ERR_INVALID, "pb_set_tuning: tc_chain must be 0, 512, 1024 or 2048");
+    if (t->red_method < 0 || t->red_method > 2) return fail(PB_ERR_INVALID, "pb_set_tuning: red_method in [0, 2]");
+    if (t->red_warps < 0 || t->red_warps > 8) return fail(PB_ERR_INVALID, "pb_set_tuning: red_warps in [0, 8]");
+    if (t->red_waves < 0 || t->red_waves > 32) return fail(PB_ERR_INVALID, "pb_set_tuning: red_waves in [0, 32]");
+    g_tuning = *t;
+    return PB_OK;
+}
+
+extern "C" int pb_get_tuning(pb_tuning_t *t) {
+    if (!t) return fail(PB_ERR_INVALID, "pb_get_tuning: NULL");
+    *t = g_tuning;
+    return PB_OK;
+}
 
 struct pb_fft_plan {
     cufftHandle h;

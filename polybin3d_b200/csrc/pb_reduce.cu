@@ -218,6 +218,152 @@ __global__ void __launch_bounds__(RED_THREADS) binred_rows_kernel(Grid g, const 
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Many rows, one lane per row.  The mode geometry (bin and deg x L_la L_lb per mode, FP64)
+// is tabulated once per call by binred_geom_kernel.  A warp then walks kz lines of the half
+// grid; each lane reads ITS row's values along the line (8 consecutive modes = one 128-byte
+// segment for complex128) while the geometry and the shared spectrum are warp-uniform
+// broadcasts.  All lanes see the same mode sequence, so a bin change is a uniform branch:
+// the sums of the current bin stay in registers and are added to the lane's slot of the
+// warp's shared-memory accumulators [bin][e][lane] only when the bin changes (no shuffles,
+// no atomics, fixed order: deterministic).  Only the part of each line inside the binned
+// range is read (|k| grows along a kz line, so it is one contiguous run of modes).
+// ------------------------------------------------------------------------------------
+constexpr int BL_MODES = 8;  // modes per lane per step
+
+__global__ void binred_geom_kernel(Grid g, RedParams p, int8_t *mbin, double *mw) {
+    __shared__ double edges[PB_RED_MAX_BINS + 1];
+    for (int i = threadIdx.x; i <= p.nk; i += blockDim.x) edges[i] = p.edges[i];
+    __syncthreads();
+    const int ne = p.n_ell;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < g.nhalf;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const Mode md = mode_of(g, idx);
+        const int bin = find_bin(edges, p.nk, md.k);
+        mbin[idx] = (int8_t)bin;
+        if (bin >= 0) {
+#pragma unroll
+            for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                if (e < ne) mw[idx * ne + e] = md.deg * legendre(p.la[e], md.mu) * legendre(p.lb[e], md.mu);
+        }
+    }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) binred_lanes_kernel(Grid g, const typename cplx<T>::type *a,
+                                                           const typename cplx<T>::type *b, int64_t row_stride,
+                                                           int n_rows, int nk, int ne, const int8_t *mbin,
+                                                           const double *mw, double *partials) {
+    using C = typename cplx<T>::type;
+    extern __shared__ __align__(16) double bl_acc[];  // [warp][bin][e][32]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int per = nk * ne;
+    double *wacc = bl_acc + (size_t)warp * per * 32;
+    for (int i = threadIdx.x; i < nw * per * 32; i += blockDim.x) bl_acc[i] = 0.0;
+    __syncthreads();
+    const int row = blockIdx.y * 32 + lane;
+    const bool live = row < n_rows;
+    const C *brow = b + (int64_t)(live ? row : 0) * row_stride;
+    const int64_t n_lines = (int64_t)g.n0 * g.n1;
+    const int nh2 = g.nh2;
+    double r[PB_RED_MAX_ELLS];
+#pragma unroll
+    for (int e = 0; e < PB_RED_MAX_ELLS; ++e) r[e] = 0.0;
+    int cur = -1;
+    auto flush = [&]() {
+#pragma unroll
+        for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+            if (e < ne) {
+                if (cur >= 0) wacc[(cur * ne + e) * 32 + lane] += r[e];
+                r[e] = 0.0;
+            }
+    };
+    for (int64_t line = (int64_t)blockIdx.x * nw + warp; line < n_lines; line += (int64_t)gridDim.x * nw) {
+        const int64_t base = line * nh2;
+        // the binned run [l_lo, l_hi) of this line
+        int l_lo = nh2, l_hi = 0;
+        for (int l0 = 0; l0 < nh2; l0 += 32) {
+            const int l = l0 + lane;
+            const bool in = l < nh2 && mbin[base + l] >= 0;
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            if (m) {
+                l_lo = min(l_lo, l0 + __ffs(m) - 1);
+                l_hi = l0 + 32 - __clz(m);
+            }
+        }
+        for (int l0 = l_lo; l0 < l_hi; l0 += BL_MODES) {
+            C v[BL_MODES];
+#pragma unroll
+            for (int k = 0; k < BL_MODES; ++k) {
+                v[k].x = 0;
+                v[k].y = 0;
+                if (live && l0 + k < l_hi) v[k] = brow[base + l0 + k];
+            }
+#pragma unroll
+            for (int k = 0; k < BL_MODES; ++k) {
+                if (l0 + k >= l_hi) break;
+                const int64_t idx = base + l0 + k;
+                const int bin = mbin[idx];
+                if (bin != cur) {
+                    flush();
+                    cur = bin;
+                }
+                if (bin < 0) continue;
+                double f;
+                if (MODE == PB_RED_CROSS) {
+                    const C u = a[idx];
+                    f = (double)u.x * (double)v[k].x + (double)u.y * (double)v[k].y;
+                } else {
+                    f = (double)v[k].x * (double)v[k].x + (double)v[k].y * (double)v[k].y;
+                }
+                const double *w = mw + idx * ne;
+#pragma unroll
+                for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
+                    if (e < ne) r[e] += f * w[e];
+            }
+        }
+    }
+    flush();
+    __syncthreads();
+    // warps' sums in fixed order -> this block's partial of each row
+    for (int i = threadIdx.x; i < per * 32; i += blockDim.x) {
+        const int ln = i & 31, be = i >> 5;  // be = bin * ne + e
+        const int rr = blockIdx.y * 32 + ln;
+        if (rr >= n_rows) continue;
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += bl_acc[((size_t)w * per + be) * 32 + ln];
+        const int bin = be / ne, e = be - bin * ne;
+        partials[((int64_t)rr * gridDim.x + blockIdx.x) * per + e * nk + bin] = s;
+    }
+}
+
+struct LanesLaunch {
+    int nw, gx;
+    size_t smem;
+    size_t geom_bytes;   // mbin (nhalf bytes, padded to 256) + mw (nhalf * n_ell doubles)
+};
+
+// the lane-per-row kernel serves many rows with small (bins x multipoles) accumulators
+static bool lanes_plan(const Grid &G, int n_rows, int nk, int n_ell, LanesLaunch *L) {
+    const pb_tuning_t &tu = tuning();
+    if (tu.red_method == 2) return false;
+    if (n_rows < (tu.red_method == 1 ? 1 : 16)) return false;
+    const size_t per_warp = (size_t)nk * n_ell * 32 * sizeof(double);
+    if (per_warp > 48 * 1024) return false;
+    const size_t fit = std::max<size_t>(1, (48 * 1024) / per_warp);
+    L->nw = tu.red_warps > 0 ? (int)std::min<size_t>((size_t)tu.red_warps, 2 * fit) : (int)std::min<size_t>(4, fit);
+    L->smem = per_warp * L->nw;
+    if (L->smem > 96 * 1024) return false;
+    const int64_t n_lines = (int64_t)G.n0 * G.n1;
+    const int groups = (n_rows + 31) / 32;
+    const int waves = tu.red_waves > 0 ? tu.red_waves : 8;
+    int64_t gx = ((int64_t)waves * num_sms() + groups - 1) / groups;
+    gx = std::min<int64_t>(gx, (n_lines + L->nw - 1) / L->nw);
+    L->gx = (int)std::max<int64_t>(1, gx);
+    L->geom_bytes = ((size_t)G.nhalf + 255) / 256 * 256 + (size_t)G.nhalf * n_ell * sizeof(double);
+    return true;
+}
+
 __global__ void binred_finalize(const double *partials, int n_blocks, int per_row, int n_rows, double scale,
                                 double *out, int accumulate) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -241,6 +387,9 @@ extern "C" int pb_bin_reduce_workspace_size(const pb_grid_t *g, int n_rows, int 
     if (!bytes) return fail(PB_ERR_INVALID, "bytes is NULL");
     if (n_rows < 1 || nk < 1 || n_ell < 1) return fail(PB_ERR_INVALID, "pb_bin_reduce: empty reduction");
     *bytes = (size_t)n_rows * red_blocks(G) * nk * n_ell * sizeof(double);
+    LanesLaunch L;
+    if (lanes_plan(G, n_rows, nk, n_ell, &L))
+        *bytes = std::max(*bytes, L.geom_bytes + (size_t)n_rows * L.gx * nk * n_ell * sizeof(double));
     return PB_OK;
 }
 
@@ -273,12 +422,50 @@ extern "C" int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const 
     }
     p.nk = nk;
     p.n_ell = n_ell;
+    if (precision != PB_F32 && precision != PB_F64) return fail(PB_ERR_INVALID, "bad precision");
     int nb = red_blocks(G);
     size_t need = (size_t)n_rows * nb * nk * n_ell * sizeof(double);
+    cudaStream_t s = as_stream(stream);
+    LanesLaunch LL;
+    if (mode != PB_RED_REAL2 && lanes_plan(G, n_rows, nk, n_ell, &LL)) {
+        // geometry table, then one lane per row (binred_lanes_kernel)
+        need = LL.geom_bytes + (size_t)n_rows * LL.gx * nk * n_ell * sizeof(double);
+        if (!workspace || workspace_bytes < need)
+            return fail(PB_ERR_WORKSPACE, "pb_bin_reduce: workspace too small (need " + std::to_string(need) + " bytes)");
+        int8_t *mbin = (int8_t *)workspace;
+        double *mw = (double *)((char *)workspace + ((size_t)G.nhalf + 255) / 256 * 256);
+        double *partials = (double *)((char *)workspace + LL.geom_bytes);
+        const int gg = (int)std::min<int64_t>((G.nhalf + 255) / 256, (int64_t)num_sms() * 8);
+        binred_geom_kernel<<<gg, 256, 0, s>>>(G, p, mbin, mw);
+        PB_LAUNCH_CHECK("pb_bin_reduce(geometry)");
+        dim3 lgrid(LL.gx, (n_rows + 31) / 32);
+        const void *rows = (mode == PB_RED_CROSS) ? b : a;
+#define PB_BL_LAUNCH(T, M)                                                                                    \
+    do {                                                                                                      \
+        PB_CUDA(cudaFuncSetAttribute(binred_lanes_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                     (int)LL.smem));                                                          \
+        binred_lanes_kernel<T, M><<<lgrid, 32 * LL.nw, LL.smem, s>>>(G, (const cplx<T>::type *)a,            \
+                                                                    (const cplx<T>::type *)rows, row_stride,  \
+                                                                    n_rows, nk, n_ell, mbin, mw, partials);   \
+    } while (0)
+        if (precision == PB_F32) {
+            if (mode == PB_RED_ABS2) PB_BL_LAUNCH(float, PB_RED_ABS2);
+            else PB_BL_LAUNCH(float, PB_RED_CROSS);
+        } else {
+            if (mode == PB_RED_ABS2) PB_BL_LAUNCH(double, PB_RED_ABS2);
+            else PB_BL_LAUNCH(double, PB_RED_CROSS);
+        }
+#undef PB_BL_LAUNCH
+        PB_LAUNCH_CHECK("pb_bin_reduce(lanes)");
+        const int per = nk * n_ell;
+        const int total = per * n_rows;
+        binred_finalize<<<(total + 255) / 256, 256, 0, s>>>(partials, LL.gx, per, n_rows, scale, out, accumulate);
+        PB_LAUNCH_CHECK("pb_bin_reduce(finalize)");
+        return PB_OK;
+    }
     if (!workspace || workspace_bytes < need)
         return fail(PB_ERR_WORKSPACE, "pb_bin_reduce: workspace too small (need " + std::to_string(need) + " bytes)");
     double *partials = (double *)workspace;
-    cudaStream_t s = as_stream(stream);
     if (mode != PB_RED_REAL2) {
         // spectra: mode geometry once per tile for a group of rows (binred_rows_kernel)
         const int per = nk * n_ell;
@@ -477,9 +664,12 @@ extern "C" int pb_shell_rows(const pb_grid_t *g, int precision, const void *F, i
 // The array's host-side name is only a stand-in for the device symbol, so its device
 // address is looked up once per device with cudaGetSymbolAddress, with that device
 // current, on the first call made on that device; make that first call before any stream
-// capture.  All calls share the one array: calls whose kernels overlap on the GPU (other
-// streams, other host threads) race on it and must be serialised by the caller.  Each call
-// writes every partial it later reads, so nothing is carried over from the previous call.
+// capture.  The address is kept for the life of the process: a program that resets the
+// device (cudaDeviceReset) must not call this entry point afterwards.  All calls share the
+// one array: calls whose kernels overlap on the GPU (other streams, other host threads)
+// race on it and must be serialised by the caller.  Each call writes every partial it later
+// reads, so nothing is carried over from the previous call.  Spectra go through the same
+// deterministic multi-row kernel as pb_bin_reduce, with as many blocks per row as fit.
 // ------------------------------------------------------------------------------------
 #include <mutex>
 
@@ -552,21 +742,40 @@ extern "C" int pb_bin_reduce_noalloc(const pb_grid_t *g, int precision, int mode
     st = binred_scratch_address(&partials);
     if (st) return st;
     int nb = (int)std::min<int64_t>(red_blocks(G), fit);
-    dim3 grid(nb, n_rows);
     cudaStream_t s = as_stream(stream);
-#define PB_RED_LAUNCH(T, M)                                                                        \
-    binred_kernel<T, M><<<grid, RED_THREADS, 0, s>>>(G, (const cplx<T>::type *)a, (const cplx<T>::type *)b, \
-                                                      (const T *)a, row_stride, p, partials)
-    if (precision == PB_F32) {
-        if (mode == PB_RED_ABS2) PB_RED_LAUNCH(float, PB_RED_ABS2);
-        else if (mode == PB_RED_CROSS) PB_RED_LAUNCH(float, PB_RED_CROSS);
-        else PB_RED_LAUNCH(float, PB_RED_REAL2);
+    if (mode != PB_RED_REAL2) {
+        // spectra: the deterministic multi-row kernel of pb_bin_reduce (its accumulators are
+        // dynamic shared memory, not device memory), on the block count that fits the array
+        const int per = nk * n_ell;
+        const int rpg = std::max(1, std::min(n_rows, RR_ACC_DOUBLES / per));
+        const size_t smem = rr_acc_len(rpg, n_ell, nk) * sizeof(double) + (size_t)n_ell * RR_TILE * sizeof(double) +
+                            (size_t)RR_TILE * (sizeof(double2) + sizeof(int));
+        dim3 rgrid(nb, (n_rows + rpg - 1) / rpg);
+#define PB_RR_LAUNCH(T, M)                                                                                   \
+    do {                                                                                                     \
+        PB_CUDA(cudaFuncSetAttribute(binred_rows_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)smem));                                                            \
+        binred_rows_kernel<T, M><<<rgrid, RED_THREADS, smem, s>>>(G, (const cplx<T>::type *)a,              \
+                                                                  (const cplx<T>::type *)b, row_stride, p,   \
+                                                                  n_rows, rpg, partials);                    \
+    } while (0)
+        if (precision == PB_F32) {
+            if (mode == PB_RED_ABS2) PB_RR_LAUNCH(float, PB_RED_ABS2);
+            else PB_RR_LAUNCH(float, PB_RED_CROSS);
+        } else {
+            if (mode == PB_RED_ABS2) PB_RR_LAUNCH(double, PB_RED_ABS2);
+            else PB_RR_LAUNCH(double, PB_RED_CROSS);
+        }
+#undef PB_RR_LAUNCH
     } else {
-        if (mode == PB_RED_ABS2) PB_RED_LAUNCH(double, PB_RED_ABS2);
-        else if (mode == PB_RED_CROSS) PB_RED_LAUNCH(double, PB_RED_CROSS);
-        else PB_RED_LAUNCH(double, PB_RED_REAL2);
+        dim3 grid(nb, n_rows);
+        if (precision == PB_F32)
+            binred_kernel<float, PB_RED_REAL2><<<grid, RED_THREADS, 0, s>>>(G, nullptr, nullptr, (const float *)a,
+                                                                            row_stride, p, partials);
+        else
+            binred_kernel<double, PB_RED_REAL2><<<grid, RED_THREADS, 0, s>>>(G, nullptr, nullptr, (const double *)a,
+                                                                             row_stride, p, partials);
     }
-#undef PB_RED_LAUNCH
     PB_LAUNCH_CHECK("pb_bin_reduce_noalloc");
     int per_row = nk * n_ell;
     int total = per_row * n_rows;

@@ -1,24 +1,30 @@
 // Tensor-core (tcgen05, sm_100a) triplet contraction
 //   out[t] = scale * sum_x A[i1](x) B[i2](x) C[i3](x)
-// as the GEMM  D[c_row, pair] = sum_x C_row(x) P_pair(x)  with P_pair = A[i1] * B[i2].
+// as the GEMM  D[pair, c] = sum_x P_pair(x) C_c(x)  with P_pair = A[i1] * B[i2].
 //
-// Operands, per tile of TC_KT voxels, in shared memory in the UMMA K-major no-swizzle
-// layout (core matrix = 8 rows x 16 B; K chunks LBO apart, padded by 16 B so the producing
-// stores are bank-conflict free; 8-row groups 128 B apart):
-//   * MMA A = the C maps split into bf16 hi and lo, rows interleaved (row 2j = hi of map j,
-//     row 2j + 1 = lo), M = 64 (n_c <= 32) or 128 (n_c <= 64);
-//   * MMA B = the pair products split into bf16 hi and lo parts, N <= 256 pairs per tile.
-// Per 16-voxel K step and pair tile two MMAs (kind::f16, FP32 accumulate in TMEM),
-// C x P_hi and C x P_lo, give all four hi/lo terms; the hi and lo rows of a map sit in
-// neighbouring TMEM lanes and are summed with one shuffle when the accumulators are read.
+// Operands per tile of T voxels (T = 32 or 64; K steps of 16 voxels):
+//   * MMA A = the pair products, in TENSOR MEMORY: one TMEM lane per pair (M = 128 pairs per
+//     M-tile, up to TC_MAX_MT M-tiles), split into bf16 hi and lo parts, written by the
+//     producer warps with tcgen05.st (two bf16 per 32-bit column, even voxel in the low half);
+//   * MMA B = the C maps split into bf16 hi (rows 0..nc_pad-1) and lo (rows nc_pad..), in
+//     shared memory in the UMMA K-major no-swizzle layout (core matrix = 8 rows x 16 B, K
+//     chunks LBO apart, padded by 16 B so the splitting stores are bank-conflict free).
+// Per K step and M-tile two MMAs (kind::f16, FP32 accumulate in TMEM):
+//   D[:, 0:2 nc_pad] += P_hi [C_hi; C_lo]^T   and   D[:, 0:nc_pad] += P_lo C_hi^T,
+// i.e. the hi*hi, hi*lo and lo*hi terms (lo*lo, ~2^-18 relative, is dropped).  The pair
+// products never pass through shared memory: only the staged fp32 map rows (TMA, 128-byte
+// swizzle, so that the 32 lanes of a producer warp -- 32 pairs reading up to 8 different
+// rows at the same voxels -- hit distinct banks) and the small C operand do.
 //
-// Warp roles (16 warps): producers write the operands from fp32 tiles staged in a ring
-// by TMA (cp.async when rows are not 16-byte aligned); one warp stages, one lane issues the
-// MMAs; they synchronise through mbarriers only.  Every TC_CHAIN tiles the accumulators are
-// folded (tcgen05.ld) into FP64 sums in shared memory, double buffered in TMEM when both
-// sets fit.  Every mbarrier wait is bounded; on timeout the CTA records an error in the
-// workspace, stops issuing work, drains (bounded) and frees TMEM, and the finalize kernel
-// writes NaN outputs.
+// Warp roles (16 warps): 0 stages tiles (TMA, or cp.async when rows are not 16-byte
+// aligned), 1 issues the MMAs (one lane), 2-3 split the C maps, 4-7 fold accumulators
+// (warp w reads TMEM lane quarter w % 4), 8-15 produce pair products (two warps per lane
+// quarter, each taking half of a tile's K steps).  They synchronise through mbarriers
+// only.  Every `chain` tiles (1024 voxels by default) the accumulators are folded
+// (tcgen05.ld) into FP64 sums in shared memory, double buffered in TMEM when both sets fit.
+// Every mbarrier wait is bounded; on timeout the CTA records an error in the workspace,
+// stops issuing work, drains (bounded) and frees TMEM, and the finalize kernel writes NaN
+// outputs.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -28,42 +34,36 @@
 
 namespace pb {
 
-constexpr int TC_KT = 64;                  // voxels per tile (4 MMA K steps of 16)
-constexpr int TC_NCHUNK = TC_KT / 8;       // 16-byte K chunks per tile
-constexpr int TC_STAGE_LD = TC_KT;         // fp32 staging row stride (elements; TMA box rows are dense)
-constexpr int TC_STAGES = 4;               // staging ring depth (tiles in flight per CTA)
-#ifndef TC_NBUF
-#define TC_NBUF 3
-#endif
-// operand buffers: producers run TC_NBUF - 1 tiles ahead of the MMAs, which hides the
-// commit -> mbarrier -> wake-up round trip of the tensor-core pipe behind operand building
-constexpr int TC_OPBUF = TC_NBUF;
-constexpr int TC_CHAIN = 16;               // tiles accumulated in TMEM between FP64 folds
-constexpr int TC_MAX_NT = 4;               // pair tiles (N <= 256 each)
-constexpr int TC_MAX_NC = 64;              // C maps (M = 2 * n_c <= 128)
+constexpr int TC_MAX_MT = 4;                // pair M-tiles of 128 lanes (<= 512 pairs per launch)
+constexpr int TC_MAX_NC = 64;               // C maps per launch
+constexpr int TC_CHAIN_VOX = 1024;          // default voxels accumulated in TMEM (FP32) between FP64 folds
+constexpr int TC_MAX_STAGES = 6;
+constexpr int TC_MAX_NBUF = 4;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 
+constexpr int TC_WARPS = 16;
+constexpr int TC_THREADS = 32 * TC_WARPS;
+constexpr int TC_LOADW = 0, TC_MMAW = 1, TC_CW0 = 2, TC_NCW = 2, TC_FOLD0 = 4, TC_PW0 = 8, TC_PW = 2;
+static_assert(TC_FOLD0 % 4 == 0 && TC_PW0 % 4 == 0, "TMEM lane quarter of warp w is w % 4");
+
 struct TcGeom {
-    int n_rows;                 // staged map rows
-    int off_b, off_c;           // first staged row of the B and C map sets
-    int load_b, load_c;         // B / C rows staged from their own pointers (else they lie in A's rows)
-    int n_pairs, n_c;
-    int M;                      // MMA M: 64 or 128 (C-map rows, hi/lo interleaved)
-    int a_lbo, a_bytes;         // C operand: K-chunk stride, bytes per buffer
-    int n_nt;                   // pair tiles
-    int nt_start[TC_MAX_NT];    // first pair of each tile
-    int nt_n[TC_MAX_NT];        // MMA N of each tile (pair count padded)
-    int nt_col[TC_MAX_NT];      // TMEM column offset of each tile
-    int nt_lbo[TC_MAX_NT];      // K-chunk stride of each tile's operand
-    int nt_off[TC_MAX_NT];      // byte offset of each tile's hi part (lo part follows)
-    int b_bytes;                // pair operand bytes per buffer
-    int ntot;                   // TMEM columns of one accumulator set
+    int T;                      // voxels per tile
+    int n_rows;                 // staged rows (each loaded set padded to 8 rows)
+    int rows_a, rows_b, rows_c; // rows loaded from each set's tensor map (0: the set is rows of another)
+    int off_b, off_c;           // first staged row of the B and C maps
+    int n_pairs, n_c, nc_pad;   // nc_pad = n_c rounded up to 16
+    int n_mt;                   // pair M-tiles
+    int nstage, nbuf, dsets;
+    int pcol0, dcol0, tmem_cols;
+    int half_bytes;             // one 32-voxel half of a stage: n_rows x 128 B
     int stage_bytes;
-    int tmem_cols, dsets;
-    int table_bytes;            // pair table staged in shared memory
-    int acc_ld;                 // row stride (doubles) of the FP64 accumulators [n_c][acc_ld], = 2 mod 16
-    int acc_bytes;
+    int cop_lbo, cop_bytes;     // C operand: K-chunk stride, bytes per buffer
+    int acc_ld;                 // row stride (doubles) of the FP64 sums [pair][acc_ld], odd
+    int acc_bytes;              // rounded to 1024
     int smem_bytes;
+    int chain;                  // tiles accumulated in TMEM between FP64 folds
+    int n_cons;                 // arrivals per stage / operand buffer: active producer warps + C warps
+    int pw_active;              // bit q: pair warps of lane quarter q have pairs
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -89,8 +89,7 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-// try_wait with a suspend-time hint: the waiting thread sleeps until the phase completes
-// or ~0.1 ms passes, instead of spinning on issue slots the producer warps need
+// try_wait with a suspend-time hint (the thread may sleep until the phase completes)
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -98,7 +97,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(100000u)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
         : "memory");
     return ok != 0;
 }
@@ -112,18 +111,37 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return true;
 }
 
+// lane 0 waits (bounded), the warp learns the outcome
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int lane) {
+    bool good = true;
+    if (lane == 0) good = mbar_wait_bounded(bar, parity);
+    return __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
+// D (TMEM) (+)= A (TMEM, M = 128 lanes x 16 bf16) x B (shared memory descriptor)^T
+__device__ __forceinline__ void umma_ts_bf16(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
     uint32_t z = 0;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -132,130 +150,93 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                  : "memory");
 }
 
-// 32 lanes x 8 columns of 32-bit accumulators; tmem_ld_wait() before the values are used
-__device__ __forceinline__ void tmem_ld8_issue(uint32_t taddr, float (&v)[8]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+// 32 lanes x 8 columns of 32-bit values from registers into TMEM (lane quarter of the warp)
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"r"(taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+
+// 32 lanes x 16 columns of 32-bit accumulators; tmem_ld_wait() before the values are used
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+__device__ __forceinline__ void cp4(uint32_t smem, const void *gmem, int valid_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem), "l"(gmem), "r"(valid_bytes));
 }
 
-__device__ __forceinline__ void cp16(void *smem, const void *gmem, int valid_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem),
-                 "r"(valid_bytes));
-}
-__device__ __forceinline__ void cp4(void *smem, const void *gmem, int valid_bytes) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem),
-                 "r"(valid_bytes));
-}
-
-// split 8 fp32 values into packed bf16 hi and lo parts (hi = rn(x), lo = rn(x - hi))
-__device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo) {
-    uint32_t h[4], l[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        __nv_bfloat162 hh = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
-        float2 hf = __bfloat1622float2(hh);
-        __nv_bfloat162 ll = __floats2bfloat162_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
-        h[i] = *reinterpret_cast<uint32_t *>(&hh);
-        l[i] = *reinterpret_cast<uint32_t *>(&ll);
-    }
-    hi = make_uint4(h[0], h[1], h[2], h[3]);
-    lo = make_uint4(l[0], l[1], l[2], l[3]);
-}
-
-__device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+__device__ __forceinline__ void tma_load_2d(uint32_t smem_dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-            smem_u32(smem_dst)),
+            smem_dst),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
+// bf16 hi = rn(x), lo = rn(x - hi) of two fp32 values, packed (first value in the low half)
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    float2 hf = __bfloat1622float2(h);
+    __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+    hi = *reinterpret_cast<uint32_t *>(&h);
+    lo = *reinterpret_cast<uint32_t *>(&l);
 }
 
-// Warp roles: warps 0..TC_PROD-1 produce operands, warp TC_PROD stages tiles (TMA, or
-// cp.async), warp TC_PROD+1 issues MMAs, warps TC_FOLD0.. fold the TMEM accumulators of each
-// finished chain into the FP64 sums while the producers go on with the next one.
-#ifndef TC_NPROD
-#define TC_NPROD 14
-#endif
-#ifndef TC_NUPT
-#define TC_NUPT 3
-#endif
-constexpr int TC_PROD = TC_NPROD;  // producer warps
-constexpr int TC_UPT = TC_NUPT;    // units per producer thread handled with hoisted loads
-constexpr int TC_FOLDW = 4;        // fold warps, one per TMEM lane quarter
-constexpr int TC_THREADS = 32 * (TC_PROD + 2 + TC_FOLDW);
-constexpr int TC_LOADW = TC_PROD;  // staging warp
-constexpr int TC_MMAW = TC_PROD + 1;
-constexpr int TC_FOLD0 = TC_PROD + 2;
-static_assert(TC_FOLD0 % 4 == 0, "fold warp w reads TMEM lane quarter w % 4: they must start on a multiple of 4");
+// byte offset of the 16-byte chunk `ch` (4 voxels) of staged row r within a 32-voxel half
+// (TMA 128-byte swizzle: chunk index XOR row mod 8)
+__device__ __forceinline__ uint32_t stage_off(int r, int ch) { return (uint32_t)r * 128u + (uint32_t)((ch ^ (r & 7)) << 4); }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t *bar) {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-
+template <int T>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     triplet_tc_kernel(const float *A, int n_a, const float *B, int n_b, const float *C, int n_c, int64_t n_vox,
                       int use_tma, const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                       const __grid_constant__ CUtensorMap map_c, const int32_t *pairs, const __grid_constant__ TcGeom geo,
                       double *partials, int *err) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    // [FP64 accumulators][stage ring][C operand x2][pair operand x2][pairs]; bases computed
-    // arithmetically (runtime-indexed pointer arrays would live in local memory)
+    constexpr int KS = T / 16;       // MMA K steps per tile
+    constexpr int HALVES = T / 32;   // 32-voxel swizzled halves per stage
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // [FP64 sums][stage ring][C operand buffers][pair rows], from a 1024-byte boundary of the
+    // shared window (the 128-byte swizzle atom of the staged rows)
+    unsigned char *const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     double *const acc = (double *)smem;
     unsigned char *const stage0 = smem + geo.acc_bytes;
-    unsigned char *const abuf0 = stage0 + TC_STAGES * geo.stage_bytes;
-    unsigned char *const bbuf0 = abuf0 + TC_OPBUF * geo.a_bytes;
-    int32_t *const spairs = (int32_t *)(bbuf0 + TC_OPBUF * geo.b_bytes);
-    auto stage = [&](int k) { return (float *)(stage0 + k * geo.stage_bytes); };
+    unsigned char *const cop0 = stage0 + geo.nstage * geo.stage_bytes;
+    int32_t *const spairs = (int32_t *)(cop0 + geo.nbuf * geo.cop_bytes);
 
-    __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES];
-    __shared__ __align__(8) uint64_t opready[TC_OPBUF], opfree[TC_OPBUF], accready[2], accfree[2];
+    __shared__ __align__(8) uint64_t full[TC_MAX_STAGES], empty[TC_MAX_STAGES];
+    __shared__ __align__(8) uint64_t opready[TC_MAX_NBUF], opfree[TC_MAX_NBUF], accready[2], accfree[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int64_t n_tiles = (n_vox + TC_KT - 1) / TC_KT;
+    const int64_t n_tiles = (n_vox + T - 1) / T;
     const int64_t my_tiles = n_tiles > blockIdx.x ? (n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
-    // operand buffers start at zero: padding rows stay zero for the whole kernel
-    for (int i = tid; i < TC_OPBUF * (geo.a_bytes + geo.b_bytes) / 16; i += TC_THREADS)
-        reinterpret_cast<uint4 *>(abuf0)[i] = make_uint4(0, 0, 0, 0);
+    // C operand buffers start at zero (the padding rows nc_pad > n_c stay zero)
+    for (int i = tid; i < geo.nbuf * geo.cop_bytes / 16; i += TC_THREADS)
+        reinterpret_cast<uint4 *>(cop0)[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < 2 * geo.n_pairs; i += TC_THREADS) spairs[i] = pairs[i];
-    for (int i = tid; i < n_c * geo.acc_ld; i += TC_THREADS) acc[i] = 0.0;
+    for (int i = tid; i < geo.n_pairs * geo.acc_ld; i += TC_THREADS) acc[i] = 0.0;
     if (tid == 0) {
-        for (int k = 0; k < TC_STAGES; ++k) {
+        for (int k = 0; k < geo.nstage; ++k) {
             mbar_init(&full[k], use_tma ? 1 : 32);
-            mbar_init(&empty[k], TC_PROD);
+            mbar_init(&empty[k], geo.n_cons);
         }
-        for (int k = 0; k < TC_OPBUF; ++k) {
-            mbar_init(&opready[k], TC_PROD);
+        for (int k = 0; k < geo.nbuf; ++k) {
+            mbar_init(&opready[k], geo.n_cons);
             mbar_init(&opfree[k], 1);
         }
         for (int k = 0; k < 2; ++k) {
             mbar_init(&accready[k], 1);
-            mbar_init(&accfree[k], TC_FOLDW);
+            mbar_init(&accfree[k], 4);
         }
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -275,34 +256,38 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == TC_LOADW) {
         // ---------------- staging warp ----------------
         for (int64_t it = 0; it < my_tiles; ++it) {
-            const int slot = (int)(it % TC_STAGES);
-            if (it >= TC_STAGES) {
-                bool good = true;
-                if (lane == 0) good = mbar_wait_bounded(&empty[slot], (uint32_t)(((it - TC_STAGES) / TC_STAGES) & 1));
-                good = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
-                if (!good) { atomicExch(&abort_flag, 1); break; }
+            const int slot = (int)(it % geo.nstage);
+            if (it >= geo.nstage && !warp_wait(&empty[slot], (uint32_t)(((it - geo.nstage) / geo.nstage) & 1), lane)) {
+                atomicExch(&abort_flag, 1);
+                break;
             }
             if (*(volatile int *)&abort_flag) break;
-            const int64_t v0 = (blockIdx.x + it * (int64_t)gridDim.x) * TC_KT;
-            float *dst = stage(slot);
+            const int64_t v0 = (blockIdx.x + it * (int64_t)gridDim.x) * T;
+            const uint32_t dst = smem_u32(stage0 + slot * geo.stage_bytes);
             if (use_tma) {
                 if (lane == 0) {
-                    mbar_expect_tx(&full[slot], (uint32_t)(geo.n_rows * TC_KT * 4));
-                    tma_load_2d(dst, &map_a, (int)v0, 0, &full[slot]);
-                    if (geo.load_b) tma_load_2d(dst + geo.off_b * TC_STAGE_LD, &map_b, (int)v0, 0, &full[slot]);
-                    if (geo.load_c) tma_load_2d(dst + geo.off_c * TC_STAGE_LD, &map_c, (int)v0, 0, &full[slot]);
+                    mbar_expect_tx(&full[slot], (uint32_t)(HALVES * (geo.rows_a + geo.rows_b + geo.rows_c) * 128));
+#pragma unroll
+                    for (int h = 0; h < HALVES; ++h) {
+                        const uint32_t d = dst + h * geo.half_bytes;
+                        tma_load_2d(d, &map_a, (int)(v0 + 32 * h), 0, &full[slot]);
+                        if (geo.rows_b) tma_load_2d(d + geo.off_b * 128, &map_b, (int)(v0 + 32 * h), 0, &full[slot]);
+                        if (geo.rows_c) tma_load_2d(d + geo.off_c * 128, &map_c, (int)(v0 + 32 * h), 0, &full[slot]);
+                    }
                 }
             } else {
-                for (int e = lane; e < geo.n_rows * TC_KT; e += 32) {
-                    int r = e / TC_KT, v = e - r * TC_KT;
+                const int nload = geo.rows_a + geo.rows_b + geo.rows_c;
+                for (int e = lane; e < nload * T; e += 32) {
+                    const int q = e / T, v = e - q * T;
                     const float *src;
-                    int m;
-                    if (r < n_a) { src = A; m = r; }
-                    else if (geo.load_b && r < geo.off_b + n_b) { src = B; m = r - geo.off_b; }
-                    else { src = C; m = r - geo.off_c; }
-                    int64_t x = v0 + v;
-                    bool ok = x < n_vox;
-                    cp4(dst + r * TC_STAGE_LD + v, src + (int64_t)m * n_vox + (ok ? x : 0), ok ? 4 : 0);
+                    int m, r;
+                    if (q < geo.rows_a) { src = A; m = q; r = q; }
+                    else if (q < geo.rows_a + geo.rows_b) { src = B; m = q - geo.rows_a; r = geo.off_b + m; }
+                    else { src = C; m = q - geo.rows_a - geo.rows_b; r = geo.off_c + m; }
+                    const int64_t x = v0 + v;
+                    const bool ok = x < n_vox;
+                    const uint32_t d = dst + (v >> 5) * geo.half_bytes + stage_off(r, (v & 31) >> 2) + (v & 3) * 4;
+                    cp4(d, src + (int64_t)m * n_vox + (ok ? x : 0), ok ? 4 : 0);
                 }
                 cp_async_mbar_arrive_noinc(&full[slot]);
             }
@@ -310,11 +295,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else if (warp == TC_MMAW) {
         // ---------------- MMA lane ----------------
         if (lane == 0) {
-            const uint64_t adesc0 = umma_desc(0, geo.a_lbo, 128);
+            const uint32_t idesc_hi = umma_idesc_bf16_f32(128, 2 * geo.nc_pad);
+            const uint32_t idesc_lo = umma_idesc_bf16_f32(128, geo.nc_pad);
             int chain = 0, chain_pos = 0;
             for (int64_t it = 0; it < my_tiles; ++it) {
-                const int buf = (int)(it % TC_OPBUF);
-                if (!mbar_wait_bounded(&opready[buf], (uint32_t)((it / TC_OPBUF) & 1))) {
+                const int buf = (int)(it % geo.nbuf);
+                if (!mbar_wait_bounded(&opready[buf], (uint32_t)((it / geo.nbuf) & 1))) {
                     atomicExch(&abort_flag, 1);
                     break;
                 }
@@ -328,132 +314,58 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (*(volatile int *)&abort_flag) break;
                 tc_fence_after();
                 const int dset = chain % geo.dsets;
-                const uint32_t asm_ = smem_u32(abuf0 + buf * geo.a_bytes);
-                const uint32_t bsm = smem_u32(bbuf0 + buf * geo.b_bytes);
-                for (int t = 0; t < geo.n_nt; ++t) {
-                    const uint32_t d = tmem + (uint32_t)(dset * geo.ntot + geo.nt_col[t]);
-                    const uint32_t idesc = umma_idesc_bf16_f32(geo.M, geo.nt_n[t]);
-                    const uint64_t bdesc0 = umma_desc(0, geo.nt_lbo[t], 128);
-                    const uint32_t bhi = bsm + geo.nt_off[t];
-                    const uint32_t part = TC_NCHUNK * geo.nt_lbo[t];
+                const uint32_t csm = smem_u32(cop0 + buf * geo.cop_bytes);
+                for (int mt = 0; mt < geo.n_mt; ++mt) {
+                    const uint32_t d = tmem + (uint32_t)(geo.dcol0 + (dset * geo.n_mt + mt) * 2 * geo.nc_pad);
+                    const uint32_t a = tmem + (uint32_t)(geo.pcol0 + (buf * geo.n_mt + mt) * T);
 #pragma unroll
-                    for (int s2 = 0; s2 < TC_NCHUNK / 2; ++s2) {
-                        const uint64_t adesc = adesc0 | (uint64_t)(((asm_ + 2 * s2 * geo.a_lbo) >> 4) & 0x3FFF);
-                        const uint32_t bh = bhi + 2 * s2 * geo.nt_lbo[t];
-                        const uint64_t dh = bdesc0 | (uint64_t)((bh >> 4) & 0x3FFF);
-                        const uint64_t dl = bdesc0 | (uint64_t)(((bh + part) >> 4) & 0x3FFF);
-                        umma_bf16(d, adesc, dh, idesc, (chain_pos > 0 || s2 > 0) ? 1u : 0u);
-                        umma_bf16(d, adesc, dl, idesc, 1u);
+                    for (int ks = 0; ks < KS; ++ks) {
+                        const uint64_t bdesc = umma_desc(csm + 2 * ks * geo.cop_lbo, geo.cop_lbo, 128);
+                        umma_ts_bf16(d, a + 16 * ks, bdesc, idesc_hi, (chain_pos > 0 || ks > 0) ? 1u : 0u);
+                        umma_ts_bf16(d, a + 16 * ks + 8, bdesc, idesc_lo, 1u);
                     }
                 }
                 umma_commit(&opfree[buf]);
                 last_issued = (int)it;
-                if (++chain_pos == TC_CHAIN || it + 1 == my_tiles) {
+                if (++chain_pos == geo.chain || it + 1 == my_tiles) {
                     umma_commit(&accready[dset]);  // the chain's sums are complete in TMEM
                     chain_pos = 0;
                     ++chain;
                 }
             }
         }
-    } else if (warp < TC_PROD) {
-        // ---------------- producer warps ----------------
-        // Units of 8 voxels; K chunk c holds tile voxels {4c..4c+3, 32+4c..32+4c+3} for both
-        // operands (the sum over K is order-free), so the 8 lanes of one row read 128
-        // contiguous bytes.  Pair units (pair, chunk) first, then C-map units (map, chunk),
-        // dealt round-robin; a thread's units are the same every tile, so their offsets
-        // are computed once and the TC_UPT units of a tile are loaded before they are
-        // converted (the load latencies overlap).
-        const int n_unit_p = geo.n_pairs * TC_NCHUNK;
-        const int n_unit = n_unit_p + n_c * TC_NCHUNK;
-        constexpr int R4 = TC_STAGE_LD / 4;
-        constexpr int NPT = 32 * TC_PROD;
-        auto unit_info = [&](int u, int &ra, int &rb, int &dst, int &lo, bool &is_pair) {
-            const int c = u & (TC_NCHUNK - 1);
-            is_pair = u < n_unit_p;
-            if (is_pair) {
-                const int p = u >> 3;
-                ra = spairs[2 * p] * R4 + c;
-                rb = (geo.off_b + spairs[2 * p + 1]) * R4 + c;
-                int t = 0;
-                while (t + 1 < geo.n_nt && p >= geo.nt_start[t + 1]) ++t;
-                const int r = p - geo.nt_start[t];
-                dst = geo.nt_off[t] + c * geo.nt_lbo[t] + (r >> 3) * 128 + (r & 7) * 16;
-                lo = TC_NCHUNK * geo.nt_lbo[t];
-            } else {
-                const int j = (u - n_unit_p) >> 3;
-                ra = (geo.off_c + j) * R4 + c;
-                rb = ra;
-                const int m = 2 * j;  // hi row; the lo row 2j+1 is the next core-matrix row
-                dst = c * geo.a_lbo + (m >> 3) * 128 + (m & 7) * 16;
-                lo = 16;
-            }
-        };
-        int u_ra[TC_UPT], u_rb[TC_UPT], u_dst[TC_UPT], u_lo[TC_UPT];
-        bool u_ok[TC_UPT], u_pair[TC_UPT];
-#pragma unroll
-        for (int k = 0; k < TC_UPT; ++k) {
-            const int u = tid + k * NPT;
-            u_ok[k] = u < n_unit;
-            u_ra[k] = u_rb[k] = u_dst[k] = u_lo[k] = 0;
-            u_pair[k] = false;
-            if (u_ok[k]) unit_info(u, u_ra[k], u_rb[k], u_dst[k], u_lo[k], u_pair[k]);
-        }
+    } else if (warp >= TC_CW0 && warp < TC_CW0 + TC_NCW) {
+        // ---------------- C-map splitting warps ----------------
+        // unit (map j, 8-voxel chunk c8): two 16-byte reads of the staged row, bf16 hi to
+        // row j and lo to row nc_pad + j of the B operand (K chunk c8)
+        const int ct = tid - 32 * TC_CW0;
+        const int n_unit = n_c * (T / 8);
         for (int64_t it = 0; it < my_tiles; ++it) {
-            const int buf = (int)(it % TC_OPBUF);
-            const int slot = (int)(it % TC_STAGES);
-            bool good = true;
-            if (lane == 0) {
-                good = mbar_wait_bounded(&full[slot], (uint32_t)((it / TC_STAGES) & 1));
-                if (good && it >= TC_OPBUF)
-                    good = mbar_wait_bounded(&opfree[buf], (uint32_t)(((it - TC_OPBUF) / TC_OPBUF) & 1));
+            const int buf = (int)(it % geo.nbuf);
+            const int slot = (int)(it % geo.nstage);
+            if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane) ||
+                (it >= geo.nbuf && !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane))) {
+                atomicExch(&abort_flag, 1);
+                break;
             }
-            good = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
-            if (!good) { atomicExch(&abort_flag, 1); break; }
             if (*(volatile int *)&abort_flag) break;
-            const float4 *st4 = reinterpret_cast<const float4 *>(stage(slot));
-            unsigned char *ab = abuf0 + buf * geo.a_bytes;
-            unsigned char *bb = bbuf0 + buf * geo.b_bytes;
-            float4 va0[TC_UPT], va1[TC_UPT], vb0[TC_UPT], vb1[TC_UPT];
-#pragma unroll
-            for (int k = 0; k < TC_UPT; ++k) {
-                if (u_ok[k]) {
-                    va0[k] = st4[u_ra[k]];
-                    va1[k] = st4[u_ra[k] + 8];
-                    if (u_pair[k]) {
-                        vb0[k] = st4[u_rb[k]];
-                        vb1[k] = st4[u_rb[k] + 8];
-                    } else {
-                        vb0[k] = make_float4(1.f, 1.f, 1.f, 1.f);
-                        vb1[k] = vb0[k];
-                    }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < TC_UPT; ++k) {
-                if (!u_ok[k]) continue;
-                float x[8] = {va0[k].x * vb0[k].x, va0[k].y * vb0[k].y, va0[k].z * vb0[k].z, va0[k].w * vb0[k].w,
-                              va1[k].x * vb1[k].x, va1[k].y * vb1[k].y, va1[k].z * vb1[k].z, va1[k].w * vb1[k].w};
-                uint4 hi, lo;
-                split8(x, hi, lo);
-                unsigned char *dst = (u_pair[k] ? bb : ab) + u_dst[k];
-                *reinterpret_cast<uint4 *>(dst) = hi;
-                *reinterpret_cast<uint4 *>(dst + u_lo[k]) = lo;
-            }
-            // units beyond TC_UPT per thread (only for very large pair / map counts)
-            for (int u = tid + TC_UPT * NPT; u < n_unit; u += NPT) {
-                int ra, rb, dsto, loo;
-                bool isp;
-                unit_info(u, ra, rb, dsto, loo, isp);
-                float4 a0 = st4[ra], a1 = st4[ra + 8];
-                float4 b0 = isp ? st4[rb] : make_float4(1.f, 1.f, 1.f, 1.f);
-                float4 b1 = isp ? st4[rb + 8] : make_float4(1.f, 1.f, 1.f, 1.f);
-                float x[8] = {a0.x * b0.x, a0.y * b0.y, a0.z * b0.z, a0.w * b0.w,
-                              a1.x * b1.x, a1.y * b1.y, a1.z * b1.z, a1.w * b1.w};
-                uint4 hi, lo;
-                split8(x, hi, lo);
-                unsigned char *dst = (isp ? bb : ab) + dsto;
-                *reinterpret_cast<uint4 *>(dst) = hi;
-                *reinterpret_cast<uint4 *>(dst + loo) = lo;
+            const unsigned char *st = stage0 + slot * geo.stage_bytes;
+            unsigned char *cb = cop0 + buf * geo.cop_bytes;
+            for (int u = ct; u < n_unit; u += 32 * TC_NCW) {
+                const int j = u / (T / 8), c8 = u - j * (T / 8);
+                const int r = geo.off_c + j;
+                const unsigned char *hb = st + (c8 >> 2) * geo.half_bytes;
+                const float4 x0 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3)));
+                const float4 x1 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3) + 1));
+                uint32_t h[4], l[4];
+                split2(x0.x, x0.y, h[0], l[0]);
+                split2(x0.z, x0.w, h[1], l[1]);
+                split2(x1.x, x1.y, h[2], l[2]);
+                split2(x1.z, x1.w, h[3], l[3]);
+                unsigned char *dh = cb + c8 * geo.cop_lbo + (j >> 3) * 128 + (j & 7) * 16;
+                unsigned char *dl = cb + c8 * geo.cop_lbo + ((geo.nc_pad + j) >> 3) * 128 + (j & 7) * 16;
+                *reinterpret_cast<uint4 *>(dh) = make_uint4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint4 *>(dl) = make_uint4(l[0], l[1], l[2], l[3]);
             }
             fence_async_smem();
             __syncwarp();
@@ -462,53 +374,95 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 mbar_arrive(&opready[buf]);
             }
         }
-    }
-    if (warp >= TC_FOLD0) {
+    } else if (warp >= TC_PW0) {
+        // ---------------- pair-product warps ----------------
+        // lane quarter q = warp % 4, half g of each tile's K steps; TMEM lane 32 q + lane of
+        // M-tile mt holds pair 128 mt + 32 q + lane
+        const int q = warp & 3, g = (warp - TC_PW0) >> 2;
+        if ((geo.pw_active >> q) & 1) {
+            uint32_t ra[TC_MAX_MT], rb[TC_MAX_MT];
+            bool ok[TC_MAX_MT];
+#pragma unroll
+            for (int mt = 0; mt < TC_MAX_MT; ++mt) {
+                const int p = 128 * mt + 32 * q + lane;
+                ok[mt] = mt < geo.n_mt && p < geo.n_pairs;
+                ra[mt] = ok[mt] ? (uint32_t)spairs[2 * p] : 0u;
+                rb[mt] = ok[mt] ? (uint32_t)(geo.off_b + spairs[2 * p + 1]) : 0u;
+            }
+            const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
+            for (int64_t it = 0; it < my_tiles; ++it) {
+                const int buf = (int)(it % geo.nbuf);
+                const int slot = (int)(it % geo.nstage);
+                if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane) ||
+                    (it >= geo.nbuf && !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane))) {
+                    atomicExch(&abort_flag, 1);
+                    break;
+                }
+                if (*(volatile int *)&abort_flag) break;
+                tc_fence_after();
+                const unsigned char *st = stage0 + slot * geo.stage_bytes;
+#pragma unroll
+                for (int mt = 0; mt < TC_MAX_MT; ++mt) {
+                    if (mt >= geo.n_mt || 128 * mt + 32 * q >= geo.n_pairs) break;
+                    const uint32_t tcol = tq + (uint32_t)(geo.pcol0 + (buf * geo.n_mt + mt) * T);
+#pragma unroll
+                    for (int kk = 0; kk < KS / TC_PW; ++kk) {
+                        const int ks = g * (KS / TC_PW) + kk;
+                        const unsigned char *hb = st + (ks >> 1) * geo.half_bytes;
+                        uint32_t hi[8], lo[8];
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const int ch = 4 * (ks & 1) + c;
+                            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+                            if (ok[mt]) {
+                                a = *reinterpret_cast<const float4 *>(hb + stage_off(ra[mt], ch));
+                                b = *reinterpret_cast<const float4 *>(hb + stage_off(rb[mt], ch));
+                            }
+                            split2(a.x * b.x, a.y * b.y, hi[2 * c], lo[2 * c]);
+                            split2(a.z * b.z, a.w * b.w, hi[2 * c + 1], lo[2 * c + 1]);
+                        }
+                        tmem_st8(tcol + 16 * ks, hi);
+                        tmem_st8(tcol + 16 * ks + 8, lo);
+                    }
+                }
+                tmem_st_wait();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&empty[slot]);
+                    mbar_arrive(&opready[buf]);
+                }
+            }
+        }
+    } else if (warp >= TC_FOLD0 && warp < TC_FOLD0 + 4) {
         // ---------------- fold warps ----------------
-        // chain c lives in accumulator set c % dsets; its last MMAs commit accready
-        const int q = warp & 3;  // TMEM lane quarter
-        // D row held by this lane: M = 64 -> rows 16q..16q+15 in lanes 0..15
-        const int m = geo.M == 64 ? (lane < 16 ? 16 * q + lane : -1) : 32 * q + lane;
-        const int j = m >= 0 ? (m >> 1) : -1;
-        // after the hi + lo shuffle both lanes of a map hold its sums: the hi lane adds the
-        // even columns of each group of 8, the lo lane the odd ones; with the accumulator row
-        // stride = 2 mod 16 the 16 lanes of one store hit 16 different bank pairs
-        const bool writer = m >= 0 && j < n_c;
-        const int half = m & 1;
-        const int ngrp = geo.ntot / 8;
-        const int64_t n_chains = (my_tiles + TC_CHAIN - 1) / TC_CHAIN;
+        // chain c lives in accumulator set c % dsets; lane quarter q holds pairs 128 mt + 32 q + lane
+        const int q = warp & 3;
+        const int64_t n_chains = (my_tiles + geo.chain - 1) / geo.chain;
         for (int64_t c = 0; c < n_chains; ++c) {
             const int dset = (int)(c % geo.dsets);
-            bool good = true;
-            if (lane == 0) good = mbar_wait_bounded(&accready[dset], (uint32_t)((c / geo.dsets) & 1));
-            good = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
-            if (!good) { atomicExch(&abort_flag, 1); break; }
+            if (!warp_wait(&accready[dset], (uint32_t)((c / geo.dsets) & 1), lane)) {
+                atomicExch(&abort_flag, 1);
+                break;
+            }
             tc_fence_after();
-            const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(dset * geo.ntot);
-            for (int cc = 0; cc < ngrp; cc += 2) {
-                // two column groups per TMEM wait
-                const int cc2 = cc + 1;
-                float v[2][8];
-                tmem_ld8_issue(tbase + cc * 8, v[0]);
-                if (cc2 < ngrp) tmem_ld8_issue(tbase + cc2 * 8, v[1]);
-                tmem_ld_wait();
+            for (int mt = 0; mt < geo.n_mt; ++mt) {
+                const int p0 = 128 * mt + 32 * q;
+                if (p0 >= geo.n_pairs) break;
+                const int p = p0 + lane;
+                double *arow = acc + (size_t)min(p, geo.n_pairs - 1) * geo.acc_ld;
+                const uint32_t tb = tmem + ((uint32_t)(32 * q) << 16) +
+                                    (uint32_t)(geo.dcol0 + (dset * geo.n_mt + mt) * 2 * geo.nc_pad);
+                for (int j0 = 0; j0 < geo.nc_pad; j0 += 16) {
+                    uint32_t h[16], l[16];
+                    tmem_ld16_issue(tb + j0, h);
+                    tmem_ld16_issue(tb + geo.nc_pad + j0, l);
+                    tmem_ld_wait();
+                    if (p < geo.n_pairs) {
 #pragma unroll
-                for (int g2 = 0; g2 < 2; ++g2) {
-                    const int c8 = cc + g2;
-                    if (c8 >= ngrp) break;
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) v[g2][k] += __shfl_xor_sync(0xffffffffu, v[g2][k], 1);
-                    if (writer) {
-                        const int col0 = c8 * 8;
-                        int t = 0;
-                        while (t + 1 < geo.n_nt && col0 >= geo.nt_col[t + 1]) ++t;
-                        const int pend = (t + 1 < geo.n_nt) ? geo.nt_start[t + 1] : geo.n_pairs;
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const float val = half ? v[g2][2 * k + 1] : v[g2][2 * k];
-                            const int p = geo.nt_start[t] + (col0 + 2 * k + half - geo.nt_col[t]);
-                            if (p < pend) acc[j * geo.acc_ld + p] += (double)val;
-                        }
+                        for (int k = 0; k < 16; ++k)
+                            if (j0 + k < n_c)
+                                arow[j0 + k] += (double)__uint_as_float(h[k]) + (double)__uint_as_float(l[k]);
                     }
                 }
             }
@@ -520,7 +474,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // ---------------- teardown ----------------
     if (warp == TC_MMAW && lane == 0 && last_issued >= 0) {
         // the MMAs of the last tile must drain before TMEM is freed (bounded)
-        mbar_wait_bounded(&opfree[last_issued % TC_OPBUF], (uint32_t)((last_issued / TC_OPBUF) & 1));
+        mbar_wait_bounded(&opfree[last_issued % geo.nbuf], (uint32_t)((last_issued / geo.nbuf) & 1));
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     tc_fence_before();
@@ -530,7 +484,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     double *part = partials + (size_t)blockIdx.x * geo.n_pairs * n_c;
     for (int i = tid; i < geo.n_pairs * n_c; i += TC_THREADS) {
         const int p = i / n_c;
-        part[i] = acc[(i - p * n_c) * geo.acc_ld + p];
+        part[i] = acc[(size_t)p * geo.acc_ld + (i - p * n_c)];
     }
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(geo.tmem_cols));
@@ -561,52 +515,71 @@ __global__ void triplet_tc_finalize(const double *partials, int n_cta, int n_pai
 }
 
 struct TcRows {
-    int n_rows, off_b, off_c, load_b, load_c;
+    int n_rows, rows_a, rows_b, rows_c, off_b, off_c;
 };
 
-static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, TcGeom *g) {
+static int pad8(int x) { return (x + 7) & ~7; }
+
+static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g) {
     memset(g, 0, sizeof(*g));
-    const int n_rows = rw.n_rows;
-    g->n_rows = n_rows;
+    g->T = T;
+    g->n_rows = rw.n_rows;
+    g->rows_a = rw.rows_a;
+    g->rows_b = rw.rows_b;
+    g->rows_c = rw.rows_c;
     g->off_b = rw.off_b;
     g->off_c = rw.off_c;
-    g->load_b = rw.load_b;
-    g->load_c = rw.load_c;
     g->n_pairs = n_pairs;
     g->n_c = n_c;
     if (n_c > TC_MAX_NC) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 64 C maps");
-    g->M = (2 * n_c <= 64) ? 64 : 128;
-    g->a_lbo = (g->M / 8) * 128 + 16;
-    g->a_bytes = TC_NCHUNK * g->a_lbo;
-    const int gran = g->M == 64 ? 8 : 16;  // MMA N granularity
-    g->n_nt = (g->n_pairs + 255) / 256;
-    if (g->n_nt > TC_MAX_NT) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 1024 pairs");
-    int col = 0, off = 0;
-    for (int t = 0; t < g->n_nt; ++t) {
-        g->nt_start[t] = t * 256;
-        int np = std::min(256, g->n_pairs - t * 256);
-        g->nt_n[t] = std::max(gran, (np + gran - 1) / gran * gran);
-        g->nt_col[t] = col;
-        col += g->nt_n[t];
-        g->nt_lbo[t] = (g->nt_n[t] / 8) * 128 + 16;
-        g->nt_off[t] = off;
-        off += 2 * TC_NCHUNK * g->nt_lbo[t];
-    }
-    g->b_bytes = off;
-    g->ntot = col;
-    if (g->ntot > 512) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: accumulators exceed TMEM");
-    g->dsets = (2 * g->ntot <= 512) ? 2 : 1;
+    g->nc_pad = (n_c + 15) / 16 * 16;
+    g->n_mt = (n_pairs + 127) / 128;
+    if (g->n_mt > TC_MAX_MT) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 512 pairs");
+    // TMEM: nbuf pair-operand buffers (n_mt x T columns each) + dsets accumulator sets
+    // (n_mt x 2 nc_pad columns each), 512 columns in all
+    const int pcols = g->n_mt * T, dcols = g->n_mt * 2 * g->nc_pad;
+    g->nbuf = 0;
+    for (int ds = 2; ds >= 1 && !g->nbuf; --ds)
+        for (int nb = TC_MAX_NBUF; nb >= 2; --nb)
+            if (nb * pcols + ds * dcols <= 512) {
+                g->nbuf = nb;
+                g->dsets = ds;
+                break;
+            }
+    if (!g->nbuf) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: operands exceed TMEM");
+    g->pcol0 = 0;
+    g->dcol0 = g->nbuf * pcols;
     int cols = 32;
-    while (cols < g->dsets * g->ntot) cols *= 2;
+    while (cols < g->dcol0 + g->dsets * dcols) cols *= 2;
     g->tmem_cols = cols;
-    g->stage_bytes = n_rows * TC_STAGE_LD * 4;
-    g->table_bytes = (int)(2 * g->n_pairs * sizeof(int32_t));
-    g->acc_ld = g->n_pairs + (2 - g->n_pairs % 16 + 16) % 16;
-    g->acc_bytes = (n_c * g->acc_ld * 8 + 127) / 128 * 128;
-    g->smem_bytes = g->acc_bytes + TC_STAGES * g->stage_bytes + TC_OPBUF * (g->a_bytes + g->b_bytes) +
-                    (g->table_bytes + 15) / 16 * 16;
-    if (g->smem_bytes > 225 * 1024)
-        return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: tile too large for shared memory");
+    g->half_bytes = rw.n_rows * 128;
+    g->stage_bytes = (T / 32) * g->half_bytes;
+    g->cop_lbo = (2 * g->nc_pad / 8) * 128 + 16;
+    g->cop_bytes = ((T / 8) * g->cop_lbo + 127) / 128 * 128;
+    g->acc_ld = g->nc_pad + 1;
+    g->acc_bytes = (n_pairs * g->acc_ld * 8 + 1023) / 1024 * 1024;
+    const int table = (2 * n_pairs * 4 + 15) / 16 * 16;
+    const int fixed = 1024 + g->acc_bytes + g->nbuf * g->cop_bytes + table;
+    const int budget = 225 * 1024;
+    int ns = std::min(TC_MAX_STAGES, (budget - fixed) / std::max(1, g->stage_bytes));
+    const int want = tuning().tc_stages > 0 ? tuning().tc_stages
+                                            : std::max(2, (64 * 1024) / std::max(1, g->stage_bytes));  // ~64 KB
+    ns = std::min(ns, want);
+    if (ns < 2) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: tile too large for shared memory");
+    g->nstage = ns;
+    g->smem_bytes = 1024 + g->acc_bytes + ns * g->stage_bytes + g->nbuf * g->cop_bytes + table;
+    g->pw_active = 0;
+    int pw = 0;
+    for (int q = 0; q < 4; ++q) {
+        bool any = false;
+        for (int mt = 0; mt < g->n_mt; ++mt) any = any || (128 * mt + 32 * q < n_pairs);
+        if (any) {
+            g->pw_active |= 1 << q;
+            pw += TC_PW;
+        }
+    }
+    g->n_cons = pw + TC_NCW;
+    g->chain = std::max(1, (tuning().tc_chain > 0 ? tuning().tc_chain : TC_CHAIN_VOX) / T);
     return PB_OK;
 }
 
@@ -630,7 +603,7 @@ static EncodeTiledFn encode_tiled() {
 }
 
 static int tc_grid(int64_t n_vox) {
-    int64_t n_tiles = (n_vox + TC_KT - 1) / TC_KT;
+    int64_t n_tiles = (n_vox + 31) / 32;
     return (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, num_sms()));
 }
 
@@ -647,8 +620,11 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
     PB_CUDA(cudaGetDevice(&dev));
     PB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
     if (major != 10) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction needs an sm_100 device");
+    if (n_a > 256 || n_b > 256 || n_c > TC_MAX_NC)
+        return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 256 maps in a set");
     // staged rows: A's maps, then B's and C's unless they are rows of A already (the same
-    // maps, or a contiguous run of them: B = A + k maps) or C is B
+    // maps, or a contiguous run of them: B = A + k maps) or C is B; each loaded set starts
+    // on a multiple of 8 rows (1024 bytes per 32-voxel half: the swizzle atom)
     const size_t map_bytes = (size_t)n_vox * 4;
     auto rows_of_a = [&](const void *P, int n_p, int *k) {
         if ((const char *)P < (const char *)A) return false;
@@ -657,30 +633,32 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
         *k = (int)(d / map_bytes);
         return *k + n_p <= n_a && d / map_bytes < (size_t)n_a;
     };
-    TcRows rw{n_a, 0, 0, 0, 0};
+    TcRows rw{pad8(n_a), n_a, 0, 0, 0, 0};
     if (!rows_of_a(B, n_b, &rw.off_b)) {
         rw.off_b = rw.n_rows;
-        rw.load_b = 1;
-        rw.n_rows += n_b;
+        rw.rows_b = n_b;
+        rw.n_rows += pad8(n_b);
     }
     if (!rows_of_a(C, n_c, &rw.off_c)) {
-        if (rw.load_b && C == B && n_c <= n_b) {
+        if (rw.rows_b && C == B && n_c <= n_b) {
             rw.off_c = rw.off_b;
         } else {
             rw.off_c = rw.n_rows;
-            rw.load_c = 1;
-            rw.n_rows += n_c;
+            rw.rows_c = n_c;
+            rw.n_rows += pad8(n_c);
         }
     }
-    // pairs go through in chunks small enough for shared memory and TMEM (the FP64
-    // accumulators and the pair operands grow with the pair count)
+    // pairs go through in chunks that fit TMEM and shared memory (the accumulators and the
+    // pair operands grow with the pair count)
     const int n_pairs = counts[1];
+    int T = tuning().tc_tile == 32 ? 32 : 64;
     TcGeom g;
-    int chunk = std::min(n_pairs, 512);
-    int st = tc_geometry(rw, chunk, n_c, &g);
-    while (st == PB_ERR_UNSUPPORTED && chunk > 16 && n_c <= TC_MAX_NC) {
-        chunk = (chunk + 1) / 2;
-        st = tc_geometry(rw, chunk, n_c, &g);
+    int chunk = std::min(n_pairs, 128 * TC_MAX_MT);
+    int st = tc_geometry(rw, chunk, n_c, T, &g);
+    while (st == PB_ERR_UNSUPPORTED && (T == 64 || chunk > 16)) {
+        if (T == 64) T = 32;
+        else chunk = (chunk + 1) / 2;
+        st = tc_geometry(rw, chunk, n_c, T, &g);
     }
     if (st) return st;
     int gx = tc_grid(n_vox);
@@ -689,9 +667,9 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
         return fail(PB_ERR_WORKSPACE, "pb_triplet_contract(tc): workspace too small (need " + std::to_string(need) + ")");
     int *err = (int *)workspace;
     double *partials = (double *)((char *)workspace + 256);
-    // TMA staging needs 16-byte aligned rows and at most 256 rows per map set
+    // TMA staging needs 16-byte aligned rows
     int use_tma = ((n_vox % 4) == 0) && (((uintptr_t)A & 15) == 0) && (((uintptr_t)B & 15) == 0) &&
-                  (((uintptr_t)C & 15) == 0) && n_a <= 256 && n_b <= 256 && n_c <= 256 && n_vox < (1LL << 31);
+                  (((uintptr_t)C & 15) == 0) && n_vox < (1LL << 31);
     CUtensorMap maps[3];
     memset(maps, 0, sizeof(maps));
     EncodeTiledFn enc = use_tma ? encode_tiled() : nullptr;
@@ -702,12 +680,11 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
         for (int k = 0; k < 3 && use_tma; ++k) {
             cuuint64_t dims[2] = {(cuuint64_t)n_vox, (cuuint64_t)rows[k]};
             cuuint64_t strides[1] = {(cuuint64_t)n_vox * 4};
-            cuuint32_t box[2] = {(cuuint32_t)TC_KT, (cuuint32_t)rows[k]};
+            cuuint32_t box[2] = {32u, (cuuint32_t)rows[k]};
             cuuint32_t estr[2] = {1, 1};
-            CUresult r = enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(bases[k]),
-                                                dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            CUresult r = enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(bases[k]), dims, strides,
+                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             if (r != CUDA_SUCCESS) use_tma = 0;
         }
     }
@@ -718,15 +695,25 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
     for (int p_lo = 0; p_lo < n_pairs; p_lo += chunk) {
         const int pk = std::min(chunk, n_pairs - p_lo);
         TcGeom gk;
-        st = tc_geometry(rw, pk, n_c, &gk);
+        st = tc_geometry(rw, pk, n_c, T, &gk);
         if (st) return st;
         if (gk.smem_bytes > smem_max) {
-            PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, gk.smem_bytes));
+            if (T == 64)
+                PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             gk.smem_bytes));
+            else
+                PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             gk.smem_bytes));
             smem_max = gk.smem_bytes;
         }
-        triplet_tc_kernel<<<gx, TC_THREADS, gk.smem_bytes, s>>>(
-            (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
-            maps[2], pairs + 2 * p_lo, gk, partials + (size_t)gx * p_lo * n_c, err);
+        if (T == 64)
+            triplet_tc_kernel<64><<<gx, TC_THREADS, gk.smem_bytes, s>>>(
+                (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
+                maps[2], pairs + 2 * p_lo, gk, partials + (size_t)gx * p_lo * n_c, err);
+        else
+            triplet_tc_kernel<32><<<gx, TC_THREADS, gk.smem_bytes, s>>>(
+                (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
+                maps[2], pairs + 2 * p_lo, gk, partials + (size_t)gx * p_lo * n_c, err);
         PB_LAUNCH_CHECK("pb_triplet_contract(tc)");
     }
     triplet_tc_finalize<<<(counts[3] + 7) / 8, 256, 0, s>>>(partials, gx, n_pairs, chunk, n_c,

@@ -11,6 +11,7 @@ import torch
 from . import _native as nat
 from . import covariance
 from . import pointing
+from . import autotune
 from . import realisations
 
 
@@ -331,11 +332,11 @@ class PSpec:
                 self._pointing()(qr, True, out=qr)
                 Q = b.fft_r2c(qr, out=Q)
                 b.n_FFTs_forward += self.N_bins
-            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, self.k_bins, self._ells(self.Nl),
-                           scaling, fish[i], b.ws)
+            autotune.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, self.k_bins,
+                                self._ells(self.Nl), scaling, fish[i], b.ws)
             if theory is not None:                                       # pspec.py:395-402
-                nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, theory[0],
-                               self._ells(theory[1]), scaling, bm[i], b.ws)
+                autotune.bin_reduce(grid, F64, nat.PB_RED_CROSS, Ainv[i], Q, self.N_bins, theory[0],
+                                    self._ells(theory[1]), scaling, bm[i], b.ws)
         return fish if theory is None else (fish, bm)
 
     def _xi_grids(self, Pk_cov):
@@ -438,7 +439,8 @@ class PSpec:
 
         def cross(a, edges):
             out = torch.empty((self.N_bins, len(edges) - 1), dtype=torch.float64, device=b.device)
-            nat.bin_reduce(grid, F64, nat.PB_RED_CROSS, a, Q, self.N_bins, edges, [(0, 0)], scaling, out, b.ws)
+            autotune.bin_reduce(grid, F64, nat.PB_RED_CROSS, a, Q, self.N_bins, edges, [(0, 0)], scaling, out,
+                                b.ws)
             return out
 
         fish[:, :Nk] = cross(Ainv, self.k_bins)

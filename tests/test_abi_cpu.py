@@ -173,3 +173,21 @@ def test_bilinear_plan_host_logic():
     bad = np.array([5], dtype=np.int32)
     assert lib.pb_bilinear_plan(4, 3, nat.hptr(o[:1]), nat.hptr(bad), nat.hptr(j[:1]), nat.hptr(c[:1]), 1, None,
                                 ctypes.byref(nb), nat.hptr(n)) != 0
+
+
+def test_tuning_settings_round_trip_and_checks():
+    """pb_set_tuning / pb_get_tuning need no device: settings are per host thread, zero means
+    the default, out-of-range values are refused and NULL restores every default."""
+    nat.set_tuning({"tc_tile": 32, "tc_stages": 3, "tc_chain": 2048, "red_method": 1, "red_warps": 2,
+                    "red_waves": 4})
+    try:
+        assert nat.get_tuning() == {"tc_tile": 32, "tc_stages": 3, "tc_chain": 2048, "red_method": 1,
+                                    "red_warps": 2, "red_waves": 4}
+        for bad in ({"tc_tile": 48}, {"tc_stages": 9}, {"tc_chain": 1000}, {"red_method": 3}, {"red_warps": 9},
+                    {"red_waves": -1}):
+            with pytest.raises(ValueError):
+                nat.set_tuning(bad)
+        assert nat.get_tuning()["tc_tile"] == 32  # a refused setting leaves the previous one
+    finally:
+        nat.set_tuning(None)
+    assert all(v == 0 for v in nat.get_tuning().values())

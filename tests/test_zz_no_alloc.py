@@ -72,6 +72,32 @@ def test_noalloc_matches_workspace_entry_point_twice(prec, cdt):
         assert np.max(np.abs(o - r)) <= 1e-10 * np.max(np.abs(r))
 
 
+def test_noalloc_at_the_scratch_limit_and_mode_counts():
+    """1000 rows x 64 bins x 4 multipoles = 256000 doubles per block: only one block per row
+    fits the fixed array, so the entry point runs the reduction on a one-block grid; it must
+    still equal the workspace entry point, and so must the mode counts (REAL2, no input)."""
+    lib = nat.load()
+    n, L = 32, 500.0
+    g = _grid(n, L)
+    kF = 2 * np.pi / L
+    edges = np.ascontiguousarray(np.linspace(kF, 0.35, 65))
+    ells = np.ascontiguousarray(np.array([0, 0, 2, 0, 4, 0, 2, 2], dtype=np.int32))
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    shape = (n, n, n // 2 + 1)
+    a = torch.randn(shape, dtype=torch.complex128, device="cuda", generator=gen)
+    b = torch.randn((1000,) + shape, dtype=torch.complex128, device="cuda", generator=gen)
+    for _ in range(2):
+        ref = _reference_reduce(lib, g, nat.PB_F64, nat.PB_RED_CROSS, a, b, 1000, edges, ells)
+        got = _noalloc_reduce(lib, g, nat.PB_F64, nat.PB_RED_CROSS, a, b, 1000, edges, ells)
+        r, o = ref.cpu().numpy(), got.cpu().numpy()
+        assert np.all(np.isfinite(o))
+        assert np.max(np.abs(o - r)) <= 1e-10 * np.max(np.abs(r))
+    one = np.ascontiguousarray(np.array([0, 0], dtype=np.int32))
+    ref = _reference_reduce(lib, g, nat.PB_F64, nat.PB_RED_REAL2, None, None, 1, edges, one).cpu().numpy()
+    got = _noalloc_reduce(lib, g, nat.PB_F64, nat.PB_RED_REAL2, None, None, 1, edges, one).cpu().numpy()
+    assert np.array_equal(got, ref)
+
+
 def test_noalloc_rejects_oversized_reduction():
     lib = nat.load()
     g = _grid(16, 300.0)
