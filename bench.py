@@ -268,7 +268,7 @@ def run_ours(args, rank, world, local):
 
     def step(i, record=False):
         x = resident[i % n_pool]
-        xk = base.fft_r2c(x)
+        xk = bs._data_spectrum(x)
         w = bs._data_weight(torch.float32)
         G = bs._g_maps(xk, w, 1.0)
         plan = bs._plan("b3", G.shape[0], G.shape[0], G.shape[0], bs._triplet_index())

@@ -76,6 +76,10 @@ typedef struct pb_tuning {
     int32_t red_method;  /* k-bin reduction of many rows: 1 lane per row, 2 mode tiles (0: auto) */
     int32_t red_warps;   /* lane-per-row reduction: warps per block, 1..8 (0: as 48 KB fit)   */
     int32_t red_waves;   /* lane-per-row reduction: blocks per SM per 32-row group, 1..32 (0: 8) */
+    int32_t tc_wait;     /* tensor-core contraction waits: 1 suspending try_wait, 2 polling   */
+                         /* test_wait on the MMA / operand path (0: 1)                        */
+    int32_t tc_dsets;    /* its TMEM accumulator sets, 1 or 2 (0: 2 when they fit); one set   */
+                         /* leaves columns for more operand buffers                           */
 } pb_tuning_t;
 PB_API int pb_set_tuning(const pb_tuning_t *t); /* NULL restores the defaults               */
 PB_API int pb_get_tuning(pb_tuning_t *t);

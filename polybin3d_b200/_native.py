@@ -37,7 +37,8 @@ class PBGrid(ctypes.Structure):
 
 class PBTuning(ctypes.Structure):
     _fields_ = [("tc_tile", ctypes.c_int32), ("tc_stages", ctypes.c_int32), ("tc_chain", ctypes.c_int32),
-                ("red_method", ctypes.c_int32), ("red_warps", ctypes.c_int32), ("red_waves", ctypes.c_int32)]
+                ("red_method", ctypes.c_int32), ("red_warps", ctypes.c_int32), ("red_waves", ctypes.c_int32),
+                ("tc_wait", ctypes.c_int32), ("tc_dsets", ctypes.c_int32)]
 
 
 TUNING_FIELDS = [f for f, _ in PBTuning._fields_]

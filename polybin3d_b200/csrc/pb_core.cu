@@ -23,7 +23,7 @@ int cuda_check(cudaError_t e, const char *where) {
     return fail(PB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-static thread_local pb_tuning_t g_tuning = {0, 0, 0, 0, 0, 0};
+static thread_local pb_tuning_t g_tuning = {0, 0, 0, 0, 0, 0, 0, 0};
 
 const pb_tuning_t &tuning() { return g_tuning; }
 
@@ -207,7 +207,7 @@ extern "C" const char *pb_last_error(void) { return g_last_error.c_str(); }
 
 extern "C" int pb_set_tuning(const pb_tuning_t *t) {
     if (!t) {
-        g_tuning = pb_tuning_t{0, 0, 0, 0, 0, 0};
+        g_tuning = pb_tuning_t{0, 0, 0, 0, 0, 0, 0, 0};
         return PB_OK;
     }
     if (t->tc_tile != 0 && t->tc_tile != 32 && t->tc_tile != 64)
@@ -219,6 +219,8 @@ extern "C" int pb_set_tuning(const pb_tuning_t *t) {
     if (t->red_method < 0 || t->red_method > 2) return fail(PB_ERR_INVALID, "pb_set_tuning: red_method in [0, 2]");
     if (t->red_warps < 0 || t->red_warps > 8) return fail(PB_ERR_INVALID, "pb_set_tuning: red_warps in [0, 8]");
     if (t->red_waves < 0 || t->red_waves > 32) return fail(PB_ERR_INVALID, "pb_set_tuning: red_waves in [0, 32]");
+    if (t->tc_wait < 0 || t->tc_wait > 2) return fail(PB_ERR_INVALID, "pb_set_tuning: tc_wait in [0, 2]");
+    if (t->tc_dsets < 0 || t->tc_dsets > 2) return fail(PB_ERR_INVALID, "pb_set_tuning: tc_dsets in [0, 2]");
     g_tuning = *t;
     return PB_OK;
 }

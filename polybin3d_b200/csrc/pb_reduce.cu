@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(RED_THREADS) binred_rows_kernel(Grid g, const 
 // no atomics, fixed order: deterministic).  Only the part of each line inside the binned
 // range is read (|k| grows along a kz line, so it is one contiguous run of modes).
 // ------------------------------------------------------------------------------------
-constexpr int BL_MODES = 8;  // modes per lane per step
+constexpr int BL_MODES = 4;  // modes per lane per step (the next step's values load meanwhile)
 
 __global__ void binred_geom_kernel(Grid g, RedParams p, int8_t *mbin, double *mw) {
     __shared__ double edges[PB_RED_MAX_BINS + 1];
@@ -249,15 +249,16 @@ __global__ void binred_geom_kernel(Grid g, RedParams p, int8_t *mbin, double *mw
     }
 }
 
-template <typename T, int MODE>
+template <typename T, int MODE, int NE>
 __global__ void __launch_bounds__(256) binred_lanes_kernel(Grid g, const typename cplx<T>::type *a,
                                                            const typename cplx<T>::type *b, int64_t row_stride,
-                                                           int n_rows, int nk, int ne, const int8_t *mbin,
-                                                           const double *mw, double *partials) {
+                                                           int n_rows, int nk, const int8_t *mbin, const double *mw,
+                                                           double *partials) {
     using C = typename cplx<T>::type;
+    constexpr int S = BL_MODES;
     extern __shared__ __align__(16) double bl_acc[];  // [warp][bin][e][32]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int per = nk * ne;
+    const int per = nk * NE;
     double *wacc = bl_acc + (size_t)warp * per * 32;
     for (int i = threadIdx.x; i < nw * per * 32; i += blockDim.x) bl_acc[i] = 0.0;
     __syncthreads();
@@ -266,18 +267,10 @@ __global__ void __launch_bounds__(256) binred_lanes_kernel(Grid g, const typenam
     const C *brow = b + (int64_t)(live ? row : 0) * row_stride;
     const int64_t n_lines = (int64_t)g.n0 * g.n1;
     const int nh2 = g.nh2;
-    double r[PB_RED_MAX_ELLS];
+    double r[NE];
 #pragma unroll
-    for (int e = 0; e < PB_RED_MAX_ELLS; ++e) r[e] = 0.0;
+    for (int e = 0; e < NE; ++e) r[e] = 0.0;
     int cur = -1;
-    auto flush = [&]() {
-#pragma unroll
-        for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
-            if (e < ne) {
-                if (cur >= 0) wacc[(cur * ne + e) * 32 + lane] += r[e];
-                r[e] = 0.0;
-            }
-    };
     for (int64_t line = (int64_t)blockIdx.x * nw + warp; line < n_lines; line += (int64_t)gridDim.x * nw) {
         const int64_t base = line * nh2;
         // the binned run [l_lo, l_hi) of this line
@@ -291,48 +284,76 @@ __global__ void __launch_bounds__(256) binred_lanes_kernel(Grid g, const typenam
                 l_hi = l0 + 32 - __clz(m);
             }
         }
-        for (int l0 = l_lo; l0 < l_hi; l0 += BL_MODES) {
-            C v[BL_MODES];
+        if (l_lo >= l_hi) continue;
+        // software pipeline: the row values of step s + 1 are in flight while step s is summed
+        C v[S];
 #pragma unroll
-            for (int k = 0; k < BL_MODES; ++k) {
-                v[k].x = 0;
-                v[k].y = 0;
-                if (live && l0 + k < l_hi) v[k] = brow[base + l0 + k];
+        for (int k = 0; k < S; ++k) {
+            v[k].x = 0;
+            v[k].y = 0;
+            if (live && l_lo + k < l_hi) v[k] = brow[base + l_lo + k];
+        }
+        for (int l0 = l_lo; l0 < l_hi; l0 += S) {
+            C nv[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                nv[k].x = 0;
+                nv[k].y = 0;
+                if (live && l0 + S + k < l_hi) nv[k] = brow[base + l0 + S + k];
             }
+            // this step's geometry and shared spectrum, loaded before any of it is used
+            int bn[S];
+            C av[S];
+            double w[S][NE];
 #pragma unroll
-            for (int k = 0; k < BL_MODES; ++k) {
-                if (l0 + k >= l_hi) break;
+            for (int k = 0; k < S; ++k) {
                 const int64_t idx = base + l0 + k;
-                const int bin = mbin[idx];
-                if (bin != cur) {
-                    flush();
-                    cur = bin;
-                }
-                if (bin < 0) continue;
-                double f;
+                const bool in = l0 + k < l_hi;
+                bn[k] = in ? (int)mbin[idx] : -2;
                 if (MODE == PB_RED_CROSS) {
-                    const C u = a[idx];
-                    f = (double)u.x * (double)v[k].x + (double)u.y * (double)v[k].y;
-                } else {
-                    f = (double)v[k].x * (double)v[k].x + (double)v[k].y * (double)v[k].y;
+                    av[k].x = 0;
+                    av[k].y = 0;
+                    if (in) av[k] = a[idx];
                 }
-                const double *w = mw + idx * ne;
 #pragma unroll
-                for (int e = 0; e < PB_RED_MAX_ELLS; ++e)
-                    if (e < ne) r[e] += f * w[e];
+                for (int e = 0; e < NE; ++e) w[k][e] = in ? mw[idx * NE + e] : 0.0;
             }
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                if (bn[k] == -2) break;
+                if (bn[k] != cur) {
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) {
+                        if (cur >= 0) wacc[(cur * NE + e) * 32 + lane] += r[e];
+                        r[e] = 0.0;
+                    }
+                    cur = bn[k];
+                }
+                if (bn[k] < 0) continue;
+                double f;
+                if (MODE == PB_RED_CROSS)
+                    f = (double)av[k].x * (double)v[k].x + (double)av[k].y * (double)v[k].y;
+                else
+                    f = (double)v[k].x * (double)v[k].x + (double)v[k].y * (double)v[k].y;
+#pragma unroll
+                for (int e = 0; e < NE; ++e) r[e] += f * w[k][e];
+            }
+#pragma unroll
+            for (int k = 0; k < S; ++k) v[k] = nv[k];
         }
     }
-    flush();
+#pragma unroll
+    for (int e = 0; e < NE; ++e)
+        if (cur >= 0) wacc[(cur * NE + e) * 32 + lane] += r[e];
     __syncthreads();
     // warps' sums in fixed order -> this block's partial of each row
     for (int i = threadIdx.x; i < per * 32; i += blockDim.x) {
-        const int ln = i & 31, be = i >> 5;  // be = bin * ne + e
+        const int ln = i & 31, be = i >> 5;  // be = bin * NE + e
         const int rr = blockIdx.y * 32 + ln;
         if (rr >= n_rows) continue;
         double s = 0.0;
         for (int w = 0; w < nw; ++w) s += bl_acc[((size_t)w * per + be) * 32 + ln];
-        const int bin = be / ne, e = be - bin * ne;
+        const int bin = be / NE, e = be - bin * NE;
         partials[((int64_t)rr * gridDim.x + blockIdx.x) * per + e * nk + bin] = s;
     }
 }
@@ -440,21 +461,34 @@ extern "C" int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const 
         PB_LAUNCH_CHECK("pb_bin_reduce(geometry)");
         dim3 lgrid(LL.gx, (n_rows + 31) / 32);
         const void *rows = (mode == PB_RED_CROSS) ? b : a;
-#define PB_BL_LAUNCH(T, M)                                                                                    \
-    do {                                                                                                      \
-        PB_CUDA(cudaFuncSetAttribute(binred_lanes_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                     (int)LL.smem));                                                          \
-        binred_lanes_kernel<T, M><<<lgrid, 32 * LL.nw, LL.smem, s>>>(G, (const cplx<T>::type *)a,            \
-                                                                    (const cplx<T>::type *)rows, row_stride,  \
-                                                                    n_rows, nk, n_ell, mbin, mw, partials);   \
+#define PB_BL_LAUNCH(T, M, NE)                                                                                  \
+    do {                                                                                                        \
+        PB_CUDA(cudaFuncSetAttribute(binred_lanes_kernel<T, M, NE>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)LL.smem));                                                            \
+        binred_lanes_kernel<T, M, NE><<<lgrid, 32 * LL.nw, LL.smem, s>>>(G, (const cplx<T>::type *)a,          \
+                                                                        (const cplx<T>::type *)rows, row_stride, \
+                                                                        n_rows, nk, mbin, mw, partials);         \
     } while (0)
+#define PB_BL_NE(T, M)                                        \
+    switch (n_ell) {                                          \
+        case 1: PB_BL_LAUNCH(T, M, 1); break;                 \
+        case 2: PB_BL_LAUNCH(T, M, 2); break;                 \
+        case 3: PB_BL_LAUNCH(T, M, 3); break;                 \
+        case 4: PB_BL_LAUNCH(T, M, 4); break;                 \
+        case 5: PB_BL_LAUNCH(T, M, 5); break;                 \
+        case 6: PB_BL_LAUNCH(T, M, 6); break;                 \
+        case 7: PB_BL_LAUNCH(T, M, 7); break;                 \
+        case 8: PB_BL_LAUNCH(T, M, 8); break;                 \
+        default: PB_BL_LAUNCH(T, M, 9); break;                \
+    }
         if (precision == PB_F32) {
-            if (mode == PB_RED_ABS2) PB_BL_LAUNCH(float, PB_RED_ABS2);
-            else PB_BL_LAUNCH(float, PB_RED_CROSS);
+            if (mode == PB_RED_ABS2) PB_BL_NE(float, PB_RED_ABS2)
+            else PB_BL_NE(float, PB_RED_CROSS)
         } else {
-            if (mode == PB_RED_ABS2) PB_BL_LAUNCH(double, PB_RED_ABS2);
-            else PB_BL_LAUNCH(double, PB_RED_CROSS);
+            if (mode == PB_RED_ABS2) PB_BL_NE(double, PB_RED_ABS2)
+            else PB_BL_NE(double, PB_RED_CROSS)
         }
+#undef PB_BL_NE
 #undef PB_BL_LAUNCH
         PB_LAUNCH_CHECK("pb_bin_reduce(lanes)");
         const int per = nk * n_ell;

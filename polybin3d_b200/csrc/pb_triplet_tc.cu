@@ -62,6 +62,7 @@ struct TcGeom {
     int acc_bytes;              // rounded to 1024
     int smem_bytes;
     int chain;                  // tiles accumulated in TMEM between FP64 folds
+    int poll;                   // 1: the MMA lane and the operand producers poll their barriers
     int n_cons;                 // arrivals per stage / operand buffer: active producer warps + C warps
     int pw_active;              // bit q: pair warps of lane quarter q have pairs
 };
@@ -102,9 +103,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// bounded wait: false on timeout
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// non-blocking probe of a phase
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait: false on timeout.  poll != 0: spin on test_wait (the waiter reacts at once;
+// used on the operand / MMA path), else a suspending try_wait
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int poll = 0) {
     long long t0 = clock64();
+    if (poll) {
+        while (!mbar_test_wait(bar, parity)) {
+            if (clock64() - t0 > TC_WAIT_CYCLES) return false;
+        }
+        return true;
+    }
     while (!mbar_try_wait(bar, parity)) {
         if (clock64() - t0 > TC_WAIT_CYCLES) return false;
     }
@@ -112,9 +133,9 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 }
 
 // lane 0 waits (bounded), the warp learns the outcome
-__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int lane) {
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int lane, int poll = 0) {
     bool good = true;
-    if (lane == 0) good = mbar_wait_bounded(bar, parity);
+    if (lane == 0) good = mbar_wait_bounded(bar, parity, poll);
     return __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
 }
 
@@ -300,13 +321,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             int chain = 0, chain_pos = 0;
             for (int64_t it = 0; it < my_tiles; ++it) {
                 const int buf = (int)(it % geo.nbuf);
-                if (!mbar_wait_bounded(&opready[buf], (uint32_t)((it / geo.nbuf) & 1))) {
+                if (!mbar_wait_bounded(&opready[buf], (uint32_t)((it / geo.nbuf) & 1), geo.poll)) {
                     atomicExch(&abort_flag, 1);
                     break;
                 }
                 if (chain_pos == 0 && chain >= geo.dsets) {
                     const int pc = chain - geo.dsets;
-                    if (!mbar_wait_bounded(&accfree[pc % geo.dsets], (uint32_t)((pc / geo.dsets) & 1))) {
+                    if (!mbar_wait_bounded(&accfree[pc % geo.dsets], (uint32_t)((pc / geo.dsets) & 1), geo.poll)) {
                         atomicExch(&abort_flag, 1);
                         break;
                     }
@@ -343,8 +364,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int64_t it = 0; it < my_tiles; ++it) {
             const int buf = (int)(it % geo.nbuf);
             const int slot = (int)(it % geo.nstage);
-            if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane) ||
-                (it >= geo.nbuf && !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane))) {
+            if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane, geo.poll) ||
+                (it >= geo.nbuf &&
+                 !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane, geo.poll))) {
                 atomicExch(&abort_flag, 1);
                 break;
             }
@@ -393,8 +415,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int64_t it = 0; it < my_tiles; ++it) {
                 const int buf = (int)(it % geo.nbuf);
                 const int slot = (int)(it % geo.nstage);
-                if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane) ||
-                    (it >= geo.nbuf && !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane))) {
+                if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane, geo.poll) ||
+                    (it >= geo.nbuf &&
+                     !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane, geo.poll))) {
                     atomicExch(&abort_flag, 1);
                     break;
                 }
@@ -539,7 +562,7 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     // (n_mt x 2 nc_pad columns each), 512 columns in all
     const int pcols = g->n_mt * T, dcols = g->n_mt * 2 * g->nc_pad;
     g->nbuf = 0;
-    for (int ds = 2; ds >= 1 && !g->nbuf; --ds)
+    for (int ds = tuning().tc_dsets == 1 ? 1 : 2; ds >= 1 && !g->nbuf; --ds)
         for (int nb = TC_MAX_NBUF; nb >= 2; --nb)
             if (nb * pcols + ds * dcols <= 512) {
                 g->nbuf = nb;
@@ -580,6 +603,7 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     }
     g->n_cons = pw + TC_NCW;
     g->chain = std::max(1, (tuning().tc_chain > 0 ? tuning().tc_chain : TC_CHAIN_VOX) / T);
+    g->poll = tuning().tc_wait == 2 ? 1 : 0;
     return PB_OK;
 }
 

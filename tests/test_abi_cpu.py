@@ -178,13 +178,13 @@ def test_bilinear_plan_host_logic():
 def test_tuning_settings_round_trip_and_checks():
     """pb_set_tuning / pb_get_tuning need no device: settings are per host thread, zero means
     the default, out-of-range values are refused and NULL restores every default."""
-    nat.set_tuning({"tc_tile": 32, "tc_stages": 3, "tc_chain": 2048, "red_method": 1, "red_warps": 2,
-                    "red_waves": 4})
+    cfg = {"tc_tile": 32, "tc_stages": 3, "tc_chain": 2048, "red_method": 1, "red_warps": 2, "red_waves": 4,
+           "tc_wait": 2, "tc_dsets": 1}
+    nat.set_tuning(cfg)
     try:
-        assert nat.get_tuning() == {"tc_tile": 32, "tc_stages": 3, "tc_chain": 2048, "red_method": 1,
-                                    "red_warps": 2, "red_waves": 4}
+        assert nat.get_tuning() == cfg
         for bad in ({"tc_tile": 48}, {"tc_stages": 9}, {"tc_chain": 1000}, {"red_method": 3}, {"red_warps": 9},
-                    {"red_waves": -1}):
+                    {"red_waves": -1}, {"tc_wait": 3}, {"tc_dsets": 3}):
             with pytest.raises(ValueError):
                 nat.set_tuning(bad)
         assert nat.get_tuning()["tc_tile"] == 32  # a refused setting leaves the previous one
