@@ -15,6 +15,12 @@
 // products never pass through shared memory: only the staged fp32 map rows (TMA, 128-byte
 // swizzle, so that the 32 lanes of a producer warp -- 32 pairs reading up to 8 different
 // rows at the same voxels -- hit distinct banks) and the small C operand do.
+// Side pairs: when the pair count exceeds a multiple of 128 by at most 16 (the 256^3
+// bispectrum's 136 = 128 + 8), the extra pairs do not get a 128-lane M-tile of their own:
+// their products go to a small shared-memory operand S (bf16 hi rows, then lo rows) and one
+// more MMA per K step, D2[C rows, S rows] += [C_hi; C_lo] S^T (C as the A operand, M = 64 or
+// 128), gives all four hi/lo terms.  That keeps the tensor memory for operand buffers and
+// the producer work of one lane quarter from doubling.
 //
 // Warp roles (16 warps): 0 stages tiles (TMA, or cp.async when rows are not 16-byte
 // aligned), 1 issues the MMAs (one lane), 2-3 split the C maps, 4-7 fold accumulators
@@ -35,6 +41,7 @@
 namespace pb {
 
 constexpr int TC_MAX_MT = 4;                // pair M-tiles of 128 lanes (<= 512 pairs per launch)
+constexpr int TC_MAX_SIDE = 16;             // side pairs (shared-memory operand)
 constexpr int TC_MAX_NC = 64;               // C maps per launch
 constexpr int TC_CHAIN_VOX = 1024;          // default voxels accumulated in TMEM (FP32) between FP64 folds
 constexpr int TC_MAX_STAGES = 6;
@@ -51,8 +58,13 @@ struct TcGeom {
     int n_rows;                 // staged rows (each loaded set padded to 8 rows)
     int rows_a, rows_b, rows_c; // rows loaded from each set's tensor map (0: the set is rows of another)
     int off_b, off_c;           // first staged row of the B and C maps
-    int n_pairs, n_c, nc_pad;   // nc_pad = n_c rounded up to 16
+    int n_pairs, n_c, nc_pad;   // nc_pad = n_c rounded up to 16 (32 or 64 with side pairs)
+    int n_tp;                   // pairs in tensor memory (the first n_tp of the launch)
     int n_mt;                   // pair M-tiles
+    int n_side, ns_pad;         // side pairs (after the n_tp) and their operand rows per part (8, 16)
+    int side_lbo, side_bytes;   // side operand: K-chunk stride, bytes per buffer
+    int d2col0;                 // TMEM column of the side accumulators of set 0 (2 ns_pad per set)
+    int acc2_off;               // byte offset of the side FP64 sums [2][n_side][n_c] after acc
     int nstage, nbuf, dsets;
     int pcol0, dcol0, tmem_cols;
     int half_bytes;             // one 32-voxel half of a stage: n_rows x 128 B
@@ -211,6 +223,48 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_
     lo = *reinterpret_cast<uint32_t *>(&l);
 }
 
+// packed fp32x2 arithmetic (one instruction for two lanes' worth of values)
+__device__ __forceinline__ unsigned long long f2pack(float a, float b) {
+    return ((unsigned long long)__float_as_uint(b) << 32) | __float_as_uint(a);
+}
+__device__ __forceinline__ unsigned long long fmul2(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long fsub2(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+// bf16 hi = rn(x), lo = rn(x - hi) of a packed pair (first value in the low half)
+__device__ __forceinline__ void split2p(unsigned long long x, uint32_t &hi, uint32_t &lo) {
+    const float x0 = __uint_as_float((uint32_t)x), x1 = __uint_as_float((uint32_t)(x >> 32));
+    __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    hi = *reinterpret_cast<uint32_t *>(&h);
+    // the bf16 pair back to fp32: low half << 16, high half masked
+    const unsigned long long hf = ((unsigned long long)(hi & 0xFFFF0000u) << 32) | (uint32_t)(hi << 16);
+    const unsigned long long r = fsub2(x, hf);
+    __nv_bfloat162 l = __floats2bfloat162_rn(__uint_as_float((uint32_t)r), __uint_as_float((uint32_t)(r >> 32)));
+    lo = *reinterpret_cast<uint32_t *>(&l);
+}
+// the products of 4 + 4 voxels of two staged rows, split: hi[0..1], lo[0..1] per float4 pair
+__device__ __forceinline__ void prod_split4(const float4 &a, const float4 &b, uint32_t *hi, uint32_t *lo) {
+    split2p(fmul2(f2pack(a.x, a.y), f2pack(b.x, b.y)), hi[0], lo[0]);
+    split2p(fmul2(f2pack(a.z, a.w), f2pack(b.z, b.w)), hi[1], lo[1]);
+}
+
+// D (TMEM) (+)= A (shared memory descriptor) x B (shared memory descriptor)^T
+__device__ __forceinline__ void umma_ss_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+    uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
 // byte offset of the 16-byte chunk `ch` (4 voxels) of staged row r within a 32-voxel half
 // (TMA 128-byte swizzle: chunk index XOR row mod 8)
 __device__ __forceinline__ uint32_t stage_off(int r, int ch) { return (uint32_t)r * 128u + (uint32_t)((ch ^ (r & 7)) << 4); }
@@ -230,7 +284,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     double *const acc = (double *)smem;
     unsigned char *const stage0 = smem + geo.acc_bytes;
     unsigned char *const cop0 = stage0 + geo.nstage * geo.stage_bytes;
-    int32_t *const spairs = (int32_t *)(cop0 + geo.nbuf * geo.cop_bytes);
+    unsigned char *const sop0 = cop0 + geo.nbuf * geo.cop_bytes;
+    int32_t *const spairs = (int32_t *)(sop0 + geo.nbuf * geo.side_bytes);
+    double *const acc2 = (double *)(smem + geo.acc2_off);  // [2 (C hi / lo rows)][n_side][n_c]
 
     __shared__ __align__(8) uint64_t full[TC_MAX_STAGES], empty[TC_MAX_STAGES];
     __shared__ __align__(8) uint64_t opready[TC_MAX_NBUF], opfree[TC_MAX_NBUF], accready[2], accfree[2];
@@ -242,10 +298,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int64_t my_tiles = n_tiles > blockIdx.x ? (n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
     // C operand buffers start at zero (the padding rows nc_pad > n_c stay zero)
-    for (int i = tid; i < geo.nbuf * geo.cop_bytes / 16; i += TC_THREADS)
+    for (int i = tid; i < geo.nbuf * (geo.cop_bytes + geo.side_bytes) / 16; i += TC_THREADS)
         reinterpret_cast<uint4 *>(cop0)[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < 2 * geo.n_side * n_c; i += TC_THREADS) acc2[i] = 0.0;
     for (int i = tid; i < 2 * geo.n_pairs; i += TC_THREADS) spairs[i] = pairs[i];
-    for (int i = tid; i < geo.n_pairs * geo.acc_ld; i += TC_THREADS) acc[i] = 0.0;
+    for (int i = tid; i < geo.n_tp * geo.acc_ld; i += TC_THREADS) acc[i] = 0.0;
     if (tid == 0) {
         for (int k = 0; k < geo.nstage; ++k) {
             mbar_init(&full[k], use_tma ? 1 : 32);
@@ -336,6 +393,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tc_fence_after();
                 const int dset = chain % geo.dsets;
                 const uint32_t csm = smem_u32(cop0 + buf * geo.cop_bytes);
+                if (geo.n_side) {
+                    const uint32_t d2 = tmem + (uint32_t)(geo.d2col0 + dset * 2 * geo.ns_pad);
+                    const uint32_t ssm = smem_u32(sop0 + buf * geo.side_bytes);
+                    const uint32_t idesc_s = umma_idesc_bf16_f32(2 * geo.nc_pad, 2 * geo.ns_pad);
+#pragma unroll
+                    for (int ks = 0; ks < KS; ++ks)
+                        umma_ss_bf16(d2, umma_desc(csm + 2 * ks * geo.cop_lbo, geo.cop_lbo, 128),
+                                     umma_desc(ssm + 2 * ks * geo.side_lbo, geo.side_lbo, 128), idesc_s,
+                                     (chain_pos > 0 || ks > 0) ? 1u : 0u);
+                }
                 for (int mt = 0; mt < geo.n_mt; ++mt) {
                     const uint32_t d = tmem + (uint32_t)(geo.dcol0 + (dset * geo.n_mt + mt) * 2 * geo.nc_pad);
                     const uint32_t a = tmem + (uint32_t)(geo.pcol0 + (buf * geo.n_mt + mt) * T);
@@ -361,6 +428,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // row j and lo to row nc_pad + j of the B operand (K chunk c8)
         const int ct = tid - 32 * TC_CW0;
         const int n_unit = n_c * (T / 8);
+        const int n_all = n_unit + geo.n_side * (T / 8);
         for (int64_t it = 0; it < my_tiles; ++it) {
             const int buf = (int)(it % geo.nbuf);
             const int slot = (int)(it % geo.nstage);
@@ -373,19 +441,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (*(volatile int *)&abort_flag) break;
             const unsigned char *st = stage0 + slot * geo.stage_bytes;
             unsigned char *cb = cop0 + buf * geo.cop_bytes;
-            for (int u = ct; u < n_unit; u += 32 * TC_NCW) {
-                const int j = u / (T / 8), c8 = u - j * (T / 8);
-                const int r = geo.off_c + j;
-                const unsigned char *hb = st + (c8 >> 2) * geo.half_bytes;
-                const float4 x0 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3)));
-                const float4 x1 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3) + 1));
+            unsigned char *sb = sop0 + buf * geo.side_bytes;
+            for (int u = ct; u < n_all; u += 32 * TC_NCW) {
                 uint32_t h[4], l[4];
-                split2(x0.x, x0.y, h[0], l[0]);
-                split2(x0.z, x0.w, h[1], l[1]);
-                split2(x1.x, x1.y, h[2], l[2]);
-                split2(x1.z, x1.w, h[3], l[3]);
-                unsigned char *dh = cb + c8 * geo.cop_lbo + (j >> 3) * 128 + (j & 7) * 16;
-                unsigned char *dl = cb + c8 * geo.cop_lbo + ((geo.nc_pad + j) >> 3) * 128 + (j & 7) * 16;
+                unsigned char *dh, *dl;
+                if (u < n_unit) {
+                    // C map j, 8 voxels: bf16 hi to row j, lo to row nc_pad + j
+                    const int j = u / (T / 8), c8 = u - j * (T / 8);
+                    const int r = geo.off_c + j;
+                    const unsigned char *hb = st + (c8 >> 2) * geo.half_bytes;
+                    const float4 x0 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3)));
+                    const float4 x1 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3) + 1));
+                    split2p(f2pack(x0.x, x0.y), h[0], l[0]);
+                    split2p(f2pack(x0.z, x0.w), h[1], l[1]);
+                    split2p(f2pack(x1.x, x1.y), h[2], l[2]);
+                    split2p(f2pack(x1.z, x1.w), h[3], l[3]);
+                    dh = cb + c8 * geo.cop_lbo + (j >> 3) * 128 + (j & 7) * 16;
+                    dl = cb + c8 * geo.cop_lbo + ((geo.nc_pad + j) >> 3) * 128 + (j & 7) * 16;
+                } else {
+                    // side pair sp, 8 voxels: products split, hi to row sp, lo to row ns_pad + sp
+                    const int v = u - n_unit;
+                    const int sp = v / (T / 8), c8 = v - sp * (T / 8);
+                    const int ra = spairs[2 * (geo.n_tp + sp)], rb = geo.off_b + spairs[2 * (geo.n_tp + sp) + 1];
+                    const unsigned char *hb = st + (c8 >> 2) * geo.half_bytes;
+                    const int ch = 2 * (c8 & 3);
+                    prod_split4(*reinterpret_cast<const float4 *>(hb + stage_off(ra, ch)),
+                                *reinterpret_cast<const float4 *>(hb + stage_off(rb, ch)), h, l);
+                    prod_split4(*reinterpret_cast<const float4 *>(hb + stage_off(ra, ch + 1)),
+                                *reinterpret_cast<const float4 *>(hb + stage_off(rb, ch + 1)), h + 2, l + 2);
+                    dh = sb + c8 * geo.side_lbo + (sp >> 3) * 128 + (sp & 7) * 16;
+                    dl = sb + c8 * geo.side_lbo + ((geo.ns_pad + sp) >> 3) * 128 + (sp & 7) * 16;
+                }
                 *reinterpret_cast<uint4 *>(dh) = make_uint4(h[0], h[1], h[2], h[3]);
                 *reinterpret_cast<uint4 *>(dl) = make_uint4(l[0], l[1], l[2], l[3]);
             }
@@ -407,7 +493,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
             for (int mt = 0; mt < TC_MAX_MT; ++mt) {
                 const int p = 128 * mt + 32 * q + lane;
-                ok[mt] = mt < geo.n_mt && p < geo.n_pairs;
+                ok[mt] = mt < geo.n_mt && p < geo.n_tp;
                 ra[mt] = ok[mt] ? (uint32_t)spairs[2 * p] : 0u;
                 rb[mt] = ok[mt] ? (uint32_t)(geo.off_b + spairs[2 * p + 1]) : 0u;
             }
@@ -426,7 +512,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const unsigned char *st = stage0 + slot * geo.stage_bytes;
 #pragma unroll
                 for (int mt = 0; mt < TC_MAX_MT; ++mt) {
-                    if (mt >= geo.n_mt || 128 * mt + 32 * q >= geo.n_pairs) break;
+                    if (mt >= geo.n_mt || 128 * mt + 32 * q >= geo.n_tp) break;
                     const uint32_t tcol = tq + (uint32_t)(geo.pcol0 + (buf * geo.n_mt + mt) * T);
 #pragma unroll
                     for (int kk = 0; kk < KS / TC_PW; ++kk) {
@@ -441,8 +527,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                 a = *reinterpret_cast<const float4 *>(hb + stage_off(ra[mt], ch));
                                 b = *reinterpret_cast<const float4 *>(hb + stage_off(rb[mt], ch));
                             }
-                            split2(a.x * b.x, a.y * b.y, hi[2 * c], lo[2 * c]);
-                            split2(a.z * b.z, a.w * b.w, hi[2 * c + 1], lo[2 * c + 1]);
+                            prod_split4(a, b, hi + 2 * c, lo + 2 * c);
                         }
                         tmem_st8(tcol + 16 * ks, hi);
                         tmem_st8(tcol + 16 * ks + 8, lo);
@@ -469,11 +554,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             tc_fence_after();
+            if (geo.n_side) {
+                // D2 row m (C hi rows m < nc_pad, lo rows after): M = 64 keeps rows 16 q .. 16 q + 15
+                // in lanes 0..15 of lane quarter q, M = 128 row 32 q + lane
+                const int m = (2 * geo.nc_pad == 64) ? (lane < 16 ? 16 * q + lane : -1) : 32 * q + lane;
+                const int h2 = m >= 0 ? m / geo.nc_pad : 0, j = m >= 0 ? m - h2 * geo.nc_pad : 0;
+                const uint32_t tb = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(geo.d2col0 + dset * 2 * geo.ns_pad);
+                uint32_t v0[16], v1[16];
+                tmem_ld16_issue(tb, v0);
+                if (geo.ns_pad == 16) tmem_ld16_issue(tb + 16, v1);
+                tmem_ld_wait();
+                if (m >= 0 && j < n_c) {
+                    double *a2 = acc2 + (size_t)h2 * geo.n_side * n_c + j;
+#pragma unroll
+                    for (int sp = 0; sp < TC_MAX_SIDE; ++sp) {
+                        if (sp >= geo.n_side) break;
+                        // column sp holds the S_hi products, column ns_pad + sp the S_lo ones
+                        const float x_hi = __uint_as_float(v0[sp]);
+                        const float x_lo = __uint_as_float(geo.ns_pad == 8 ? v0[(8 + sp) & 15] : v1[sp]);
+                        a2[(size_t)sp * n_c] += (double)x_hi + (double)x_lo;
+                    }
+                }
+            }
             for (int mt = 0; mt < geo.n_mt; ++mt) {
                 const int p0 = 128 * mt + 32 * q;
-                if (p0 >= geo.n_pairs) break;
+                if (p0 >= geo.n_tp) break;
                 const int p = p0 + lane;
-                double *arow = acc + (size_t)min(p, geo.n_pairs - 1) * geo.acc_ld;
+                double *arow = acc + (size_t)min(p, geo.n_tp - 1) * geo.acc_ld;
                 const uint32_t tb = tmem + ((uint32_t)(32 * q) << 16) +
                                     (uint32_t)(geo.dcol0 + (dset * geo.n_mt + mt) * 2 * geo.nc_pad);
                 for (int j0 = 0; j0 < geo.nc_pad; j0 += 16) {
@@ -481,7 +588,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     tmem_ld16_issue(tb + j0, h);
                     tmem_ld16_issue(tb + geo.nc_pad + j0, l);
                     tmem_ld_wait();
-                    if (p < geo.n_pairs) {
+                    if (p < geo.n_tp) {
 #pragma unroll
                         for (int k = 0; k < 16; ++k)
                             if (j0 + k < n_c)
@@ -506,8 +613,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (tid == 0 && abort_flag) atomicExch(err, PB_ERR_TIMEOUT);
     double *part = partials + (size_t)blockIdx.x * geo.n_pairs * n_c;
     for (int i = tid; i < geo.n_pairs * n_c; i += TC_THREADS) {
-        const int p = i / n_c;
-        part[i] = acc[(size_t)p * geo.acc_ld + (i - p * n_c)];
+        const int p = i / n_c, j = i - p * n_c;
+        part[i] = p < geo.n_tp ? acc[(size_t)p * geo.acc_ld + j]
+                               : acc2[(size_t)(p - geo.n_tp) * n_c + j] +
+                                     acc2[(size_t)(geo.n_side + p - geo.n_tp) * n_c + j];
     }
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(geo.tmem_cols));
@@ -555,12 +664,17 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     g->n_pairs = n_pairs;
     g->n_c = n_c;
     if (n_c > TC_MAX_NC) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 64 C maps");
-    g->nc_pad = (n_c + 15) / 16 * 16;
-    g->n_mt = (n_pairs + 127) / 128;
+    const int rem = n_pairs % 128;
+    g->n_side = (n_pairs > 128 && rem > 0 && rem <= TC_MAX_SIDE) ? rem : 0;
+    g->n_tp = n_pairs - g->n_side;
+    // the side MMA takes the C operand as its A operand: M = 2 nc_pad must be 64 or 128
+    g->nc_pad = g->n_side ? (n_c <= 32 ? 32 : 64) : (n_c + 15) / 16 * 16;
+    g->ns_pad = g->n_side <= 8 ? 8 : 16;
+    g->n_mt = (g->n_tp + 127) / 128;
     if (g->n_mt > TC_MAX_MT) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 512 pairs");
     // TMEM: nbuf pair-operand buffers (n_mt x T columns each) + dsets accumulator sets
-    // (n_mt x 2 nc_pad columns each), 512 columns in all
-    const int pcols = g->n_mt * T, dcols = g->n_mt * 2 * g->nc_pad;
+    // (n_mt x 2 nc_pad columns each, plus 2 ns_pad for the side pairs), 512 columns in all
+    const int pcols = g->n_mt * T, dcols = g->n_mt * 2 * g->nc_pad + (g->n_side ? 2 * g->ns_pad : 0);
     g->nbuf = 0;
     for (int ds = tuning().tc_dsets == 1 ? 1 : 2; ds >= 1 && !g->nbuf; --ds)
         for (int nb = TC_MAX_NBUF; nb >= 2; --nb)
@@ -572,6 +686,7 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     if (!g->nbuf) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: operands exceed TMEM");
     g->pcol0 = 0;
     g->dcol0 = g->nbuf * pcols;
+    g->d2col0 = g->dcol0 + g->dsets * g->n_mt * 2 * g->nc_pad;
     int cols = 32;
     while (cols < g->dcol0 + g->dsets * dcols) cols *= 2;
     g->tmem_cols = cols;
@@ -579,10 +694,13 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     g->stage_bytes = (T / 32) * g->half_bytes;
     g->cop_lbo = (2 * g->nc_pad / 8) * 128 + 16;
     g->cop_bytes = ((T / 8) * g->cop_lbo + 127) / 128 * 128;
+    g->side_lbo = g->n_side ? (2 * g->ns_pad / 8) * 128 + 16 : 0;
+    g->side_bytes = g->n_side ? ((T / 8) * g->side_lbo + 127) / 128 * 128 : 0;
     g->acc_ld = g->nc_pad + 1;
-    g->acc_bytes = (n_pairs * g->acc_ld * 8 + 1023) / 1024 * 1024;
+    g->acc2_off = g->n_tp * g->acc_ld * 8;
+    g->acc_bytes = (g->acc2_off + 2 * g->n_side * n_c * 8 + 1023) / 1024 * 1024;
     const int table = (2 * n_pairs * 4 + 15) / 16 * 16;
-    const int fixed = 1024 + g->acc_bytes + g->nbuf * g->cop_bytes + table;
+    const int fixed = 1024 + g->acc_bytes + g->nbuf * (g->cop_bytes + g->side_bytes) + table;
     const int budget = 225 * 1024;
     int ns = std::min(TC_MAX_STAGES, (budget - fixed) / std::max(1, g->stage_bytes));
     const int want = tuning().tc_stages > 0 ? tuning().tc_stages
@@ -590,12 +708,12 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     ns = std::min(ns, want);
     if (ns < 2) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: tile too large for shared memory");
     g->nstage = ns;
-    g->smem_bytes = 1024 + g->acc_bytes + ns * g->stage_bytes + g->nbuf * g->cop_bytes + table;
+    g->smem_bytes = 1024 + g->acc_bytes + ns * g->stage_bytes + g->nbuf * (g->cop_bytes + g->side_bytes) + table;
     g->pw_active = 0;
     int pw = 0;
     for (int q = 0; q < 4; ++q) {
         bool any = false;
-        for (int mt = 0; mt < g->n_mt; ++mt) any = any || (128 * mt + 32 * q < n_pairs);
+        for (int mt = 0; mt < g->n_mt; ++mt) any = any || (128 * mt + 32 * q < g->n_tp);
         if (any) {
             g->pw_active |= 1 << q;
             pw += TC_PW;
