@@ -73,6 +73,10 @@ SIGNATURES = {
     "pb_triplet_plan": ([_I, _I, _I, _P, _I, _P, ctypes.POINTER(_SZ), _P], _I),
     "pb_triplet_workspace_size": ([_I, _I, _I64, _P, _I, ctypes.POINTER(_SZ)], _I),
     "pb_triplet_contract": ([_I, _I, _P, _I, _P, _I, _P, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
+    "pb_tiled_maps_bytes": ([_I, _I64, ctypes.POINTER(_SZ)], _I),
+    "pb_tile_maps": ([_P, _I, _I64, _P, _P], _I),
+    "pb_triplet_contract_tiled": ([_I, _P, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
+    "pb_shell_synth_tiled": ([_GP, _P, _I, _P, _I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P], _I),
     "pb_elementwise": ([_I, _I, _I64, _P, _P, _I64, _P, _P, _D, _P, _P], _I),
     "pb_grf_from_noise": ([_GP, _I, _P, _P, _I, _P, _D, _P, _P], _I),
     "pb_grf_philox": ([_GP, _I, _P, _I, _P, _D, _P, _P], _I),
@@ -314,6 +318,60 @@ class TripletPlan:
         _count(2)
         return out
 
+    def contract_tiled(self, tiled, out, ws, method=PB_TRIPLET_TC, scale=1.0):
+        """The contraction with A = B = C = a TiledMaps set (plan made for n_a = n_b = n_c = its maps)."""
+        if not (self.n_a == self.n_b == self.n_c == tiled.n_maps):
+            raise ValueError("contract_tiled: the plan was made for %d/%d/%d maps, the set holds %d"
+                             % (self.n_a, self.n_b, self.n_c, tiled.n_maps))
+        buf = ws.get(self.workspace_bytes(PB_F32, method, tiled.n_vox), "triplet")
+        check(load().pb_triplet_contract_tiled(method, ptr(tiled.data), tiled.n_maps, tiled.n_vox, ptr(self.table),
+                                               hptr(self.counts), float(scale), ptr(out), ptr(buf), buf.numel(),
+                                               stream_ptr()), "pb_triplet_contract_tiled")
+        _count(2)
+        return out
+
+
+def tiled_maps_bytes(n_maps, n_vox):
+    nbytes = ctypes.c_size_t()
+    check(load().pb_tiled_maps_bytes(int(n_maps), int(n_vox), ctypes.byref(nbytes)), "pb_tiled_maps_bytes")
+    return nbytes.value
+
+
+def tiled_index(n_maps, n_vox):
+    """Host int64 array [n_maps, n_vox]: element of each voxel of each map in a tiled set."""
+    R = (n_maps + 7) // 8 * 8
+    v = np.arange(n_vox, dtype=np.int64)[None, :]
+    m = np.arange(n_maps, dtype=np.int64)[:, None]
+    w = v & 31
+    return ((v >> 5) * R + m) * 32 + ((((w >> 2) ^ (m & 7)) << 2) | (w & 3))
+
+
+class TiledMaps:
+    """A tiled map set (include/polybin3d_b200.h): n_maps f32 maps on `shape`, stored as
+    32-voxel slabs in the tensor-core contraction's staging layout.  data: flat float32."""
+
+    def __init__(self, n_maps, shape, device, data=None):
+        self.n_maps, self.shape = int(n_maps), tuple(int(n) for n in shape)
+        self.n_vox = int(np.prod(self.shape))
+        n = tiled_maps_bytes(self.n_maps, self.n_vox) // 4
+        self.data = torch.empty(n, dtype=torch.float32, device=device) if data is None else data
+        if self.data.numel() < n or self.data.dtype != torch.float32:
+            raise ValueError("TiledMaps: data must hold %d float32 values" % n)
+
+    @classmethod
+    def from_maps(cls, maps):
+        """Tile (n_maps, *shape) float32 device maps (pb_tile_maps)."""
+        maps = maps.contiguous()
+        t = cls(maps.shape[0], maps.shape[1:], maps.device)
+        check(load().pb_tile_maps(ptr(maps), t.n_maps, t.n_vox, ptr(t.data), stream_ptr()), "pb_tile_maps")
+        _count(1)
+        return t
+
+    def to_maps(self):
+        """(n_maps, *shape) copy in the plain layout (a device gather)."""
+        idx = torch.as_tensor(tiled_index(self.n_maps, self.n_vox), device=self.data.device)
+        return self.data[idx].reshape((self.n_maps,) + self.shape)
+
 
 def pair_products(X, Y, pairs, Z=None, U=None, s=1.0, out=None):
     """out[p] = s*(X[i]Y[j] - Z[i]U[j]) for host (i, j) pairs; X.. are (n, ...) real maps."""
@@ -372,8 +430,11 @@ def binned_filter(grid, src, out, edges, ells, coef, w=None, wpow=0, scale=1.0):
 def shell_synth(grid, precision, src, out, maps, out_n, ws, w=None, src_stride=None):
     """Real maps out[m] = unnormalised c2r on grid out_n of the filter `maps` (entries
     (src_idx, lo, hi, l1, l2, scale, wpow) as spectral_filter) in one pruned pass per chunk
-    of 64 maps.  Raises NotImplementedError when the band limits do not allow it."""
+    of 64 maps.  out: a (n_maps, *out_n) tensor, or a TiledMaps set of f32 maps (one pass:
+    at most 64 maps).  Raises NotImplementedError when the band limits do not allow it."""
     lib = load()
+    if isinstance(out, TiledMaps):
+        return _shell_synth_tiled(lib, grid, precision, src, out, maps, out_n, ws, w, src_stride)
     on = np.ascontiguousarray(out_n, dtype=np.int32)
     stride = src_stride if src_stride is not None else (src[0].numel() if src is not None and src.dim() == 4 else 0)
     c0 = 0
@@ -406,6 +467,32 @@ def shell_synth(grid, precision, src, out, maps, out_n, ws, w=None, src_stride=N
                                  ptr(out[c0:c0 + len(chunk)]), ptr(buf), buf.numel(), stream_ptr()), "pb_shell_synth")
         _count(3)
         c0 += nc
+    return out
+
+
+def _shell_synth_tiled(lib, grid, precision, src, out, maps, out_n, ws, w, src_stride):
+    if precision != PB_F32:
+        raise ValueError("shell_synth: a tiled set holds f32 maps")
+    if len(maps) != out.n_maps or tuple(int(n) for n in out_n) != out.shape:
+        raise ValueError("shell_synth: the tiled set holds %d maps on %s" % (out.n_maps, out.shape))
+    if len(maps) > SYNTH_MAX_MAPS:
+        raise NotImplementedError("shell_synth: a tiled set is synthesised in one pass of at most 64 maps")
+    on = np.ascontiguousarray(out_n, dtype=np.int32)
+    stride = src_stride if src_stride is not None else (src[0].numel() if src is not None and src.dim() == 4 else 0)
+    arr = np.asarray(maps, dtype=np.float64)
+    si = np.ascontiguousarray(arr[:, 0].astype(np.int32))
+    lo, hi, sc = (np.ascontiguousarray(arr[:, k]) for k in (1, 2, 5))
+    l1, l2, wp = (np.ascontiguousarray(arr[:, k].astype(np.int32)) for k in (3, 4, 6))
+    nbytes = ctypes.c_size_t()
+    check(lib.pb_shell_synth_workspace_size(ctypes.byref(grid), hptr(on), precision, len(maps), hptr(hi),
+                                            ctypes.byref(nbytes)), "pb_shell_synth_workspace_size")
+    if nbytes.value > SYNTH_WS_BYTES:
+        raise NotImplementedError("shell_synth: a tiled set's transform workspace exceeds SYNTH_WS_BYTES")
+    buf = ws.get(nbytes.value, "synth")
+    check(lib.pb_shell_synth_tiled(ctypes.byref(grid), hptr(on), precision, ptr(src), stride, len(maps), hptr(si),
+                                   hptr(lo), hptr(hi), hptr(l1), hptr(l2), hptr(sc), hptr(wp), ptr(w),
+                                   ptr(out.data), ptr(buf), buf.numel(), stream_ptr()), "pb_shell_synth_tiled")
+    _count(3)
     return out
 
 

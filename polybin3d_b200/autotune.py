@@ -5,8 +5,9 @@ candidate setting of pb_tuning_t (include/polybin3d_b200.h) with CUDA events on 
 stream, keeps the fastest and stores it in a JSON file, so later calls -- and later
 processes -- set the winner before launching.  Tuned shapes:
 
-* the tensor-core triplet contraction: voxels per tile (64 / 32), staging ring depth,
-  voxels summed in TMEM between FP64 folds;
+* the tensor-core triplet contraction (from plain maps and from a tiled set): voxels per
+  tile (128 / 64 / 32), staging ring depth, voxels summed in TMEM between FP64 folds, the
+  barrier-wait form;
 * the k-bin reduction of many rows (>= 16): lane-per-row kernel (warps per block, blocks
   per SM) against the mode-tile kernel.
 
@@ -26,6 +27,9 @@ from . import _native as nat
 
 TC_CANDIDATES = [{}, {"tc_tile": 32}, {"tc_chain": 2048}, {"tc_tile": 32, "tc_chain": 2048}, {"tc_stages": 3},
                  {"tc_tile": 32, "tc_stages": 4}]
+# from a tiled map set (one contiguous copy per tile): 128-voxel tiles by default
+TC_TILED_CANDIDATES = [{}, {"tc_tile": 64}, {"tc_stages": 3}, {"tc_wait": 2}, {"tc_chain": 2048},
+                       {"tc_tile": 64, "tc_stages": 6}]
 RED_CANDIDATES = [{}, {"red_method": 2}, {"red_method": 1, "red_warps": 2},
                   {"red_method": 1, "red_warps": 2, "red_waves": 16}, {"red_method": 1, "red_warps": 4, "red_waves": 4},
                   {"red_method": 1, "red_waves": 16}]
@@ -142,6 +146,14 @@ def contract(plan, A, B, C, out, ws, method, scale):
     cfg = tuner().choose(key, TC_CANDIDATES, lambda: plan.contract(A, B, C, out, ws, method=method, scale=scale))
     with applied(cfg):
         return plan.contract(A, B, C, out, ws, method=method, scale=scale)
+
+
+def contract_tiled(plan, tiled, out, ws, scale):
+    """plan.contract_tiled with the tuned launch shape for this shape."""
+    key = "tct|%s|%d|%d|%d" % (device_tag(tiled.data.device), tiled.n_vox, tiled.n_maps, plan.n_pairs)
+    cfg = tuner().choose(key, TC_TILED_CANDIDATES, lambda: plan.contract_tiled(tiled, out, ws, scale=scale))
+    with applied(cfg):
+        return plan.contract_tiled(tiled, out, ws, scale=scale)
 
 
 def bin_reduce(grid, precision, mode, a, b, n_rows, edges, ells, scale, out, ws, accumulate=False, row_stride=0):

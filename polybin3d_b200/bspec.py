@@ -338,6 +338,13 @@ class BSpec:
         # spec: (bin, l1, l2, scale[, source index]); the sources lie src_stride apart
         maps = [(sp[4] if len(sp) > 4 else 0, ks[sp[0]], ks[sp[0] + 1], sp[1], sp[2], sp[3] / b.nreal, wp)
                 for sp in specs]
+        if isinstance(out, nat.TiledMaps):
+            # a tiled set comes from the pruned synthesis only (one pass)
+            if self.synthesis == 'cufft' or not self._synth_ok.get(dims, True):
+                raise NotImplementedError("tiled maps need the pruned synthesis")
+            nat.shell_synth(b.grid, prec, src, out, maps, dims, b.ws, w=w, src_stride=b.nhalf)
+            b.n_FFTs_reverse += len(specs)
+            return out
         if self.synthesis != 'cufft' and self._synth_ok.get(dims, True):
             if out is None:
                 out = torch.empty((len(specs),) + tuple(dims), dtype=dtype, device=b.device)
@@ -482,8 +489,7 @@ class BSpec:
                 w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), rd)
             scale = 1.0
         if not linear:
-            G = self._g_maps(xk, w, scale)
-            return self._contract('b3', G, G, G, self._triplet_index())
+            return self._b3_sums(xk, w, scale)
         # data maps and one simulation's maps side by side: X = [g; g_ii]
         n = self.Nl * self.Nk_squeeze
         X = torch.empty((2 * n,) + tuple(self.map_grid), dtype=rd, device=b.device)
@@ -495,6 +501,54 @@ class BSpec:
             self._g_maps(self._sim_spectrum(ii, rd), None, 1.0, out=S)
             b1 += self._set_sums('b1', X, n, ((0, 1, 1), (1, 0, 1), (1, 1, 0)))
         return out - b1 / self.N_it
+
+    def _b3_sums(self, xk, w, scale):
+        """FP64 sums B3[i] = assemble_b3 of the g-maps of one weighted spectrum.  With the
+        tensor-core contraction the g-maps are synthesised straight into a tiled set (the
+        contraction's staging layout: each tile of voxels of all maps is one contiguous
+        copy), else into plain maps."""
+        idx = self._triplet_index()
+        dt = xk.real.dtype
+        if self._tiled_ok(dt):
+            T = self._g_maps_tiled(xk, w, scale)
+            if T is not None:
+                plan = self._plan('b3', T.n_maps, T.n_maps, T.n_maps, idx)
+                out = torch.empty(plan.n_trip, dtype=torch.float64, device=self.base.device)
+                try:
+                    return autotune.contract_tiled(plan, T, out, self.base.ws, self._grid_scale(T.shape))
+                except NotImplementedError:
+                    if self.contraction == 'tc':
+                        raise
+                    self._tiled = False
+                    plan.tc_unsupported = True
+        G = self._g_maps(xk, w, scale)
+        return self._contract('b3', G, G, G, idx)
+
+    def _tiled_ok(self, dtype):
+        return (getattr(self, '_tiled', True) and self.synthesis != 'cufft' and
+                self._method(dtype) == nat.PB_TRIPLET_TC and self.Nl * self.Nk_squeeze <= 64)
+
+    def _grid_scale(self, shape):
+        """Factor taking sums over the (dealiased) map grid `shape` to full-grid sums."""
+        b = self.base
+        if tuple(shape) != tuple(int(n) for n in b.gridsize):
+            return float(np.prod(b.gridsize)) / float(np.prod(shape))
+        return 1.0
+
+    def _g_maps_tiled(self, xk, w, scale):
+        """The g-maps of _g_maps as a tiled set, or None when the pruned synthesis cannot
+        make them (the caller takes the plain path)."""
+        b = self.base
+        T = nat.TiledMaps(self.Nl * self.Nk_squeeze, self.map_grid, b.device)
+        try:
+            if b.sightline == 'local' and self.lmax > 0:
+                self._g_maps_local(xk, w, scale, out=T)
+            else:
+                self._g_maps(xk, w, scale, out=T)
+        except NotImplementedError:
+            self._tiled = False
+            return None
+        return T
 
     def _set_sums(self, key, X, n, terms):
         """FP64 sum over `terms` (ta, tb, tc) of the triplet sums

@@ -91,4 +91,21 @@ template <typename T> struct cplx;
 template <> struct cplx<float> { using type = float2; };
 template <> struct cplx<double> { using type = double2; };
 
+// ---- tiled map sets ---------------------------------------------------------------
+// n_maps f32 maps of n_vox voxels as 32-voxel slabs: slab s holds voxels 32 s .. 32 s + 31
+// of rows 0 .. R-1 (R = n_maps rounded up to 8), 128 bytes per row, the 16-byte chunk c
+// (4 voxels) of row r at chunk position c ^ (r mod 8).  Slabs run to a multiple of 4 (128
+// voxels), so any tile of 32, 64 or 128 voxels is one contiguous block laid out as the
+// tensor-core contraction stages it in shared memory (the 128-byte swizzle).
+constexpr int TILED_SLAB = 32, TILED_ALIGN = 128;
+__host__ __device__ __forceinline__ int tiled_rows(int n_maps) { return (n_maps + 7) & ~7; }
+__host__ __device__ __forceinline__ int64_t tiled_slabs(int64_t n_vox) {
+    return (n_vox + TILED_ALIGN - 1) / TILED_ALIGN * (TILED_ALIGN / TILED_SLAB);
+}
+// element index of voxel v of map m in a set of `rows` rows
+__host__ __device__ __forceinline__ int64_t tiled_index(int64_t v, int m, int rows) {
+    const int w = (int)(v & 31);
+    return ((v >> 5) * rows + m) * 32 + ((((w >> 2) ^ (m & 7)) << 2) | (w & 3));
+}
+
 }  // namespace pb

@@ -210,8 +210,8 @@ extern "C" int pb_set_tuning(const pb_tuning_t *t) {
         g_tuning = pb_tuning_t{0, 0, 0, 0, 0, 0, 0, 0};
         return PB_OK;
     }
-    if (t->tc_tile != 0 && t->tc_tile != 32 && t->tc_tile != 64)
-        return fail(PB_ERR_INVALID, "pb_set_tuning: tc_tile must be 0, 32 or 64");
+    if (t->tc_tile != 0 && t->tc_tile != 32 && t->tc_tile != 64 && t->tc_tile != 128)
+        return fail(PB_ERR_INVALID, "pb_set_tuning: tc_tile must be 0, 32, 64 or 128");
     if (t->tc_stages != 0 && (t->tc_stages < 2 || t->tc_stages > 6))
         return fail(PB_ERR_INVALID, "pb_set_tuning: tc_stages must be 0 or in [2, 6]");
     if (t->tc_chain != 0 && t->tc_chain != 512 && t->tc_chain != 1024 && t->tc_chain != 2048)

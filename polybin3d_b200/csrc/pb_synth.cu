@@ -55,6 +55,7 @@ struct SynthParams {
     int64_t src_stride;
     FftAxis ax, ay, az;
     int c1;                     // S1 column chunks per plane (max over maps)
+    int tiled_rows;             // 0: out is [map][x][y][z]; else a tiled set of this many rows
     SynthMap maps[SY_MAX_MAPS];
 };
 
@@ -575,7 +576,14 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
     const int K = mp.kz_max;
     make_twiddles<T>(tw, n);  // made visible by the barrier after the first pass
     const int64_t plane = (int64_t)p.m0 * p.m1;
-    T *o = out + (int64_t)m * p.m0 * p.m1 * p.m2 + ((int64_t)x * p.m1 + y0) * p.m2;
+    // voxel v0 + yy m2 + z of map m: plain [map][voxel] rows, or the slab layout of a tiled set
+    const int64_t v0 = ((int64_t)x * p.m1 + y0) * p.m2;
+    T *const o = out + (int64_t)m * plane * p.m2 + v0;
+    const int trows = p.tiled_rows;
+    auto put = [&](int yy, int z, T val) {
+        if (trows) out[tiled_index(v0 + (int64_t)yy * p.m2 + z, m, trows)] = val;
+        else o[(int64_t)yy * p.m2 + z] = val;
+    };
     if constexpr (N > 0 && pass_count(N) >= 2) {
         // first pass straight from H (a warp reads the (y, y+1) pairs of 32 lines at one kz:
         // 512 contiguous bytes; it needs no twiddles), last pass straight to the real rows
@@ -615,8 +623,8 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
                 return r;
             },
             [&](int line, int z, C v) {
-                o[(int64_t)(2 * line) * p.m2 + z] = v.x;
-                o[(int64_t)(2 * line + 1) * p.m2 + z] = v.y;
+                put(2 * line, z, v.x);
+                put(2 * line + 1, z, v.y);
             });
         return;
     }
@@ -659,11 +667,10 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int yy = warp; yy < ny; yy += nw) {
         const C *row = res + (int64_t)(yy >> 1) * ld;
-        T *orow = o + (int64_t)yy * p.m2;
         if (yy & 1)
-            for (int z = lane; z < n; z += 32) orow[z] = row[z].y;
+            for (int z = lane; z < n; z += 32) put(yy, z, row[z].y);
         else
-            for (int z = lane; z < n; z += 32) orow[z] = row[z].x;
+            for (int z = lane; z < n; z += 32) put(yy, z, row[z].x);
     }
 }
 
@@ -872,21 +879,34 @@ extern "C" int pb_shell_synth_workspace_size(const pb_grid_t *g, const int32_t *
     return PB_OK;
 }
 
-extern "C" int pb_shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
-                              int64_t src_stride, int n_maps, const int32_t *src_idx, const double *lo,
-                              const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
-                              const int32_t *wpow, const void *w, void *out, void *workspace, size_t workspace_bytes,
-                              void *stream) {
+static int shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src, int64_t src_stride,
+                       int n_maps, const int32_t *src_idx, const double *lo, const double *hi, const int32_t *l1,
+                       const int32_t *l2, const double *scale, const int32_t *wpow, const void *w, void *out,
+                       void *workspace, size_t workspace_bytes, void *stream, bool tiled) {
     if (!out || !lo || !hi || !l1 || !l2 || !scale) return fail(PB_ERR_INVALID, "pb_shell_synth: NULL argument");
     SynthLayout L;
     int st = synth_layout(g, out_n, precision, n_maps, lo, hi, src_idx, l1, l2, scale, wpow, src_stride, &L);
     if (st) return st;
+    cudaStream_t s = as_stream(stream);
+    if (tiled) {
+        if (precision != PB_F32) return fail(PB_ERR_INVALID, "pb_shell_synth_tiled: tiled sets hold f32 maps");
+        if ((uintptr_t)out & 15) return fail(PB_ERR_INVALID, "pb_shell_synth_tiled: output not 16-byte aligned");
+        L.p.tiled_rows = tiled_rows(n_maps);
+        // the voxels past the grid in the last 128-voxel tile read as zeros (the z pass then
+        // writes every voxel of the grid; padding rows past n_maps are never read)
+        const int64_t n_vox = (int64_t)L.p.m0 * L.p.m1 * L.p.m2;
+        const int64_t rows = L.p.tiled_rows;
+        if (n_vox % TILED_ALIGN) {
+            const int64_t first = tiled_slabs(n_vox) - TILED_ALIGN / TILED_SLAB;
+            PB_CUDA(cudaMemsetAsync((float *)out + first * rows * TILED_SLAB, 0,
+                                    (size_t)(TILED_ALIGN / TILED_SLAB) * rows * TILED_SLAB * sizeof(float), s));
+        }
+    }
     for (int m = 0; m < n_maps; ++m)
         if (L.p.maps[m].wpow != 0 && !w) return fail(PB_ERR_INVALID, "pb_shell_synth: wpow set but weight grid is NULL");
     const size_t c = precision == PB_F64 ? 16 : 8;
     const size_t need = (size_t)(L.u_elems + L.h_elems) * c + 256;
     if (!workspace || workspace_bytes < need) return fail(PB_ERR_INVALID, "pb_shell_synth: workspace too small");
-    cudaStream_t s = as_stream(stream);
     char *ws = (char *)(((uintptr_t)workspace + 255) & ~(uintptr_t)255);
     if (precision == PB_F32) {
         float2 *U = (float2 *)ws;
@@ -896,4 +916,22 @@ extern "C" int pb_shell_synth(const pb_grid_t *g, const int32_t *out_n, int prec
         st = launch_synth<double>(L, (const double2 *)src, (const double *)w, U, U + L.u_elems, (double *)out, s);
     }
     return st;
+}
+
+extern "C" int pb_shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
+                              int64_t src_stride, int n_maps, const int32_t *src_idx, const double *lo,
+                              const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
+                              const int32_t *wpow, const void *w, void *out, void *workspace, size_t workspace_bytes,
+                              void *stream) {
+    return shell_synth(g, out_n, precision, src, src_stride, n_maps, src_idx, lo, hi, l1, l2, scale, wpow, w, out,
+                       workspace, workspace_bytes, stream, false);
+}
+
+extern "C" int pb_shell_synth_tiled(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
+                                    int64_t src_stride, int n_maps, const int32_t *src_idx, const double *lo,
+                                    const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
+                                    const int32_t *wpow, const void *w, void *out, void *workspace,
+                                    size_t workspace_bytes, void *stream) {
+    return shell_synth(g, out_n, precision, src, src_stride, n_maps, src_idx, lo, hi, l1, l2, scale, wpow, w, out,
+                       workspace, workspace_bytes, stream, true);
 }

@@ -2,7 +2,7 @@
 //   out[t] = scale * sum_x A[i1](x) B[i2](x) C[i3](x)
 // as the GEMM  D[pair, c] = sum_x P_pair(x) C_c(x)  with P_pair = A[i1] * B[i2].
 //
-// Operands per tile of T voxels (T = 32 or 64; K steps of 16 voxels):
+// Operands per tile of T voxels (T = 32, 64 or 128; K steps of 16 voxels):
 //   * MMA A = the pair products, in TENSOR MEMORY: one TMEM lane per pair (M = 128 pairs per
 //     M-tile, up to TC_MAX_MT M-tiles), split into bf16 hi and lo parts, written by the
 //     producer warps with tcgen05.st (two bf16 per 32-bit column, even voxel in the low half);
@@ -22,8 +22,13 @@
 // 128), gives all four hi/lo terms.  That keeps the tensor memory for operand buffers and
 // the producer work of one lane quarter from doubling.
 //
-// Warp roles (16 warps): 0 stages tiles (TMA, or cp.async when rows are not 16-byte
-// aligned), 1 issues the MMAs (one lane), 2-3 split the C maps, 4-7 fold accumulators
+// Staging: from a tiled map set (A = B = C = one set in the slab layout of tiled_index, whose
+// tiles are laid out as a stage) each tile is ONE contiguous bulk copy (cp.async.bulk, 16 KB
+// for 32 maps at T = 128); from plain [map][voxel] arrays, 32-voxel 2-D TMA boxes of every
+// staged row (TMA, or 4-byte cp.async when rows are not 16-byte aligned).  The contiguous copy
+// streams at several times the rate of the boxes, whose 128-byte rows are scattered over the
+// maps.
+// Warp roles (16 warps): 0 stages tiles, 1 issues the MMAs (one lane), 2-3 split the C maps, 4-7 fold accumulators
 // (warp w reads TMEM lane quarter w % 4), 8-15 produce pair products (two warps per lane
 // quarter, each taking half of a tile's K steps).  They synchronise through mbarriers
 // only.  Every `chain` tiles (1024 voxels by default) the accumulators are folded
@@ -47,6 +52,9 @@ constexpr int TC_CHAIN_VOX = 1024;          // default voxels accumulated in TME
 constexpr int TC_MAX_STAGES = 6;
 constexpr int TC_MAX_NBUF = 4;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
+
+// how a CTA stages its tiles
+constexpr int TC_STAGE_CPASYNC = 0, TC_STAGE_TMA = 1, TC_STAGE_BULK = 2;
 
 constexpr int TC_WARPS = 16;
 constexpr int TC_THREADS = 32 * TC_WARPS;
@@ -206,6 +214,15 @@ __device__ __forceinline__ void cp4(uint32_t smem, const void *gmem, int valid_b
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem), "l"(gmem), "r"(valid_bytes));
 }
 
+// contiguous global -> shared copy completing on an mbarrier (both addresses 16-byte
+// aligned, size a multiple of 16); no multicast
+__device__ __forceinline__ void bulk_load(uint32_t smem_dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_dst),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 __device__ __forceinline__ void tma_load_2d(uint32_t smem_dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
@@ -272,7 +289,7 @@ __device__ __forceinline__ uint32_t stage_off(int r, int ch) { return (uint32_t)
 template <int T>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     triplet_tc_kernel(const float *A, int n_a, const float *B, int n_b, const float *C, int n_c, int64_t n_vox,
-                      int use_tma, const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                      int stage_mode, const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                       const __grid_constant__ CUtensorMap map_c, const int32_t *pairs, const __grid_constant__ TcGeom geo,
                       double *partials, int *err) {
     constexpr int KS = T / 16;       // MMA K steps per tile
@@ -305,7 +322,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int i = tid; i < geo.n_tp * geo.acc_ld; i += TC_THREADS) acc[i] = 0.0;
     if (tid == 0) {
         for (int k = 0; k < geo.nstage; ++k) {
-            mbar_init(&full[k], use_tma ? 1 : 32);
+            mbar_init(&full[k], stage_mode == TC_STAGE_CPASYNC ? 32 : 1);
             mbar_init(&empty[k], geo.n_cons);
         }
         for (int k = 0; k < geo.nbuf; ++k) {
@@ -342,7 +359,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (*(volatile int *)&abort_flag) break;
             const int64_t v0 = (blockIdx.x + it * (int64_t)gridDim.x) * T;
             const uint32_t dst = smem_u32(stage0 + slot * geo.stage_bytes);
-            if (use_tma) {
+            if (stage_mode == TC_STAGE_BULK) {
+                // the tile's HALVES slabs of the tiled set: one contiguous block
+                if (lane == 0) {
+                    mbar_expect_tx(&full[slot], (uint32_t)geo.stage_bytes);
+                    bulk_load(dst, A + (v0 >> 5) * (int64_t)geo.n_rows * 32, (uint32_t)geo.stage_bytes, &full[slot]);
+                }
+            } else if (stage_mode == TC_STAGE_TMA) {
                 if (lane == 0) {
                     mbar_expect_tx(&full[slot], (uint32_t)(HALVES * (geo.rows_a + geo.rows_b + geo.rows_c) * 128));
 #pragma unroll
@@ -755,13 +778,71 @@ int triplet_tc_workspace_size(int64_t n_vox, const int32_t *counts, int n_c, siz
     return PB_OK;
 }
 
-int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void *C, int n_c, int64_t n_vox,
-                      const unsigned char *table, const int32_t *counts, double scale, double *out, void *workspace,
-                      size_t workspace_bytes, cudaStream_t s) {
+// The pair chunks, launches and finalize of one contraction whose staged rows `rw` and
+// staging mode are set; T0 is the preferred tile (smaller tiles, then smaller pair chunks,
+// when a shape does not fit TMEM or shared memory).
+static int run_triplet_tc(const float *A, int n_a, const float *B, int n_b, const float *C, int n_c, int64_t n_vox,
+                          const TcRows &rw, int stage_mode, const CUtensorMap *maps, int T0,
+                          const unsigned char *table, const int32_t *counts, double scale, double *out,
+                          void *workspace, size_t workspace_bytes, cudaStream_t s, const char *who) {
+    const int n_pairs = counts[1];
+    int T = T0;
+    TcGeom g;
+    int chunk = std::min(n_pairs, 128 * TC_MAX_MT);
+    int st = tc_geometry(rw, chunk, n_c, T, &g);
+    while (st == PB_ERR_UNSUPPORTED && (T > 32 || chunk > 16)) {
+        if (T > 32) T /= 2;
+        else chunk = (chunk + 1) / 2;
+        st = tc_geometry(rw, chunk, n_c, T, &g);
+    }
+    if (st) return st;
+    int gx = tc_grid(n_vox);
+    size_t need = 256 + (size_t)gx * n_pairs * n_c * sizeof(double);
+    if (!workspace || workspace_bytes < need)
+        return fail(PB_ERR_WORKSPACE, std::string(who) + ": workspace too small (need " + std::to_string(need) + ")");
+    int *err = (int *)workspace;
+    double *partials = (double *)((char *)workspace + 256);
+    TableLayout L = table_layout(counts);
+    PB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    const int32_t *pairs = (const int32_t *)(table + L.off_pairs);
+    auto kernel_of = [](int t) {
+        return t == 128 ? triplet_tc_kernel<128> : (t == 64 ? triplet_tc_kernel<64> : triplet_tc_kernel<32>);
+    };
+    int smem_max = 0;
+    for (int p_lo = 0; p_lo < n_pairs; p_lo += chunk) {
+        const int pk = std::min(chunk, n_pairs - p_lo);
+        TcGeom gk;
+        st = tc_geometry(rw, pk, n_c, T, &gk);
+        if (st) return st;
+        if (gk.smem_bytes > smem_max) {
+            PB_CUDA(cudaFuncSetAttribute(kernel_of(T), cudaFuncAttributeMaxDynamicSharedMemorySize, gk.smem_bytes));
+            smem_max = gk.smem_bytes;
+        }
+        kernel_of(T)<<<gx, TC_THREADS, gk.smem_bytes, s>>>(A, n_a, B, n_b, C, n_c, n_vox, stage_mode, maps[0],
+                                                           maps[1], maps[2], pairs + 2 * p_lo, gk,
+                                                           partials + (size_t)gx * p_lo * n_c, err);
+        PB_LAUNCH_CHECK(who);
+    }
+    triplet_tc_finalize<<<(counts[3] + 7) / 8, 256, 0, s>>>(partials, gx, n_pairs, chunk, n_c,
+                                                               (const int32_t *)(table + L.off_tmap), counts[3],
+                                                               scale, out, err);
+    PB_LAUNCH_CHECK(who);
+    return PB_OK;
+}
+
+static int check_device() {
     int dev = 0, major = 0;
     PB_CUDA(cudaGetDevice(&dev));
     PB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
     if (major != 10) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction needs an sm_100 device");
+    return PB_OK;
+}
+
+int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void *C, int n_c, int64_t n_vox,
+                      const unsigned char *table, const int32_t *counts, double scale, double *out, void *workspace,
+                      size_t workspace_bytes, cudaStream_t s) {
+    int st = check_device();
+    if (st) return st;
     if (n_a > 256 || n_b > 256 || n_c > TC_MAX_NC)
         return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 256 maps in a set");
     // staged rows: A's maps, then B's and C's unless they are rows of A already (the same
@@ -790,36 +871,19 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
             rw.n_rows += pad8(n_c);
         }
     }
-    // pairs go through in chunks that fit TMEM and shared memory (the accumulators and the
-    // pair operands grow with the pair count)
-    const int n_pairs = counts[1];
-    int T = tuning().tc_tile == 32 ? 32 : 64;
-    TcGeom g;
-    int chunk = std::min(n_pairs, 128 * TC_MAX_MT);
-    int st = tc_geometry(rw, chunk, n_c, T, &g);
-    while (st == PB_ERR_UNSUPPORTED && (T == 64 || chunk > 16)) {
-        if (T == 64) T = 32;
-        else chunk = (chunk + 1) / 2;
-        st = tc_geometry(rw, chunk, n_c, T, &g);
-    }
-    if (st) return st;
-    int gx = tc_grid(n_vox);
-    size_t need = 256 + (size_t)gx * n_pairs * n_c * sizeof(double);
-    if (!workspace || workspace_bytes < need)
-        return fail(PB_ERR_WORKSPACE, "pb_triplet_contract(tc): workspace too small (need " + std::to_string(need) + ")");
-    int *err = (int *)workspace;
-    double *partials = (double *)((char *)workspace + 256);
     // TMA staging needs 16-byte aligned rows
-    int use_tma = ((n_vox % 4) == 0) && (((uintptr_t)A & 15) == 0) && (((uintptr_t)B & 15) == 0) &&
-                  (((uintptr_t)C & 15) == 0) && n_vox < (1LL << 31);
+    int stage_mode = ((n_vox % 4) == 0) && (((uintptr_t)A & 15) == 0) && (((uintptr_t)B & 15) == 0) &&
+                             (((uintptr_t)C & 15) == 0) && n_vox < (1LL << 31)
+                         ? TC_STAGE_TMA
+                         : TC_STAGE_CPASYNC;
     CUtensorMap maps[3];
     memset(maps, 0, sizeof(maps));
-    EncodeTiledFn enc = use_tma ? encode_tiled() : nullptr;
-    if (!enc) use_tma = 0;
-    if (use_tma) {
+    EncodeTiledFn enc = stage_mode == TC_STAGE_TMA ? encode_tiled() : nullptr;
+    if (!enc) stage_mode = TC_STAGE_CPASYNC;
+    if (stage_mode == TC_STAGE_TMA) {
         const void *bases[3] = {A, B, C};
         const int rows[3] = {n_a, n_b, n_c};
-        for (int k = 0; k < 3 && use_tma; ++k) {
+        for (int k = 0; k < 3 && stage_mode == TC_STAGE_TMA; ++k) {
             cuuint64_t dims[2] = {(cuuint64_t)n_vox, (cuuint64_t)rows[k]};
             cuuint64_t strides[1] = {(cuuint64_t)n_vox * 4};
             cuuint32_t box[2] = {32u, (cuuint32_t)rows[k]};
@@ -827,42 +891,29 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
             CUresult r = enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(bases[k]), dims, strides,
                              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-            if (r != CUDA_SUCCESS) use_tma = 0;
+            if (r != CUDA_SUCCESS) stage_mode = TC_STAGE_CPASYNC;
         }
     }
-    TableLayout L = table_layout(counts);
-    PB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-    const int32_t *pairs = (const int32_t *)(table + L.off_pairs);
-    int smem_max = 0;
-    for (int p_lo = 0; p_lo < n_pairs; p_lo += chunk) {
-        const int pk = std::min(chunk, n_pairs - p_lo);
-        TcGeom gk;
-        st = tc_geometry(rw, pk, n_c, T, &gk);
-        if (st) return st;
-        if (gk.smem_bytes > smem_max) {
-            if (T == 64)
-                PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             gk.smem_bytes));
-            else
-                PB_CUDA(cudaFuncSetAttribute(triplet_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             gk.smem_bytes));
-            smem_max = gk.smem_bytes;
-        }
-        if (T == 64)
-            triplet_tc_kernel<64><<<gx, TC_THREADS, gk.smem_bytes, s>>>(
-                (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
-                maps[2], pairs + 2 * p_lo, gk, partials + (size_t)gx * p_lo * n_c, err);
-        else
-            triplet_tc_kernel<32><<<gx, TC_THREADS, gk.smem_bytes, s>>>(
-                (const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, use_tma, maps[0], maps[1],
-                maps[2], pairs + 2 * p_lo, gk, partials + (size_t)gx * p_lo * n_c, err);
-        PB_LAUNCH_CHECK("pb_triplet_contract(tc)");
-    }
-    triplet_tc_finalize<<<(counts[3] + 7) / 8, 256, 0, s>>>(partials, gx, n_pairs, chunk, n_c,
-                                                               (const int32_t *)(table + L.off_tmap), counts[3],
-                                                               scale, out, err);
-    PB_LAUNCH_CHECK("pb_triplet_contract(tc finalize)");
-    return PB_OK;
+    const int T = tuning().tc_tile ? tuning().tc_tile : 64;
+    return run_triplet_tc((const float *)A, n_a, (const float *)B, n_b, (const float *)C, n_c, n_vox, rw, stage_mode,
+                          maps, T, table, counts, scale, out, workspace, workspace_bytes, s, "pb_triplet_contract(tc)");
+}
+
+int launch_triplet_tc_tiled(const float *maps, int n_maps, int64_t n_vox, const unsigned char *table,
+                            const int32_t *counts, double scale, double *out, void *workspace, size_t workspace_bytes,
+                            cudaStream_t s) {
+    int st = check_device();
+    if (st) return st;
+    if (n_maps > TC_MAX_NC)
+        return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 64 maps in a tiled set");
+    if ((uintptr_t)maps & 15) return fail(PB_ERR_INVALID, "pb_triplet_contract_tiled: maps not 16-byte aligned");
+    // every staged row is a row of the one set: A = B = C
+    const TcRows rw{pad8(n_maps), n_maps, 0, 0, 0, 0};
+    CUtensorMap none[3];
+    memset(none, 0, sizeof(none));
+    const int T = tuning().tc_tile ? tuning().tc_tile : 128;
+    return run_triplet_tc(maps, n_maps, maps, n_maps, maps, n_maps, n_vox, rw, TC_STAGE_BULK, none, T, table, counts,
+                          scale, out, workspace, workspace_bytes, s, "pb_triplet_contract_tiled");
 }
 
 }  // namespace pb

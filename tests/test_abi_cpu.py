@@ -191,3 +191,30 @@ def test_tuning_settings_round_trip_and_checks():
     finally:
         nat.set_tuning(None)
     assert all(v == 0 for v in nat.get_tuning().values())
+
+
+def test_tiled_map_layout_host_side():
+    """Tiled map sets: the size covers whole 128-voxel tiles of 8-row groups, the element
+    index (as the header states it) is a one-to-one map into that size, each 32-voxel slab
+    row is 128 contiguous bytes, and the converters refuse bad arguments without a device."""
+    lib = nat.load()
+    for n_maps, n_vox in ((1, 1), (5, 1000), (32, 192 ** 3 // 64), (33, 50_003)):
+        R = (n_maps + 7) // 8 * 8
+        slabs = (n_vox + 127) // 128 * 4
+        assert nat.tiled_maps_bytes(n_maps, n_vox) == slabs * R * 32 * 4
+        idx = nat.tiled_index(n_maps, n_vox)
+        assert idx.min() >= 0 and idx.max() < slabs * R * 32
+        assert len(np.unique(idx)) == idx.size
+        # voxels 32 s .. 32 s + 31 of a row fill one 128-byte row of slab s
+        v = np.arange(n_vox)
+        for m in (0, n_maps - 1):
+            assert np.all(idx[m] // 32 == (v // 32) * R + m)
+    nb = ctypes.c_size_t()
+    assert lib.pb_tiled_maps_bytes(0, 10, ctypes.byref(nb)) != 0
+    assert lib.pb_tiled_maps_bytes(4, 0, ctypes.byref(nb)) != 0
+    assert lib.pb_tile_maps(None, 4, 100, None, None) != 0
+    counts = np.ones(4, dtype=np.int32)
+    out = np.zeros(1)
+    # only the tensor-core method reads a tiled set; NULL maps are refused first
+    assert lib.pb_triplet_contract_tiled(nat.PB_TRIPLET_TC, None, 4, 100, nat.hptr(counts), nat.hptr(counts), 1.0,
+                                         nat.hptr(out), None, 0, None) != 0
