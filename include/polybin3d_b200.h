@@ -73,7 +73,8 @@ typedef struct pb_tuning {
     int32_t tc_tile;     /* tensor-core contraction: voxels per tile, 32, 64 or 128 (0: 64,   */
                          /* 128 from a tiled map set)                                        */
     int32_t tc_stages;   /* its staging ring depth in tiles, 2..6 (0: what ~64 KB holds)     */
-    int32_t tc_chain;    /* voxels summed in TMEM between FP64 folds: 512, 1024, 2048 (0: 1024) */
+    int32_t tc_chain;    /* voxels summed in TMEM between FP64 folds: 256 .. 2048 (0: 512);    */
+                         /* changes the FP32 rounding, so the autotuner leaves it alone      */
     int32_t red_method;  /* k-bin reduction of many rows: 1 lane per row, 2 mode tiles (0: auto) */
     int32_t red_warps;   /* lane-per-row reduction: warps per block, 1..8 (0: as 48 KB fit)   */
     int32_t red_waves;   /* lane-per-row reduction: blocks per SM per 32-row group, 1..32 (0: 8) */
@@ -141,13 +142,14 @@ PB_API int pb_shell_synth(const pb_grid_t *g, const int32_t *out_n, int precisio
                           const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
                           const int32_t *wpow, const void *w, void *out, void *workspace,
                           size_t workspace_bytes, void *stream);
-/* The same maps written as a tiled map set (f32 only; see pb_tiled_maps_bytes for the      */
-/* layout and the size of `out`), ready for pb_triplet_contract_tiled.                   */
+/* The same maps written as a tiled map set (f32 only; the first n_factor maps are the    */
+/* pair factors; see pb_tiled_maps_bytes for the layout and the size of `out`), ready for */
+/* pb_triplet_contract_tiled.                                                            */
 PB_API int pb_shell_synth_tiled(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
-                                int64_t src_stride, int n_maps, const int32_t *src_idx, const double *lo,
-                                const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
-                                const int32_t *wpow, const void *w, void *out, void *workspace,
-                                size_t workspace_bytes, void *stream);
+                                int64_t src_stride, int n_maps, int n_factor, const int32_t *src_idx,
+                                const double *lo, const double *hi, const int32_t *l1, const int32_t *l2,
+                                const double *scale, const int32_t *wpow, const void *w, void *out,
+                                void *workspace, size_t workspace_bytes, void *stream);
 
 /* Binned-weight filter (the backward of the k-bin reduction):                           */
 /*   out(k) = scale * src(k) * w(k)^wpow * sum_e coef[e][b(k)] L_{ells[e]}(mu),           */
@@ -199,7 +201,7 @@ PB_API int pb_bin_reduce(const pb_grid_t *g, int precision, int mode, const void
 /* method PB_TRIPLET_TC: f32 maps; tcgen05 tensor cores (sm_100a).  The pair products    */
 /*   A[i1]*B[i2] (MMA M, 128 pairs per M-tile, in tensor memory) and the C maps (MMA N)   */
 /*   are split into bf16 hi + lo; per 16 voxels two MMAs accumulate the hi*hi, hi*lo and  */
-/*   lo*hi terms in FP32 in TMEM, folded into FP64 every 1024 voxels.  Any pair count (in */
+/*   lo*hi terms in FP32 in TMEM, folded into FP64 every 512 voxels.  Any pair count (in  */
 /*   launches of up to 512 pairs); at most 64 C maps and 256 maps per set (else           */
 /*   PB_ERR_UNSUPPORTED).                                                                */
 /* Output FP64 on the device, deterministic for a given device.                          */
@@ -217,23 +219,29 @@ PB_API int pb_triplet_contract(int precision, int method, const void *A, int n_a
                                size_t workspace_bytes, void *stream);
 
 /* Tiled map sets: the tensor-core contraction's staging layout in device memory, so that */
-/* a tile of voxels of every map is one contiguous copy.  n_maps f32 maps of n_vox voxels */
-/* as 32-voxel slabs: slab s holds voxels 32s..32s+31 of rows 0..R-1 (R = n_maps rounded  */
-/* up to 8), 128 bytes per row, the 16-byte chunk c (voxels 4c..4c+3 of the slab) of row  */
-/* r at chunk position c XOR (r mod 8); the slabs run to a multiple of 4 (128 voxels) and */
-/* voxels past n_vox hold zeros.  Element of voxel v, map m:                             */
-/*   ((v / 32) R + m) 32 + 4 ((v mod 32) / 4 XOR m mod 8) + v mod 4                       */
-/* pb_tile_maps converts [n_maps][n_vox] maps; pb_shell_synth_tiled writes the layout     */
-/* directly.  pb_triplet_contract_tiled is pb_triplet_contract with A = B = C = the set    */
-/* (table and counts from pb_triplet_plan(n_maps, n_maps, n_maps, ...), workspace from    */
-/* pb_triplet_workspace_size(PB_F32, PB_TRIPLET_TC, n_vox, counts, n_maps)); method       */
-/* PB_TRIPLET_TC only.  No reference counterpart (the reference's maps are plain numpy    */
-/* arrays); the contraction replaces the same assemble_b3 call.                          */
-PB_API int pb_tiled_maps_bytes(int n_maps, int64_t n_vox, size_t *bytes);
-PB_API int pb_tile_maps(const void *maps, int n_maps, int64_t n_vox, void *tiled, void *stream);
-PB_API int pb_triplet_contract_tiled(int method, const void *maps, int n_maps, int64_t n_vox, const void *table,
-                                     const int32_t *counts, double scale, double *out, void *workspace,
-                                     size_t workspace_bytes, void *stream);
+/* one contiguous copy stages a tile of 128 voxels.  n_maps f32 maps of n_vox voxels, of  */
+/* which the first n_factor (1 <= n_factor <= n_maps) are pair factors.  Per tile t, at    */
+/* byte t * 512 (F + P) (F = n_factor rounded up to 8, P = n_maps rounded up to 16):       */
+/*  - factor slabs, 4 x F x 128 bytes: slab s (voxels 32s..32s+31 of the tile), row m     */
+/*    (factor map m) holds the FP32 values, 16-byte chunk c (voxels 4c..4c+3) at chunk     */
+/*    position c XOR (m mod 8);                                                           */
+/*  - C operand, 8 x 2P x 32 bytes: step k (voxels 16k..16k+15 of the tile), row r holds   */
+/*    the bf16 hi part rn(x) of map r (r < P) or the lo part rn(x - hi) of map r - P, the   */
+/*    16-byte half h (voxels 8h..8h+7) at half position h XOR ((r / 4) mod 2) -- the        */
+/*    32-byte-swizzled K-major layout of a tcgen05 MMA operand, one K step per 8-row atom. */
+/* Voxels past n_vox hold zeros.  pb_tile_maps converts [n_maps][n_vox] maps;              */
+/* pb_shell_synth_tiled writes the layout directly.  pb_triplet_contract_tiled is          */
+/* pb_triplet_contract with A = B = C = the set (table and counts from pb_triplet_plan(    */
+/* n_maps, n_maps, n_maps, ...) whose pair indices i1, i2 are below n_factor -- other      */
+/* pairs make the call's outputs NaN -- and workspace from pb_triplet_workspace_size(      */
+/* PB_F32, PB_TRIPLET_TC, n_vox, counts, n_maps)); method PB_TRIPLET_TC only, at most 64   */
+/* maps.  No reference counterpart (the reference's maps are plain numpy arrays); the     */
+/* contraction replaces the same assemble_b3 call.                                       */
+PB_API int pb_tiled_maps_bytes(int n_maps, int n_factor, int64_t n_vox, size_t *bytes);
+PB_API int pb_tile_maps(const void *maps, int n_maps, int n_factor, int64_t n_vox, void *tiled, void *stream);
+PB_API int pb_triplet_contract_tiled(int method, const void *maps, int n_maps, int n_factor, int64_t n_vox,
+                                     const void *table, const int32_t *counts, double scale, double *out,
+                                     void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Bilinear maps (the adjoint of the triplet contraction with respect to its maps):       */

@@ -73,10 +73,10 @@ SIGNATURES = {
     "pb_triplet_plan": ([_I, _I, _I, _P, _I, _P, ctypes.POINTER(_SZ), _P], _I),
     "pb_triplet_workspace_size": ([_I, _I, _I64, _P, _I, ctypes.POINTER(_SZ)], _I),
     "pb_triplet_contract": ([_I, _I, _P, _I, _P, _I, _P, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
-    "pb_tiled_maps_bytes": ([_I, _I64, ctypes.POINTER(_SZ)], _I),
-    "pb_tile_maps": ([_P, _I, _I64, _P, _P], _I),
-    "pb_triplet_contract_tiled": ([_I, _P, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
-    "pb_shell_synth_tiled": ([_GP, _P, _I, _P, _I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P], _I),
+    "pb_tiled_maps_bytes": ([_I, _I, _I64, ctypes.POINTER(_SZ)], _I),
+    "pb_tile_maps": ([_P, _I, _I, _I64, _P, _P], _I),
+    "pb_triplet_contract_tiled": ([_I, _P, _I, _I, _I64, _P, _P, _D, _P, _P, _SZ, _P], _I),
+    "pb_shell_synth_tiled": ([_GP, _P, _I, _P, _I64, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P], _I),
     "pb_elementwise": ([_I, _I, _I64, _P, _P, _I64, _P, _P, _D, _P, _P], _I),
     "pb_grf_from_noise": ([_GP, _I, _P, _P, _I, _P, _D, _P, _P], _I),
     "pb_grf_philox": ([_GP, _I, _P, _I, _P, _D, _P, _P], _I),
@@ -299,6 +299,7 @@ class TripletPlan:
                                   hptr(self.counts)), "pb_triplet_plan")
         self.host_table = host
         self.n_items, self.n_pairs = int(self.counts[0]), int(self.counts[1])
+        self.factor_max = int(idx[:, :2].max()) if len(idx) else -1
         self.table = torch.from_numpy(host).to(device)
 
     def workspace_bytes(self, precision, method, n_vox):
@@ -319,58 +320,84 @@ class TripletPlan:
         return out
 
     def contract_tiled(self, tiled, out, ws, method=PB_TRIPLET_TC, scale=1.0):
-        """The contraction with A = B = C = a TiledMaps set (plan made for n_a = n_b = n_c = its maps)."""
-        if not (self.n_a == self.n_b == self.n_c == tiled.n_maps):
-            raise ValueError("contract_tiled: the plan was made for %d/%d/%d maps, the set holds %d"
-                             % (self.n_a, self.n_b, self.n_c, tiled.n_maps))
+        """The contraction with A = B = C = a TiledMaps set (plan made for n_a = n_b = n_c = its
+        maps, pair factors among its first n_factor maps)."""
+        if not (self.n_a == self.n_b == self.n_c == tiled.n_maps) or self.factor_max >= tiled.n_factor:
+            raise ValueError("contract_tiled: the plan (%d/%d/%d maps, pair factors up to %d) does not fit a set of "
+                             "%d maps with %d factor maps" % (self.n_a, self.n_b, self.n_c, self.factor_max,
+                                                               tiled.n_maps, tiled.n_factor))
         buf = ws.get(self.workspace_bytes(PB_F32, method, tiled.n_vox), "triplet")
-        check(load().pb_triplet_contract_tiled(method, ptr(tiled.data), tiled.n_maps, tiled.n_vox, ptr(self.table),
-                                               hptr(self.counts), float(scale), ptr(out), ptr(buf), buf.numel(),
-                                               stream_ptr()), "pb_triplet_contract_tiled")
+        check(load().pb_triplet_contract_tiled(method, ptr(tiled.data), tiled.n_maps, tiled.n_factor, tiled.n_vox,
+                                               ptr(self.table), hptr(self.counts), float(scale), ptr(out), ptr(buf),
+                                               buf.numel(), stream_ptr()), "pb_triplet_contract_tiled")
         _count(2)
         return out
 
 
-def tiled_maps_bytes(n_maps, n_vox):
+def tiled_maps_bytes(n_maps, n_factor, n_vox):
     nbytes = ctypes.c_size_t()
-    check(load().pb_tiled_maps_bytes(int(n_maps), int(n_vox), ctypes.byref(nbytes)), "pb_tiled_maps_bytes")
+    check(load().pb_tiled_maps_bytes(int(n_maps), int(n_factor), int(n_vox), ctypes.byref(nbytes)),
+          "pb_tiled_maps_bytes")
     return nbytes.value
 
 
-def tiled_index(n_maps, n_vox):
-    """Host int64 array [n_maps, n_vox]: element of each voxel of each map in a tiled set."""
-    R = (n_maps + 7) // 8 * 8
+def _tiled_dims(n_maps, n_factor):
+    F, P = (n_factor + 7) // 8 * 8, (n_maps + 15) // 16 * 16
+    return F, P, 512 * (F + P)
+
+
+def tiled_factor_offsets(n_maps, n_factor, n_vox):
+    """Host int64 [n_factor, n_vox]: byte offset of each voxel of each factor map (FP32)."""
+    F, P, tb = _tiled_dims(n_maps, n_factor)
     v = np.arange(n_vox, dtype=np.int64)[None, :]
-    m = np.arange(n_maps, dtype=np.int64)[:, None]
-    w = v & 31
-    return ((v >> 5) * R + m) * 32 + ((((w >> 2) ^ (m & 7)) << 2) | (w & 3))
+    m = np.arange(n_factor, dtype=np.int64)[:, None]
+    w = v & 127
+    return (v >> 7) * tb + ((w >> 5) * F + m) * 128 + ((((w & 31) >> 2) ^ (m & 7)) << 4) + (w & 3) * 4
+
+
+def tiled_c_offsets(n_maps, n_factor, n_vox):
+    """Host int64 [2, n_maps, n_vox]: byte offsets of the bf16 hi (0) and lo (1) parts."""
+    F, P, tb = _tiled_dims(n_maps, n_factor)
+    v = np.arange(n_vox, dtype=np.int64)[None, None, :]
+    r = np.arange(n_maps, dtype=np.int64)[None, :, None] + np.asarray([0, P], dtype=np.int64)[:, None, None]
+    w = v & 127
+    return ((v >> 7) * tb + 512 * F + (w >> 4) * 64 * P + (r >> 3) * 256 + (r & 7) * 32 +
+            ((((w & 15) >> 3) ^ ((r >> 2) & 1)) << 4) + (w & 7) * 2)
 
 
 class TiledMaps:
-    """A tiled map set (include/polybin3d_b200.h): n_maps f32 maps on `shape`, stored as
-    32-voxel slabs in the tensor-core contraction's staging layout.  data: flat float32."""
+    """A tiled map set (include/polybin3d_b200.h): n_maps f32 maps on `shape`, the first
+    n_factor kept in FP32 as pair factors and every map split into bf16 hi + lo parts, per
+    tile of 128 voxels in the tensor-core contraction's staging layout.  data: uint8 bytes."""
 
-    def __init__(self, n_maps, shape, device, data=None):
-        self.n_maps, self.shape = int(n_maps), tuple(int(n) for n in shape)
+    def __init__(self, n_maps, n_factor, shape, device, data=None):
+        self.n_maps, self.n_factor, self.shape = int(n_maps), int(n_factor), tuple(int(n) for n in shape)
         self.n_vox = int(np.prod(self.shape))
-        n = tiled_maps_bytes(self.n_maps, self.n_vox) // 4
-        self.data = torch.empty(n, dtype=torch.float32, device=device) if data is None else data
-        if self.data.numel() < n or self.data.dtype != torch.float32:
-            raise ValueError("TiledMaps: data must hold %d float32 values" % n)
+        n = tiled_maps_bytes(self.n_maps, self.n_factor, self.n_vox)
+        self.data = torch.empty(n, dtype=torch.uint8, device=device) if data is None else data
+        if self.data.numel() < n or self.data.dtype != torch.uint8:
+            raise ValueError("TiledMaps: data must hold %d bytes" % n)
 
     @classmethod
-    def from_maps(cls, maps):
+    def from_maps(cls, maps, n_factor):
         """Tile (n_maps, *shape) float32 device maps (pb_tile_maps)."""
         maps = maps.contiguous()
-        t = cls(maps.shape[0], maps.shape[1:], maps.device)
-        check(load().pb_tile_maps(ptr(maps), t.n_maps, t.n_vox, ptr(t.data), stream_ptr()), "pb_tile_maps")
+        t = cls(maps.shape[0], n_factor, maps.shape[1:], maps.device)
+        check(load().pb_tile_maps(ptr(maps), t.n_maps, t.n_factor, t.n_vox, ptr(t.data), stream_ptr()),
+              "pb_tile_maps")
         _count(1)
         return t
 
-    def to_maps(self):
-        """(n_maps, *shape) copy in the plain layout (a device gather)."""
-        idx = torch.as_tensor(tiled_index(self.n_maps, self.n_vox), device=self.data.device)
-        return self.data[idx].reshape((self.n_maps,) + self.shape)
+    def factor_maps(self):
+        """(n_factor, *shape) float32: the FP32 factor maps (a device gather)."""
+        off = torch.as_tensor(tiled_factor_offsets(self.n_maps, self.n_factor, self.n_vox) // 4, device=self.data.device)
+        return self.data.view(torch.float32)[off].reshape((self.n_factor,) + self.shape)
+
+    def split_parts(self):
+        """(hi, lo): (n_maps, *shape) bfloat16 parts of every map (a device gather)."""
+        off = torch.as_tensor(tiled_c_offsets(self.n_maps, self.n_factor, self.n_vox) // 2, device=self.data.device)
+        x = self.data.view(torch.bfloat16)[off]
+        return x[0].reshape((self.n_maps,) + self.shape), x[1].reshape((self.n_maps,) + self.shape)
 
 
 def pair_products(X, Y, pairs, Z=None, U=None, s=1.0, out=None):
@@ -489,7 +516,8 @@ def _shell_synth_tiled(lib, grid, precision, src, out, maps, out_n, ws, w, src_s
     if nbytes.value > SYNTH_WS_BYTES:
         raise NotImplementedError("shell_synth: a tiled set's transform workspace exceeds SYNTH_WS_BYTES")
     buf = ws.get(nbytes.value, "synth")
-    check(lib.pb_shell_synth_tiled(ctypes.byref(grid), hptr(on), precision, ptr(src), stride, len(maps), hptr(si),
+    check(lib.pb_shell_synth_tiled(ctypes.byref(grid), hptr(on), precision, ptr(src), stride, len(maps),
+                                   out.n_factor, hptr(si),
                                    hptr(lo), hptr(hi), hptr(l1), hptr(l2), hptr(sc), hptr(wp), ptr(w),
                                    ptr(out.data), ptr(buf), buf.numel(), stream_ptr()), "pb_shell_synth_tiled")
     _count(3)

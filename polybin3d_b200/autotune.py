@@ -6,8 +6,8 @@ stream, keeps the fastest and stores it in a JSON file, so later calls -- and la
 processes -- set the winner before launching.  Tuned shapes:
 
 * the tensor-core triplet contraction (from plain maps and from a tiled set): voxels per
-  tile (128 / 64 / 32), staging ring depth, voxels summed in TMEM between FP64 folds, the
-  barrier-wait form;
+  tile (plain maps: 64 / 32), staging ring depth, the barrier-wait form, accumulator sets
+  (never the TMEM chain length, which changes the FP32 rounding);
 * the k-bin reduction of many rows (>= 16): lane-per-row kernel (warps per block, blocks
   per SM) against the mode-tile kernel.
 
@@ -25,11 +25,11 @@ import torch
 
 from . import _native as nat
 
-TC_CANDIDATES = [{}, {"tc_tile": 32}, {"tc_chain": 2048}, {"tc_tile": 32, "tc_chain": 2048}, {"tc_stages": 3},
-                 {"tc_tile": 32, "tc_stages": 4}]
-# from a tiled map set (one contiguous copy per tile): 128-voxel tiles by default
-TC_TILED_CANDIDATES = [{}, {"tc_tile": 64}, {"tc_stages": 3}, {"tc_wait": 2}, {"tc_chain": 2048},
-                       {"tc_tile": 64, "tc_stages": 6}]
+# (launch shapes only: the TMEM chain length changes the FP32 rounding and stays fixed)
+TC_CANDIDATES = [{}, {"tc_tile": 32}, {"tc_stages": 3}, {"tc_tile": 32, "tc_stages": 4}, {"tc_wait": 2},
+                 {"tc_dsets": 1}]
+# from a tiled map set (one contiguous copy per 128-voxel tile)
+TC_TILED_CANDIDATES = [{}, {"tc_wait": 2}, {"tc_stages": 4}, {"tc_dsets": 1}, {"tc_wait": 2, "tc_dsets": 1}]
 RED_CANDIDATES = [{}, {"red_method": 2}, {"red_method": 1, "red_warps": 2},
                   {"red_method": 1, "red_warps": 2, "red_waves": 16}, {"red_method": 1, "red_warps": 4, "red_waves": 4},
                   {"red_method": 1, "red_waves": 16}]
@@ -150,7 +150,8 @@ def contract(plan, A, B, C, out, ws, method, scale):
 
 def contract_tiled(plan, tiled, out, ws, scale):
     """plan.contract_tiled with the tuned launch shape for this shape."""
-    key = "tct|%s|%d|%d|%d" % (device_tag(tiled.data.device), tiled.n_vox, tiled.n_maps, plan.n_pairs)
+    key = "tct|%s|%d|%d|%d|%d" % (device_tag(tiled.data.device), tiled.n_vox, tiled.n_maps, tiled.n_factor,
+                                  plan.n_pairs)
     cfg = tuner().choose(key, TC_TILED_CANDIDATES, lambda: plan.contract_tiled(tiled, out, ws, scale=scale))
     with applied(cfg):
         return plan.contract_tiled(tiled, out, ws, scale=scale)

@@ -539,7 +539,8 @@ class BSpec:
         """The g-maps of _g_maps as a tiled set, or None when the pruned synthesis cannot
         make them (the caller takes the plain path)."""
         b = self.base
-        T = nat.TiledMaps(self.Nl * self.Nk_squeeze, self.map_grid, b.device)
+        # the monopole maps (the first Nk_squeeze) are the pair factors of every triplet
+        T = nat.TiledMaps(self.Nl * self.Nk_squeeze, self.Nk_squeeze, self.map_grid, b.device)
         try:
             if b.sightline == 'local' and self.lmax > 0:
                 self._g_maps_local(xk, w, scale, out=T)

@@ -92,20 +92,37 @@ template <> struct cplx<float> { using type = float2; };
 template <> struct cplx<double> { using type = double2; };
 
 // ---- tiled map sets ---------------------------------------------------------------
-// n_maps f32 maps of n_vox voxels as 32-voxel slabs: slab s holds voxels 32 s .. 32 s + 31
-// of rows 0 .. R-1 (R = n_maps rounded up to 8), 128 bytes per row, the 16-byte chunk c
-// (4 voxels) of row r at chunk position c ^ (r mod 8).  Slabs run to a multiple of 4 (128
-// voxels), so any tile of 32, 64 or 128 voxels is one contiguous block laid out as the
-// tensor-core contraction stages it in shared memory (the 128-byte swizzle).
-constexpr int TILED_SLAB = 32, TILED_ALIGN = 128;
-__host__ __device__ __forceinline__ int tiled_rows(int n_maps) { return (n_maps + 7) & ~7; }
-__host__ __device__ __forceinline__ int64_t tiled_slabs(int64_t n_vox) {
-    return (n_vox + TILED_ALIGN - 1) / TILED_ALIGN * (TILED_ALIGN / TILED_SLAB);
+// n_maps f32 maps of n_vox voxels stored per tile of 128 voxels in the tensor-core
+// contraction's staging layout, so that one contiguous copy stages a tile.  The first
+// n_factor maps (the pair factors) are kept in FP32; every map is also kept split into bf16
+// hi + lo parts, the MMA's operand.  Tile t = [factor slabs][C operand], 512 (F + P) bytes:
+//  * factor slabs: 4 slabs of 32 voxels x F rows (F = n_factor rounded up to 8) x 128 bytes,
+//    the 16-byte chunk c (voxels 4c..4c+3 of the slab) of row m at chunk position c ^ (m % 8);
+//  * C operand: 8 steps of 16 voxels x 2P rows x 32 bytes (P = n_maps rounded up to 16;
+//    rows 0..P-1 the hi parts, P..2P-1 the lo parts), the 16-byte half h (voxels 8h..8h+7
+//    of the step) of row r at half position h ^ ((r / 4) % 2): the 32-byte-swizzled K-major
+//    layout of a tcgen05 operand (8-row atoms of 256 bytes, one MMA K step each), so every
+//    MMA reads one contiguous block and 16 voxels of a map are one 32-byte sector.
+// Voxels past n_vox hold zeros.
+constexpr int TILED_VOX = 128;
+__host__ __device__ __forceinline__ int tiled_frows(int n_factor) { return (n_factor + 7) & ~7; }
+__host__ __device__ __forceinline__ int tiled_cpad(int n_maps) { return (n_maps + 15) & ~15; }
+__host__ __device__ __forceinline__ int64_t tiled_tile_bytes(int n_maps, int n_factor) {
+    return 512 * (int64_t)(tiled_frows(n_factor) + tiled_cpad(n_maps));
 }
-// element index of voxel v of map m in a set of `rows` rows
-__host__ __device__ __forceinline__ int64_t tiled_index(int64_t v, int m, int rows) {
-    const int w = (int)(v & 31);
-    return ((v >> 5) * rows + m) * 32 + ((((w >> 2) ^ (m & 7)) << 2) | (w & 3));
+__host__ __device__ __forceinline__ int64_t tiled_tiles(int64_t n_vox) { return (n_vox + TILED_VOX - 1) / TILED_VOX; }
+// byte offset of voxel v of factor map m (FP32)
+__host__ __device__ __forceinline__ int64_t tiled_factor_byte(int64_t v, int m, int n_maps, int n_factor) {
+    const int w = (int)(v & (TILED_VOX - 1));
+    return (v >> 7) * tiled_tile_bytes(n_maps, n_factor) + ((w >> 5) * tiled_frows(n_factor) + m) * 128 +
+           ((((w & 31) >> 2) ^ (m & 7)) << 4) + (w & 3) * 4;
+}
+// byte offset of voxel v of C-operand row r (bf16; r < P: hi part of map r, else lo part of map r - P)
+__host__ __device__ __forceinline__ int64_t tiled_c_byte(int64_t v, int r, int n_maps, int n_factor) {
+    const int w = (int)(v & (TILED_VOX - 1));
+    const int P = tiled_cpad(n_maps);
+    return (v >> 7) * tiled_tile_bytes(n_maps, n_factor) + 512 * tiled_frows(n_factor) + (w >> 4) * 64 * P +
+           (r >> 3) * 256 + (r & 7) * 32 + ((((w & 15) >> 3) ^ ((r >> 2) & 1)) << 4) + (w & 7) * 2;
 }
 
 }  // namespace pb

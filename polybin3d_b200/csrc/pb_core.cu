@@ -214,8 +214,8 @@ extern "C" int pb_set_tuning(const pb_tuning_t *t) {
         return fail(PB_ERR_INVALID, "pb_set_tuning: tc_tile must be 0, 32, 64 or 128");
     if (t->tc_stages != 0 && (t->tc_stages < 2 || t->tc_stages > 6))
         return fail(PB_ERR_INVALID, "pb_set_tuning: tc_stages must be 0 or in [2, 6]");
-    if (t->tc_chain != 0 && t->tc_chain != 512 && t->tc_chain != 1024 && t->tc_chain != 2048)
-        return fail(PB_ERR_INVALID, "pb_set_tuning: tc_chain must be 0, 512, 1024 or 2048");
+    if (t->tc_chain != 0 && t->tc_chain != 256 && t->tc_chain != 512 && t->tc_chain != 1024 && t->tc_chain != 2048)
+        return fail(PB_ERR_INVALID, "pb_set_tuning: tc_chain must be 0, 256, 512, 1024 or 2048");
     if (t->red_method < 0 || t->red_method > 2) return fail(PB_ERR_INVALID, "pb_set_tuning: red_method in [0, 2]");
     if (t->red_warps < 0 || t->red_warps > 8) return fail(PB_ERR_INVALID, "pb_set_tuning: red_warps in [0, 8]");
     if (t->red_waves < 0 || t->red_waves > 32) return fail(PB_ERR_INVALID, "pb_set_tuning: red_waves in [0, 32]");

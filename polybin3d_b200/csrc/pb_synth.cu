@@ -19,6 +19,7 @@
 #include <cmath>
 #include <type_traits>
 #include <vector>
+#include <cuda_bf16.h>
 #include "pb_common.cuh"
 
 namespace pb {
@@ -55,7 +56,8 @@ struct SynthParams {
     int64_t src_stride;
     FftAxis ax, ay, az;
     int c1;                     // S1 column chunks per plane (max over maps)
-    int tiled_rows;             // 0: out is [map][x][y][z]; else a tiled set of this many rows
+    int tiled;                  // 0: out is [map][x][y][z]; 1: a tiled set (see tiled_c_byte)
+    int t_maps, t_factor;       // the tiled set's map and factor-map counts
     SynthMap maps[SY_MAX_MAPS];
 };
 
@@ -579,10 +581,20 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
     // voxel v0 + yy m2 + z of map m: plain [map][voxel] rows, or the slab layout of a tiled set
     const int64_t v0 = ((int64_t)x * p.m1 + y0) * p.m2;
     T *const o = out + (int64_t)m * plane * p.m2 + v0;
-    const int trows = p.tiled_rows;
+    const int tiled = p.tiled;
     auto put = [&](int yy, int z, T val) {
-        if (trows) out[tiled_index(v0 + (int64_t)yy * p.m2 + z, m, trows)] = val;
-        else o[(int64_t)yy * p.m2 + z] = val;
+        if (!tiled) {
+            o[(int64_t)yy * p.m2 + z] = val;
+            return;
+        }
+        // FP32 copy of a factor map, bf16 hi and lo parts of every map
+        const int64_t v = v0 + (int64_t)yy * p.m2 + z;
+        char *const base = reinterpret_cast<char *>(out);
+        if (m < p.t_factor) *reinterpret_cast<float *>(base + tiled_factor_byte(v, m, p.t_maps, p.t_factor)) = (float)val;
+        const __nv_bfloat16 hi = __float2bfloat16_rn((float)val);
+        const __nv_bfloat16 lo = __float2bfloat16_rn((float)val - __bfloat162float(hi));
+        *reinterpret_cast<__nv_bfloat16 *>(base + tiled_c_byte(v, m, p.t_maps, p.t_factor)) = hi;
+        *reinterpret_cast<__nv_bfloat16 *>(base + tiled_c_byte(v, tiled_cpad(p.t_maps) + m, p.t_maps, p.t_factor)) = lo;
     };
     if constexpr (N > 0 && pass_count(N) >= 2) {
         // first pass straight from H (a warp reads the (y, y+1) pairs of 32 lines at one kz:
@@ -882,7 +894,7 @@ extern "C" int pb_shell_synth_workspace_size(const pb_grid_t *g, const int32_t *
 static int shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src, int64_t src_stride,
                        int n_maps, const int32_t *src_idx, const double *lo, const double *hi, const int32_t *l1,
                        const int32_t *l2, const double *scale, const int32_t *wpow, const void *w, void *out,
-                       void *workspace, size_t workspace_bytes, void *stream, bool tiled) {
+                       void *workspace, size_t workspace_bytes, void *stream, bool tiled, int n_factor) {
     if (!out || !lo || !hi || !l1 || !l2 || !scale) return fail(PB_ERR_INVALID, "pb_shell_synth: NULL argument");
     SynthLayout L;
     int st = synth_layout(g, out_n, precision, n_maps, lo, hi, src_idx, l1, l2, scale, wpow, src_stride, &L);
@@ -891,15 +903,17 @@ static int shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, 
     if (tiled) {
         if (precision != PB_F32) return fail(PB_ERR_INVALID, "pb_shell_synth_tiled: tiled sets hold f32 maps");
         if ((uintptr_t)out & 15) return fail(PB_ERR_INVALID, "pb_shell_synth_tiled: output not 16-byte aligned");
-        L.p.tiled_rows = tiled_rows(n_maps);
-        // the voxels past the grid in the last 128-voxel tile read as zeros (the z pass then
-        // writes every voxel of the grid; padding rows past n_maps are never read)
+        if (n_factor < 1 || n_factor > n_maps)
+            return fail(PB_ERR_INVALID, "pb_shell_synth_tiled: n_factor must be in [1, n_maps]");
+        L.p.tiled = 1;
+        L.p.t_maps = n_maps;
+        L.p.t_factor = n_factor;
+        // the voxels past the grid in the last tile read as zeros (the z pass then writes
+        // every voxel of the grid; padding rows are never read)
         const int64_t n_vox = (int64_t)L.p.m0 * L.p.m1 * L.p.m2;
-        const int64_t rows = L.p.tiled_rows;
-        if (n_vox % TILED_ALIGN) {
-            const int64_t first = tiled_slabs(n_vox) - TILED_ALIGN / TILED_SLAB;
-            PB_CUDA(cudaMemsetAsync((float *)out + first * rows * TILED_SLAB, 0,
-                                    (size_t)(TILED_ALIGN / TILED_SLAB) * rows * TILED_SLAB * sizeof(float), s));
+        if (n_vox % TILED_VOX) {
+            const int64_t tb = tiled_tile_bytes(n_maps, n_factor);
+            PB_CUDA(cudaMemsetAsync((char *)out + (tiled_tiles(n_vox) - 1) * tb, 0, (size_t)tb, s));
         }
     }
     for (int m = 0; m < n_maps; ++m)
@@ -924,14 +938,14 @@ extern "C" int pb_shell_synth(const pb_grid_t *g, const int32_t *out_n, int prec
                               const int32_t *wpow, const void *w, void *out, void *workspace, size_t workspace_bytes,
                               void *stream) {
     return shell_synth(g, out_n, precision, src, src_stride, n_maps, src_idx, lo, hi, l1, l2, scale, wpow, w, out,
-                       workspace, workspace_bytes, stream, false);
+                       workspace, workspace_bytes, stream, false, 0);
 }
 
 extern "C" int pb_shell_synth_tiled(const pb_grid_t *g, const int32_t *out_n, int precision, const void *src,
-                                    int64_t src_stride, int n_maps, const int32_t *src_idx, const double *lo,
-                                    const double *hi, const int32_t *l1, const int32_t *l2, const double *scale,
-                                    const int32_t *wpow, const void *w, void *out, void *workspace,
-                                    size_t workspace_bytes, void *stream) {
+                                    int64_t src_stride, int n_maps, int n_factor, const int32_t *src_idx,
+                                    const double *lo, const double *hi, const int32_t *l1, const int32_t *l2,
+                                    const double *scale, const int32_t *wpow, const void *w, void *out,
+                                    void *workspace, size_t workspace_bytes, void *stream) {
     return shell_synth(g, out_n, precision, src, src_stride, n_maps, src_idx, lo, hi, l1, l2, scale, wpow, w, out,
-                       workspace, workspace_bytes, stream, true);
+                       workspace, workspace_bytes, stream, true, n_factor);
 }

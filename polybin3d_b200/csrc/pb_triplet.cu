@@ -13,6 +13,7 @@
 #include <set>
 #include <string>
 #include <vector>
+#include <cuda_bf16.h>
 #include "pb_common.cuh"
 #include "pb_triplet.cuh"
 
@@ -303,26 +304,21 @@ int launch_triplet_simt(int precision, const void *A, int n_a, const void *B, in
 
 static size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// plain [n_maps][n_vox] maps -> tiled set: one thread per 16-byte chunk of the output (the
-// 8 chunks of a slab row are 8 consecutive threads: 128-byte stores; the loads read the 4
-// voxels that land there); padding rows and voxels past n_vox are written as zeros
-__global__ void tile_maps_kernel(const float *maps, int n_maps, int64_t n_vox, int rows, int64_t n_chunks,
-                                 float4 *out) {
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n_chunks;
-         q += (int64_t)gridDim.x * blockDim.x) {
-        const int cp = (int)(q & 7);
-        const int64_t sr = q >> 3;
-        const int r = (int)(sr % rows);
-        const int64_t slab = sr / rows;
-        const int64_t v = slab * 32 + 4 * (cp ^ (r & 7));
-        float x[4] = {0.f, 0.f, 0.f, 0.f};
-        if (r < n_maps) {
-            const float *src = maps + (int64_t)r * n_vox;
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                if (v + e < n_vox) x[e] = src[v + e];
-        }
-        out[q] = make_float4(x[0], x[1], x[2], x[3]);
+// plain [n_maps][n_vox] maps -> tiled set (the buffer is zeroed first): one thread per
+// (map, voxel), consecutive threads on consecutive voxels of a map (128-byte runs of the
+// factor slabs and of the operand rows)
+__global__ void tile_maps_kernel(const float *maps, int n_maps, int n_factor, int64_t n_vox, char *out) {
+    const int64_t total = (int64_t)n_maps * n_vox;
+    const int P = tiled_cpad(n_maps);
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int m = (int)(q / n_vox);
+        const int64_t v = q - (int64_t)m * n_vox;
+        const float x = maps[q];
+        if (m < n_factor) *reinterpret_cast<float *>(out + tiled_factor_byte(v, m, n_maps, n_factor)) = x;
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+        *reinterpret_cast<__nv_bfloat16 *>(out + tiled_c_byte(v, m, n_maps, n_factor)) = hi;
+        *reinterpret_cast<__nv_bfloat16 *>(out + tiled_c_byte(v, P + m, n_maps, n_factor)) = lo;
     }
 }
 
@@ -433,35 +429,39 @@ extern "C" int pb_triplet_contract(int precision, int method, const void *A, int
                                counts[0], counts[3], scale, out, workspace, workspace_bytes, as_stream(stream));
 }
 
-extern "C" int pb_tiled_maps_bytes(int n_maps, int64_t n_vox, size_t *bytes) {
+extern "C" int pb_tiled_maps_bytes(int n_maps, int n_factor, int64_t n_vox, size_t *bytes) {
     if (!bytes) return fail(PB_ERR_INVALID, "pb_tiled_maps_bytes: bytes is NULL");
     if (n_maps < 1 || n_vox < 1) return fail(PB_ERR_INVALID, "pb_tiled_maps_bytes: empty map set");
-    *bytes = (size_t)tiled_slabs(n_vox) * tiled_rows(n_maps) * TILED_SLAB * sizeof(float);
+    if (n_factor < 1 || n_factor > n_maps) return fail(PB_ERR_INVALID, "pb_tiled_maps_bytes: n_factor not in [1, n_maps]");
+    *bytes = (size_t)(tiled_tiles(n_vox) * tiled_tile_bytes(n_maps, n_factor));
     return PB_OK;
 }
 
-extern "C" int pb_tile_maps(const void *maps, int n_maps, int64_t n_vox, void *tiled, void *stream) {
+extern "C" int pb_tile_maps(const void *maps, int n_maps, int n_factor, int64_t n_vox, void *tiled, void *stream) {
     if (!maps || !tiled) return fail(PB_ERR_INVALID, "pb_tile_maps: NULL argument");
     if (n_maps < 1 || n_vox < 1) return fail(PB_ERR_INVALID, "pb_tile_maps: empty map set");
+    if (n_factor < 1 || n_factor > n_maps) return fail(PB_ERR_INVALID, "pb_tile_maps: n_factor not in [1, n_maps]");
     if ((uintptr_t)tiled & 15) return fail(PB_ERR_INVALID, "pb_tile_maps: output not 16-byte aligned");
-    const int rows = tiled_rows(n_maps);
-    const int64_t n_chunks = tiled_slabs(n_vox) * rows * 8;
-    const int64_t blocks = std::min<int64_t>((n_chunks + 255) / 256, (int64_t)num_sms() * 16);
-    tile_maps_kernel<<<(int)blocks, 256, 0, as_stream(stream)>>>((const float *)maps, n_maps, n_vox, rows, n_chunks,
-                                                                 (float4 *)tiled);
+    cudaStream_t s = as_stream(stream);
+    PB_CUDA(cudaMemsetAsync(tiled, 0, (size_t)(tiled_tiles(n_vox) * tiled_tile_bytes(n_maps, n_factor)), s));
+    const int64_t total = (int64_t)n_maps * n_vox;
+    const int64_t blocks = std::min<int64_t>((total + 255) / 256, (int64_t)num_sms() * 16);
+    tile_maps_kernel<<<(int)blocks, 256, 0, s>>>((const float *)maps, n_maps, n_factor, n_vox, (char *)tiled);
     PB_LAUNCH_CHECK("pb_tile_maps");
     return PB_OK;
 }
 
-extern "C" int pb_triplet_contract_tiled(int method, const void *maps, int n_maps, int64_t n_vox, const void *table,
-                                         const int32_t *counts, double scale, double *out, void *workspace,
-                                         size_t workspace_bytes, void *stream) {
+extern "C" int pb_triplet_contract_tiled(int method, const void *maps, int n_maps, int n_factor, int64_t n_vox,
+                                         const void *table, const int32_t *counts, double scale, double *out,
+                                         void *workspace, size_t workspace_bytes, void *stream) {
     if (!maps || !table || !out) return fail(PB_ERR_INVALID, "pb_triplet_contract_tiled: NULL argument");
     int st = check_counts(counts);
     if (st) return st;
     if (n_vox < 1 || n_maps < 1) return fail(PB_ERR_INVALID, "pb_triplet_contract_tiled: empty contraction");
+    if (n_factor < 1 || n_factor > n_maps)
+        return fail(PB_ERR_INVALID, "pb_triplet_contract_tiled: n_factor not in [1, n_maps]");
     if (method != PB_TRIPLET_TC)
         return fail(PB_ERR_UNSUPPORTED, "pb_triplet_contract_tiled: only the tensor-core method reads tiled sets");
-    return launch_triplet_tc_tiled((const float *)maps, n_maps, n_vox, (const unsigned char *)table, counts, scale,
-                                   out, workspace, workspace_bytes, as_stream(stream));
+    return launch_triplet_tc_tiled((const char *)maps, n_maps, n_factor, n_vox, (const unsigned char *)table, counts,
+                                   scale, out, workspace, workspace_bytes, as_stream(stream));
 }

@@ -38,8 +38,9 @@ int triplet_tc_workspace_size(int64_t n_vox, const int32_t *counts, int n_c, siz
 int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void *C, int n_c, int64_t n_vox,
                       const unsigned char *table, const int32_t *counts, double scale, double *out, void *workspace,
                       size_t workspace_bytes, cudaStream_t s);
-// the same contraction with A = B = C = one tiled map set of n_maps maps (tiled_index)
-int launch_triplet_tc_tiled(const float *maps, int n_maps, int64_t n_vox, const unsigned char *table,
+// the same contraction with A = B = C = one tiled map set (tiled_factor_byte, tiled_c_byte);
+// pair factors are among its first n_factor maps
+int launch_triplet_tc_tiled(const char *maps, int n_maps, int n_factor, int64_t n_vox, const unsigned char *table,
                             const int32_t *counts, double scale, double *out, void *workspace, size_t workspace_bytes,
                             cudaStream_t s);
 

@@ -31,7 +31,7 @@
 // Warp roles (16 warps): 0 stages tiles, 1 issues the MMAs (one lane), 2-3 split the C maps, 4-7 fold accumulators
 // (warp w reads TMEM lane quarter w % 4), 8-15 produce pair products (two warps per lane
 // quarter, each taking half of a tile's K steps).  They synchronise through mbarriers
-// only.  Every `chain` tiles (1024 voxels by default) the accumulators are folded
+// only.  Every `chain` tiles (512 voxels by default) the accumulators are folded
 // (tcgen05.ld) into FP64 sums in shared memory, double buffered in TMEM when both sets fit.
 // Every mbarrier wait is bounded; on timeout the CTA records an error in the workspace,
 // stops issuing work, drains (bounded) and frees TMEM, and the finalize kernel writes NaN
@@ -48,13 +48,16 @@ namespace pb {
 constexpr int TC_MAX_MT = 4;                // pair M-tiles of 128 lanes (<= 512 pairs per launch)
 constexpr int TC_MAX_SIDE = 16;             // side pairs (shared-memory operand)
 constexpr int TC_MAX_NC = 64;               // C maps per launch
-constexpr int TC_CHAIN_VOX = 1024;          // default voxels accumulated in TMEM (FP32) between FP64 folds
+// default voxels accumulated in TMEM between FP64 folds: the tensor core's FP32 accumulation
+// loses about half an ulp per K step (measured on positive-mean maps: mean relative error
+// -4e-7 after 256 voxels, -9e-7 after 512, -2e-6 after 1024, -5e-6 after 2048)
+constexpr int TC_CHAIN_VOX = 512;
 constexpr int TC_MAX_STAGES = 6;
 constexpr int TC_MAX_NBUF = 4;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 
 // how a CTA stages its tiles
-constexpr int TC_STAGE_CPASYNC = 0, TC_STAGE_TMA = 1, TC_STAGE_BULK = 2;
+constexpr int TC_STAGE_CPASYNC = 0, TC_STAGE_TMA = 1, TC_STAGE_TILED = 2;
 
 constexpr int TC_WARPS = 16;
 constexpr int TC_THREADS = 32 * TC_WARPS;
@@ -85,6 +88,10 @@ struct TcGeom {
     int poll;                   // 1: the MMA lane and the operand producers poll their barriers
     int n_cons;                 // arrivals per stage / operand buffer: active producer warps + C warps
     int pw_active;              // bit q: pair warps of lane quarter q have pairs
+    int split_c;                // 1: the C operand is part of the staged tile (a tiled set), bf16 hi/lo in
+                                // the 32-byte-swizzled K-major layout at byte c_off of the stage
+    int c_off;
+    int pair_lim;               // pair factor rows must lie below this
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -98,6 +105,14 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
     d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
     d |= (uint64_t)1 << 46;
     return d;
+}
+
+// descriptor of a 32-byte-swizzled K-major operand (8-row atoms of 256 bytes, 256-aligned,
+// one atom column = one K step of 16 bf16): LBO unused (1), SBO 256 bytes between 8-row
+// atoms, version 1, layout type SWIZZLE_32B (6) [61,64)
+__device__ __forceinline__ uint64_t umma_desc_sw32(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(256 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)6 << 61);
 }
 
 __host__ __device__ constexpr uint32_t umma_idesc_bf16_f32(int M, int N) {
@@ -151,6 +166,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     }
     return true;
 }
+
+// slot of a ring of n buffers and the parity of its current use (no division per tile)
+struct Ring {
+    int idx = 0, phase = 0;
+    __device__ __forceinline__ void next(int n) {
+        if (++idx == n) {
+            idx = 0;
+            phase ^= 1;
+        }
+    }
+};
 
 // lane 0 waits (bounded), the warp learns the outcome
 __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int lane, int poll = 0) {
@@ -312,18 +338,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t n_tiles = (n_vox + T - 1) / T;
-    const int64_t my_tiles = n_tiles > blockIdx.x ? (n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const int my_tiles = n_tiles > blockIdx.x ? (int)((n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
 
     // C operand buffers start at zero (the padding rows nc_pad > n_c stay zero)
     for (int i = tid; i < geo.nbuf * (geo.cop_bytes + geo.side_bytes) / 16; i += TC_THREADS)
         reinterpret_cast<uint4 *>(cop0)[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < 2 * geo.n_side * n_c; i += TC_THREADS) acc2[i] = 0.0;
-    for (int i = tid; i < 2 * geo.n_pairs; i += TC_THREADS) spairs[i] = pairs[i];
+    int bad_rows = 0;
+    for (int i = tid; i < 2 * geo.n_pairs; i += TC_THREADS) {
+        spairs[i] = pairs[i];
+        bad_rows |= (pairs[i] < 0 || pairs[i] >= geo.pair_lim);
+    }
     for (int i = tid; i < geo.n_tp * geo.acc_ld; i += TC_THREADS) acc[i] = 0.0;
     if (tid == 0) {
         for (int k = 0; k < geo.nstage; ++k) {
             mbar_init(&full[k], stage_mode == TC_STAGE_CPASYNC ? 32 : 1);
-            mbar_init(&empty[k], geo.n_cons);
+            mbar_init(&empty[k], geo.split_c ? 1 : geo.n_cons);
         }
         for (int k = 0; k < geo.nbuf; ++k) {
             mbar_init(&opready[k], geo.n_cons);
@@ -343,27 +373,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     fence_async_smem();
     tc_fence_before();
+    // a pair row outside its map set (a plan made for other sets) stops the CTA before any work
+    if (__syncthreads_or(bad_rows) && tid == 0) abort_flag = 1;
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    int last_issued = -1;  // MMA lane: last tile whose MMAs were committed
+    int last_issued = -1;  // MMA lane: last tile whose MMAs were committed, its operand buffer and use parity
+    int last_buf = 0, last_phase = 0;
+    const bool rejected = abort_flag != 0;  // bad pair rows: no role starts
 
-    if (warp == TC_LOADW) {
+    if (rejected) {
+    } else if (warp == TC_LOADW) {
         // ---------------- staging warp ----------------
-        for (int64_t it = 0; it < my_tiles; ++it) {
-            const int slot = (int)(it % geo.nstage);
-            if (it >= geo.nstage && !warp_wait(&empty[slot], (uint32_t)(((it - geo.nstage) / geo.nstage) & 1), lane)) {
+        Ring st;
+        for (int it = 0; it < my_tiles; ++it, st.next(geo.nstage)) {
+            const int slot = st.idx;
+            if (it >= geo.nstage && !warp_wait(&empty[slot], (uint32_t)(st.phase ^ 1), lane)) {
                 atomicExch(&abort_flag, 1);
                 break;
             }
             if (*(volatile int *)&abort_flag) break;
             const int64_t v0 = (blockIdx.x + it * (int64_t)gridDim.x) * T;
             const uint32_t dst = smem_u32(stage0 + slot * geo.stage_bytes);
-            if (stage_mode == TC_STAGE_BULK) {
-                // the tile's HALVES slabs of the tiled set: one contiguous block
+            if (stage_mode == TC_STAGE_TILED) {
+                // tile v0 / T of the tiled set: one contiguous block
                 if (lane == 0) {
                     mbar_expect_tx(&full[slot], (uint32_t)geo.stage_bytes);
-                    bulk_load(dst, A + (v0 >> 5) * (int64_t)geo.n_rows * 32, (uint32_t)geo.stage_bytes, &full[slot]);
+                    bulk_load(dst, reinterpret_cast<const char *>(A) + (v0 / T) * (int64_t)geo.stage_bytes,
+                              (uint32_t)geo.stage_bytes, &full[slot]);
                 }
             } else if (stage_mode == TC_STAGE_TMA) {
                 if (lane == 0) {
@@ -399,31 +436,43 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const uint32_t idesc_hi = umma_idesc_bf16_f32(128, 2 * geo.nc_pad);
             const uint32_t idesc_lo = umma_idesc_bf16_f32(128, geo.nc_pad);
             int chain = 0, chain_pos = 0;
-            for (int64_t it = 0; it < my_tiles; ++it) {
-                const int buf = (int)(it % geo.nbuf);
-                if (!mbar_wait_bounded(&opready[buf], (uint32_t)((it / geo.nbuf) & 1), geo.poll)) {
+            Ring bf, st, ds;
+            for (int it = 0; it < my_tiles; ++it, bf.next(geo.nbuf), st.next(geo.nstage)) {
+                const int buf = bf.idx;
+                if (!mbar_wait_bounded(&opready[buf], (uint32_t)bf.phase, geo.poll)) {
                     atomicExch(&abort_flag, 1);
                     break;
                 }
                 if (chain_pos == 0 && chain >= geo.dsets) {
-                    const int pc = chain - geo.dsets;
-                    if (!mbar_wait_bounded(&accfree[pc % geo.dsets], (uint32_t)((pc / geo.dsets) & 1), geo.poll)) {
+                    // the fold of the chain that used this accumulator set before
+                    if (!mbar_wait_bounded(&accfree[ds.idx], (uint32_t)(ds.phase ^ 1), geo.poll)) {
                         atomicExch(&abort_flag, 1);
                         break;
                     }
                 }
+                const int slot = st.idx;
+                // the C operand of a tiled set is read from the stage itself
+                if (geo.split_c && !mbar_wait_bounded(&full[slot], (uint32_t)st.phase, geo.poll)) {
+                    atomicExch(&abort_flag, 1);
+                    break;
+                }
                 if (*(volatile int *)&abort_flag) break;
                 tc_fence_after();
-                const int dset = chain % geo.dsets;
-                const uint32_t csm = smem_u32(cop0 + buf * geo.cop_bytes);
+                const int dset = ds.idx;
+                const uint32_t csm = geo.split_c ? smem_u32(stage0 + slot * geo.stage_bytes + geo.c_off)
+                                                 : smem_u32(cop0 + buf * geo.cop_bytes);
+                // K step ks of the C operand: 16 voxels of every row
+                auto cdesc = [&](int ks) -> uint64_t {
+                    if (geo.split_c) return umma_desc_sw32(csm + ks * 64 * geo.nc_pad);
+                    return umma_desc(csm + 2 * ks * geo.cop_lbo, geo.cop_lbo, 128);
+                };
                 if (geo.n_side) {
                     const uint32_t d2 = tmem + (uint32_t)(geo.d2col0 + dset * 2 * geo.ns_pad);
                     const uint32_t ssm = smem_u32(sop0 + buf * geo.side_bytes);
                     const uint32_t idesc_s = umma_idesc_bf16_f32(2 * geo.nc_pad, 2 * geo.ns_pad);
 #pragma unroll
                     for (int ks = 0; ks < KS; ++ks)
-                        umma_ss_bf16(d2, umma_desc(csm + 2 * ks * geo.cop_lbo, geo.cop_lbo, 128),
-                                     umma_desc(ssm + 2 * ks * geo.side_lbo, geo.side_lbo, 128), idesc_s,
+                        umma_ss_bf16(d2, cdesc(ks), umma_desc(ssm + 2 * ks * geo.side_lbo, geo.side_lbo, 128), idesc_s,
                                      (chain_pos > 0 || ks > 0) ? 1u : 0u);
                 }
                 for (int mt = 0; mt < geo.n_mt; ++mt) {
@@ -431,17 +480,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint32_t a = tmem + (uint32_t)(geo.pcol0 + (buf * geo.n_mt + mt) * T);
 #pragma unroll
                     for (int ks = 0; ks < KS; ++ks) {
-                        const uint64_t bdesc = umma_desc(csm + 2 * ks * geo.cop_lbo, geo.cop_lbo, 128);
+                        const uint64_t bdesc = cdesc(ks);
                         umma_ts_bf16(d, a + 16 * ks, bdesc, idesc_hi, (chain_pos > 0 || ks > 0) ? 1u : 0u);
                         umma_ts_bf16(d, a + 16 * ks + 8, bdesc, idesc_lo, 1u);
                     }
                 }
                 umma_commit(&opfree[buf]);
-                last_issued = (int)it;
+                if (geo.split_c) umma_commit(&empty[slot]);  // the stage is free once its MMAs are done
+                last_issued = it;
+                last_buf = buf;
+                last_phase = bf.phase;
                 if (++chain_pos == geo.chain || it + 1 == my_tiles) {
                     umma_commit(&accready[dset]);  // the chain's sums are complete in TMEM
                     chain_pos = 0;
                     ++chain;
+                    ds.next(geo.dsets);
                 }
             }
         }
@@ -450,14 +503,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // unit (map j, 8-voxel chunk c8): two 16-byte reads of the staged row, bf16 hi to
         // row j and lo to row nc_pad + j of the B operand (K chunk c8)
         const int ct = tid - 32 * TC_CW0;
-        const int n_unit = n_c * (T / 8);
+        const int n_unit = geo.split_c ? 0 : n_c * (T / 8);  // a tiled set carries the split C maps
         const int n_all = n_unit + geo.n_side * (T / 8);
-        for (int64_t it = 0; it < my_tiles; ++it) {
-            const int buf = (int)(it % geo.nbuf);
-            const int slot = (int)(it % geo.nstage);
-            if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane, geo.poll) ||
-                (it >= geo.nbuf &&
-                 !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane, geo.poll))) {
+        Ring bf, st;
+        for (int it = 0; it < my_tiles; ++it, bf.next(geo.nbuf), st.next(geo.nstage)) {
+            const int buf = bf.idx, slot = st.idx;
+            if (!warp_wait(&full[slot], (uint32_t)st.phase, lane, geo.poll) ||
+                (it >= geo.nbuf && !warp_wait(&opfree[buf], (uint32_t)(bf.phase ^ 1), lane, geo.poll))) {
                 atomicExch(&abort_flag, 1);
                 break;
             }
@@ -501,7 +553,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             fence_async_smem();
             __syncwarp();
             if (lane == 0) {
-                mbar_arrive(&empty[slot]);
+                if (!geo.split_c) mbar_arrive(&empty[slot]);
                 mbar_arrive(&opready[buf]);
             }
         }
@@ -521,12 +573,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 rb[mt] = ok[mt] ? (uint32_t)(geo.off_b + spairs[2 * p + 1]) : 0u;
             }
             const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
-            for (int64_t it = 0; it < my_tiles; ++it) {
-                const int buf = (int)(it % geo.nbuf);
-                const int slot = (int)(it % geo.nstage);
-                if (!warp_wait(&full[slot], (uint32_t)((it / geo.nstage) & 1), lane, geo.poll) ||
-                    (it >= geo.nbuf &&
-                     !warp_wait(&opfree[buf], (uint32_t)(((it - geo.nbuf) / geo.nbuf) & 1), lane, geo.poll))) {
+            Ring bf, st;
+            for (int it = 0; it < my_tiles; ++it, bf.next(geo.nbuf), st.next(geo.nstage)) {
+                const int buf = bf.idx, slot = st.idx;
+                if (!warp_wait(&full[slot], (uint32_t)st.phase, lane, geo.poll) ||
+                    (it >= geo.nbuf && !warp_wait(&opfree[buf], (uint32_t)(bf.phase ^ 1), lane, geo.poll))) {
                     atomicExch(&abort_flag, 1);
                     break;
                 }
@@ -560,7 +611,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) {
-                    mbar_arrive(&empty[slot]);
+                    if (!geo.split_c) mbar_arrive(&empty[slot]);
                     mbar_arrive(&opready[buf]);
                 }
             }
@@ -569,10 +620,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---------------- fold warps ----------------
         // chain c lives in accumulator set c % dsets; lane quarter q holds pairs 128 mt + 32 q + lane
         const int q = warp & 3;
-        const int64_t n_chains = (my_tiles + geo.chain - 1) / geo.chain;
-        for (int64_t c = 0; c < n_chains; ++c) {
-            const int dset = (int)(c % geo.dsets);
-            if (!warp_wait(&accready[dset], (uint32_t)((c / geo.dsets) & 1), lane)) {
+        const int n_chains = (my_tiles + geo.chain - 1) / geo.chain;
+        Ring ds;
+        for (int c = 0; c < n_chains; ++c, ds.next(geo.dsets)) {
+            const int dset = ds.idx;
+            if (!warp_wait(&accready[dset], (uint32_t)ds.phase, lane)) {
                 atomicExch(&abort_flag, 1);
                 break;
             }
@@ -627,7 +679,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // ---------------- teardown ----------------
     if (warp == TC_MMAW && lane == 0 && last_issued >= 0) {
         // the MMAs of the last tile must drain before TMEM is freed (bounded)
-        mbar_wait_bounded(&opfree[last_issued % geo.nbuf], (uint32_t)((last_issued / geo.nbuf) & 1));
+        mbar_wait_bounded(&opfree[last_buf], (uint32_t)last_phase);
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     tc_fence_before();
@@ -671,6 +723,8 @@ __global__ void triplet_tc_finalize(const double *partials, int n_cta, int n_pai
 
 struct TcRows {
     int n_rows, rows_a, rows_b, rows_c, off_b, off_c;
+    int tiled;     // 1: one tiled set; n_rows = its factor rows, the C operand in the tile
+    int pair_lim;  // pair factor indices must lie below this
 };
 
 static int pad8(int x) { return (x + 7) & ~7; }
@@ -687,11 +741,20 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     g->n_pairs = n_pairs;
     g->n_c = n_c;
     if (n_c > TC_MAX_NC) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 64 C maps");
+    g->split_c = rw.tiled;
+    g->pair_lim = rw.pair_lim;
+    if (rw.tiled && T != TILED_VOX) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: tiled sets take 128-voxel tiles");
     const int rem = n_pairs % 128;
     g->n_side = (n_pairs > 128 && rem > 0 && rem <= TC_MAX_SIDE) ? rem : 0;
+    // the side MMA takes the C operand as its A operand: M = 2 nc_pad must be 64 or 128 (a tiled
+    // set's operand has its own row padding: without a fitting one the side pairs get an M-tile)
+    if (rw.tiled) {
+        g->nc_pad = tiled_cpad(n_c);
+        if (g->nc_pad != 32 && g->nc_pad != 64) g->n_side = 0;
+    } else {
+        g->nc_pad = g->n_side ? (n_c <= 32 ? 32 : 64) : (n_c + 15) / 16 * 16;
+    }
     g->n_tp = n_pairs - g->n_side;
-    // the side MMA takes the C operand as its A operand: M = 2 nc_pad must be 64 or 128
-    g->nc_pad = g->n_side ? (n_c <= 32 ? 32 : 64) : (n_c + 15) / 16 * 16;
     g->ns_pad = g->n_side <= 8 ? 8 : 16;
     g->n_mt = (g->n_tp + 127) / 128;
     if (g->n_mt > TC_MAX_MT) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 512 pairs");
@@ -717,6 +780,12 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     g->stage_bytes = (T / 32) * g->half_bytes;
     g->cop_lbo = (2 * g->nc_pad / 8) * 128 + 16;
     g->cop_bytes = ((T / 8) * g->cop_lbo + 127) / 128 * 128;
+    if (rw.tiled) {
+        // [factor slabs][C operand: 8 K steps x 2 nc_pad rows x 32 B], as tiled_tile_bytes
+        g->c_off = g->stage_bytes;
+        g->stage_bytes += 2 * 2 * g->nc_pad * 128;
+        g->cop_bytes = 0;
+    }
     g->side_lbo = g->n_side ? (2 * g->ns_pad / 8) * 128 + 16 : 0;
     g->side_bytes = g->n_side ? ((T / 8) * g->side_lbo + 127) / 128 * 128 : 0;
     g->acc_ld = g->nc_pad + 1;
@@ -726,7 +795,9 @@ static int tc_geometry(const TcRows &rw, int n_pairs, int n_c, int T, TcGeom *g)
     const int fixed = 1024 + g->acc_bytes + g->nbuf * (g->cop_bytes + g->side_bytes) + table;
     const int budget = 225 * 1024;
     int ns = std::min(TC_MAX_STAGES, (budget - fixed) / std::max(1, g->stage_bytes));
+    // a tiled set's stage stays until its MMAs are done: as many as fit
     const int want = tuning().tc_stages > 0 ? tuning().tc_stages
+                     : rw.tiled             ? TC_MAX_STAGES
                                             : std::max(2, (64 * 1024) / std::max(1, g->stage_bytes));  // ~64 KB
     ns = std::min(ns, want);
     if (ns < 2) return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: tile too large for shared memory");
@@ -790,8 +861,8 @@ static int run_triplet_tc(const float *A, int n_a, const float *B, int n_b, cons
     TcGeom g;
     int chunk = std::min(n_pairs, 128 * TC_MAX_MT);
     int st = tc_geometry(rw, chunk, n_c, T, &g);
-    while (st == PB_ERR_UNSUPPORTED && (T > 32 || chunk > 16)) {
-        if (T > 32) T /= 2;
+    while (st == PB_ERR_UNSUPPORTED && ((T > 32 && !rw.tiled) || chunk > 16)) {
+        if (T > 32 && !rw.tiled) T /= 2;
         else chunk = (chunk + 1) / 2;
         st = tc_geometry(rw, chunk, n_c, T, &g);
     }
@@ -856,7 +927,7 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
         *k = (int)(d / map_bytes);
         return *k + n_p <= n_a && d / map_bytes < (size_t)n_a;
     };
-    TcRows rw{pad8(n_a), n_a, 0, 0, 0, 0};
+    TcRows rw{pad8(n_a), n_a, 0, 0, 0, 0, 0, std::max(n_a, n_b)};
     if (!rows_of_a(B, n_b, &rw.off_b)) {
         rw.off_b = rw.n_rows;
         rw.rows_b = n_b;
@@ -899,7 +970,7 @@ int launch_triplet_tc(const void *A, int n_a, const void *B, int n_b, const void
                           maps, T, table, counts, scale, out, workspace, workspace_bytes, s, "pb_triplet_contract(tc)");
 }
 
-int launch_triplet_tc_tiled(const float *maps, int n_maps, int64_t n_vox, const unsigned char *table,
+int launch_triplet_tc_tiled(const char *maps, int n_maps, int n_factor, int64_t n_vox, const unsigned char *table,
                             const int32_t *counts, double scale, double *out, void *workspace, size_t workspace_bytes,
                             cudaStream_t s) {
     int st = check_device();
@@ -907,12 +978,13 @@ int launch_triplet_tc_tiled(const float *maps, int n_maps, int64_t n_vox, const 
     if (n_maps > TC_MAX_NC)
         return fail(PB_ERR_UNSUPPORTED, "tensor-core contraction: more than 64 maps in a tiled set");
     if ((uintptr_t)maps & 15) return fail(PB_ERR_INVALID, "pb_triplet_contract_tiled: maps not 16-byte aligned");
-    // every staged row is a row of the one set: A = B = C
-    const TcRows rw{pad8(n_maps), n_maps, 0, 0, 0, 0};
+    // A = B = C = the set: the staged factor rows are its first n_factor maps, the C operand
+    // (all maps) comes with the tile
+    const TcRows rw{tiled_frows(n_factor), n_factor, 0, 0, 0, 0, 1, n_factor};
     CUtensorMap none[3];
     memset(none, 0, sizeof(none));
-    const int T = tuning().tc_tile ? tuning().tc_tile : 128;
-    return run_triplet_tc(maps, n_maps, maps, n_maps, maps, n_maps, n_vox, rw, TC_STAGE_BULK, none, T, table, counts,
+    const float *f = reinterpret_cast<const float *>(maps);
+    return run_triplet_tc(f, n_maps, f, n_maps, f, n_maps, n_vox, rw, TC_STAGE_TILED, none, TILED_VOX, table, counts,
                           scale, out, workspace, workspace_bytes, s, "pb_triplet_contract_tiled");
 }
 

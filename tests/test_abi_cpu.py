@@ -194,27 +194,33 @@ def test_tuning_settings_round_trip_and_checks():
 
 
 def test_tiled_map_layout_host_side():
-    """Tiled map sets: the size covers whole 128-voxel tiles of 8-row groups, the element
-    index (as the header states it) is a one-to-one map into that size, each 32-voxel slab
-    row is 128 contiguous bytes, and the converters refuse bad arguments without a device."""
+    """Tiled map sets: the size covers whole 128-voxel tiles of [factor slabs][C operand], the
+    byte offsets of the FP32 factor values and of the bf16 hi / lo parts (as the header states
+    them) never collide and stay inside that size, a map's 32 (factor) consecutive voxels fill
+    one 128-byte row and 16 (operand) one 32-byte sector, and the converters refuse bad
+    arguments without a device."""
     lib = nat.load()
-    for n_maps, n_vox in ((1, 1), (5, 1000), (32, 192 ** 3 // 64), (33, 50_003)):
-        R = (n_maps + 7) // 8 * 8
-        slabs = (n_vox + 127) // 128 * 4
-        assert nat.tiled_maps_bytes(n_maps, n_vox) == slabs * R * 32 * 4
-        idx = nat.tiled_index(n_maps, n_vox)
-        assert idx.min() >= 0 and idx.max() < slabs * R * 32
-        assert len(np.unique(idx)) == idx.size
-        # voxels 32 s .. 32 s + 31 of a row fill one 128-byte row of slab s
+    for n_maps, n_factor, n_vox in ((1, 1, 1), (5, 3, 1000), (32, 16, 192 ** 3 // 64), (33, 33, 50_003)):
+        F, P = (n_factor + 7) // 8 * 8, (n_maps + 15) // 16 * 16
+        size = (n_vox + 127) // 128 * 512 * (F + P)
+        assert nat.tiled_maps_bytes(n_maps, n_factor, n_vox) == size
+        fo = nat.tiled_factor_offsets(n_maps, n_factor, n_vox)
+        co = nat.tiled_c_offsets(n_maps, n_factor, n_vox)
+        assert fo.min() >= 0 and fo.max() + 4 <= size and co.min() >= 0 and co.max() + 2 <= size
+        spans = np.concatenate([(fo // 4).reshape(-1) * 2, (fo // 4).reshape(-1) * 2 + 1, (co // 2).reshape(-1)])
+        assert len(np.unique(spans)) == spans.size  # in 2-byte units: no overlaps
         v = np.arange(n_vox)
+        for m in (0, n_factor - 1):
+            assert np.all(fo[m] // 128 == fo[m][v - v % 32] // 128)
         for m in (0, n_maps - 1):
-            assert np.all(idx[m] // 32 == (v // 32) * R + m)
+            assert np.all(co[0, m] // 32 == co[0, m][v - v % 16] // 32)
     nb = ctypes.c_size_t()
-    assert lib.pb_tiled_maps_bytes(0, 10, ctypes.byref(nb)) != 0
-    assert lib.pb_tiled_maps_bytes(4, 0, ctypes.byref(nb)) != 0
-    assert lib.pb_tile_maps(None, 4, 100, None, None) != 0
+    assert lib.pb_tiled_maps_bytes(0, 1, 10, ctypes.byref(nb)) != 0
+    assert lib.pb_tiled_maps_bytes(4, 5, 10, ctypes.byref(nb)) != 0
+    assert lib.pb_tiled_maps_bytes(4, 0, 10, ctypes.byref(nb)) != 0
+    assert lib.pb_tile_maps(None, 4, 2, 100, None, None) != 0
     counts = np.ones(4, dtype=np.int32)
     out = np.zeros(1)
-    # only the tensor-core method reads a tiled set; NULL maps are refused first
-    assert lib.pb_triplet_contract_tiled(nat.PB_TRIPLET_TC, None, 4, 100, nat.hptr(counts), nat.hptr(counts), 1.0,
+    # NULL maps and a factor count outside [1, n_maps] are refused before any device work
+    assert lib.pb_triplet_contract_tiled(nat.PB_TRIPLET_TC, None, 4, 2, 100, nat.hptr(counts), nat.hptr(counts), 1.0,
                                          nat.hptr(out), None, 0, None) != 0

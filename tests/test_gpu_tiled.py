@@ -1,9 +1,11 @@
-"""Tiled map sets (the tensor-core contraction's staging layout in device memory):
-conversion round trip, the pruned synthesis writing the layout directly (identical values
-to its plain output), and the tensor-core contraction from a tiled set (one contiguous bulk
-copy per tile) against FP64 sums and against the same contraction from plain maps; the
-bispectrum estimator through the tiled path against the plain path."""
+"""Tiled map sets (the tensor-core contraction's staging layout in device memory: FP32 pair
+factor maps and the bf16 hi/lo C operand per 128-voxel tile): conversion, the pruned
+synthesis writing the layout directly (identical values to its plain output), and the
+tensor-core contraction from a tiled set (one contiguous bulk copy per tile, the MMA reading
+the operand from the staged tile) against FP64 sums and against the same contraction from
+plain maps; the bispectrum estimator through the tiled path against the plain path."""
 import contextlib
+import ctypes
 import io
 
 import numpy as np
@@ -39,30 +41,47 @@ def reference(G, idx):
     return out
 
 
-@pytest.mark.parametrize("n_maps,n_vox", [(5, 50_003), (32, 64 ** 3), (33, 1000)])
-def test_tile_maps_round_trip(n_maps, n_vox):
+def split(G):
+    hi = G.to(torch.bfloat16)
+    return hi, (G - hi.float()).to(torch.bfloat16)
+
+
+def covered(T):
+    """Bool mask over T.data of the bytes the layout assigns to the set's voxels."""
+    hit = torch.zeros(T.data.numel(), dtype=torch.bool, device=T.data.device)
+    fo = torch.as_tensor(nat.tiled_factor_offsets(T.n_maps, T.n_factor, T.n_vox), device=hit.device).reshape(-1)
+    co = torch.as_tensor(nat.tiled_c_offsets(T.n_maps, T.n_factor, T.n_vox), device=hit.device).reshape(-1)
+    for o, w in ((fo, 4), (co, 2)):
+        for k in range(w):
+            hit[o + k] = True
+    return hit
+
+
+@pytest.mark.parametrize("n_maps,n_factor,n_vox", [(5, 3, 50_003), (32, 16, 64 ** 3), (33, 33, 1000)])
+def test_tile_maps_round_trip(n_maps, n_factor, n_vox):
     torch.manual_seed(0)
     G = torch.randn(n_maps, n_vox, device="cuda")
-    T = nat.TiledMaps.from_maps(G)
-    assert torch.equal(T.to_maps(), G)
-    # everything the index does not reach (padding rows, voxels past n_vox) is zero
-    hit = torch.zeros(T.data.numel(), dtype=torch.bool, device="cuda")
-    hit[torch.as_tensor(nat.tiled_index(n_maps, n_vox), device="cuda").reshape(-1)] = True
-    assert torch.count_nonzero(T.data[~hit]) == 0
+    T = nat.TiledMaps.from_maps(G, n_factor)
+    assert torch.equal(T.factor_maps(), G[:n_factor])
+    hi, lo = T.split_parts()
+    rh, rl = split(G)
+    assert torch.equal(hi, rh) and torch.equal(lo, rl)
+    # padding rows and the voxels past n_vox are zero
+    assert torch.count_nonzero(T.data[~covered(T)]) == 0
 
 
 @tc
 @pytest.mark.parametrize("n_vox", [64 ** 3, 50_003, 128])
-@pytest.mark.parametrize("cfg", [{}, {"tc_tile": 64}, {"tc_tile": 32}, {"tc_stages": 2}])
+@pytest.mark.parametrize("cfg", [{}, {"tc_stages": 2}, {"tc_wait": 2}, {"tc_dsets": 1}])
 def test_contract_tiled_matches_fp64(n_vox, cfg):
-    """32 maps, 136 pairs (128 in tensor memory + 8 side pairs), 888 triplets."""
+    """32 maps (16 pair factors), 136 pairs (128 in tensor memory + 8 side pairs), 888 triplets."""
     torch.manual_seed(1)
     idx = bk_like_triplets()
     G = torch.randn(32, n_vox, device="cuda")
     ref = reference(G, torch.as_tensor(idx, device="cuda").long()).cpu().numpy()
     ws = nat.Workspace(torch.device("cuda"))
     plan = nat.TripletPlan(32, 32, 32, idx, torch.device("cuda"))
-    T = nat.TiledMaps.from_maps(G)
+    T = nat.TiledMaps.from_maps(G, 16)
     out = torch.empty(len(idx), dtype=torch.float64, device="cuda")
     nat.set_tuning(cfg)
     try:
@@ -82,8 +101,8 @@ def test_contract_tiled_matches_fp64(n_vox, cfg):
 @tc
 @pytest.mark.parametrize("nk", [24, 12])
 def test_contract_tiled_other_shapes(nk):
-    """48 maps / 300 pairs (pair M-tiles that do not fit 128-voxel operand buffers: smaller
-    tiles) and 24 maps / 78 pairs (one partly filled M-tile)."""
+    """48 maps / 300 pairs (M-tiles that do not fit two 128-voxel operand buffers: pair
+    chunks) and 24 maps / 78 pairs (one partly filled M-tile, operand rows padded to 32)."""
     torch.manual_seed(2)
     idx = bk_like_triplets(nk=nk, lmax=2)
     n = 2 * nk
@@ -92,19 +111,30 @@ def test_contract_tiled_other_shapes(nk):
     ws = nat.Workspace(torch.device("cuda"))
     plan = nat.TripletPlan(n, n, n, idx, torch.device("cuda"))
     out = torch.empty(len(idx), dtype=torch.float64, device="cuda")
-    plan.contract_tiled(nat.TiledMaps.from_maps(G), out, ws)
+    plan.contract_tiled(nat.TiledMaps.from_maps(G, nk), out, ws)
     got = out.cpu().numpy()
     assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-5
 
 
 @tc
-def test_contract_tiled_refuses_a_foreign_plan():
+def test_contract_tiled_rejects_pairs_outside_the_factor_maps():
+    """A plan whose pair factors are not among the set's factor maps: the Python wrapper
+    refuses it, and through the C ABI the kernel rejects it before any work (NaN outputs)."""
+    torch.manual_seed(3)
     G = torch.randn(8, 4096, device="cuda")
-    idx = np.asarray([(0, 1, 2), (1, 2, 3)], dtype=np.int32)
-    plan = nat.TripletPlan(8, 8, 4, idx, torch.device("cuda"))
+    idx = np.asarray([(0, 1, 2), (1, 5, 3)], dtype=np.int32)
+    plan = nat.TripletPlan(8, 8, 8, idx, torch.device("cuda"))
+    T = nat.TiledMaps.from_maps(G, 4)
+    ws = nat.Workspace(torch.device("cuda"))
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
     with pytest.raises(ValueError):
-        plan.contract_tiled(nat.TiledMaps.from_maps(G), torch.empty(2, dtype=torch.float64, device="cuda"),
-                            nat.Workspace(torch.device("cuda")))
+        plan.contract_tiled(T, out, ws)
+    buf = ws.get(plan.workspace_bytes(nat.PB_F32, nat.PB_TRIPLET_TC, T.n_vox), "triplet")
+    st = nat.load().pb_triplet_contract_tiled(nat.PB_TRIPLET_TC, nat.ptr(T.data), 8, 4, T.n_vox, nat.ptr(plan.table),
+                                              nat.hptr(plan.counts), 1.0, nat.ptr(out), nat.ptr(buf), buf.numel(),
+                                              nat.stream_ptr())
+    assert st == 0
+    assert torch.isnan(out).all()
 
 
 def quiet(fn, *a, **k):
@@ -114,8 +144,9 @@ def quiet(fn, *a, **k):
 
 @pytest.mark.parametrize("N", [40, 64])
 def test_shell_synth_tiled_equals_plain(N):
-    """The g-maps written as a tiled set hold exactly the values of the plain synthesis (the
-    40^3 grid's 30^3 map grid ends in a partly filled 128-voxel tile)."""
+    """The g-maps written as a tiled set hold exactly the values (FP32 factors, bf16 parts) of
+    the plain synthesis (the 40^3 grid's 30^3 map grid ends in a partly filled tile, whose
+    padding reads as zeros)."""
     import polybin3d_b200 as pb
     from polybin3d_b200 import synthetic
     L = 1000.0
@@ -125,15 +156,19 @@ def test_shell_synth_tiled_equals_plain(N):
     x = b.as_device(synthetic.lognormal(N, L, seed=3))
     xk = bs._data_spectrum(x)
     w = bs._data_weight(torch.float32)
-    G = bs._g_maps(xk, w, 1.0)
+    G = bs._g_maps(xk, w, 1.0).reshape(2 * bs.Nk_squeeze, -1)
     T = bs._g_maps_tiled(xk, w, 1.0)
-    assert T is not None and T.shape == tuple(G.shape[1:])
-    assert torch.equal(T.to_maps(), G)
+    assert T is not None and T.n_vox == G.shape[1] and T.n_factor == bs.Nk_squeeze
+    assert torch.equal(T.factor_maps().reshape(T.n_factor, -1), G[:T.n_factor])
+    hi, lo = T.split_parts()
+    rh, rl = split(G)
+    assert torch.equal(hi.reshape(T.n_maps, -1), rh) and torch.equal(lo.reshape(T.n_maps, -1), rl)
     if T.n_vox % 128:
-        hit = torch.zeros(T.data.numel(), dtype=torch.bool, device=T.data.device)
-        hit[torch.as_tensor(nat.tiled_index(T.n_maps, T.n_vox), device=hit.device).reshape(-1)] = True
-        tail = torch.arange(T.data.numel(), device=hit.device) >= (T.data.numel() - 4 * 32 * ((T.n_maps + 7) // 8 * 8))
-        assert torch.count_nonzero(T.data[~hit & tail]) == 0
+        nv = (T.n_vox + 127) // 128 * 128
+        fo = nat.tiled_factor_offsets(T.n_maps, T.n_factor, nv)[:, T.n_vox:].reshape(-1)
+        co = nat.tiled_c_offsets(T.n_maps, T.n_factor, nv)[:, :, T.n_vox:].reshape(-1)
+        pad = torch.as_tensor(np.concatenate([fo, fo + 1, fo + 2, fo + 3, co, co + 1]), device=T.data.device)
+        assert torch.count_nonzero(T.data[pad]) == 0
 
 
 @tc
