@@ -9,7 +9,9 @@ processes -- set the winner before launching.  Tuned shapes:
   tile (plain maps: 64 / 32), staging ring depth, the barrier-wait form, accumulator sets
   (never the TMEM chain length, which changes the FP32 rounding);
 * the k-bin reduction of many rows (>= 16): lane-per-row kernel (warps per block, blocks
-  per SM) against the mode-tile kernel.
+  per SM) against the mode-tile kernel;
+* routes that do the same work two ways (choose_route): the bispectrum's cubic sums from
+  plain maps or from a tiled set (synthesis and contraction timed together).
 
 Settings change launch shapes only; results agree to FP summation order.  Nothing is timed
 while a CUDA graph is being captured (the default or the cached setting is used), and
@@ -104,6 +106,39 @@ class Tuner:
             self.timings[key] = times
             self._save()
         return self.table[key]
+
+
+    def choose_route(self, key, runs, reps=3):
+        """The name of the fastest of `runs` (name -> callable doing the same work two ways),
+        cached like a setting; the first name when tuning is off or a graph is being captured."""
+        names = list(runs)
+        with self.lock:
+            hit = self.table.get(key)
+        if hit is not None and hit.get("route") in runs:
+            return hit["route"]
+        if not enabled() or torch.cuda.is_current_stream_capturing():
+            return names[0]
+        times = []
+        for name in names:
+            try:
+                runs[name]()  # warm-up (its own tuning, module load)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    runs[name]()
+                e1.record()
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1) / reps)
+            except (NotImplementedError, ValueError, MemoryError):
+                times.append(float("inf"))
+        best = int(np.argmin(times))
+        if not np.isfinite(times[best]):
+            best = 0
+        with self.lock:
+            self.table[key] = {"route": names[best]}
+            self.timings[key] = times
+            self._save()
+        return names[best]
 
 
 _TUNER = None

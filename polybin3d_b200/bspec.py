@@ -504,25 +504,44 @@ class BSpec:
 
     def _b3_sums(self, xk, w, scale):
         """FP64 sums B3[i] = assemble_b3 of the g-maps of one weighted spectrum.  With the
-        tensor-core contraction the g-maps are synthesised straight into a tiled set (the
-        contraction's staging layout: each tile of voxels of all maps is one contiguous
-        copy), else into plain maps."""
-        idx = self._triplet_index()
-        dt = xk.real.dtype
-        if self._tiled_ok(dt):
-            T = self._g_maps_tiled(xk, w, scale)
-            if T is not None:
-                plan = self._plan('b3', T.n_maps, T.n_maps, T.n_maps, idx)
-                out = torch.empty(plan.n_trip, dtype=torch.float64, device=self.base.device)
-                try:
-                    return autotune.contract_tiled(plan, T, out, self.base.ws, self._grid_scale(T.shape))
-                except NotImplementedError:
-                    if self.contraction == 'tc':
-                        raise
-                    self._tiled = False
-                    plan.tc_unsupported = True
+        tensor-core contraction there are two routes: the g-maps synthesised straight into a
+        tiled set (the contraction's staging layout: each tile of voxels of all maps is one
+        contiguous copy and the MMA operand comes pre-split), or plain maps staged by 2-D TMA
+        boxes.  The faster for this shape (synthesis and contraction timed together) is found
+        once and cached by the autotuner; the two agree to FP32 rounding."""
+        if self._tiled_ok(xk.real.dtype) and self._b3_route(xk, w, scale) == "tiled":
+            out = self._b3_tiled(xk, w, scale)
+            if out is not None:
+                return out
+        return self._b3_plain(xk, w, scale)
+
+    def _b3_plain(self, xk, w, scale):
         G = self._g_maps(xk, w, scale)
-        return self._contract('b3', G, G, G, idx)
+        return self._contract('b3', G, G, G, self._triplet_index())
+
+    def _b3_tiled(self, xk, w, scale):
+        """The tiled route, or None when a tiled set cannot be made or contracted here."""
+        T = self._g_maps_tiled(xk, w, scale)
+        if T is None:
+            return None
+        plan = self._plan('b3', T.n_maps, T.n_maps, T.n_maps, self._triplet_index())
+        out = torch.empty(plan.n_trip, dtype=torch.float64, device=self.base.device)
+        try:
+            return autotune.contract_tiled(plan, T, out, self.base.ws, self._grid_scale(T.shape))
+        except NotImplementedError:
+            if self.contraction == 'tc':
+                raise
+            self._tiled = False
+            return None
+
+    def _b3_route(self, xk, w, scale):
+        b = self.base
+        key = "b3route|%s|%s|%d|%d|%s" % (autotune.device_tag(b.device), ",".join(str(int(n)) for n in self.map_grid),
+                                          self.Nl * self.Nk_squeeze, self.Nk_squeeze, b.sightline)
+        def tiled():
+            if self._b3_tiled(xk, w, scale) is None:
+                raise NotImplementedError("no tiled set for this shape")
+        return autotune.tuner().choose_route(key, {"tiled": tiled, "plain": lambda: self._b3_plain(xk, w, scale)})
 
     def _tiled_ok(self, dtype):
         return (getattr(self, '_tiled', True) and self.synthesis != 'cufft' and

@@ -556,6 +556,60 @@ __global__ void __launch_bounds__(SY_THREADS) synth_y_kernel(SynthParams p, cons
     }
 }
 
+// ---- tiled-set output ------------------------------------------------------------------
+// voxel v of map m into a tiled set: FP32 copy of a factor map, bf16 hi and lo parts
+__device__ __forceinline__ void tiled_put(const SynthParams &p, int m, int64_t v, float val, char *out) {
+    if (m < p.t_factor) *reinterpret_cast<float *>(out + tiled_factor_byte(v, m, p.t_maps, p.t_factor)) = val;
+    const __nv_bfloat16 hi = __float2bfloat16_rn(val);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(val - __bfloat162float(hi));
+    *reinterpret_cast<__nv_bfloat16 *>(out + tiled_c_byte(v, m, p.t_maps, p.t_factor)) = hi;
+    *reinterpret_cast<__nv_bfloat16 *>(out + tiled_c_byte(v, tiled_cpad(p.t_maps) + m, p.t_maps, p.t_factor)) = lo;
+}
+
+// A block's staged values of map m (rows of NN voxels, row stride lds in stg; voxels v0 ..
+// v0 + rows NN - 1) into a tiled set.  Each warp takes 64 consecutive voxels, a lane two
+// neighbours: two 128-byte rows of factor slabs (8-byte stores) and four 32-byte K-step rows
+// each of the hi and lo parts (bf16x2 stores), so the stores fill whole sectors; offsets inside
+// a tile are per lane and fixed, the tile base per warp chunk.  Per voxel (tiled_put) when the
+// run is not 64-aligned.
+template <int NN>
+__device__ void flush_tiled(const SynthParams &p, int m, int64_t v0, int rows, int lds, const float *stg, char *out) {
+    const int count = rows * NN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if ((NN & 1) != 0 || (v0 & 63) != 0 || (count & 63) != 0) {
+        for (int i = threadIdx.x; i < count; i += blockDim.x) {
+            const int r = i / NN, z = i - r * NN;
+            tiled_put(p, m, v0 + i, stg[r * lds + z], out);
+        }
+        return;
+    }
+    const int F = tiled_frows(p.t_factor), P = tiled_cpad(p.t_maps);
+    const int64_t tb = tiled_tile_bytes(p.t_maps, p.t_factor);
+    const bool factor = m < p.t_factor;
+    // lane j holds voxels 2j, 2j + 1 of the chunk: slab j / 16, 4-voxel chunk (j % 16) / 2 of
+    // it; K step j / 8, 8-voxel half (j / 4) % 2, element 2 (j % 4)
+    const uint32_t off_f = (uint32_t)(lane >> 4) * F * 128u + (uint32_t)m * 128u +
+                           ((((uint32_t)(lane & 15) >> 1) ^ ((uint32_t)m & 7u)) << 4) + (lane & 1) * 8;
+    auto c_off = [&](int r) {
+        return (uint32_t)((lane >> 3) * 64 * P + (r >> 3) * 256 + (r & 7) * 32 +
+                          ((((lane >> 2) & 1) ^ ((r >> 2) & 1)) << 4) + (lane & 3) * 4);
+    };
+    const uint32_t off_hi = c_off(m), off_lo = c_off(P + m);
+    for (int u = warp * 64; u < count; u += nw * 64) {
+        const int i = u + 2 * lane, r = i / NN, z = i - r * NN;  // NN even: both voxels in row r
+        const float x0 = stg[r * lds + z], x1 = stg[r * lds + z + 1];
+        const int64_t v = v0 + u;  // 64-aligned: two slabs, four K steps of one tile
+        const int w = (int)(v & (TILED_VOX - 1));
+        char *const tile = out + (v >> 7) * tb;
+        if (factor) *reinterpret_cast<float2 *>(tile + (w >> 5) * F * 128 + off_f) = make_float2(x0, x1);
+        const __nv_bfloat162 hb = __floats2bfloat162_rn(x0, x1);
+        const __nv_bfloat162 lb = __floats2bfloat162_rn(x0 - __low2float(hb), x1 - __high2float(hb));
+        char *const cop = tile + 512 * F + (w >> 4) * 64 * P;
+        *reinterpret_cast<__nv_bfloat162 *>(cop + off_hi) = hb;
+        *reinterpret_cast<__nv_bfloat162 *>(cop + off_lo) = lb;
+    }
+}
+
 // ---- S3: real transform along z, two output lines per complex transform -----------------
 template <typename T, int N>
 __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, const typename cplx<T>::type *H,
@@ -583,20 +637,15 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
     T *const o = out + (int64_t)m * plane * p.m2 + v0;
     const int tiled = p.tiled;
     auto put = [&](int yy, int z, T val) {
-        if (!tiled) {
-            o[(int64_t)yy * p.m2 + z] = val;
-            return;
-        }
-        // FP32 copy of a factor map, bf16 hi and lo parts of every map
-        const int64_t v = v0 + (int64_t)yy * p.m2 + z;
-        char *const base = reinterpret_cast<char *>(out);
-        if (m < p.t_factor) *reinterpret_cast<float *>(base + tiled_factor_byte(v, m, p.t_maps, p.t_factor)) = (float)val;
-        const __nv_bfloat16 hi = __float2bfloat16_rn((float)val);
-        const __nv_bfloat16 lo = __float2bfloat16_rn((float)val - __bfloat162float(hi));
-        *reinterpret_cast<__nv_bfloat16 *>(base + tiled_c_byte(v, m, p.t_maps, p.t_factor)) = hi;
-        *reinterpret_cast<__nv_bfloat16 *>(base + tiled_c_byte(v, tiled_cpad(p.t_maps) + m, p.t_maps, p.t_factor)) = lo;
+        if (!tiled) o[(int64_t)yy * p.m2 + z] = val;
+        else tiled_put(p, m, v0 + (int64_t)yy * p.m2 + z, (float)val, reinterpret_cast<char *>(out));
     };
     if constexpr (N > 0 && pass_count(N) >= 2) {
+        // a tiled set's rows (2 L lines of n values) are staged in the transform buffer the last
+        // pass does not read (b1 after an even number of shared-memory passes, else b0) and
+        // written out together
+        float *const stg = reinterpret_cast<float *>((pass_count(N) - 2) % 2 == 0 ? b1 : b0);
+        constexpr int LDS = N + 1;  // odd row stride: the last pass's lanes write different rows
         // first pass straight from H (a warp reads the (y, y+1) pairs of 32 lines at one kz:
         // 512 contiguous bytes; it needs no twiddles), last pass straight to the real rows
         const C *hb = H + mp.h_off + (int64_t)x * p.m1 + y0;
@@ -635,9 +684,18 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
                 return r;
             },
             [&](int line, int z, C v) {
-                put(2 * line, z, v.x);
-                put(2 * line + 1, z, v.y);
+                if (tiled) {
+                    stg[(2 * line) * LDS + z] = (float)v.x;
+                    stg[(2 * line + 1) * LDS + z] = (float)v.y;
+                } else {
+                    put(2 * line, z, v.x);
+                    put(2 * line + 1, z, v.y);
+                }
             });
+        if (tiled) {
+            __syncthreads();
+            flush_tiled<N>(p, m, v0, ny, LDS, stg, reinterpret_cast<char *>(out));
+        }
         return;
     }
     // line-fastest: consecutive threads read consecutive (y, y+1) pairs of one kz row
@@ -684,6 +742,64 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
         else
             for (int z = lane; z < n; z += 32) put(yy, z, row[z].x);
     }
+}
+
+// ---- S3 for a tiled set: a block per (x, 2 LY y-lines, group of SY_TMAPS maps) --------------
+// Its L = SY_TMAPS LY complex lines are (map, y pair) combinations (line l: map g0 SY_TMAPS +
+// l / LY, y pair l % LY), so the block writes neighbouring maps' rows of the same tiles -- one
+// 8-row atom of each factor slab and K step -- together instead of one map's row in many tiles.
+constexpr int SY_TMAPS = 8;
+
+template <int N>
+__global__ void __launch_bounds__(SY_THREADS_Z) synth_z_tiled_kernel(SynthParams p, const float2 *H, char *out) {
+    extern __shared__ __align__(16) unsigned char sy_smem[];
+    const FftAxis &az = p.az;
+    const int L = 1 << az.lshift, LY = L / SY_TMAPS;
+    float2 *tw = reinterpret_cast<float2 *>(sy_smem);
+    float2 *b0 = tw + N;
+    float2 *b1 = b0 + L * (N + 1);
+    const int ychunks = (p.m1 + 2 * LY - 1) / (2 * LY), mgroups = (p.n_maps + SY_TMAPS - 1) / SY_TMAPS;
+    int b = blockIdx.x;
+    const int g0 = b % mgroups;
+    b /= mgroups;
+    const int yc = b % ychunks, x = b / ychunks;
+    const int y0 = yc * 2 * LY, ny = min(2 * LY, p.m1 - y0);
+    const int nm = min(SY_TMAPS, p.n_maps - SY_TMAPS * g0);
+    make_twiddles<float>(tw, N);  // made visible by the barrier after the first pass
+    const int64_t plane = (int64_t)p.m0 * p.m1;
+    float *const stg = reinterpret_cast<float *>((pass_count(N) - 2) % 2 == 0 ? b1 : b0);
+    constexpr int LDS = N + 1;
+    line_ifft_io<float, N, true>(
+        b0, b1, nm * LY, az.lshift, tw,
+        [&](int line, int e) -> float2 {
+            const int mi = line / LY, y = y0 + 2 * (line - mi * LY);
+            const SynthMap &mp = p.maps[SY_TMAPS * g0 + mi];
+            const int K = mp.kz_max;
+            int kz;
+            bool mirror = false;
+            if (y >= p.m1) return make_float2(0.f, 0.f);
+            if (e <= K) {
+                kz = e;
+            } else if (e >= N - K) {
+                kz = N - e;
+                mirror = true;
+            } else {
+                return make_float2(0.f, 0.f);
+            }
+            // the (y, y + 1) pair of line: one 16-byte load (m1 even)
+            const float4 q = *reinterpret_cast<const float4 *>(H + mp.h_off + kz * plane + (int64_t)x * p.m1 + y);
+            const float2 a = make_float2(q.x, q.y), c = make_float2(q.z, q.w);
+            if (kz == 0) return make_float2(a.x, c.x);
+            return mirror ? make_float2(a.x + c.y, c.x - a.y) : make_float2(a.x - c.y, a.y + c.x);
+        },
+        [&](int line, int z, float2 v) {
+            stg[(2 * line) * LDS + z] = v.x;
+            stg[(2 * line + 1) * LDS + z] = v.y;
+        });
+    __syncthreads();
+    const int64_t v0 = ((int64_t)x * p.m1 + y0) * p.m2;
+    for (int mi = 0; mi < nm; ++mi)
+        flush_tiled<N>(p, SY_TMAPS * g0 + mi, v0, ny, LDS, stg + 2 * mi * LY * LDS, out);
 }
 
 // ---- host side ----------------------------------------------------------------------------
@@ -813,6 +929,12 @@ static int synth_layout(const pb_grid_t *g, const int32_t *out_n, int precision,
 }
 
 
+// dynamic shared memory of a transform kernel
+template <typename K>
+static cudaError_t set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // Lengths with a compile-time kernel; any other supported length runs the run-time form.
 template <typename F>
 static void with_length(int n, F &&f) {
@@ -837,11 +959,12 @@ static int launch_synth(const SynthLayout &L, const typename cplx<T>::type *src,
     const SynthParams &p = L.p;
     const size_t c = sizeof(typename cplx<T>::type);
     auto smem = [&](const FftAxis &a) { return (size_t)(2 * (1 << a.lshift) * (a.n + 1) + a.n) * c; };
+    const size_t smem_z = smem(p.az);
     cudaError_t e = cudaSuccess;
     with_length(p.ax.n, [&](auto NC) {
         constexpr int N = decltype(NC)::value;
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(synth_x_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem(p.ax));
+            e = set_smem(synth_x_kernel<T, N>, smem(p.ax));
         if (e == cudaSuccess) {
             synth_x_kernel<T, N><<<L.nb1, SY_THREADS, smem(p.ax), s>>>(p, src, w, U);
             e = cudaGetLastError();
@@ -851,7 +974,7 @@ static int launch_synth(const SynthLayout &L, const typename cplx<T>::type *src,
     with_length(p.ay.n, [&](auto NC) {
         constexpr int N = decltype(NC)::value;
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(synth_y_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem(p.ay));
+            e = set_smem(synth_y_kernel<T, N>, smem(p.ay));
         if (e == cudaSuccess) {
             synth_y_kernel<T, N><<<L.nb2, SY_THREADS, smem(p.ay), s>>>(p, U, H);
             e = cudaGetLastError();
@@ -860,10 +983,26 @@ static int launch_synth(const SynthLayout &L, const typename cplx<T>::type *src,
     if (e != cudaSuccess) return cuda_check(e, "pb_shell_synth (y)");
     with_length(p.az.n, [&](auto NC) {
         constexpr int N = decltype(NC)::value;
+        if constexpr (std::is_same<T, float>::value && N > 0 && pass_count(N) >= 2) {
+            // a tiled set: blocks over groups of maps (rows of neighbouring maps written together)
+            const int Lz = 1 << p.az.lshift;
+            if (p.tiled && p.m1 % 2 == 0 && Lz >= SY_TMAPS) {
+                const int LY = Lz / SY_TMAPS;
+                const int64_t nb = (int64_t)p.m0 * ((p.m1 + 2 * LY - 1) / (2 * LY)) *
+                                   ((p.n_maps + SY_TMAPS - 1) / SY_TMAPS);
+                if (e == cudaSuccess)
+                    e = set_smem(synth_z_tiled_kernel<N>, smem_z);
+                if (e == cudaSuccess) {
+                    synth_z_tiled_kernel<N><<<(unsigned)nb, SY_THREADS_Z, smem_z, s>>>(p, H, reinterpret_cast<char *>(out));
+                    e = cudaGetLastError();
+                }
+                return;
+            }
+        }
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(synth_z_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem(p.az));
+            e = set_smem(synth_z_kernel<T, N>, smem_z);
         if (e == cudaSuccess) {
-            synth_z_kernel<T, N><<<L.nb3, SY_THREADS_Z, smem(p.az), s>>>(p, H, out);
+            synth_z_kernel<T, N><<<L.nb3, SY_THREADS_Z, smem_z, s>>>(p, H, out);
             e = cudaGetLastError();
         }
     });

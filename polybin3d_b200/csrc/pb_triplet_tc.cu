@@ -563,16 +563,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // M-tile mt holds pair 128 mt + 32 q + lane
         const int q = warp & 3, g = (warp - TC_PW0) >> 2;
         if ((geo.pw_active >> q) & 1) {
-            uint32_t ra[TC_MAX_MT], rb[TC_MAX_MT];
-            bool ok[TC_MAX_MT];
-#pragma unroll
-            for (int mt = 0; mt < TC_MAX_MT; ++mt) {
-                const int p = 128 * mt + 32 * q + lane;
-                ok[mt] = mt < geo.n_mt && p < geo.n_tp;
-                ra[mt] = ok[mt] ? (uint32_t)spairs[2 * p] : 0u;
-                rb[mt] = ok[mt] ? (uint32_t)(geo.off_b + spairs[2 * p + 1]) : 0u;
-            }
+            // one copy of the K-step body (the M-tile loop is not unrolled: the role's code stays
+            // small next to the other roles'); a lane past the pair count reads row 0 and its
+            // TMEM lane is never read out
             const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
+            const uint32_t half = (uint32_t)geo.half_bytes;
             Ring bf, st;
             for (int it = 0; it < my_tiles; ++it, bf.next(geo.nbuf), st.next(geo.nstage)) {
                 const int buf = bf.idx, slot = st.idx;
@@ -583,24 +578,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 if (*(volatile int *)&abort_flag) break;
                 tc_fence_after();
-                const unsigned char *st = stage0 + slot * geo.stage_bytes;
-#pragma unroll
-                for (int mt = 0; mt < TC_MAX_MT; ++mt) {
-                    if (mt >= geo.n_mt || 128 * mt + 32 * q >= geo.n_tp) break;
+                // this warp's K steps start in slab (g * KS / TC_PW) / 2 of the stage
+                const unsigned char *sg = stage0 + slot * geo.stage_bytes + (g * (KS / TC_PW) >> 1) * half;
+#pragma unroll 1
+                for (int mt = 0; mt < geo.n_mt; ++mt) {
+                    const int p0 = 128 * mt + 32 * q;
+                    if (p0 >= geo.n_tp) break;
+                    const int p = min(p0 + lane, geo.n_tp - 1);
+                    const uint32_t ra = (uint32_t)spairs[2 * p], rb = (uint32_t)(geo.off_b + spairs[2 * p + 1]);
                     const uint32_t tcol = tq + (uint32_t)(geo.pcol0 + (buf * geo.n_mt + mt) * T);
 #pragma unroll
                     for (int kk = 0; kk < KS / TC_PW; ++kk) {
                         const int ks = g * (KS / TC_PW) + kk;
-                        const unsigned char *hb = st + (ks >> 1) * geo.half_bytes;
+                        // KS / TC_PW is even (T >= 64) or 1: (ks & 1) and the slab step are compile-time
+                        const unsigned char *hb = sg + ((KS / TC_PW) >= 2 ? (kk >> 1) * half : 0u);
+                        const int odd = (KS / TC_PW) >= 2 ? (kk & 1) : (ks & 1);
                         uint32_t hi[8], lo[8];
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
-                            const int ch = 4 * (ks & 1) + c;
-                            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-                            if (ok[mt]) {
-                                a = *reinterpret_cast<const float4 *>(hb + stage_off(ra[mt], ch));
-                                b = *reinterpret_cast<const float4 *>(hb + stage_off(rb[mt], ch));
-                            }
+                            const int ch = 4 * odd + c;
+                            const float4 a = *reinterpret_cast<const float4 *>(hb + stage_off(ra, ch));
+                            const float4 b = *reinterpret_cast<const float4 *>(hb + stage_off(rb, ch));
                             prod_split4(a, b, hi + 2 * c, lo + 2 * c);
                         }
                         tmem_st8(tcol + 16 * ks, hi);

@@ -172,22 +172,29 @@ def test_shell_synth_tiled_equals_plain(N):
 
 
 @tc
-def test_bk_ideal_tiled_path_matches_plain_path():
-    """Bk_ideal (mixed precision, tensor cores) through the tiled set and through plain maps:
-    the same sums up to FP32 accumulation order within tiles."""
+def test_bk_routes_agree():
+    """The bispectrum's cubic sums through the tiled set and through plain maps (mixed
+    precision, tensor cores) on one field: the same sums up to FP32 accumulation order within
+    tiles; Bk_numerator_ideal returns the route the autotuner picked."""
     import polybin3d_b200 as pb
     from polybin3d_b200 import synthetic
     N, L = 64, 1000.0
     b = quiet(pb.PolyBin3D, [L] * 3, [N] * 3, pixel_window="tsc", backend="cuda", precision="mixed")
     bs = quiet(pb.BSpec, b, np.linspace(2 * np.pi / L, 0.15, 9), lmax=2, contraction="tc")
     bs.sym_factor = np.ones(bs.N_bins)
-    x = synthetic.lognormal(N, L, seed=4)
+    field = synthetic.lognormal(N, L, seed=4)
     assert bs._tiled_ok(torch.float32)
-    tiled = quiet(bs.Bk_numerator_ideal, x)
-    assert getattr(bs, "_tiled", True)
-    bs._tiled = False
-    plain = quiet(bs.Bk_numerator_ideal, x)
+    x = b.as_device(field)
+    xk = bs._data_spectrum(x)
+    w = bs._data_weight(torch.float32)
+    scale = 1.0 / bs.cube_mask_mean ** (1. / 3.)
+    tiled = bs._b3_tiled(xk, w, scale).cpu().numpy()
+    plain = bs._b3_plain(xk, w, scale).cpu().numpy()
     nb = len(plain) // 2
     for j in range(2):
         a, r = tiled[j * nb:(j + 1) * nb], plain[j * nb:(j + 1) * nb]
         assert np.max(np.abs(a - r)) / np.max(np.abs(r)) < 1e-6
+    num = quiet(bs.Bk_numerator_ideal, field)
+    norm = b.volume / float(b.gridsize.prod())
+    ref = tiled if bs._b3_route(xk, w, scale) == "tiled" else plain
+    assert np.max(np.abs(num / norm - ref)) / np.max(np.abs(ref)) < 1e-12
