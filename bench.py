@@ -1,6 +1,7 @@
 """Benchmark: Bk_ideal fields/s at 256^3 (16 bins, lmax=2, TSC, mixed precision).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--contraction auto|tc|simt]
+                    [--workload ...] [--route auto|plain|tiled]
 
 One step = one float32 lognormal field through BSpec.Bk_ideal: r2c, the synthesis of the
 32 bin-filtered maps (Theta_b L_l / W_TSC) on the dealiased 192^3 grid (pb_shell_synth:
@@ -82,6 +83,9 @@ def parse():
     p.add_argument("--workload", default="headline", choices=["headline", "bk256", "bk512grad"] + sorted(FISHER))
     p.add_argument("--contraction", default="auto", choices=["auto", "tc", "simt"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    # the bispectrum's cubic-sum route: auto (the autotuner's choice, as Bk_ideal uses it), or one
+    # of the two pinned (for profiling a kernel of that route)
+    p.add_argument("--route", default="auto", choices=["auto", "plain", "tiled"])
     a = p.parse_args()
     if a.steps is None:
         a.steps = {"headline": 50, "bk256": 50, "bk512grad": 16}.get(a.workload, 6)
@@ -279,7 +283,9 @@ def run_ours(args, rank, world, local):
         w = bs._data_weight(torch.float32)
         idx = bs._triplet_index()
         if "tiled" not in route:
-            route["tiled"] = bs._tiled_ok(torch.float32) and bs._b3_route(xk, w, 1.0) == "tiled"
+            ok = bs._tiled_ok(torch.float32)
+            route["tiled"] = ok and (bs._b3_route(xk, w, 1.0) == "tiled" if args.route == "auto"
+                                     else args.route == "tiled")
         tiled = route["tiled"]
         if tiled:
             G = bs._g_maps_tiled(xk, w, 1.0)

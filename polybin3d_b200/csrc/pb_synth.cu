@@ -612,7 +612,8 @@ __device__ void flush_tiled(const SynthParams &p, int m, int64_t v0, int rows, i
 
 // ---- S3: real transform along z, two output lines per complex transform -----------------
 template <typename T, int N>
-__global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, const typename cplx<T>::type *H,
+// (FP32: two 768-thread blocks resident per SM, 42 registers; FP64 keeps its registers)
+__global__ void __launch_bounds__(SY_THREADS_Z, sizeof(T) == 4 ? 2 : 1) synth_z_kernel(SynthParams p, const typename cplx<T>::type *H,
                                                              T *out) {
     using C = typename cplx<T>::type;
     extern __shared__ __align__(16) unsigned char sy_smem[];
@@ -748,13 +749,13 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_kernel(SynthParams p, co
 // Its L = SY_TMAPS LY complex lines are (map, y pair) combinations (line l: map g0 SY_TMAPS +
 // l / LY, y pair l % LY), so the block writes neighbouring maps' rows of the same tiles -- one
 // 8-row atom of each factor slab and K step -- together instead of one map's row in many tiles.
-constexpr int SY_TMAPS = 8;
+constexpr int SY_TMAPS = 8;  // a power of two (line -> map by shift)
 
 template <int N>
-__global__ void __launch_bounds__(SY_THREADS_Z) synth_z_tiled_kernel(SynthParams p, const float2 *H, char *out) {
+__global__ void __launch_bounds__(SY_THREADS_Z, 2) synth_z_tiled_kernel(SynthParams p, const float2 *H, char *out) {
     extern __shared__ __align__(16) unsigned char sy_smem[];
     const FftAxis &az = p.az;
-    const int L = 1 << az.lshift, LY = L / SY_TMAPS;
+    const int L = 1 << az.lshift, LY = L / SY_TMAPS, ly_shift = az.lshift - 3;  // SY_TMAPS = 8
     float2 *tw = reinterpret_cast<float2 *>(sy_smem);
     float2 *b0 = tw + N;
     float2 *b1 = b0 + L * (N + 1);
@@ -772,7 +773,7 @@ __global__ void __launch_bounds__(SY_THREADS_Z) synth_z_tiled_kernel(SynthParams
     line_ifft_io<float, N, true>(
         b0, b1, nm * LY, az.lshift, tw,
         [&](int line, int e) -> float2 {
-            const int mi = line / LY, y = y0 + 2 * (line - mi * LY);
+            const int mi = line >> ly_shift, y = y0 + 2 * (line & (LY - 1));
             const SynthMap &mp = p.maps[SY_TMAPS * g0 + mi];
             const int K = mp.kz_max;
             int kz;
