@@ -566,18 +566,20 @@ __device__ __forceinline__ void tiled_put(const SynthParams &p, int m, int64_t v
     *reinterpret_cast<__nv_bfloat16 *>(out + tiled_c_byte(v, tiled_cpad(p.t_maps) + m, p.t_maps, p.t_factor)) = lo;
 }
 
-// A block's staged values of map m (rows of NN voxels, row stride lds in stg; voxels v0 ..
-// v0 + rows NN - 1) into a tiled set.  Each warp takes 64 consecutive voxels, a lane two
-// neighbours: two 128-byte rows of factor slabs (8-byte stores) and four 32-byte K-step rows
-// each of the hi and lo parts (bf16x2 stores), so the stores fill whole sectors; offsets inside
-// a tile are per lane and fixed, the tile base per warp chunk.  Per voxel (tiled_put) when the
-// run is not 64-aligned.
+// Staged values of map m (rows of NN voxels, row stride lds in stg; voxels v0 .. v0 + rows NN
+// - 1) into a tiled set, by warps wk = 0 .. nw - 1 of a group (the caller's warp index in it).
+// Each warp takes 64 consecutive voxels per step, a lane two neighbours: two 128-byte rows of
+// factor slabs (8-byte stores) and four 32-byte K-step rows each of the hi and lo parts
+// (bf16x2 stores), so the stores fill whole sectors; offsets inside a tile are per lane and
+// computed once per map, the tile base per chunk.  Per voxel (tiled_put) when the run is not
+// 64-aligned.
 template <int NN>
-__device__ void flush_tiled(const SynthParams &p, int m, int64_t v0, int rows, int lds, const float *stg, char *out) {
+__device__ void flush_tiled(const SynthParams &p, int m, int64_t v0, int rows, int lds, const float *stg, char *out,
+                            int wk, int nw) {
     const int count = rows * NN;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
     if ((NN & 1) != 0 || (v0 & 63) != 0 || (count & 63) != 0) {
-        for (int i = threadIdx.x; i < count; i += blockDim.x) {
+        for (int i = wk * 32 + lane; i < count; i += nw * 32) {
             const int r = i / NN, z = i - r * NN;
             tiled_put(p, m, v0 + i, stg[r * lds + z], out);
         }
@@ -595,7 +597,7 @@ __device__ void flush_tiled(const SynthParams &p, int m, int64_t v0, int rows, i
                           ((((lane >> 2) & 1) ^ ((r >> 2) & 1)) << 4) + (lane & 3) * 4);
     };
     const uint32_t off_hi = c_off(m), off_lo = c_off(P + m);
-    for (int u = warp * 64; u < count; u += nw * 64) {
+    for (int u = wk * 64; u < count; u += nw * 64) {
         const int i = u + 2 * lane, r = i / NN, z = i - r * NN;  // NN even: both voxels in row r
         const float x0 = stg[r * lds + z], x1 = stg[r * lds + z + 1];
         const int64_t v = v0 + u;  // 64-aligned: two slabs, four K steps of one tile
@@ -695,7 +697,7 @@ __global__ void __launch_bounds__(SY_THREADS_Z, sizeof(T) == 4 ? 2 : 1) synth_z_
             });
         if (tiled) {
             __syncthreads();
-            flush_tiled<N>(p, m, v0, ny, LDS, stg, reinterpret_cast<char *>(out));
+            flush_tiled<N>(p, m, v0, ny, LDS, stg, reinterpret_cast<char *>(out), threadIdx.x >> 5, blockDim.x >> 5);
         }
         return;
     }
@@ -799,8 +801,10 @@ __global__ void __launch_bounds__(SY_THREADS_Z, 2) synth_z_tiled_kernel(SynthPar
         });
     __syncthreads();
     const int64_t v0 = ((int64_t)x * p.m1 + y0) * p.m2;
-    for (int mi = 0; mi < nm; ++mi)
-        flush_tiled<N>(p, SY_TMAPS * g0 + mi, v0, ny, LDS, stg + 2 * mi * LY * LDS, out);
+    // a group of warps per map, so each warp sets up one map's offsets and stores many chunks
+    const int nwb = blockDim.x >> 5, wpm = max(1, nwb / nm), warp = threadIdx.x >> 5;
+    for (int mi = warp / wpm; mi < nm; mi += max(1, nwb / wpm))
+        flush_tiled<N>(p, SY_TMAPS * g0 + mi, v0, ny, LDS, stg + 2 * mi * LY * LDS, out, warp % wpm, wpm);
 }
 
 // ---- host side ----------------------------------------------------------------------------
