@@ -70,8 +70,8 @@ PB_API const char *pb_last_error(void);
 /* counterpart (the reference has no launch configuration).                              */
 /* ---------------------------------------------------------------------------------- */
 typedef struct pb_tuning {
-    int32_t tc_tile;     /* tensor-core contraction: voxels per tile, 32, 64 or 128 (0: 64,   */
-                         /* 128 from a tiled map set)                                        */
+    int32_t tc_tile;     /* tensor-core contraction: voxels per tile, 32, 64 or 128 (0: 128, */
+                         /* smaller when a shape does not fit; a tiled map set takes 128)    */
     int32_t tc_stages;   /* its staging ring depth in tiles, 2..6 (0: what ~64 KB holds)     */
     int32_t tc_chain;    /* voxels summed in TMEM between FP64 folds: 256 .. 2048 (0: 512);    */
                          /* changes the FP32 rounding, so the autotuner leaves it alone      */

@@ -6,7 +6,7 @@ stream, keeps the fastest and stores it in a JSON file, so later calls -- and la
 processes -- set the winner before launching.  Tuned shapes:
 
 * the tensor-core triplet contraction (from plain maps and from a tiled set): voxels per
-  tile (plain maps: 64 / 32), staging ring depth, the barrier-wait form, accumulator sets
+  tile (plain maps: 128 / 64), staging ring depth, the barrier-wait form, accumulator sets
   (never the TMEM chain length, which changes the FP32 rounding);
 * the k-bin reduction of many rows (>= 16): lane-per-row kernel (warps per block, blocks
   per SM) against the mode-tile kernel;
@@ -28,7 +28,7 @@ import torch
 from . import _native as nat
 
 # (launch shapes only: the TMEM chain length changes the FP32 rounding and stays fixed)
-TC_CANDIDATES = [{}, {"tc_tile": 32}, {"tc_stages": 3}, {"tc_tile": 32, "tc_stages": 4}, {"tc_wait": 2},
+TC_CANDIDATES = [{}, {"tc_wait": 2}, {"tc_tile": 64}, {"tc_tile": 64, "tc_wait": 2}, {"tc_stages": 6},
                  {"tc_dsets": 1}]
 # from a tiled map set (one contiguous copy per 128-voxel tile)
 TC_TILED_CANDIDATES = [{}, {"tc_wait": 2}, {"tc_stages": 4}, {"tc_dsets": 1}, {"tc_wait": 2, "tc_dsets": 1}]

@@ -144,3 +144,24 @@ def test_bilinear_maps(dtype, tol):
     scale = ref.abs().max()
     assert float((out - ref).abs().max() / scale) < tol
     assert float(out[n_out - 1].abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("tile", [128, 64, 32])
+def test_tc_tile_sizes(tile):
+    """The tensor-core contraction from plain maps at each tile size (128 by default; 64 and 32
+    when a shape needs them or the autotuner picks them), ragged voxel count included."""
+    if not (nat.tc_built() and torch.cuda.get_device_capability()[0] == 10):
+        pytest.skip("tensor-core contraction needs sm_100")
+    torch.manual_seed(9)
+    idx = bk_like_triplets()
+    G = torch.randn(32, 50_003, device="cuda")
+    ref = reference(G, G, G, torch.as_tensor(idx, device="cuda").long()).cpu().numpy()
+    ws = nat.Workspace(torch.device("cuda"))
+    plan = nat.TripletPlan(32, 32, 32, idx, torch.device("cuda"))
+    out = torch.empty(len(idx), dtype=torch.float64, device="cuda")
+    nat.set_tuning({"tc_tile": tile})
+    try:
+        plan.contract(G, G, G, out, ws, method=nat.PB_TRIPLET_TC)
+    finally:
+        nat.set_tuning(None)
+    assert np.max(np.abs(out.cpu().numpy() - ref)) / np.max(np.abs(ref)) < 1e-5
