@@ -10,6 +10,7 @@ realisations of 203 bins).
 Without an initialised process group (or with one rank) nothing is exchanged.
 """
 import atexit
+import gc
 import multiprocessing
 import os
 from collections import deque
@@ -198,8 +199,18 @@ class CapturedBatch:
         torch.cuda.synchronize(base.device)
         c0 = (base.n_FFTs_forward, base.n_FFTs_reverse, nat.LAUNCHES[0])
         self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
-            self.out = fn(self.seeds)
+        # a finalizer that frees device memory (an unreferenced FFT plan, workspace or tensor
+        # of earlier work) must not run inside the capture: a cudaFree there invalidates it.
+        # Collect first, and keep the collector off while capturing.
+        gc.collect()
+        was_enabled = gc.isenabled()
+        gc.disable()
+        try:
+            with torch.cuda.graph(self.graph):
+                self.out = fn(self.seeds)
+        finally:
+            if was_enabled:
+                gc.enable()
         self.delta = (base.n_FFTs_forward - c0[0], base.n_FFTs_reverse - c0[1], nat.LAUNCHES[0] - c0[2])
         self.keep = list(base.ws.bufs.values())
 
