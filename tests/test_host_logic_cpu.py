@@ -78,3 +78,22 @@ def test_real_harmonics_all_l():
 def test_wide_angle_derivative_coefficients():
     for k in (np.linspace(0.01, 0.12, 7), np.geomspace(0.01, 0.2, 5)):
         assert np.array_equal(PSpec.derivative_coefficient(k), O.OraclePSpec.derivative_coefficient(k))
+
+
+def test_route_chooser_cache_and_disabled(tmp_path, monkeypatch):
+    """autotune.Tuner.choose_route: a cached winner is returned without running anything; with
+    tuning off the first route is taken, also without running anything."""
+    import json
+    from polybin3d_b200 import autotune
+
+    def never():
+        raise AssertionError("a route ran")
+
+    path = tmp_path / "tuning.json"
+    path.write_text(json.dumps({"b3route|dev|192,192,192|32|16|global": {"route": "plain"}}))
+    monkeypatch.setenv("PB_TUNING_CACHE", str(path))
+    t = autotune.Tuner()
+    assert t.choose_route("b3route|dev|192,192,192|32|16|global", {"tiled": never, "plain": never}) == "plain"
+    monkeypatch.setenv("PB_AUTOTUNE", "0")
+    assert t.choose_route("another|key", {"tiled": never, "plain": never}) == "tiled"
+    assert "another|key" not in json.loads(path.read_text())
