@@ -7,7 +7,8 @@ One step = one float32 lognormal field through BSpec.Bk_ideal: r2c, the synthesi
 32 bin-filtered maps (Theta_b L_l / W_TSC) on the dealiased 192^3 grid (pb_shell_synth:
 band-limited filter and inverse transform as pruned passes), the tensor-core triplet
 contraction over 888 bin triplets, and the inverse ideal Fisher (cached, as the reference
-caches it).  `value` times that on device-resident fields; `e2e` times the
+caches it).  The maps and the contraction take the route Bk_ideal takes: plain maps or a
+tiled map set, whichever the autotuner timed faster for this shape (--route pins one).  `value` times that on device-resident fields; `e2e` times the
 public call Bk_ideal(field) on pinned host fields, H2D copy and result readback included.
 Under torchrun every rank runs independent fields (replicas: a 256^3 field does not
 shard), timing is the max over ranks and `value` counts all ranks' fields.
