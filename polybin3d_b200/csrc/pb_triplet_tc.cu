@@ -296,6 +296,13 @@ __device__ __forceinline__ void prod_split4(const float4 &a, const float4 &b, ui
     split2p(fmul2(f2pack(a.x, a.y), f2pack(b.x, b.y)), hi[0], lo[0]);
     split2p(fmul2(f2pack(a.z, a.w), f2pack(b.z, b.w)), hi[1], lo[1]);
 }
+// 8 staged voxels (two float4) split: hi[0..3], lo[0..3]
+__device__ __forceinline__ void split4(const float4 &x0, const float4 &x1, uint32_t *hi, uint32_t *lo) {
+    split2p(f2pack(x0.x, x0.y), hi[0], lo[0]);
+    split2p(f2pack(x0.z, x0.w), hi[1], lo[1]);
+    split2p(f2pack(x1.x, x1.y), hi[2], lo[2]);
+    split2p(f2pack(x1.z, x1.w), hi[3], lo[3]);
+}
 
 // D (TMEM) (+)= A (shared memory descriptor) x B (shared memory descriptor)^T
 __device__ __forceinline__ void umma_ss_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -504,7 +511,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // row j and lo to row nc_pad + j of the B operand (K chunk c8)
         const int ct = tid - 32 * TC_CW0;
         const int n_unit = geo.split_c ? 0 : n_c * (T / 8);  // a tiled set carries the split C maps
-        const int n_all = n_unit + geo.n_side * (T / 8);
+        const int n_sunit = geo.n_side * (T / 8);
         Ring bf, st;
         for (int it = 0; it < my_tiles; ++it, bf.next(geo.nbuf), st.next(geo.nstage)) {
             const int buf = bf.idx, slot = st.idx;
@@ -517,38 +524,66 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const unsigned char *st = stage0 + slot * geo.stage_bytes;
             unsigned char *cb = cop0 + buf * geo.cop_bytes;
             unsigned char *sb = sop0 + buf * geo.side_bytes;
-            for (int u = ct; u < n_all; u += 32 * TC_NCW) {
-                uint32_t h[4], l[4];
-                unsigned char *dh, *dl;
-                if (u < n_unit) {
-                    // C map j, 8 voxels: bf16 hi to row j, lo to row nc_pad + j
-                    const int j = u / (T / 8), c8 = u - j * (T / 8);
-                    const int r = geo.off_c + j;
-                    const unsigned char *hb = st + (c8 >> 2) * geo.half_bytes;
-                    const float4 x0 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3)));
-                    const float4 x1 = *reinterpret_cast<const float4 *>(hb + stage_off(r, 2 * (c8 & 3) + 1));
-                    split2p(f2pack(x0.x, x0.y), h[0], l[0]);
-                    split2p(f2pack(x0.z, x0.w), h[1], l[1]);
-                    split2p(f2pack(x1.x, x1.y), h[2], l[2]);
-                    split2p(f2pack(x1.z, x1.w), h[3], l[3]);
-                    dh = cb + c8 * geo.cop_lbo + (j >> 3) * 128 + (j & 7) * 16;
-                    dl = cb + c8 * geo.cop_lbo + ((geo.nc_pad + j) >> 3) * 128 + (j & 7) * 16;
-                } else {
-                    // side pair sp, 8 voxels: products split, hi to row sp, lo to row ns_pad + sp
-                    const int v = u - n_unit;
-                    const int sp = v / (T / 8), c8 = v - sp * (T / 8);
-                    const int ra = spairs[2 * (geo.n_tp + sp)], rb = geo.off_b + spairs[2 * (geo.n_tp + sp) + 1];
-                    const unsigned char *hb = st + (c8 >> 2) * geo.half_bytes;
-                    const int ch = 2 * (c8 & 3);
-                    prod_split4(*reinterpret_cast<const float4 *>(hb + stage_off(ra, ch)),
-                                *reinterpret_cast<const float4 *>(hb + stage_off(rb, ch)), h, l);
-                    prod_split4(*reinterpret_cast<const float4 *>(hb + stage_off(ra, ch + 1)),
-                                *reinterpret_cast<const float4 *>(hb + stage_off(rb, ch + 1)), h + 2, l + 2);
-                    dh = sb + c8 * geo.side_lbo + (sp >> 3) * 128 + (sp & 7) * 16;
-                    dl = sb + c8 * geo.side_lbo + ((geo.ns_pad + sp) >> 3) * 128 + (sp & 7) * 16;
+            // two units per step with both units' shared-memory reads ahead of both units' stores:
+            // the stores could alias the next reads as far as the compiler can tell, which would
+            // serialise the steps on the read latency; a second unit past the end re-reads the
+            // first and is not stored
+            constexpr int CS = 32 * TC_NCW;
+            for (int u = ct; u < n_unit; u += 2 * CS) {
+                // C map j, 8 voxels: bf16 hi to row j, lo to row nc_pad + j of the B operand (K chunk c8)
+                const bool two = u + CS < n_unit;
+                const int u1 = two ? u + CS : u;
+                const int j0 = u / (T / 8), c0 = u - j0 * (T / 8);
+                const int j1 = u1 / (T / 8), c1 = u1 - j1 * (T / 8);
+                const unsigned char *b0 = st + (c0 >> 2) * geo.half_bytes, *b1 = st + (c1 >> 2) * geo.half_bytes;
+                const int r0 = geo.off_c + j0, r1 = geo.off_c + j1;
+                const float4 x0 = *reinterpret_cast<const float4 *>(b0 + stage_off(r0, 2 * (c0 & 3)));
+                const float4 x1 = *reinterpret_cast<const float4 *>(b0 + stage_off(r0, 2 * (c0 & 3) + 1));
+                const float4 y0 = *reinterpret_cast<const float4 *>(b1 + stage_off(r1, 2 * (c1 & 3)));
+                const float4 y1 = *reinterpret_cast<const float4 *>(b1 + stage_off(r1, 2 * (c1 & 3) + 1));
+                uint32_t h[8], l[8];
+                split4(x0, x1, h, l);
+                split4(y0, y1, h + 4, l + 4);
+                unsigned char *e0 = cb + c0 * geo.cop_lbo + (j0 & 7) * 16;
+                *reinterpret_cast<uint4 *>(e0 + (j0 >> 3) * 128) = make_uint4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint4 *>(e0 + ((geo.nc_pad + j0) >> 3) * 128) = make_uint4(l[0], l[1], l[2], l[3]);
+                if (two) {
+                    unsigned char *e1 = cb + c1 * geo.cop_lbo + (j1 & 7) * 16;
+                    *reinterpret_cast<uint4 *>(e1 + (j1 >> 3) * 128) = make_uint4(h[4], h[5], h[6], h[7]);
+                    *reinterpret_cast<uint4 *>(e1 + ((geo.nc_pad + j1) >> 3) * 128) = make_uint4(l[4], l[5], l[6], l[7]);
                 }
-                *reinterpret_cast<uint4 *>(dh) = make_uint4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<uint4 *>(dl) = make_uint4(l[0], l[1], l[2], l[3]);
+            }
+            for (int v = ct; v < n_sunit; v += 2 * CS) {
+                // side pair sp, 8 voxels: products split, hi to row sp, lo to row ns_pad + sp
+                const bool two = v + CS < n_sunit;
+                const int v1 = two ? v + CS : v;
+                const int s0 = v / (T / 8), c0 = v - s0 * (T / 8);
+                const int s1 = v1 / (T / 8), c1 = v1 - s1 * (T / 8);
+                const int ra0 = spairs[2 * (geo.n_tp + s0)], rb0 = geo.off_b + spairs[2 * (geo.n_tp + s0) + 1];
+                const int ra1 = spairs[2 * (geo.n_tp + s1)], rb1 = geo.off_b + spairs[2 * (geo.n_tp + s1) + 1];
+                const unsigned char *b0 = st + (c0 >> 2) * geo.half_bytes, *b1 = st + (c1 >> 2) * geo.half_bytes;
+                const int ch0 = 2 * (c0 & 3), ch1 = 2 * (c1 & 3);
+                const float4 a00 = *reinterpret_cast<const float4 *>(b0 + stage_off(ra0, ch0));
+                const float4 b00 = *reinterpret_cast<const float4 *>(b0 + stage_off(rb0, ch0));
+                const float4 a01 = *reinterpret_cast<const float4 *>(b0 + stage_off(ra0, ch0 + 1));
+                const float4 b01 = *reinterpret_cast<const float4 *>(b0 + stage_off(rb0, ch0 + 1));
+                const float4 a10 = *reinterpret_cast<const float4 *>(b1 + stage_off(ra1, ch1));
+                const float4 b10 = *reinterpret_cast<const float4 *>(b1 + stage_off(rb1, ch1));
+                const float4 a11 = *reinterpret_cast<const float4 *>(b1 + stage_off(ra1, ch1 + 1));
+                const float4 b11 = *reinterpret_cast<const float4 *>(b1 + stage_off(rb1, ch1 + 1));
+                uint32_t h[8], l[8];
+                prod_split4(a00, b00, h, l);
+                prod_split4(a01, b01, h + 2, l + 2);
+                prod_split4(a10, b10, h + 4, l + 4);
+                prod_split4(a11, b11, h + 6, l + 6);
+                unsigned char *e0 = sb + c0 * geo.side_lbo + (s0 & 7) * 16;
+                *reinterpret_cast<uint4 *>(e0 + (s0 >> 3) * 128) = make_uint4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint4 *>(e0 + ((geo.ns_pad + s0) >> 3) * 128) = make_uint4(l[0], l[1], l[2], l[3]);
+                if (two) {
+                    unsigned char *e1 = sb + c1 * geo.side_lbo + (s1 & 7) * 16;
+                    *reinterpret_cast<uint4 *>(e1 + (s1 >> 3) * 128) = make_uint4(h[4], h[5], h[6], h[7]);
+                    *reinterpret_cast<uint4 *>(e1 + ((geo.ns_pad + s1) >> 3) * 128) = make_uint4(l[4], l[5], l[6], l[7]);
+                }
             }
             fence_async_smem();
             __syncwarp();
