@@ -47,7 +47,7 @@ WORKLOAD = "Bk_ideal 256^3 box 2000 Mpc/h, TSC, lmax=2, 16 linear bins 2pi/2000.
 # maps (16 pair factors) on the 192^3 grid (1,358,954,496 algorithmic bytes), and from the
 # 32 plain FP32 maps (905,969,664 algorithmic bytes)
 TC_TRAFFIC_TILED = 1_359_059_000 + 5_238_784
-TC_TRAFFIC_PLAIN = 911_428_352
+TC_TRAFFIC_PLAIN = 906_144_256 + 3_914_752
 
 
 FISHER = {
