@@ -280,20 +280,21 @@ def run_ours(args, rank, world, local):
         # the public Bk_ideal path (BSpec._b3_sums): with the tensor-core contraction, the route
         # (g-maps into a tiled set, or plain maps) the autotuner found faster for this shape
         x = resident[i % n_pool]
-        xk = bs._data_spectrum(x)
-        w = bs._data_weight(torch.float32)
+        f32 = torch.float32
+        xk = bs._data_spectrum(x, keep64=True)  # FP64 transform, read as it is by the synthesis
+        w = bs._data_weight(f32)
         idx = bs._triplet_index()
         if "tiled" not in route:
-            ok = bs._tiled_ok(torch.float32)
-            route["tiled"] = ok and (bs._b3_route(xk, w, 1.0) == "tiled" if args.route == "auto"
+            ok = bs._tiled_ok(f32)
+            route["tiled"] = ok and (bs._b3_route(xk, w, 1.0, f32) == "tiled" if args.route == "auto"
                                      else args.route == "tiled")
         tiled = route["tiled"]
         if tiled:
-            G = bs._g_maps_tiled(xk, w, 1.0)
+            G = bs._g_maps_tiled(xk, w, 1.0, f32)
             plan = bs._plan("b3", G.n_maps, G.n_maps, G.n_maps, idx)
             run = lambda: autotune.contract_tiled(plan, G, out, base.ws, bs._grid_scale(G.shape))
         else:
-            G = bs._g_maps(xk, w, 1.0)
+            G = bs._g_maps(xk, w, 1.0, rd=f32)
             plan = bs._plan("b3", G.shape[0], G.shape[0], G.shape[0], idx)
             run = lambda: autotune.contract(plan, G, G, G, out, base.ws, method, 1.0)
         used["plan"] = plan

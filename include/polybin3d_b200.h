@@ -46,6 +46,9 @@ extern "C" {
 
 #define PB_F32 0
 #define PB_F64 1
+/* pb_shell_synth / pb_shell_synth_tiled only: FP32 maps (and FP32 w) from a complex FP64  */
+/* source spectrum, which the first pass reads and filters in FP64 before rounding once   */
+#define PB_F32_SRC_F64 2
 
 typedef struct pb_grid {
     int32_t n[3];      /* real-space grid; n[2] even                                        */
@@ -267,11 +270,14 @@ PB_API int pb_bilinear_maps(int precision, int64_t n_vox, const void *G, int n_g
 /* Real-space elementwise products.                                                      */
 /*   PB_EW_MUL      : out = s * x * y                  (prod_real, utils.pyx:248-260)     */
 /*   PB_EW_PRODDIFF : out = s * (x*y - z*u)            (prod_real_diff, utils.pyx:371-383)*/
+/*   PB_EW_WIDEN    : out = (double) x, exact; x FP32 (precision PB_F32), out FP64; y, z, */
+/*                    u, s unused (the FP32 data field before an FP64 r2c, base.py:176-198)*/
 /* n elements; y is read at i % y_period when y_period > 0 (one mask over a batch of     */
-/* maps; MUL only); z/u may be NULL where unused; out may alias x.                       */
+/* maps; MUL only); z/u may be NULL where unused; out may alias x (not for WIDEN).       */
 /* ---------------------------------------------------------------------------------- */
 #define PB_EW_MUL 0
 #define PB_EW_PRODDIFF 1
+#define PB_EW_WIDEN 2
 PB_API int pb_elementwise(int precision, int op, int64_t n, const void *x, const void *y, int64_t y_period,
                           const void *z, const void *u, double s, void *out, void *stream);
 

@@ -15,10 +15,11 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpb_b200.so")
 
 PB_F32, PB_F64 = 0, 1
+PB_F32_SRC_F64 = 2  # shell_synth only: FP32 maps from a complex128 source
 PB_FFT_R2C, PB_FFT_C2R = 0, 1
 PB_RED_ABS2, PB_RED_CROSS, PB_RED_REAL2 = 0, 1, 2
 PB_TRIPLET_SIMT, PB_TRIPLET_TC = 0, 1
-PB_EW_MUL, PB_EW_PRODDIFF = 0, 1
+PB_EW_MUL, PB_EW_PRODDIFF, PB_EW_WIDEN = 0, 1, 2
 FILTER_MAX_MAPS = 128
 SYNTH_MAX_MAPS = 64
 SYNTH_WS_BYTES = 8 << 30  # transform workspace per pb_shell_synth call
@@ -266,6 +267,17 @@ def elementwise(op, x, y, z=None, u=None, s=1.0, out=None, y_period=0):
     return out
 
 
+def widen(x, out=None):
+    """FP64 copy of an FP32 tensor (exact), by the library's vectorised kernel."""
+    if x.dtype != torch.float32 or not x.is_contiguous():
+        raise ValueError("widen: a contiguous float32 tensor")
+    out = torch.empty(x.shape, dtype=torch.float64, device=x.device) if out is None else out
+    check(load().pb_elementwise(PB_F32, PB_EW_WIDEN, x.numel(), ptr(x), None, 0, None, None, 0.0, ptr(out),
+                                stream_ptr()), "pb_elementwise")
+    _count(1)
+    return out
+
+
 def grf_philox(grid, precision, seeds, amp, scale, out):
     """Half-spectrum GRFs from on-device Philox noise; seeds: device int64 (n_batch,)."""
     check(load().pb_grf_philox(ctypes.byref(grid), precision, ptr(seeds), seeds.numel(), ptr(amp), float(scale),
@@ -498,7 +510,7 @@ def shell_synth(grid, precision, src, out, maps, out_n, ws, w=None, src_stride=N
 
 
 def _shell_synth_tiled(lib, grid, precision, src, out, maps, out_n, ws, w, src_stride):
-    if precision != PB_F32:
+    if precision not in (PB_F32, PB_F32_SRC_F64):
         raise ValueError("shell_synth: a tiled set holds f32 maps")
     if len(maps) != out.n_maps or tuple(int(n) for n in out_n) != out.shape:
         raise ValueError("shell_synth: the tiled set holds %d maps on %s" % (out.n_maps, out.shape))

@@ -333,6 +333,9 @@ class BSpec:
         ks = self.k_bins_squeeze
         cd = torch.complex128 if dtype == torch.float64 else torch.complex64
         prec = nat.precision_of(dtype)
+        # FP32 maps from an FP64 spectrum: the pruned synthesis reads it as it is
+        src64 = src is not None and src.dtype == torch.complex128 and dtype == torch.float32
+        sprec = nat.PB_F32_SRC_F64 if src64 else prec
         dims = self.map_grid if coarse else tuple(int(n) for n in b.gridsize)
         wp = 0 if w is None else 1
         # spec: (bin, l1, l2, scale[, source index]); the sources lie src_stride apart
@@ -342,20 +345,22 @@ class BSpec:
             # a tiled set comes from the pruned synthesis only (one pass)
             if self.synthesis == 'cufft' or not self._synth_ok.get(dims, True):
                 raise NotImplementedError("tiled maps need the pruned synthesis")
-            nat.shell_synth(b.grid, prec, src, out, maps, dims, b.ws, w=w, src_stride=b.nhalf)
+            nat.shell_synth(b.grid, sprec, src, out, maps, dims, b.ws, w=w, src_stride=b.nhalf)
             b.n_FFTs_reverse += len(specs)
             return out
         if self.synthesis != 'cufft' and self._synth_ok.get(dims, True):
             if out is None:
                 out = torch.empty((len(specs),) + tuple(dims), dtype=dtype, device=b.device)
             try:
-                nat.shell_synth(b.grid, prec, src, out, maps, dims, b.ws, w=w, src_stride=b.nhalf)
+                nat.shell_synth(b.grid, sprec, src, out, maps, dims, b.ws, w=w, src_stride=b.nhalf)
                 b.n_FFTs_reverse += len(specs)
                 return out
             except NotImplementedError:
                 if self.synthesis == 'pruned':
                     raise
                 self._synth_ok[dims] = False
+        if src64:
+            src = src.to(cd)
         hs = (dims[0], dims[1], dims[2] // 2 + 1)
         half = torch.empty((len(specs),) + hs, dtype=cd, device=b.device)
         nat.spectral_filter(b.grid, prec, src, half, maps, w=w, src_stride=b.nhalf,
@@ -421,12 +426,16 @@ class BSpec:
         ab = self.all_bins
         return np.stack([ab[:, 0], ab[:, 1], (ab[:, 3] // 2) * self.Nk_squeeze + ab[:, 2]], axis=1).astype(np.int32)
 
-    def _g_maps(self, xk, w, scale, out=None):
-        """All Nl x Nk_squeeze bin-filtered maps g[l/2, b] of one weighted spectrum."""
+    def _g_maps(self, xk, w, scale, out=None, rd=None):
+        """All Nl x Nk_squeeze bin-filtered maps g[l/2, b] of one weighted spectrum, as real
+        maps of dtype rd (default: the spectrum's; FP32 maps may come from an FP64 spectrum)."""
+        rd = rd or xk.real.dtype
         if self.base.sightline == 'local' and self.lmax > 0:
+            if xk.real.dtype != rd:
+                xk = xk.to(torch.complex64 if rd == torch.float32 else torch.complex128)
             return self._g_maps_local(xk, w, scale, out)
         specs = [(bb, l, 0, scale) for l in range(0, self.lmax + 1, 2) for bb in range(self.Nk_squeeze)]
-        return self._binned_maps(xk, specs, w, xk.real.dtype, out=out)
+        return self._binned_maps(xk, specs, w, rd, out=out)
 
     def _g_maps_local(self, xk, w, scale, out=None, coarse=True):
         """Local sightline (bspec.py:932-954): with D = scale w xk and d = irfftn(D), the
@@ -455,16 +464,18 @@ class BSpec:
         norm = b.volume / float(b.gridsize.prod()) / self.sym_factor
         return B3.cpu().numpy() * norm
 
-    def _data_spectrum(self, x):
+    def _data_spectrum(self, x, keep64=False):
         """rfftn of a data field.  With FP32 maps (precision='mixed') the transform itself runs
         in FP64 unless data_fft='fp32': the FP32 r2c's rounding (relative to the largest modes,
         so large on the weak high-k modes) is the biggest error of the mixed path on the bins
         whose triple products cancel (quadrupoles near zero); rounding the FP64 spectrum to
-        FP32 afterwards costs ~1e-7 per mode."""
+        FP32 afterwards costs ~1e-7 per mode.  keep64: return that FP64 spectrum as it is, for
+        a caller whose synthesis reads it directly (FP32 maps, no rounded copy)."""
         b = self.base
         if x.dtype == torch.float32 and self.data_fft == 'fp64':
             b.n_FFTs_forward += 1
-            return b.fft_r2c(x.double()).to(torch.complex64)
+            xk = b.fft_r2c(nat.widen(x.contiguous()))
+            return xk if keep64 else xk.to(torch.complex64)
         return b.to_fourier(x)
 
     def _bk_cubic(self, data, filtering, linear=False):
@@ -473,7 +484,7 @@ class BSpec:
         (bspec.py:958-978)."""
         b = self.base
         x = b.as_device(data)
-        xk = self._data_spectrum(x)
+        xk = self._data_spectrum(x, keep64=filtering == 'ideal' and not linear)
         rd = x.dtype
         if filtering == 'ideal':
             w = self._data_weight(rd)
@@ -489,7 +500,7 @@ class BSpec:
                 w = b.to_device_grid(('bk_invwin', id(self)), lambda: self._inv_window(), rd)
             scale = 1.0
         if not linear:
-            return self._b3_sums(xk, w, scale)
+            return self._b3_sums(xk, w, scale, rd)
         # data maps and one simulation's maps side by side: X = [g; g_ii]
         n = self.Nl * self.Nk_squeeze
         X = torch.empty((2 * n,) + tuple(self.map_grid), dtype=rd, device=b.device)
@@ -502,26 +513,28 @@ class BSpec:
             b1 += self._set_sums('b1', X, n, ((0, 1, 1), (1, 0, 1), (1, 1, 0)))
         return out - b1 / self.N_it
 
-    def _b3_sums(self, xk, w, scale):
+    def _b3_sums(self, xk, w, scale, rd=None):
         """FP64 sums B3[i] = assemble_b3 of the g-maps of one weighted spectrum.  With the
         tensor-core contraction there are two routes: the g-maps synthesised straight into a
         tiled set (the contraction's staging layout: each tile of voxels of all maps is one
         contiguous copy and the MMA operand comes pre-split), or plain maps staged by 2-D TMA
         boxes.  The faster for this shape (synthesis and contraction timed together) is found
-        once and cached by the autotuner; the two agree to FP32 rounding."""
-        if self._tiled_ok(xk.real.dtype) and self._b3_route(xk, w, scale) == "tiled":
-            out = self._b3_tiled(xk, w, scale)
+        once and cached by the autotuner; the two agree to FP32 rounding.  rd: the maps' dtype
+        (default: the spectrum's)."""
+        rd = rd or xk.real.dtype
+        if self._tiled_ok(rd) and self._b3_route(xk, w, scale, rd) == "tiled":
+            out = self._b3_tiled(xk, w, scale, rd)
             if out is not None:
                 return out
-        return self._b3_plain(xk, w, scale)
+        return self._b3_plain(xk, w, scale, rd)
 
-    def _b3_plain(self, xk, w, scale):
-        G = self._g_maps(xk, w, scale)
+    def _b3_plain(self, xk, w, scale, rd=None):
+        G = self._g_maps(xk, w, scale, rd=rd)
         return self._contract('b3', G, G, G, self._triplet_index())
 
-    def _b3_tiled(self, xk, w, scale):
+    def _b3_tiled(self, xk, w, scale, rd=None):
         """The tiled route, or None when a tiled set cannot be made or contracted here."""
-        T = self._g_maps_tiled(xk, w, scale)
+        T = self._g_maps_tiled(xk, w, scale, rd)
         if T is None:
             return None
         plan = self._plan('b3', T.n_maps, T.n_maps, T.n_maps, self._triplet_index())
@@ -534,14 +547,14 @@ class BSpec:
             self._tiled = False
             return None
 
-    def _b3_route(self, xk, w, scale):
+    def _b3_route(self, xk, w, scale, rd=None):
         b = self.base
         key = "b3route|%s|%s|%d|%d|%s" % (autotune.device_tag(b.device), ",".join(str(int(n)) for n in self.map_grid),
                                           self.Nl * self.Nk_squeeze, self.Nk_squeeze, b.sightline)
         def tiled():
-            if self._b3_tiled(xk, w, scale) is None:
+            if self._b3_tiled(xk, w, scale, rd) is None:
                 raise NotImplementedError("no tiled set for this shape")
-        return autotune.tuner().choose_route(key, {"tiled": tiled, "plain": lambda: self._b3_plain(xk, w, scale)})
+        return autotune.tuner().choose_route(key, {"tiled": tiled, "plain": lambda: self._b3_plain(xk, w, scale, rd)})
 
     def _tiled_ok(self, dtype):
         return (getattr(self, '_tiled', True) and self.synthesis != 'cufft' and
@@ -554,17 +567,14 @@ class BSpec:
             return float(np.prod(b.gridsize)) / float(np.prod(shape))
         return 1.0
 
-    def _g_maps_tiled(self, xk, w, scale):
+    def _g_maps_tiled(self, xk, w, scale, rd=None):
         """The g-maps of _g_maps as a tiled set, or None when the pruned synthesis cannot
         make them (the caller takes the plain path)."""
         b = self.base
         # the monopole maps (the first Nk_squeeze) are the pair factors of every triplet
         T = nat.TiledMaps(self.Nl * self.Nk_squeeze, self.Nk_squeeze, self.map_grid, b.device)
         try:
-            if b.sightline == 'local' and self.lmax > 0:
-                self._g_maps_local(xk, w, scale, out=T)
-            else:
-                self._g_maps(xk, w, scale, out=T)
+            self._g_maps(xk, w, scale, out=T, rd=rd or xk.real.dtype)
         except NotImplementedError:
             self._tiled = False
             return None

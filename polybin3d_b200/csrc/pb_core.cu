@@ -411,10 +411,38 @@ __global__ void ew_kernel(int op, int64_t n, const T *x, const T *y, int64_t y_p
     }
 }
 
+// FP32 -> FP64, exact: four values per step (one 16-byte read, two 16-byte writes) when both
+// arrays are 16-byte aligned, then the tail
+__global__ void widen_kernel(int64_t n, const float *x, double *out, int vec) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t done = 0;
+    if (vec) {
+        const int64_t n4 = n >> 2;
+        for (int64_t q = i; q < n4; q += stride) {
+            const float4 v = reinterpret_cast<const float4 *>(x)[q];
+            reinterpret_cast<double2 *>(out)[2 * q] = make_double2(v.x, v.y);
+            reinterpret_cast<double2 *>(out)[2 * q + 1] = make_double2(v.z, v.w);
+        }
+        done = n4 << 2;
+    }
+    for (int64_t k = done + i; k < n; k += stride) out[k] = (double)x[k];
+}
+
 extern "C" int pb_elementwise(int precision, int op, int64_t n, const void *x, const void *y, int64_t y_period,
                               const void *z, const void *u, double s, void *out, void *stream) {
     if (n < 0) return fail(PB_ERR_INVALID, "pb_elementwise: negative size");
     if (n == 0) return PB_OK;
+    if (op == PB_EW_WIDEN) {
+        if (!x || !out) return fail(PB_ERR_INVALID, "pb_elementwise: NULL argument");
+        if (precision != PB_F32) return fail(PB_ERR_INVALID, "pb_elementwise: WIDEN reads FP32 (precision PB_F32)");
+        const int vec = (((uintptr_t)x | (uintptr_t)out) & 15) == 0;
+        const int threads = 256;
+        widen_kernel<<<grid_blocks(vec ? (n + 3) / 4 : n, threads, 16), threads, 0, as_stream(stream)>>>(
+            n, (const float *)x, (double *)out, vec);
+        PB_LAUNCH_CHECK("pb_elementwise");
+        return PB_OK;
+    }
     if (!x || !y || !out) return fail(PB_ERR_INVALID, "pb_elementwise: NULL argument");
     if (op == PB_EW_PRODDIFF && (!z || !u)) return fail(PB_ERR_INVALID, "pb_elementwise: PRODDIFF needs z, u");
     if (op != PB_EW_MUL && op != PB_EW_PRODDIFF) return fail(PB_ERR_INVALID, "pb_elementwise: bad op");

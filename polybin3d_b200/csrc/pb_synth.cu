@@ -422,9 +422,11 @@ __device__ __forceinline__ int find_map(const SynthParams &p, int b, int which) 
 }
 
 // ---- S1: gather + filter + transform along x ------------------------------------------
-template <typename T, int N>
-__global__ void __launch_bounds__(SY_THREADS) synth_x_kernel(SynthParams p, const typename cplx<T>::type *src,
-                                                             const T *w, typename cplx<T>::type *U) {
+// S: the source spectrum's element type, the maps' complex type or (FP32 maps) complex FP64:
+// the filter product is formed in FP64 and rounded to T once
+template <typename T, int N, typename S = typename cplx<T>::type>
+__global__ void __launch_bounds__(SY_THREADS) synth_x_kernel(SynthParams p, const S *src, const T *w,
+                                                             typename cplx<T>::type *U) {
     using C = typename cplx<T>::type;
     extern __shared__ __align__(16) unsigned char sy_smem[];
     const FftAxis &ax = p.ax;
@@ -443,7 +445,7 @@ __global__ void __launch_bounds__(SY_THREADS) synth_x_kernel(SynthParams p, cons
     if (R < 0 || col_first > col_last) return;
     const int lines = col_last - c0 + 1;  // lines below col_first stay 0
     make_twiddles<T>(tw, n);
-    const C *s = src ? src + (int64_t)mp.src * p.src_stride : nullptr;  // NULL: unit spectrum
+    const S *s = src ? src + (int64_t)mp.src * p.src_stride : nullptr;  // NULL: unit spectrum
     const double kzz = __dmul_rn((double)kz, p.kf2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int line = warp; line < lines; line += nw) {
@@ -472,7 +474,7 @@ __global__ void __launch_bounds__(SY_THREADS) synth_x_kernel(SynthParams p, cons
                         else f = wv != 0.0 ? f / wv : 0.0;
                     }
                     if (s) {
-                        const C x = s[sidx];
+                        const S x = s[sidx];
                         v = cmake<T>((double)x.x * f, (double)x.y * f);
                     } else {
                         v = cmake<T>(f, 0.0);
@@ -958,9 +960,9 @@ static void with_length(int n, F &&f) {
     }
 }
 
-template <typename T>
-static int launch_synth(const SynthLayout &L, const typename cplx<T>::type *src, const T *w,
-                        typename cplx<T>::type *U, typename cplx<T>::type *H, T *out, cudaStream_t s) {
+template <typename T, typename S = typename cplx<T>::type>
+static int launch_synth(const SynthLayout &L, const S *src, const T *w, typename cplx<T>::type *U,
+                        typename cplx<T>::type *H, T *out, cudaStream_t s) {
     const SynthParams &p = L.p;
     const size_t c = sizeof(typename cplx<T>::type);
     auto smem = [&](const FftAxis &a) { return (size_t)(2 * (1 << a.lshift) * (a.n + 1) + a.n) * c; };
@@ -969,9 +971,9 @@ static int launch_synth(const SynthLayout &L, const typename cplx<T>::type *src,
     with_length(p.ax.n, [&](auto NC) {
         constexpr int N = decltype(NC)::value;
         if (e == cudaSuccess)
-            e = set_smem(synth_x_kernel<T, N>, smem(p.ax));
+            e = set_smem(synth_x_kernel<T, N, S>, smem(p.ax));
         if (e == cudaSuccess) {
-            synth_x_kernel<T, N><<<L.nb1, SY_THREADS, smem(p.ax), s>>>(p, src, w, U);
+            synth_x_kernel<T, N, S><<<L.nb1, SY_THREADS, smem(p.ax), s>>>(p, src, w, U);
             e = cudaGetLastError();
         }
     });
@@ -1024,6 +1026,7 @@ extern "C" int pb_shell_synth_workspace_size(const pb_grid_t *g, const int32_t *
     if (!bytes || !hi) return fail(PB_ERR_INVALID, "pb_shell_synth_workspace_size: NULL argument");
     if (n_maps < 1 || n_maps > SY_MAX_MAPS)
         return fail(PB_ERR_INVALID, "pb_shell_synth_workspace_size: n_maps must be in [1, 64]");
+    if (precision == PB_F32_SRC_F64) precision = PB_F32;  // the workspace holds FP32 transforms
     std::vector<double> lo(n_maps, 0.0), sc(n_maps, 1.0);
     std::vector<int32_t> zero(n_maps, 0);
     SynthLayout L;
@@ -1040,6 +1043,9 @@ static int shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, 
                        const int32_t *l2, const double *scale, const int32_t *wpow, const void *w, void *out,
                        void *workspace, size_t workspace_bytes, void *stream, bool tiled, int n_factor) {
     if (!out || !lo || !hi || !l1 || !l2 || !scale) return fail(PB_ERR_INVALID, "pb_shell_synth: NULL argument");
+    // FP32 maps from a complex FP64 source: only the x pass's reads differ
+    const bool src64 = precision == PB_F32_SRC_F64;
+    if (src64) precision = PB_F32;
     SynthLayout L;
     int st = synth_layout(g, out_n, precision, n_maps, lo, hi, src_idx, l1, l2, scale, wpow, src_stride, &L);
     if (st) return st;
@@ -1066,7 +1072,10 @@ static int shell_synth(const pb_grid_t *g, const int32_t *out_n, int precision, 
     const size_t need = (size_t)(L.u_elems + L.h_elems) * c + 256;
     if (!workspace || workspace_bytes < need) return fail(PB_ERR_INVALID, "pb_shell_synth: workspace too small");
     char *ws = (char *)(((uintptr_t)workspace + 255) & ~(uintptr_t)255);
-    if (precision == PB_F32) {
+    if (src64) {
+        float2 *U = (float2 *)ws;
+        st = launch_synth<float, double2>(L, (const double2 *)src, (const float *)w, U, U + L.u_elems, (float *)out, s);
+    } else if (precision == PB_F32) {
         float2 *U = (float2 *)ws;
         st = launch_synth<float>(L, (const float2 *)src, (const float *)w, U, U + L.u_elems, (float *)out, s);
     } else {

@@ -98,3 +98,45 @@ def test_bk_numerator_pruned_equals_cufft(pb):
         bs = quiet(pb.BSpec, b, edges, lmax=2, synthesis=mode)
         r[mode] = quiet(bs.Bk_numerator_ideal, d)
     assert np.max(np.abs(r["pruned"] - r["cufft"])) / np.max(np.abs(r["cufft"])) < 1e-12
+
+
+@pytest.mark.parametrize("case", [1, 2])
+def test_shell_synth_f32_maps_from_f64_source(pb, case):
+    """PB_F32_SRC_F64: FP32 maps (FP32 weights) read straight from a complex128 spectrum,
+    against the FP64 synthesis of the same spectrum (one FP32 rounding of the filtered modes
+    and FP32 transforms: 2e-6 of each map's largest value), and as a tiled set, whose factor
+    rows must equal the plain maps exactly."""
+    from polybin3d_b200 import _native as nat
+    N, L, outn = CASES[case]
+    outn = outn or N
+    b = quiet(pb.PolyBin3D, list(L), list(N), pixel_window="cic", backend="cuda")
+    g = torch.Generator().manual_seed(10 + case)
+    x = torch.randn((2,) + tuple(N), generator=g, dtype=torch.float64).to(b.device)
+    src = b.fft_r2c(x)
+    w64 = b.to_device_grid("window", lambda: b.pixel_window_grid, torch.float64)
+    w32 = w64.float()
+    maps = maps_for(b, outn, 12, np.random.default_rng(case))
+    ref = torch.empty((12,) + tuple(outn), dtype=torch.float64, device=b.device)
+    nat.shell_synth(b.grid, nat.PB_F64, src, ref, maps, list(outn), b.ws, w=w64)
+    out = torch.empty((12,) + tuple(outn), dtype=torch.float32, device=b.device)
+    nat.shell_synth(b.grid, nat.PB_F32_SRC_F64, src, out, maps, list(outn), b.ws, w=w32)
+    ref, o = ref.cpu().numpy(), out.cpu().numpy()
+    for m in range(12):
+        scale = np.max(np.abs(ref[m]))
+        assert np.max(np.abs(o[m] - ref[m])) / scale < 2e-6, (m, maps[m])
+    T = nat.TiledMaps(12, 4, tuple(outn), b.device)
+    nat.shell_synth(b.grid, nat.PB_F32_SRC_F64, src, T, maps, list(outn), b.ws, w=w32)
+    assert torch.equal(T.factor_maps().reshape(4, -1), out[:4].reshape(4, -1))
+
+
+@pytest.mark.parametrize("n", [1, 3, 4, 1001, 64 ** 3 + 2])
+def test_widen_exact(n):
+    """PB_EW_WIDEN: the FP32 -> FP64 copy before the data's FP64 transform, exact for every
+    length (vectorised body and scalar tail) and for an unaligned start."""
+    from polybin3d_b200 import _native as nat
+    x = torch.randn(n + 1, generator=torch.Generator().manual_seed(n)).to("cuda")
+    assert torch.equal(nat.widen(x[:n].contiguous()), x[:n].double())
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    nat.check(nat.load().pb_elementwise(nat.PB_F32, nat.PB_EW_WIDEN, n, nat.ctypes.c_void_p(x.data_ptr() + 4), None, 0,
+                                        None, None, 0.0, nat.ptr(y), nat.stream_ptr()), "pb_elementwise")
+    assert torch.equal(y, x[1:].double())

@@ -185,16 +185,17 @@ def test_bk_routes_agree():
     field = synthetic.lognormal(N, L, seed=4)
     assert bs._tiled_ok(torch.float32)
     x = b.as_device(field)
-    xk = bs._data_spectrum(x)
-    w = bs._data_weight(torch.float32)
+    f32 = torch.float32
+    xk = bs._data_spectrum(x, keep64=True)  # as Bk_ideal: FP32 maps from the FP64 transform
+    w = bs._data_weight(f32)
     scale = 1.0 / bs.cube_mask_mean ** (1. / 3.)
-    tiled = bs._b3_tiled(xk, w, scale).cpu().numpy()
-    plain = bs._b3_plain(xk, w, scale).cpu().numpy()
+    tiled = bs._b3_tiled(xk, w, scale, f32).cpu().numpy()
+    plain = bs._b3_plain(xk, w, scale, f32).cpu().numpy()
     nb = len(plain) // 2
     for j in range(2):
         a, r = tiled[j * nb:(j + 1) * nb], plain[j * nb:(j + 1) * nb]
         assert np.max(np.abs(a - r)) / np.max(np.abs(r)) < 1e-6
     num = quiet(bs.Bk_numerator_ideal, field)
     norm = b.volume / float(b.gridsize.prod())
-    ref = tiled if bs._b3_route(xk, w, scale) == "tiled" else plain
+    ref = tiled if bs._b3_route(xk, w, scale, f32) == "tiled" else plain
     assert np.max(np.abs(num / norm - ref)) / np.max(np.abs(ref)) < 1e-12
