@@ -224,3 +224,20 @@ def test_tiled_map_layout_host_side():
     # NULL maps and a factor count outside [1, n_maps] are refused before any device work
     assert lib.pb_triplet_contract_tiled(nat.PB_TRIPLET_TC, None, 4, 2, 100, nat.hptr(counts), nat.hptr(counts), 1.0,
                                          nat.hptr(out), None, 0, None) != 0
+
+
+def test_binding_constants_match_header():
+    """Every PB_* constant the Python binding defines has the header's value, and the new
+    argument values are refused where they do not apply (no device work)."""
+    src = open(HEADER).read()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"^#define (PB_[A-Z0-9_]+) +\(?(-?\d+)\)?", src, re.M)}
+    names = [k for k in dir(nat) if k.startswith("PB_")]
+    assert names
+    for k in names:
+        assert k in defs, k
+        assert getattr(nat, k) == defs[k], k
+    lib = nat.load()
+    # WIDEN reads FP32 only; NULL pointers are refused before any launch
+    assert lib.pb_elementwise(nat.PB_F64, nat.PB_EW_WIDEN, 4, None, None, 0, None, None, 0.0, None, None) != 0
+    assert lib.pb_elementwise(nat.PB_F32, nat.PB_EW_WIDEN, 4, None, None, 0, None, None, 0.0, None, None) != 0
+    assert lib.pb_elementwise(nat.PB_F32, 7, 4, None, None, 0, None, None, 0.0, None, None) != 0
